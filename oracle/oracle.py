@@ -1,0 +1,153 @@
+"""ctypes wrapper for the C restatement (oracle/_ref/liborq_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg as the checker; the product never imports it.
+Shares are numpy arrays; a shared vector is a list [S0, S1, S2].
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "liborq_oracle.so")
+
+_DT = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}
+PAIR0, PAIR1, PAIR2, G01, G02, G12, G012, LOCAL0, LOCAL1, LOCAL2 = range(10)
+
+
+def splitmix64_stream(seed: int, n: int) -> np.ndarray:
+    """SplitMix64 outputs (Steele, Lea, Flood, OOPSLA 2014) as uint64, matching
+    the sm64() input generator of ref_driver.cpp."""
+    M = (1 << 64) - 1
+    out = np.empty(n, dtype=np.uint64)
+    s = seed & M
+    for i in range(n):
+        s = (s + 0x9E3779B97F4A7C15) & M
+        z = s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        out[i] = z ^ (z >> 31)
+    return out
+
+
+def splitmix64_fast(seed: int, n: int) -> np.ndarray:
+    """Vectorised SplitMix64: state_i = seed + (i+1)*golden, then the mix."""
+    with np.errstate(over="ignore"):
+        s = np.uint64(seed) + (np.arange(1, n + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15))
+        z = s
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+class _Ctx(ctypes.Structure):
+    _fields_ = [("rk", (ctypes.c_uint32 * 60) * 10), ("nonce", ctypes.c_uint64 * 10)]
+
+
+def _lib():
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.oro_keystream.restype = ctypes.c_uint64
+    lib.oro_gen_perm.restype = ctypes.c_uint64
+    return lib
+
+
+class Oracle:
+    def __init__(self, seed: int):
+        self.lib = _lib()
+        self.ctx = _Ctx()
+        self.lib.oro_ctx_init(ctypes.byref(self.ctx), ctypes.c_uint64(seed))
+
+    # -- helpers -----------------------------------------------------------
+    @staticmethod
+    def _ptrs(arrs):
+        return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+    @staticmethod
+    def new(n, w):
+        return [np.zeros(n, dtype=_DT[w]) for _ in range(3)]
+
+    def nonce(self, stream):
+        return int(self.ctx.nonce[stream])
+
+    # -- primitives --------------------------------------------------------
+    def secret_share(self, data, arith, party=0):
+        w = data.dtype.itemsize
+        d = np.ascontiguousarray(data).view(_DT[w])
+        s = self.new(len(d), w)
+        self.lib.oro_secret_share(ctypes.byref(self.ctx), int(arith), w, ctypes.c_size_t(len(d)),
+                                  d.ctypes.data_as(ctypes.c_void_p), party, self._ptrs(s))
+        return s
+
+    def open(self, s, arith):
+        w = s[0].dtype.itemsize
+        out = np.zeros(len(s[0]), dtype=_DT[w])
+        self.lib.oro_open(int(arith), w, ctypes.c_size_t(len(out)), self._ptrs(s),
+                          out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def _bin(self, fn, x, y, ctx=True):
+        w = x[0].dtype.itemsize
+        z = self.new(len(x[0]), w)
+        args = [w, ctypes.c_size_t(len(x[0])), self._ptrs(x), self._ptrs(y), self._ptrs(z)]
+        if ctx:
+            args = [ctypes.byref(self.ctx)] + args
+        fn(*args)
+        return z
+
+    def and_b(self, x, y):
+        return self._bin(self.lib.oro_and_b, x, y)
+
+    def mul_a(self, x, y):
+        return self._bin(self.lib.oro_mul_a, x, y)
+
+    def xor_b(self, x, y):
+        return self._bin(self.lib.oro_xor_b, x, y, ctx=False)
+
+    def add_a(self, x, y):
+        return self._bin(self.lib.oro_add_a, x, y, ctx=False)
+
+    def b2a_bit(self, x):
+        w = x[0].dtype.itemsize
+        y = self.new(len(x[0]), w)
+        self.lib.oro_b2a_bit(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(x[0])), self._ptrs(x),
+                             self._ptrs(y))
+        return y
+
+    def reshare(self, s, group, arith):
+        w = s[0].dtype.itemsize
+        self.lib.oro_reshare(ctypes.byref(self.ctx), int(arith), w, ctypes.c_size_t(len(s[0])),
+                             group, self._ptrs(s))
+
+    def zero_share(self, n, w, arith):
+        r = self.new(n, w)
+        self.lib.oro_zero_share(ctypes.byref(self.ctx), int(arith), w, ctypes.c_size_t(n), self._ptrs(r))
+        return r
+
+    def gen_perm(self, stream, n):
+        p = np.zeros(n, dtype=np.int32)
+        draws = self.lib.oro_gen_perm(ctypes.byref(self.ctx), stream,
+                                      p.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(n))
+        return p, int(draws)
+
+    def keystream(self, stream, nonce0, nbytes):
+        buf = np.zeros(nbytes, dtype=np.uint8)
+        self.lib.oro_keystream(self.ctx.rk[stream], ctypes.c_uint64(nonce0),
+                               buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(nbytes))
+        return buf
+
+    def radix_sort(self, key, bits, payloads=(), desc=False):
+        """Sorts key (list of 3 uint64/uint32 share arrays) in place; payloads
+        (A-shared 64-bit) are permuted in place. Returns the A-shared perm."""
+        kw = key[0].dtype.itemsize
+        n = len(key[0])
+        pay = []
+        for p in payloads:
+            pay.extend(p)
+        pay_arr = (ctypes.c_void_p * max(1, len(pay)))(*[a.ctypes.data for a in pay])
+        perm = self.new(n, 4)
+        self.lib.oro_radix_sort(ctypes.byref(self.ctx), kw, ctypes.c_size_t(n), self._ptrs(key),
+                                bits, int(desc), len(payloads), pay_arr, self._ptrs(perm))
+        return perm

@@ -1,0 +1,676 @@
+/*
+ * orq_oracle.c — CPU restatement of ORQ's replicated-3PC local share computation.
+ *
+ * TEST INFRASTRUCTURE ONLY (see orq_oracle.h). Plain C, one thread, all three
+ * parties in one process. Each function cites the reference lines it restates;
+ * paths are relative to the ORQ source tree.
+ */
+#include "orq_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#define ORO_HAVE_AESNI 1
+#endif
+
+typedef unsigned __int128 u128;
+
+/* ------------------------------------------------------------------------- */
+/* Key derivation. The reference draws every AES key from libsodium's
+ * crypto_aead_aes256gcm_keygen (prg_algorithm.h:192-197). For reproducible
+ * runs, the test shim and this library replace that with SplitMix64 (Steele,
+ * Lea, Flood, OOPSLA 2014) keyed by (seed, party, keygen call index). */
+uint64_t oro_splitmix64(uint64_t* state) {
+    uint64_t z = (*state += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+void oro_derive_key(uint64_t seed, int party, int call, uint8_t key[32]) {
+    uint64_t st = seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(party + 1)) ^
+                  (0xABC98388FB8FAC03ull * (uint64_t)(call + 1));
+    for (int i = 0; i < 4; i++) {
+        uint64_t v = oro_splitmix64(&st);
+        for (int b = 0; b < 8; b++) key[8 * i + b] = (uint8_t)(v >> (8 * b));
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* AES-256 from FIPS-197: S-box built from the GF(2^8) inverse and the affine
+ * map, byte-oriented rounds. */
+static uint8_t g_sbox[256];
+static int g_sbox_ready = 0;
+
+static uint8_t gf_mul(uint8_t a, uint8_t b) {
+    uint8_t p = 0;
+    while (b) {
+        if (b & 1) p ^= a;
+        a = (uint8_t)((a << 1) ^ ((a & 0x80) ? 0x1B : 0));
+        b >>= 1;
+    }
+    return p;
+}
+
+static void build_sbox(void) {
+    if (g_sbox_ready) return;
+    for (int x = 0; x < 256; x++) {
+        uint8_t inv = 0;
+        if (x) {
+            for (int y = 1; y < 256; y++)
+                if (gf_mul((uint8_t)x, (uint8_t)y) == 1) {
+                    inv = (uint8_t)y;
+                    break;
+                }
+        }
+        uint8_t s = inv;
+        uint8_t r = inv;
+        for (int i = 0; i < 4; i++) {
+            r = (uint8_t)((r << 1) | (r >> 7));
+            s ^= r;
+        }
+        g_sbox[x] = s ^ 0x63;
+    }
+    g_sbox_ready = 1;
+}
+
+static uint32_t sub_word(uint32_t w) {
+    return (uint32_t)g_sbox[w & 0xff] | ((uint32_t)g_sbox[(w >> 8) & 0xff] << 8) |
+           ((uint32_t)g_sbox[(w >> 16) & 0xff] << 16) | ((uint32_t)g_sbox[w >> 24] << 24);
+}
+
+/* Round keys as little-endian words: word i holds key bytes 4i..4i+3. */
+void oro_aes256_expand(const uint8_t key[32], uint32_t rk[60]) {
+    build_sbox();
+    for (int i = 0; i < 8; i++)
+        rk[i] = (uint32_t)key[4 * i] | ((uint32_t)key[4 * i + 1] << 8) |
+                ((uint32_t)key[4 * i + 2] << 16) | ((uint32_t)key[4 * i + 3] << 24);
+    uint8_t rcon = 1;
+    for (int i = 8; i < 60; i++) {
+        uint32_t t = rk[i - 1];
+        if (i % 8 == 0) {
+            t = (t >> 8) | (t << 24); /* RotWord on the byte order */
+            t = sub_word(t) ^ rcon;
+            rcon = gf_mul(rcon, 2);
+        } else if (i % 8 == 4) {
+            t = sub_word(t);
+        }
+        rk[i] = rk[i - 8] ^ t;
+    }
+}
+
+void oro_aes256_encrypt(const uint32_t rk[60], const uint8_t in[16], uint8_t out[16]) {
+    uint8_t s[16], t[16];
+    for (int i = 0; i < 16; i++) s[i] = in[i] ^ (uint8_t)(rk[i / 4] >> (8 * (i % 4)));
+    for (int round = 1; round <= 14; round++) {
+        /* SubBytes + ShiftRows: state byte (row r, col c) is s[4c + r] */
+        for (int c = 0; c < 4; c++)
+            for (int r = 0; r < 4; r++) t[4 * c + r] = g_sbox[s[4 * ((c + r) % 4) + r]];
+        if (round != 14) {
+            for (int c = 0; c < 4; c++) {
+                uint8_t a0 = t[4 * c], a1 = t[4 * c + 1], a2 = t[4 * c + 2], a3 = t[4 * c + 3];
+                s[4 * c + 0] = gf_mul(a0, 2) ^ gf_mul(a1, 3) ^ a2 ^ a3;
+                s[4 * c + 1] = a0 ^ gf_mul(a1, 2) ^ gf_mul(a2, 3) ^ a3;
+                s[4 * c + 2] = a0 ^ a1 ^ gf_mul(a2, 2) ^ gf_mul(a3, 3);
+                s[4 * c + 3] = gf_mul(a0, 3) ^ a1 ^ a2 ^ gf_mul(a3, 2);
+            }
+        } else {
+            memcpy(s, t, 16);
+        }
+        for (int i = 0; i < 16; i++) s[i] ^= (uint8_t)(rk[4 * round + i / 4] >> (8 * (i % 4)));
+    }
+    memcpy(out, s, 16);
+}
+
+#ifdef ORO_HAVE_AESNI
+/* Same cipher on the x86 AES instructions (only a speed-up for the checker;
+ * the round keys are the FIPS-197 schedule above, read as bytes). */
+__attribute__((target("aes,sse4.1"))) static void aesni_ctr_chunk(const uint32_t rk[60],
+                                                                   uint64_t nonce, uint8_t* out,
+                                                                   size_t len) {
+    __m128i k[15];
+    for (int r = 0; r < 15; r++) k[r] = _mm_loadu_si128((const __m128i*)(rk + 4 * r));
+    uint8_t blk[16];
+    for (int b = 0; b < 8; b++) blk[b] = (uint8_t)(nonce >> (8 * b));
+    blk[8] = blk[9] = blk[10] = blk[11] = 0;
+    for (size_t j = 0; j * 16 < len; j++) {
+        uint32_t ctr = (uint32_t)(j + 2);
+        blk[12] = (uint8_t)(ctr >> 24);
+        blk[13] = (uint8_t)(ctr >> 16);
+        blk[14] = (uint8_t)(ctr >> 8);
+        blk[15] = (uint8_t)ctr;
+        __m128i s = _mm_xor_si128(_mm_loadu_si128((const __m128i*)blk), k[0]);
+        for (int r = 1; r < 14; r++) s = _mm_aesenc_si128(s, k[r]);
+        s = _mm_aesenclast_si128(s, k[14]);
+        size_t take = len - j * 16 < 16 ? len - j * 16 : 16;
+        if (take == 16)
+            _mm_storeu_si128((__m128i*)(out + j * 16), s);
+        else {
+            uint8_t t[16];
+            _mm_storeu_si128((__m128i*)t, s);
+            memcpy(out + j * 16, t, take);
+        }
+    }
+}
+#endif
+
+/* prg_algorithm.h:161-172 (1 MiB split) and :214-231 (nonce bytes, GCM). */
+uint64_t oro_keystream(const uint32_t rk[60], uint64_t nonce0, uint8_t* out, size_t nbytes) {
+    const size_t CH = (size_t)1 << 20;
+    uint64_t used = 0;
+    for (size_t off = 0; off < nbytes; off += CH, used++) {
+        size_t len = nbytes - off < CH ? nbytes - off : CH;
+        uint64_t nonce = nonce0 + used;
+#ifdef ORO_HAVE_AESNI
+        if (__builtin_cpu_supports("aes")) {
+            aesni_ctr_chunk(rk, nonce, out + off, len);
+            continue;
+        }
+#endif
+        uint8_t blk[16], ks[16];
+        for (int b = 0; b < 8; b++) blk[b] = (uint8_t)(nonce >> (8 * b));
+        blk[8] = blk[9] = blk[10] = blk[11] = 0;
+        for (size_t j = 0; j * 16 < len; j++) {
+            uint32_t ctr = (uint32_t)(j + 2);
+            blk[12] = (uint8_t)(ctr >> 24);
+            blk[13] = (uint8_t)(ctr >> 16);
+            blk[14] = (uint8_t)(ctr >> 8);
+            blk[15] = (uint8_t)ctr;
+            oro_aes256_encrypt(rk, blk, ks);
+            size_t take = len - j * 16 < 16 ? len - j * 16 : 16;
+            memcpy(out + off + j * 16, ks, take);
+        }
+    }
+    return used;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Context: which keygen call of which party keys each stream. This follows
+ * setup_random_generation (backend/common/rand_setup.h:306-381): call 0 is the
+ * local PRG; the lowest member draws each group key in the order of
+ * generateRandomnessGroups(3,2,1) = {0,1},{0,2},{1,2},{0,1,2}
+ * (core/protocols/protocol.h:309-375); P0 draws a second, discarded
+ * everyone-group key (rand_setup.h:321-325, map::insert keeps the first); the
+ * last call is the pairwise local key of setup_3pc_common_prgs
+ * (rand_setup.h:90-146): party p's get(+1) stream is keyed by its own local
+ * key and p+1's get(-1) stream by the same key. */
+void oro_ctx_init(oro_ctx* c, uint64_t seed) {
+    static const int who[ORO_NSTREAMS][2] = {
+        {0, 5}, {1, 2}, {2, 1},         /* PAIR0, PAIR1, PAIR2 */
+        {0, 1}, {0, 2}, {1, 1}, {0, 3}, /* G01, G02, G12, G012 */
+        {0, 0}, {1, 0}, {2, 0}          /* LOCAL0..2 */
+    };
+    for (int s = 0; s < ORO_NSTREAMS; s++) {
+        uint8_t key[32];
+        oro_derive_key(seed, who[s][0], who[s][1], key);
+        oro_aes256_expand(key, c->rk[s]);
+        c->nonce[s] = 0;
+    }
+}
+
+/* PRGAlgorithm::getNextBuffered (prg_algorithm.h:86-104): elements are filled
+ * in batches of at most 1 MiB; with power-of-two element sizes each batch is
+ * exactly one AES-GCM call, so the stream is the plain keystream of n*w bytes. */
+void oro_stream_fill(oro_ctx* c, int s, void* out, size_t n, int w) {
+    c->nonce[s] += oro_keystream(c->rk[s], c->nonce[s], (uint8_t*)out, n * (size_t)w);
+}
+
+/* ------------------------------------------------------------------------- */
+/* element helpers */
+static inline u128 ld(const void* p, size_t i, int w) {
+    u128 v = 0;
+    memcpy(&v, (const uint8_t*)p + i * (size_t)w, (size_t)w);
+    return v;
+}
+static inline void st(void* p, size_t i, int w, u128 v) {
+    memcpy((uint8_t*)p + i * (size_t)w, &v, (size_t)w);
+}
+static inline u128 sext(u128 v, int w) { /* sign-extend a w-byte value to 128 bits */
+    if (w == 16) return v;
+    int sh = 128 - 8 * w;
+    return (u128)(((__int128)(v << sh)) >> sh);
+}
+
+static void* xalloc(size_t bytes) {
+    void* p = calloc(bytes ? bytes : 1, 1);
+    if (!p) abort();
+    return p;
+}
+
+/* ZeroSharingGenerator::getNextBinary/Arithmetic (zero_sharing_generator.h:101-148):
+ * party p: prev = get(-1) = PAIR[p-1], next = get(+1) = PAIR[p];
+ * r_p = prev ^ next  or  prev - next. Each pairwise stream is drawn once per
+ * call (both holders consume it in lock-step). */
+void oro_zero_share(oro_ctx* c, int arith, int w, size_t n, void* r[3]) {
+    void* k[3];
+    for (int q = 0; q < 3; q++) {
+        k[q] = xalloc(n * (size_t)w);
+        oro_stream_fill(c, ORO_PAIR0 + q, k[q], n, w);
+    }
+    for (int p = 0; p < 3; p++) {
+        void* prev = k[(p + 2) % 3];
+        void* next = k[p];
+        for (size_t i = 0; i < n; i++) {
+            u128 a = ld(prev, i, w), b = ld(next, i, w);
+            st(r[p], i, w, arith ? a - b : a ^ b);
+        }
+    }
+    for (int q = 0; q < 3; q++) free(k[q]);
+}
+
+/* secret_share_b/a on the data owner (replicated_3pc.h:353-448): share_1 and
+ * share_2 from the owner's local PRG, share_3 = data ^ s1 ^ s2 (or data - s1 -
+ * s2); owner d holds (share_1, share_2), so S[(d+k)%3] = share_{k+1}. */
+void oro_secret_share(oro_ctx* c, int arith, int w, size_t n, const void* data, int d,
+                      void* s[3]) {
+    void* a = s[d % 3];
+    void* b = s[(d + 1) % 3];
+    void* e = s[(d + 2) % 3];
+    oro_stream_fill(c, ORO_LOCAL0 + d, a, n, w);
+    oro_stream_fill(c, ORO_LOCAL0 + d, b, n, w);
+    for (size_t i = 0; i < n; i++) {
+        u128 x = ld(data, i, w), u = ld(a, i, w), v = ld(b, i, w);
+        st(e, i, w, arith ? x - u - v : x ^ u ^ v);
+    }
+}
+
+/* public_share (replicated_3pc.h:456-470): P0 (x,0), P1 (0,0), P2 (0,x). */
+void oro_public_share(int w, size_t n, const void* data, void* s[3]) {
+    memcpy(s[0], data, n * (size_t)w);
+    memset(s[1], 0, n * (size_t)w);
+    memset(s[2], 0, n * (size_t)w);
+}
+
+/* open_shares_a/b (replicated_3pc.h:310-330). */
+void oro_open(int arith, int w, size_t n, void* const s[3], void* out) {
+    for (size_t i = 0; i < n; i++) {
+        u128 a = ld(s[0], i, w), b = ld(s[1], i, w), e = ld(s[2], i, w);
+        st(out, i, w, arith ? a + b + e : a ^ b ^ e);
+    }
+}
+
+void oro_xor_b(int w, size_t n, void* const x[3], void* const y[3], void* z[3]) {
+    for (int p = 0; p < 3; p++)
+        for (size_t i = 0; i < n; i++) st(z[p], i, w, ld(x[p], i, w) ^ ld(y[p], i, w));
+}
+void oro_add_a(int w, size_t n, void* const x[3], void* const y[3], void* z[3]) {
+    for (int p = 0; p < 3; p++)
+        for (size_t i = 0; i < n; i++) st(z[p], i, w, ld(x[p], i, w) + ld(y[p], i, w));
+}
+void oro_sub_a(int w, size_t n, void* const x[3], void* const y[3], void* z[3]) {
+    for (int p = 0; p < 3; p++)
+        for (size_t i = 0; i < n; i++) st(z[p], i, w, ld(x[p], i, w) - ld(y[p], i, w));
+}
+
+/* Replicated_3PC::and_b / multiply_a (replicated_3pc.h:44-67, 166-191):
+ * z_p = r_p ^ x_p&y_p ^ x_p&y_{p+1} ^ x_{p+1}&y_p, then the exchange hands
+ * z_{p+1} to party p as its second share (exchangeShares(local, remote, 2, 1)). */
+static void mult_like(oro_ctx* c, int arith, int w, size_t n, void* const x[3], void* const y[3],
+                      void* z[3]) {
+    void* r[3];
+    void* o[3];
+    for (int p = 0; p < 3; p++) {
+        r[p] = xalloc(n * (size_t)w);
+        o[p] = xalloc(n * (size_t)w);
+    }
+    oro_zero_share(c, arith, w, n, r);
+    for (int p = 0; p < 3; p++) {
+        int q = (p + 1) % 3;
+        for (size_t i = 0; i < n; i++) {
+            u128 xp = ld(x[p], i, w), xq = ld(x[q], i, w);
+            u128 yp = ld(y[p], i, w), yq = ld(y[q], i, w);
+            u128 v = ld(r[p], i, w);
+            if (arith)
+                v = v + xp * yp + xp * yq + xq * yp;
+            else
+                v = v ^ (xp & yp) ^ (xp & yq) ^ (xq & yp);
+            st(o[p], i, w, v);
+        }
+    }
+    for (int p = 0; p < 3; p++) {
+        memcpy(z[p], o[p], n * (size_t)w);
+        free(r[p]);
+        free(o[p]);
+    }
+}
+void oro_and_b(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]) {
+    mult_like(c, 0, w, n, x, y, z);
+}
+void oro_mul_a(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]) {
+    mult_like(c, 1, w, n, x, y, z);
+}
+
+/* Replicated_3PC::b2a_bit (replicated_3pc.h:220-251), in the distinct-share
+ * view: A = (r0 + ((x0^x1)&1), r1, r2), B = (r'0, r'1 + (x2&1), r'2) from two
+ * arithmetic zero-sharings, D = A - B, y = D*D (one multiply_a). */
+void oro_b2a_bit(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]) {
+    void* A[3];
+    void* B[3];
+    for (int p = 0; p < 3; p++) {
+        A[p] = xalloc(n * (size_t)w);
+        B[p] = xalloc(n * (size_t)w);
+    }
+    oro_zero_share(c, 1, w, n, A);
+    oro_zero_share(c, 1, w, n, B);
+    for (size_t i = 0; i < n; i++) {
+        u128 a = (ld(x[0], i, w) ^ ld(x[1], i, w)) & 1;
+        u128 b = ld(x[2], i, w) & 1;
+        st(A[0], i, w, ld(A[0], i, w) + a);
+        st(B[1], i, w, ld(B[1], i, w) + b);
+    }
+    for (int p = 0; p < 3; p++)
+        for (size_t i = 0; i < n; i++) st(A[p], i, w, ld(A[p], i, w) - ld(B[p], i, w));
+    oro_mul_a(c, w, n, A, A, y);
+    for (int p = 0; p < 3; p++) {
+        free(A[p]);
+        free(B[p]);
+    }
+}
+
+/* Protocol::reshare (protocol.h:500-541) with groupGetNextBinary/Arithmetic
+ * (zero_sharing_generator.h:158-183): r0, r1 from the group stream, r2 =
+ * r0^r1 (or -r0-r1); every distinct share j is re-randomised by r_j (each is
+ * held by a member of a 2-party group), the non-member receives the result. */
+void oro_reshare(oro_ctx* c, int arith, int w, size_t n, int group, void* s[3]) {
+    int stream = ORO_G01 + group;
+    void* r0 = xalloc(n * (size_t)w);
+    void* r1 = xalloc(n * (size_t)w);
+    oro_stream_fill(c, stream, r0, n, w);
+    oro_stream_fill(c, stream, r1, n, w);
+    for (size_t i = 0; i < n; i++) {
+        u128 a = ld(r0, i, w), b = ld(r1, i, w);
+        u128 e = arith ? (u128)0 - a - b : a ^ b;
+        if (arith) {
+            st(s[0], i, w, ld(s[0], i, w) + a);
+            st(s[1], i, w, ld(s[1], i, w) + b);
+            st(s[2], i, w, ld(s[2], i, w) + e);
+        } else {
+            st(s[0], i, w, ld(s[0], i, w) ^ a);
+            st(s[1], i, w, ld(s[1], i, w) ^ b);
+            st(s[2], i, w, ld(s[2], i, w) ^ e);
+        }
+    }
+    free(r0);
+    free(r1);
+}
+
+/* gen_perm (random/permutations/hm_sharded_permutation_generator.h:70-108):
+ * draws are u32 from buffers of 2^20 elements (one getNext of 4 MiB each);
+ * mask = (1 << bit_width(n)) - 1; reject r > n-1-i; swap(p[i], p[i+r]). */
+uint64_t oro_gen_perm(oro_ctx* c, int stream, int32_t* perm, size_t n) {
+    const size_t BUF = (size_t)1 << 20;
+    uint32_t* rnd = (uint32_t*)xalloc(BUF * 4);
+    for (size_t i = 0; i < n; i++) perm[i] = (int32_t)i;
+    oro_stream_fill(c, stream, rnd, BUF, 4);
+    int bits = 0;
+    while (bits < 64 && (n >> bits)) bits++;
+    uint32_t mask = (uint32_t)((1ull << bits) - 1);
+    size_t ri = 0;
+    uint64_t draws = 0;
+    for (size_t i = 0; i < n; i++) {
+        uint32_t r = (uint32_t)n;
+        while ((size_t)r > n - i - 1) {
+            r = rnd[ri] & mask;
+            ri++;
+            draws++;
+            if (ri == BUF) {
+                oro_stream_fill(c, stream, rnd, BUF, 4);
+                ri = 0;
+            }
+        }
+        size_t loc = i + r;
+        int32_t t = perm[i];
+        perm[i] = perm[loc];
+        perm[loc] = t;
+    }
+    free(rnd);
+    return draws;
+}
+
+/* ------------------------------------------------------------------------- */
+/* permutation plumbing */
+
+/* a sharded permutation: one local permutation per 2-party group */
+typedef struct {
+    int32_t* g[3];
+} sperm;
+
+static void sperm_gen(oro_ctx* c, sperm* sp, size_t n) {
+    /* HMShardedPermutationGenerator::generateBatch (hm_...generator.h:178-194):
+     * groups in order {0,1},{0,2},{1,2}. */
+    for (int g = 0; g < 3; g++) {
+        sp->g[g] = (int32_t*)xalloc(n * 4);
+        oro_gen_perm(c, ORO_G01 + g, sp->g[g], n);
+    }
+}
+static void sperm_free(sperm* sp) {
+    for (int g = 0; g < 3; g++) free(sp->g[g]);
+}
+
+/* local_apply_perm (operators/shuffle.h:113-133): new[pi[i]] = x[i] */
+static void scatter(int w, size_t n, void* x, const int32_t* pi) {
+    uint8_t* t = (uint8_t*)xalloc(n * (size_t)w);
+    for (size_t i = 0; i < n; i++) memcpy(t + (size_t)pi[i] * w, (uint8_t*)x + i * w, (size_t)w);
+    memcpy(x, t, n * (size_t)w);
+    free(t);
+}
+/* local_apply_inverse_perm (shuffle.h:250-270): new[i] = x[pi[i]] */
+static void gather(int w, size_t n, void* x, const int32_t* pi) {
+    uint8_t* t = (uint8_t*)xalloc(n * (size_t)w);
+    for (size_t i = 0; i < n; i++) memcpy(t + i * w, (uint8_t*)x + (size_t)pi[i] * w, (size_t)w);
+    memcpy(x, t, n * (size_t)w);
+    free(t);
+}
+
+/* hm_oblivious_apply_sharded_perm (shuffle.h:349-368): per group, members
+ * permute the shares they hold, then the group reshares. */
+static void apply_sharded(oro_ctx* c, int arith, int w, size_t n, void* s[3], const sperm* sp) {
+    for (int g = 0; g < 3; g++) {
+        for (int j = 0; j < 3; j++) scatter(w, n, s[j], sp->g[g]);
+        oro_reshare(c, arith, w, n, g, s);
+    }
+}
+/* hm_oblivious_apply_inverse_sharded_perm (shuffle.h:392-412): groups in
+ * reverse order, inverse (gather) application. */
+static void apply_inverse_sharded(oro_ctx* c, int arith, int w, size_t n, void* s[3],
+                                  const sperm* sp) {
+    for (int g = 2; g >= 0; g--) {
+        for (int j = 0; j < 3; j++) gather(w, n, s[j], sp->g[g]);
+        oro_reshare(c, arith, w, n, g, s);
+    }
+}
+
+/* PermutationManager queue (random/permutations/permutation_manager.h:102-181,
+ * 246-284): reserve() generates ahead; an empty queue generates on demand. */
+typedef struct {
+    sperm* q;
+    size_t head, tail, cap, n;
+} pqueue;
+
+static void pq_reserve(oro_ctx* c, pqueue* pq, size_t n, size_t count) {
+    if (pq->tail - pq->head >= count) return;
+    size_t need = count - (pq->tail - pq->head);
+    if (pq->tail + need > pq->cap) {
+        pq->cap = pq->tail + need + 8;
+        pq->q = (sperm*)realloc(pq->q, pq->cap * sizeof(sperm));
+    }
+    pq->n = n;
+    for (size_t k = 0; k < need; k++) sperm_gen(c, &pq->q[pq->tail++], n);
+}
+static sperm pq_next(oro_ctx* c, pqueue* pq, size_t n) {
+    sperm sp;
+    if (pq->tail > pq->head) return pq->q[pq->head++];
+    sperm_gen(c, &sp, n);
+    return sp;
+}
+
+/* oblivious_apply_elementwise_perm (shuffle.h:687-706): shuffle x and a copy
+ * of the (A-shared int32) permutation with the same sharded permutation, open
+ * the shuffled permutation, scatter x with it. */
+static void apply_elementwise(oro_ctx* c, pqueue* pq, int x_arith, int w, size_t n, void* x[3],
+                              int32_t* const perm[3]) {
+    int32_t* pc[3];
+    for (int j = 0; j < 3; j++) {
+        pc[j] = (int32_t*)xalloc(n * 4);
+        memcpy(pc[j], perm[j], n * 4);
+    }
+    sperm sp = pq_next(c, pq, n);
+    apply_sharded(c, x_arith, w, n, x, &sp);
+    apply_sharded(c, 1, 4, n, (void**)pc, &sp);
+    int32_t* opened = (int32_t*)xalloc(n * 4);
+    oro_open(1, 4, n, (void* const*)pc, opened);
+    for (int j = 0; j < 3; j++) scatter(w, n, x[j], opened);
+    sperm_free(&sp);
+    free(opened);
+    for (int j = 0; j < 3; j++) free(pc[j]);
+}
+
+/* ------------------------------------------------------------------------- */
+/* radix_sort (operators/radixsort.h:116-229) with pad_input/remove_padding
+ * (operators/sorting.h:405-495) and ElementwisePermutation::b2a/invert
+ * (containers/permutation.h:205-258). */
+void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int desc,
+                    int npayload, void** payloads, int32_t* perm_out[3]) {
+    pqueue pq = {0};
+    const int pw = (kw == 8) ? 16 : 8; /* PadWidth: int64 -> int128, else int64 */
+    const int full_width = (kw * 8 == bits);
+    void* P[3];
+    for (int j = 0; j < 3; j++) P[j] = xalloc(n * (size_t)pw);
+
+    /* pad_input: (v << 32) | idx, idx public-shared into S0 only */
+    for (int j = 0; j < 3; j++)
+        for (size_t i = 0; i < n; i++) {
+            u128 v = sext(ld(key[j], i, kw), kw) << 32;
+            if (j == 0) v |= (uint32_t)(desc ? (-1 - (int64_t)i) : (int64_t)i);
+            st(P[j], i, pw, v);
+        }
+    if (desc)
+        for (int j = 0; j < 3; j++)
+            for (size_t i = 0; i < n / 2; i++) {
+                u128 a = ld(P[j], i, pw), b = ld(P[j], n - 1 - i, pw);
+                st(P[j], i, pw, b);
+                st(P[j], n - 1 - i, pw, a);
+            }
+
+    /* radix_sort_body: reserve 1 permutation + (bits + 1) pairs */
+    pq_reserve(c, &pq, n, (size_t)bits + 2);
+    int32_t* vp[3];
+    int32_t* f1[3];
+    int32_t* s[3];
+    int32_t* s1v[3];
+    int32_t* t[3];
+    for (int j = 0; j < 3; j++) {
+        vp[j] = (int32_t*)xalloc(n * 4);
+        f1[j] = (int32_t*)xalloc(n * 4);
+        s[j] = (int32_t*)xalloc(2 * n * 4 + 4);
+        s1v[j] = (int32_t*)xalloc(n * 4);
+        t[j] = (int32_t*)xalloc(n * 4);
+    }
+    for (int b = 0; b < bits; b++) {
+        for (int j = 0; j < 3; j++)
+            for (size_t i = 0; i < n; i++) {
+                u128 v = sext(ld(P[j], i, pw), pw);
+                v = (u128)(((__int128)v) >> (32 + b));
+                if (full_width && b == bits - 1) v = ~v; /* inplace_invert on every share */
+                vp[j][i] = (int32_t)(uint32_t)v;
+            }
+        oro_b2a_bit(c, 4, n, (void* const*)vp, (void**)f1);
+        /* s0 = one - f1 ; s1 = f1 ; s[0] -= 1 ; prefix_sum(s) */
+        for (int j = 0; j < 3; j++) {
+            for (size_t i = 0; i < n; i++) {
+                uint32_t one = (j == 0) ? 1u : 0u;
+                s[j][i] = (int32_t)(one - (uint32_t)f1[j][i]);
+                s[j][n + i] = f1[j][i];
+            }
+            if (j == 0 && n) s[j][0] = (int32_t)((uint32_t)s[j][0] - 1u);
+            uint32_t acc = 0;
+            for (size_t i = 0; i < 2 * n; i++) {
+                acc += (uint32_t)s[j][i];
+                s[j][i] = (int32_t)acc;
+            }
+        }
+        /* s1 -= s0 ; f1 *= s1 ; s0 += f1 */
+        for (int j = 0; j < 3; j++)
+            for (size_t i = 0; i < n; i++)
+                s1v[j][i] = (int32_t)((uint32_t)s[j][n + i] - (uint32_t)s[j][i]);
+        oro_mul_a(c, 4, n, (void* const*)f1, (void* const*)s1v, (void**)t);
+        for (int j = 0; j < 3; j++)
+            for (size_t i = 0; i < n; i++)
+                t[j][i] = (int32_t)((uint32_t)s[j][i] + (uint32_t)t[j][i]);
+        apply_elementwise(c, &pq, 0, pw, n, P, t);
+    }
+
+    if (desc)
+        for (int j = 0; j < 3; j++)
+            for (size_t i = 0; i < n / 2; i++) {
+                u128 a = ld(P[j], i, pw), b = ld(P[j], n - 1 - i, pw);
+                st(P[j], i, pw, b);
+                st(P[j], n - 1 - i, pw, a);
+            }
+
+    /* remove_padding: perm = low 32 bits (B-shared); key = padded >> 32 */
+    int32_t* pm[3];
+    for (int j = 0; j < 3; j++) {
+        pm[j] = (int32_t*)xalloc(n * 4);
+        for (size_t i = 0; i < n; i++) {
+            u128 v = sext(ld(P[j], i, pw), pw);
+            pm[j][i] = (int32_t)(uint32_t)v;
+            st(key[j], i, kw, (u128)(((__int128)v) >> 32));
+        }
+    }
+    /* ElementwisePermutation::b2a (permutation.h:222-258) */
+    {
+        int32_t* pc[3];
+        for (int j = 0; j < 3; j++) {
+            pc[j] = (int32_t*)xalloc(n * 4);
+            memcpy(pc[j], pm[j], n * 4);
+        }
+        sperm sp = pq_next(c, &pq, n);
+        apply_sharded(c, 0, 4, n, (void**)pc, &sp);
+        int32_t* opened = (int32_t*)xalloc(n * 4);
+        oro_open(0, 4, n, (void* const*)pc, opened);
+        oro_public_share(4, n, opened, (void**)pm);
+        apply_inverse_sharded(c, 1, 4, n, (void**)pm, &sp);
+        sperm_free(&sp);
+        free(opened);
+        for (int j = 0; j < 3; j++) free(pc[j]);
+    }
+    if (desc) {
+        /* negate(): v *= -1 (multiply_a with a public -1) ; v += -1 */
+        int32_t* m1[3];
+        for (int j = 0; j < 3; j++) {
+            m1[j] = (int32_t*)xalloc(n * 4);
+            for (size_t i = 0; i < n; i++) m1[j][i] = (j == 0) ? -1 : 0;
+        }
+        oro_mul_a(c, 4, n, (void* const*)pm, (void* const*)m1, (void**)pm);
+        oro_add_a(4, n, (void* const*)pm, (void* const*)m1, (void**)pm);
+        for (int j = 0; j < 3; j++) free(m1[j]);
+    }
+    /* invert(): apply the permutation to a public identity */
+    {
+        int32_t* inv[3];
+        for (int j = 0; j < 3; j++) inv[j] = (int32_t*)xalloc(n * 4);
+        for (size_t i = 0; i < n; i++) inv[0][i] = (int32_t)i;
+        apply_elementwise(c, &pq, 1, 4, n, (void**)inv, pm);
+        for (int j = 0; j < 3; j++) {
+            memcpy(pm[j], inv[j], n * 4);
+            free(inv[j]);
+        }
+    }
+    for (int k = 0; k < npayload; k++) apply_elementwise(c, &pq, 1, 8, n, &payloads[3 * k], pm);
+    if (perm_out)
+        for (int j = 0; j < 3; j++) memcpy(perm_out[j], pm[j], n * 4);
+
+    for (int j = 0; j < 3; j++) {
+        free(P[j]);
+        free(vp[j]);
+        free(f1[j]);
+        free(s[j]);
+        free(s1v[j]);
+        free(t[j]);
+        free(pm[j]);
+    }
+    while (pq.head < pq.tail) sperm_free(&pq.q[pq.head++]);
+    free(pq.q);
+}

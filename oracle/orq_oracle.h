@@ -1,0 +1,101 @@
+/*
+ * orq_oracle.h — CPU restatement of ORQ's replicated-3PC share computation.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA path: only
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may load it.
+ * The product (orq_b200/, liborq_cuda.so) never links or calls it.
+ *
+ * Layout: all three parties live in one process ("loopback"). A 3PC shared
+ * vector is stored as its three distinct share arrays S[0], S[1], S[2]; party p
+ * holds the replicated pair (S[p], S[(p+1)%3]) exactly as get_shares_b/a hand
+ * them out (reference: include/core/protocols/replicated_3pc.h:353-392).
+ *
+ * Parity is pinned two ways:
+ *   - the AES-256 / GCM keystream against NIST-style known answers produced by
+ *     Python `cryptography` (tests/golden/aes_gcm_kat.json);
+ *   - every primitive and the radix sort against per-party share dumps of the
+ *     reference itself, built from its own headers with a deterministic
+ *     libsodium shim (oracle/ref_shim, oracle/Makefile) — tests/golden/*.bin.
+ */
+#ifndef ORQ_ORACLE_H
+#define ORQ_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- deterministic key derivation (shared with the shim and the device) ---- */
+uint64_t oro_splitmix64(uint64_t* state);
+/* 32-byte AES key for keygen call `call` of party `party` under `seed`. */
+void oro_derive_key(uint64_t seed, int party, int call, uint8_t key[32]);
+
+/* ---- AES-256 (FIPS-197) ---- */
+void oro_aes256_expand(const uint8_t key[32], uint32_t rk[60]);
+void oro_aes256_encrypt(const uint32_t rk[60], const uint8_t in[16], uint8_t out[16]);
+
+/* ---- GCM-mode keystream as ORQ's AESPRGAlgorithm consumes it ----
+ * (include/core/random/prg/prg_algorithm.h:161-172,214-231): the buffer is cut
+ * into 1 MiB chunks, chunk c is AES-GCM over zeros under nonce (nonce0 + c)
+ * written little-endian into the 12-byte IV; block j of a chunk is
+ * AES_K(IV || BE32(j + 2)). Returns the number of nonces consumed. */
+uint64_t oro_keystream(const uint32_t rk[60], uint64_t nonce0, uint8_t* out, size_t nbytes);
+
+/* ---- loopback context ---- */
+enum {
+    ORO_PAIR0 = 0, /* stream shared by P0/P1, keyed by P0's local key */
+    ORO_PAIR1 = 1, /* P1/P2 */
+    ORO_PAIR2 = 2, /* P2/P0 */
+    ORO_G01 = 3,
+    ORO_G02 = 4,
+    ORO_G12 = 5,
+    ORO_G012 = 6,
+    ORO_LOCAL0 = 7,
+    ORO_LOCAL1 = 8,
+    ORO_LOCAL2 = 9,
+    ORO_NSTREAMS = 10
+};
+
+typedef struct {
+    uint32_t rk[ORO_NSTREAMS][60];
+    uint64_t nonce[ORO_NSTREAMS];
+} oro_ctx;
+
+void oro_ctx_init(oro_ctx* c, uint64_t seed);
+/* getNext(Vector<T>) of n elements of w bytes from stream s. */
+void oro_stream_fill(oro_ctx* c, int s, void* out, size_t n, int w);
+
+/* ---- primitives; x, y, z are arrays of three share pointers ----
+ * w in {1,2,4,8,16} bytes. Arithmetic is mod 2^(8w). */
+void oro_secret_share(oro_ctx* c, int arith, int w, size_t n, const void* data, int data_party,
+                      void* s[3]);
+void oro_public_share(int w, size_t n, const void* data, void* s[3]);
+void oro_open(int arith, int w, size_t n, void* const s[3], void* out);
+void oro_xor_b(int w, size_t n, void* const x[3], void* const y[3], void* z[3]);
+void oro_and_b(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]);
+void oro_add_a(int w, size_t n, void* const x[3], void* const y[3], void* z[3]);
+void oro_sub_a(int w, size_t n, void* const x[3], void* const y[3], void* z[3]);
+void oro_mul_a(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]);
+void oro_b2a_bit(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]);
+void oro_reshare(oro_ctx* c, int arith, int w, size_t n, int group, void* s[3]);
+void oro_zero_share(oro_ctx* c, int arith, int w, size_t n, void* r[3]);
+
+/* Fisher–Yates from a group stream (hm_sharded_permutation_generator.h:70-108).
+ * Returns the number of u32 draws consumed. */
+uint64_t oro_gen_perm(oro_ctx* c, int stream, int32_t* perm, size_t n);
+
+/* radix_sort(v, ASC|DESC, bits) on an int32/int64 B-shared key followed by
+ * oblivious_apply_elementwise_perm of each A-shared payload (64-bit) with the
+ * returned permutation (radixsort.h:116-229, shuffle.h:687-706). The key is
+ * sorted in place; the returned elementwise permutation (A-shared int32) is
+ * written to perm_out if non-NULL. */
+void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int desc,
+                    int npayload, void** payloads /* npayload x 3 pointers, int64 */,
+                    int32_t* perm_out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

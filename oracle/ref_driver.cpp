@@ -1,0 +1,166 @@
+// ref_driver.cpp — runs ORQ's own 3PC code on seeded inputs and dumps every
+// party's local shares, so the loopback GPU path and the C restatement can be
+// compared with the reference share by share.
+//
+// TEST INFRASTRUCTURE ONLY: built from the ORQ headers by oracle/Makefile into
+// oracle/_ref/ (never shipped), launched as three local party processes by
+// oracle/run_ref.py over ORQ's NoCopy socket communicator.
+//
+// usage: ref_driver <threads> <p_factor> <batch> <op> <n> <data_seed> <outdir> [bits]
+//   threads=1 and batch=-1 give one protocol call per runtime operation, the
+//   schedule the device runtime reproduces.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+
+#include "orq.h"
+
+using namespace orq::debug;
+using namespace orq::service;
+using namespace COMPILED_MPC_PROTOCOL_NAMESPACE;
+
+static uint64_t sm64(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+struct Dumper {
+    std::ofstream f;
+    explicit Dumper(const std::string& path) : f(path, std::ios::binary) {}
+    template <typename T>
+    void rec(const std::string& name, const orq::Vector<T>& a, const orq::Vector<T>& b) {
+        uint32_t nl = name.size(), w = sizeof(T);
+        uint64_t n = a.size();
+        f.write((const char*)&nl, 4);
+        f.write(name.data(), nl);
+        f.write((const char*)&w, 4);
+        f.write((const char*)&n, 8);
+        for (uint64_t i = 0; i < n; i++) {
+            T v = a[i];
+            f.write((const char*)&v, sizeof(T));
+        }
+        for (uint64_t i = 0; i < n; i++) {
+            T v = b[i];
+            f.write((const char*)&v, sizeof(T));
+        }
+    }
+    template <typename SV>
+    void shares(const std::string& name, SV& v) {
+        rec(name, v.vector(0), v.vector(1));
+    }
+    template <typename T>
+    void plain(const std::string& name, const orq::Vector<T>& a) {
+        rec(name, a, a);
+    }
+};
+
+template <typename T>
+static orq::Vector<T> gen(size_t n, uint64_t& st, uint64_t mask) {
+    orq::Vector<T> v(n);
+    for (size_t i = 0; i < n; i++) v[i] = (T)(sm64(st) & mask);
+    return v;
+}
+
+// Sequence of primitives on width T. The restatement replays exactly this
+// sequence, so every PRG stream is consumed in the same order.
+template <typename T>
+static void run_prims(size_t n, uint64_t seed, Dumper& d, const std::string& tag) {
+    uint64_t st = seed;
+    auto x = gen<T>(n, st, ~0ull);
+    auto y = gen<T>(n, st, ~0ull);
+    BSharedVector<T> xb = secret_share_b(x, 0);
+    BSharedVector<T> yb = secret_share_b(y, 1);
+    d.shares(tag + "xb", xb);
+    d.shares(tag + "yb", yb);
+    BSharedVector<T> zb = xb & yb;
+    d.shares(tag + "and", zb);
+    BSharedVector<T> xo = xb ^ yb;
+    d.shares(tag + "xor", xo);
+    ASharedVector<T> xa = secret_share_a(x, 2);
+    ASharedVector<T> ya = secret_share_a(y, 0);
+    d.shares(tag + "xa", xa);
+    d.shares(tag + "ya", ya);
+    ASharedVector<T> za = xa * ya;
+    d.shares(tag + "mul", za);
+    ASharedVector<T> sa = xa + ya;
+    d.shares(tag + "add", sa);
+    ASharedVector<T> ba = xb.b2a_bit();
+    d.shares(tag + "b2a", ba);
+    auto o1 = zb.open();
+    auto o2 = za.open();
+    auto o3 = ba.open();
+    d.plain(tag + "open_and", o1);
+    d.plain(tag + "open_mul", o2);
+    d.plain(tag + "open_b2a", o3);
+}
+
+int main(int argc, char** argv) {
+    orq_init(argc, argv);
+    int pid = runTime->getPartyID();
+    if (argc < 8) {
+        fprintf(stderr, "usage: ref_driver t p batch op n seed outdir [bits]\n");
+        return 2;
+    }
+    std::string op = argv[4];
+    size_t n = std::stoull(argv[5]);
+    uint64_t seed = std::stoull(argv[6]);
+    std::string outdir = argv[7];
+    int bits = argc > 8 ? atoi(argv[8]) : 40;
+    Dumper d(outdir + "/p" + std::to_string(pid) + ".bin");
+
+    auto t0 = std::chrono::steady_clock::now();
+    double secs = 0;
+    if (op == "prims") {
+        run_prims<int32_t>(n, seed, d, "w4_");
+        run_prims<int64_t>(n, seed + 1, d, "w8_");
+        run_prims<int8_t>(n, seed + 2, d, "w1_");
+    } else if (op == "radix" || op == "radix_time") {
+        // radix_sort(key, ASC, bits) then apply the permutation to two
+        // A-shared payloads (key uniform in [0, 2^bits), payloads u32).
+        uint64_t st = seed;
+        uint64_t km = bits >= 64 ? ~0ull : ((1ull << bits) - 1);
+        auto key = gen<int64_t>(n, st, km);
+        auto p1 = gen<int64_t>(n, st, 0xffffffffull);
+        auto p2 = gen<int64_t>(n, st, 0xffffffffull);
+        BSharedVector<int64_t> kb = secret_share_b(key, 0);
+        ASharedVector<int64_t> a1 = secret_share_a(p1, 0);
+        ASharedVector<int64_t> a2 = secret_share_a(p2, 0);
+        t0 = std::chrono::steady_clock::now();
+        auto perm = orq::operators::radix_sort(kb, orq::operators::SortOrder::ASC, bits);
+        orq::operators::oblivious_apply_elementwise_perm(a1, perm);
+        orq::operators::oblivious_apply_elementwise_perm(a2, perm);
+        secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (op == "radix") {
+            d.shares("key", kb);
+            d.shares("pay1", a1);
+            d.shares("pay2", a2);
+            auto pa = perm.getASharedPerm();
+            d.shares("perm", pa);
+        }
+        auto ko = kb.open();
+        auto o1 = a1.open();
+        auto o2 = a2.open();
+        if (op == "radix") {
+            d.plain("open_key", ko);
+            d.plain("open_pay1", o1);
+            d.plain("open_pay2", o2);
+        }
+    } else if (op == "shuffle") {
+        uint64_t st = seed;
+        auto x = gen<int32_t>(n, st, ~0ull);
+        BSharedVector<int32_t> xb = secret_share_b(x, 0);
+        orq::operators::shuffle(xb);
+        d.shares("shuffled", xb);
+        auto o = xb.open();
+        d.plain("open_shuffled", o);
+    } else {
+        fprintf(stderr, "unknown op %s\n", op.c_str());
+        return 2;
+    }
+    if (pid == 0) printf("{\"op\": \"%s\", \"n\": %zu, \"seconds\": %.6f}\n", op.c_str(), n, secs);
+    return 0;
+}
