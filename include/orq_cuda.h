@@ -1,0 +1,140 @@
+/*
+ * orq_cuda.h — C ABI of liborq_cuda.so, the B200 loopback runtime for ORQ's
+ * replicated-3PC share computation.
+ *
+ * The library replaces, for all three parties at once on one GPU, the
+ * per-party protocol dispatch of ORQ's RunTime (include/backend/common/
+ * runtime.h:123-144, generated by runtime_declare_protocol_functions) together
+ * with the socket exchange that follows each round (the ±1 exchange becomes a
+ * property of the share layout), and the operators built from them.
+ *
+ * Conventions
+ *   - A shared vector of n elements of `width` bytes (1, 2, 4, 8 or 16) is
+ *     three device arrays S[0], S[1], S[2]; party p of the reference holds
+ *     (S[p], S[(p+1)%3]) — the layout of get_shares_b/a
+ *     (include/core/protocols/replicated_3pc.h:353-392).
+ *   - `arith` = 1 selects arithmetic shares mod 2^(8*width) (ASharedVector),
+ *     0 boolean XOR shares (BSharedVector).
+ *   - PRG keys are derived from the runtime seed exactly as the deterministic
+ *     key generator used to build the reference; every call consumes the
+ *     runtime's PRG streams in the order the reference consumes them with one
+ *     worker thread and batch size -1, so shares are bit-identical to the
+ *     reference's for the same call sequence.
+ *   - Device pointers must be cudaMalloc'd (or orqcu_malloc'd); arrays of 16-byte
+ *     elements must be 16-byte aligned. Calls are asynchronous on the runtime's
+ *     stream unless stated; results are visible after orqcu_synchronize.
+ *   - Every function returns 0 on success or a negative ORQCU_E* code;
+ *     orqcu_last_error() gives the message of the last failure on this thread.
+ */
+#ifndef ORQ_CUDA_H
+#define ORQ_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORQCU_OK 0
+#define ORQCU_EINVAL (-1)   /* bad argument (reference: assert / std::runtime_error) */
+#define ORQCU_ECUDA (-2)    /* CUDA runtime error */
+#define ORQCU_ERUNTIME (-3) /* protocol-level failure */
+#define ORQCU_ENOMEM (-4)
+
+/* PRG stream ids (include/backend/common/rand_setup.h:90-146,306-381) */
+#define ORQCU_STREAM_PAIR0 0  /* P0/P1 pairwise: P0's get(+1), P1's get(-1) */
+#define ORQCU_STREAM_PAIR1 1
+#define ORQCU_STREAM_PAIR2 2
+#define ORQCU_STREAM_G01 3    /* group {0,1} common PRG */
+#define ORQCU_STREAM_G02 4
+#define ORQCU_STREAM_G12 5
+#define ORQCU_STREAM_G012 6
+#define ORQCU_STREAM_LOCAL0 7 /* party-local PRGs */
+#define ORQCU_STREAM_LOCAL1 8
+#define ORQCU_STREAM_LOCAL2 9
+
+typedef struct orqcu_runtime orqcu_runtime;
+
+int orqcu_version(void);
+const char* orqcu_last_error(void);
+
+/* orq_init (include/backend/common/setup.h:8-58,121-129) for all three
+ * parties: keys for the 10 streams, nonces at 0. device = CUDA ordinal. */
+int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out);
+int orqcu_runtime_destroy(orqcu_runtime* rt);
+/* Run subsequent work on an existing cudaStream_t (NULL = the runtime's own). */
+int orqcu_runtime_set_stream(orqcu_runtime* rt, void* cuda_stream);
+int orqcu_synchronize(orqcu_runtime* rt);
+/* Nonce counter of a PRG stream (AESPRGAlgorithm::nonce, prg_algorithm.h:208). */
+int orqcu_get_nonce(orqcu_runtime* rt, int stream, uint64_t* nonce);
+/* Number of kernels this runtime has launched. */
+int orqcu_kernels_launched(orqcu_runtime* rt, uint64_t* count);
+
+/* device memory helpers */
+int orqcu_malloc(orqcu_runtime* rt, size_t bytes, void** dptr);
+int orqcu_free(orqcu_runtime* rt, void* dptr);
+int orqcu_memcpy_h2d(orqcu_runtime* rt, void* dst_dev, const void* src_host, size_t bytes);
+int orqcu_memcpy_d2h(orqcu_runtime* rt, void* dst_host, const void* src_dev, size_t bytes);
+
+/* Keystream of `stream` starting at nonce0 (AESPRGAlgorithm::fillBytes,
+ * prg_algorithm.h:161-172); does not advance the stream. */
+int orqcu_keystream(orqcu_runtime* rt, int stream, uint64_t nonce0, size_t nbytes, void* out_dev);
+
+/* secret_share_b / secret_share_a (replicated_3pc.h:401-448) with the owner's
+ * local PRG; data_dev is the owner's plaintext on the device. */
+int orqcu_secret_share(orqcu_runtime* rt, int arith, int width, size_t n, const void* data_dev,
+                       int data_party, void* const shares[3]);
+/* public_share (replicated_3pc.h:456-470): S0 = x, S1 = S2 = 0. */
+int orqcu_public_share(orqcu_runtime* rt, int width, size_t n, const void* data_dev,
+                       void* const shares[3]);
+/* open_shares_a / open_shares_b (replicated_3pc.h:310-330). */
+int orqcu_open(orqcu_runtime* rt, int arith, int width, size_t n, const void* const shares[3],
+               void* out_dev);
+
+/* and_b (replicated_3pc.h:166-191) fused with ZeroSharingGenerator::getNextBinary. */
+int orqcu_and_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                const void* const y[3], void* const z[3]);
+/* multiply_a (replicated_3pc.h:44-67) fused with getNextArithmetic. */
+int orqcu_multiply_a(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                     const void* const y[3], void* const z[3]);
+/* xor_b / add_a / sub_a (protocol.h:561-649): local, no randomness. */
+int orqcu_xor_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                const void* const y[3], void* const z[3]);
+int orqcu_add_a(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                const void* const y[3], void* const z[3]);
+int orqcu_sub_a(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                const void* const y[3], void* const z[3]);
+/* not_b (replicated_3pc.h:199). */
+int orqcu_not_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
+/* b2a_bit (replicated_3pc.h:220-251): LSB of a boolean sharing -> arithmetic. */
+int orqcu_b2a_bit(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
+/* Pairwise zero-sharing (zero_sharing_generator.h:101-148). */
+int orqcu_zero_share(orqcu_runtime* rt, int arith, int width, size_t n, void* const r[3]);
+/* Protocol::reshare (protocol.h:500-541), group 0={0,1}, 1={0,2}, 2={1,2}. */
+int orqcu_reshare(orqcu_runtime* rt, int arith, int width, size_t n, int group,
+                  void* const shares[3]);
+
+/* PermutationManager::reserve (permutation_manager.h:102-181): generate
+ * `count` sharded permutations of size n ahead of use. Synchronous. */
+int orqcu_reserve_permutations(orqcu_runtime* rt, size_t n, size_t count);
+/* Pop the next sharded permutation (PermutationManager::getNext) and copy its
+ * three group-local permutations ({0,1},{0,2},{1,2}; gen_perm's output,
+ * hm_sharded_permutation_generator.h:70-108) to perm_dev[g]. */
+int orqcu_next_permutation(orqcu_runtime* rt, size_t n, int32_t* const perm_dev[3]);
+/* shuffle (shuffle.h:752-757). width 4, 8 or 16. */
+int orqcu_shuffle(orqcu_runtime* rt, int arith, int width, size_t n, void* const shares[3]);
+/* oblivious_apply_elementwise_perm (shuffle.h:687-706): x permuted in place by
+ * an A-shared int32 permutation. */
+int orqcu_apply_elementwise_perm(orqcu_runtime* rt, int x_arith, int x_width, size_t n,
+                                 void* const x[3], const void* const perm[3]);
+/* radix_sort (radixsort.h:205-229): sorts the B-shared key (width 4 or 8) on its
+ * low `bits` bits (signed order when bits = 8*width), ascending; writes the
+ * A-shared int32 sorting permutation to perm_out. Synchronous. */
+int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int bits,
+                     int descending, void* const perm_out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORQ_CUDA_H */

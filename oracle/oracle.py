@@ -151,3 +151,8 @@ class Oracle:
         self.lib.oro_radix_sort(ctypes.byref(self.ctx), kw, ctypes.c_size_t(n), self._ptrs(key),
                                 bits, int(desc), len(payloads), pay_arr, self._ptrs(perm))
         return perm
+
+    def shuffle(self, s, arith):
+        w = s[0].dtype.itemsize
+        self.lib.oro_shuffle(ctypes.byref(self.ctx), int(arith), w, ctypes.c_size_t(len(s[0])),
+                             self._ptrs(s))

@@ -674,3 +674,12 @@ void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int de
     while (pq.head < pq.tail) sperm_free(&pq.q[pq.head++]);
     free(pq.q);
 }
+
+/* shuffle (operators/shuffle.h:752-757): one on-demand sharded permutation
+ * (permutation_manager.h:190-209 with an empty queue) applied with resharing. */
+void oro_shuffle(oro_ctx* c, int arith, int w, size_t n, void* s[3]) {
+    sperm sp;
+    sperm_gen(c, &sp, n);
+    apply_sharded(c, arith, w, n, s, &sp);
+    sperm_free(&sp);
+}

@@ -1,0 +1,338 @@
+"""orq_b200 — ORQ's replicated-3PC share computation on one B200.
+
+Python mirror of the reference's user-facing API (include/mpc.h,
+core/containers/{b,a}_shared_vector.h, core/operators/{radixsort,shuffle}.h)
+over the C ABI of liborq_cuda.so (include/orq_cuda.h). All three parties live
+in one process: a shared vector is the three distinct share arrays
+S[0], S[1], S[2] (party p holds S[p], S[p+1]) as one (3, n) CUDA tensor.
+
+    rt = Runtime(seed=1)                     # orq_init(argc, argv)
+    k = rt.secret_share_b(keys, party=0)     # secret_share_b(Vector, 0)
+    perm = radix_sort(k, ASC, bits=40)       # orq::operators::radix_sort
+    oblivious_apply_elementwise_perm(payload, perm)
+    k.open()                                 # BSharedVector::open()
+
+There is no CPU fallback: creating a Runtime without the compiled library or
+a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liborq_cuda.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "orq_cuda.h")
+
+ASC, DESC = 0, 1
+STREAM_PAIR0, STREAM_PAIR1, STREAM_PAIR2 = 0, 1, 2
+STREAM_G01, STREAM_G02, STREAM_G12, STREAM_G012 = 3, 4, 5, 6
+STREAM_LOCAL0, STREAM_LOCAL1, STREAM_LOCAL2 = 7, 8, 9
+
+_lib = None
+
+
+class OrqError(RuntimeError):
+    pass
+
+
+def header_symbols() -> list[str]:
+    """Entry points declared in include/orq_cuda.h."""
+    with open(HEADER) as f:
+        txt = f.read()
+    return sorted(set(re.findall(r"\b(orqcu_[a-z0-9_]+)\s*\(", txt)))
+
+
+def load_library():
+    """Load liborq_cuda.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m orq_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.orqcu_last_error.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = _lib.orqcu_last_error().decode() if _lib else "?"
+        raise OrqError(f"orqcu error {rc}: {msg}")
+
+
+def _torch():
+    import torch  # plumbing only: device memory and streams
+    return torch
+
+
+_TDT = None
+
+
+def _tdtype(width: int):
+    torch = _torch()
+    return {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64, 16: torch.int64}[width]
+
+
+def _p3(t):
+    """(3, ...) tensor -> ctypes array of the three share row pointers."""
+    return (ctypes.c_void_p * 3)(*[t[j].data_ptr() for j in range(3)])
+
+
+class Runtime:
+    """The loopback runtime for all three parties (stands in for orq_init and
+    the per-party RunTime, include/backend/common/setup.h:8-58)."""
+
+    def __init__(self, seed: int = 1, device: int = 0):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise OrqError("orq_b200 needs a CUDA device (no CPU fallback)")
+        self.lib = load_library()
+        self.device = device
+        torch.cuda.set_device(device)
+        h = ctypes.c_void_p()
+        _check(self.lib.orqcu_runtime_create(ctypes.c_uint64(seed), device, ctypes.byref(h)))
+        self.h = h
+        # run on torch's current stream so tensor ops and ORQ kernels are ordered
+        _check(self.lib.orqcu_runtime_set_stream(self.h, ctypes.c_void_p(
+            torch.cuda.current_stream(device).cuda_stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.orqcu_runtime_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state ------------------------------------------------------------
+    def nonce(self, stream: int) -> int:
+        v = ctypes.c_uint64()
+        _check(self.lib.orqcu_get_nonce(self.h, stream, ctypes.byref(v)))
+        return v.value
+
+    def kernels_launched(self) -> int:
+        v = ctypes.c_uint64()
+        _check(self.lib.orqcu_kernels_launched(self.h, ctypes.byref(v)))
+        return v.value
+
+    def synchronize(self):
+        _check(self.lib.orqcu_synchronize(self.h))
+
+    # -- sharing ----------------------------------------------------------
+    def _alloc(self, n: int, width: int):
+        torch = _torch()
+        if width == 16:
+            return torch.empty((3, n, 2), dtype=torch.int64, device=f"cuda:{self.device}")
+        return torch.empty((3, n), dtype=_tdtype(width), device=f"cuda:{self.device}")
+
+    def _to_dev(self, data, width: int):
+        torch = _torch()
+        if isinstance(data, np.ndarray):
+            data = torch.from_numpy(np.ascontiguousarray(data))
+        if data.element_size() != width:
+            raise ValueError("data element size does not match the share width")
+        return data.to(f"cuda:{self.device}").contiguous()
+
+    def secret_share_b(self, data, party: int = 0) -> "BSharedVector":
+        """secret_share_b (replicated_3pc.h:401-420): owner `party` splits data
+        with its local PRG."""
+        return BSharedVector(self, self._share(data, party, arith=False))
+
+    def secret_share_a(self, data, party: int = 0) -> "ASharedVector":
+        """secret_share_a (replicated_3pc.h:429-448)."""
+        return ASharedVector(self, self._share(data, party, arith=True))
+
+    def _share(self, data, party, arith):
+        w = data.itemsize if isinstance(data, np.ndarray) else data.element_size()
+        d = self._to_dev(data, w)
+        n = d.shape[0]
+        s = self._alloc(n, w)
+        _check(self.lib.orqcu_secret_share(self.h, int(arith), w, ctypes.c_size_t(n),
+                                           ctypes.c_void_p(d.data_ptr()), party, _p3(s)))
+        return s
+
+    def public_share(self, data, arith=True):
+        """public_share (replicated_3pc.h:456-470)."""
+        w = data.itemsize if isinstance(data, np.ndarray) else data.element_size()
+        d = self._to_dev(data, w)
+        s = self._alloc(d.shape[0], w)
+        _check(self.lib.orqcu_public_share(self.h, w, ctypes.c_size_t(d.shape[0]),
+                                           ctypes.c_void_p(d.data_ptr()), _p3(s)))
+        return (ASharedVector if arith else BSharedVector)(self, s)
+
+    def from_shares(self, shares, arith: bool):
+        """Wrap existing (3, n) device shares."""
+        return (ASharedVector if arith else BSharedVector)(self, shares)
+
+    # -- randomness -------------------------------------------------------
+    def keystream(self, stream: int, nonce0: int, nbytes: int):
+        torch = _torch()
+        out = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{self.device}")
+        _check(self.lib.orqcu_keystream(self.h, stream, ctypes.c_uint64(nonce0),
+                                        ctypes.c_size_t(nbytes), ctypes.c_void_p(out.data_ptr())))
+        return out
+
+    def zero_share(self, n: int, width: int, arith: bool):
+        s = self._alloc(n, width)
+        _check(self.lib.orqcu_zero_share(self.h, int(arith), width, ctypes.c_size_t(n), _p3(s)))
+        return s
+
+    def reserve_permutations(self, n: int, count: int):
+        """PermutationManager::reserve (permutation_manager.h:102-181)."""
+        _check(self.lib.orqcu_reserve_permutations(self.h, ctypes.c_size_t(n), ctypes.c_size_t(count)))
+
+    def next_permutation(self, n: int):
+        """The three group-local permutations of the next sharded permutation."""
+        torch = _torch()
+        out = torch.empty((3, n), dtype=torch.int32, device=f"cuda:{self.device}")
+        ptrs = (ctypes.c_void_p * 3)(*[out[g].data_ptr() for g in range(3)])
+        _check(self.lib.orqcu_next_permutation(self.h, ctypes.c_size_t(n), ptrs))
+        return out
+
+
+class SharedVector:
+    arith = False
+
+    def __init__(self, rt: Runtime, shares):
+        self.rt = rt
+        self.shares = shares
+
+    @property
+    def width(self) -> int:
+        s = self.shares
+        return 16 if s.dim() == 3 else s.element_size()
+
+    def size(self) -> int:
+        return self.shares.shape[1]
+
+    def __len__(self):
+        return self.size()
+
+    def open(self):
+        """open_shares_a/b (replicated_3pc.h:310-330); returns a device tensor."""
+        rt = self.rt
+        n, w = self.size(), self.width
+        out = rt._alloc(1, w)[0] if n == 0 else None
+        torch = _torch()
+        shape = (n, 2) if w == 16 else (n,)
+        out = torch.empty(shape, dtype=self.shares.dtype, device=self.shares.device)
+        _check(rt.lib.orqcu_open(rt.h, int(self.arith), w, ctypes.c_size_t(n), _p3(self.shares),
+                                 ctypes.c_void_p(out.data_ptr())))
+        return out
+
+    def _bin(self, other, fn, cls):
+        if other.size() != self.size() or other.width != self.width:
+            raise ValueError("size/width mismatch")
+        z = self.rt._alloc(self.size(), self.width)
+        _check(fn(self.rt.h, self.width, ctypes.c_size_t(self.size()), _p3(self.shares),
+                  _p3(other.shares), _p3(z)))
+        return cls(self.rt, z)
+
+    def _ibin(self, other, fn):
+        if other.size() != self.size() or other.width != self.width:
+            raise ValueError("size/width mismatch")
+        _check(fn(self.rt.h, self.width, ctypes.c_size_t(self.size()), _p3(self.shares),
+                  _p3(other.shares), _p3(self.shares)))
+        return self
+
+    def clone(self):
+        return type(self)(self.rt, self.shares.clone())
+
+
+class BSharedVector(SharedVector):
+    """Boolean (XOR) shares (core/containers/b_shared_vector.h)."""
+    arith = False
+
+    def __and__(self, o):
+        return self._bin(o, self.rt.lib.orqcu_and_b, BSharedVector)
+
+    def __xor__(self, o):
+        return self._bin(o, self.rt.lib.orqcu_xor_b, BSharedVector)
+
+    def __iand__(self, o):
+        return self._ibin(o, self.rt.lib.orqcu_and_b)
+
+    def __ixor__(self, o):
+        return self._ibin(o, self.rt.lib.orqcu_xor_b)
+
+    def __invert__(self):
+        z = self.rt._alloc(self.size(), self.width)
+        _check(self.rt.lib.orqcu_not_b(self.rt.h, self.width, ctypes.c_size_t(self.size()),
+                                       _p3(self.shares), _p3(z)))
+        return BSharedVector(self.rt, z)
+
+    def b2a_bit(self) -> "ASharedVector":
+        """b2a_bit (b_shared_vector.h:279-284, replicated_3pc.h:220-251)."""
+        z = self.rt._alloc(self.size(), self.width)
+        _check(self.rt.lib.orqcu_b2a_bit(self.rt.h, self.width, ctypes.c_size_t(self.size()),
+                                         _p3(self.shares), _p3(z)))
+        return ASharedVector(self.rt, z)
+
+
+class ASharedVector(SharedVector):
+    """Arithmetic shares mod 2^(8w) (core/containers/a_shared_vector.h)."""
+    arith = True
+
+    def __mul__(self, o):
+        return self._bin(o, self.rt.lib.orqcu_multiply_a, ASharedVector)
+
+    def __add__(self, o):
+        return self._bin(o, self.rt.lib.orqcu_add_a, ASharedVector)
+
+    def __sub__(self, o):
+        return self._bin(o, self.rt.lib.orqcu_sub_a, ASharedVector)
+
+    def __imul__(self, o):
+        return self._ibin(o, self.rt.lib.orqcu_multiply_a)
+
+    def __iadd__(self, o):
+        return self._ibin(o, self.rt.lib.orqcu_add_a)
+
+    def __isub__(self, o):
+        return self._ibin(o, self.rt.lib.orqcu_sub_a)
+
+
+class ElementwisePermutation(ASharedVector):
+    """A-shared int32 destination indices (core/containers/permutation.h)."""
+
+
+def reshare(v: SharedVector, group: int):
+    """Protocol::reshare (protocol.h:500-541) in place."""
+    rt = v.rt
+    _check(rt.lib.orqcu_reshare(rt.h, int(v.arith), v.width, ctypes.c_size_t(v.size()), group,
+                                _p3(v.shares)))
+
+
+def shuffle(v: SharedVector):
+    """orq::operators::shuffle (shuffle.h:752-757), in place."""
+    rt = v.rt
+    _check(rt.lib.orqcu_shuffle(rt.h, int(v.arith), v.width, ctypes.c_size_t(v.size()),
+                                _p3(v.shares)))
+
+
+def oblivious_apply_elementwise_perm(x: SharedVector, perm: ASharedVector):
+    """shuffle.h:687-706, in place on x."""
+    rt = x.rt
+    _check(rt.lib.orqcu_apply_elementwise_perm(rt.h, int(x.arith), x.width,
+                                               ctypes.c_size_t(x.size()), _p3(x.shares),
+                                               _p3(perm.shares)))
+
+
+def radix_sort(v: BSharedVector, order: int = ASC, bits: int | None = None) -> ElementwisePermutation:
+    """orq::operators::radix_sort (radixsort.h:205-229): sorts v in place and
+    returns the A-shared sorting permutation."""
+    rt = v.rt
+    if bits is None:
+        bits = 8 * v.width
+    perm = rt._alloc(v.size(), 4)
+    _check(rt.lib.orqcu_radix_sort(rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares),
+                                   bits, int(order == DESC), _p3(perm)))
+    return ElementwisePermutation(rt, perm)

@@ -1,0 +1,320 @@
+// capi.cu — extern "C" entry points (include/orq_cuda.h).
+#include <cstring>
+#include <string>
+
+#include "../../include/orq_cuda.h"
+#include "runtime.h"
+
+struct orqcu_runtime {
+    orqcu::Ctx ctx;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+int guard(F&& f) {
+    try {
+        f();
+        return ORQCU_OK;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return ORQCU_EINVAL;
+    } catch (const std::bad_alloc& e) {
+        g_err = e.what();
+        return ORQCU_ENOMEM;
+    } catch (const std::runtime_error& e) {
+        g_err = e.what();
+        return std::strstr(e.what(), "CUDA error") ? ORQCU_ECUDA : ORQCU_ERUNTIME;
+    } catch (...) {
+        g_err = "unknown error";
+        return ORQCU_ERUNTIME;
+    }
+}
+
+void need(bool ok, const char* msg) {
+    if (!ok) throw std::invalid_argument(msg);
+}
+void need_rt(orqcu_runtime* rt) { need(rt != nullptr, "null runtime"); }
+void need_w(int w) { need(w == 1 || w == 2 || w == 4 || w == 8 || w == 16, "width must be 1,2,4,8,16"); }
+void need_sh(const void* const s[3], size_t n, const char* what) {
+    if (n == 0) return;
+    need(s != nullptr && s[0] && s[1] && s[2], what);
+}
+orqcu::CSh3 c3(const void* const s[3]) { return orqcu::CSh3{{s[0], s[1], s[2]}}; }
+orqcu::Sh3 m3(void* const s[3]) { return orqcu::Sh3{{s[0], s[1], s[2]}}; }
+
+}  // namespace
+
+extern "C" {
+
+int orqcu_version(void) { return 1; }
+const char* orqcu_last_error(void) { return g_err.c_str(); }
+
+int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out) {
+    return guard([&] {
+        need(out != nullptr, "null output");
+        int ndev = 0;
+        ORQ_CUDA_CHECK(cudaGetDeviceCount(&ndev));
+        need(device >= 0 && device < ndev, "no such CUDA device");
+        ORQ_CUDA_CHECK(cudaSetDevice(device));
+        auto* rt = new orqcu_runtime();
+        rt->ctx.device = device;
+        ORQ_CUDA_CHECK(cudaDeviceGetAttribute(&rt->ctx.num_sms, cudaDevAttrMultiProcessorCount, device));
+        ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&rt->ctx.stream, cudaStreamNonBlocking));
+        rt->ctx.owns_stream = true;
+        orqcu::init_ctx_keys(rt->ctx, seed);
+        orqcu::upload_aes_tables(device);
+        *out = rt;
+    });
+}
+
+int orqcu_runtime_destroy(orqcu_runtime* rt) {
+    return guard([&] {
+        if (!rt) return;
+        cudaSetDevice(rt->ctx.device);
+        cudaStreamSynchronize(rt->ctx.stream);
+        for (auto& sp : rt->ctx.perm_queue) rt->ctx.free_perm(sp);
+        rt->ctx.perm_queue.clear();
+        if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
+        delete rt;
+    });
+}
+
+int orqcu_runtime_set_stream(orqcu_runtime* rt, void* s) {
+    return guard([&] {
+        need_rt(rt);
+        cudaSetDevice(rt->ctx.device);
+        if (s == nullptr) {
+            if (!rt->ctx.owns_stream) {
+                ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&rt->ctx.stream, cudaStreamNonBlocking));
+                rt->ctx.owns_stream = true;
+            }
+            return;
+        }
+        if (rt->ctx.owns_stream) {
+            ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+            cudaStreamDestroy(rt->ctx.stream);
+        }
+        rt->ctx.stream = (cudaStream_t)s;
+        rt->ctx.owns_stream = false;
+    });
+}
+
+int orqcu_synchronize(orqcu_runtime* rt) {
+    return guard([&] {
+        need_rt(rt);
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+    });
+}
+
+int orqcu_get_nonce(orqcu_runtime* rt, int stream, uint64_t* nonce) {
+    return guard([&] {
+        need_rt(rt);
+        need(stream >= 0 && stream < orqcu::NSTREAMS && nonce, "bad stream id");
+        *nonce = rt->ctx.nonce[stream];
+    });
+}
+
+int orqcu_kernels_launched(orqcu_runtime* rt, uint64_t* count) {
+    return guard([&] {
+        need_rt(rt);
+        need(count != nullptr, "null output");
+        *count = rt->ctx.kernels_launched;
+    });
+}
+
+int orqcu_malloc(orqcu_runtime* rt, size_t bytes, void** dptr) {
+    return guard([&] {
+        need_rt(rt);
+        need(dptr != nullptr, "null output");
+        cudaSetDevice(rt->ctx.device);
+        ORQ_CUDA_CHECK(cudaMalloc(dptr, bytes ? bytes : 1));
+    });
+}
+int orqcu_free(orqcu_runtime* rt, void* dptr) {
+    return guard([&] {
+        need_rt(rt);
+        ORQ_CUDA_CHECK(cudaFree(dptr));
+    });
+}
+int orqcu_memcpy_h2d(orqcu_runtime* rt, void* dst, const void* src, size_t bytes) {
+    return guard([&] {
+        need_rt(rt);
+        if (!bytes) return;
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, rt->ctx.stream));
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+    });
+}
+int orqcu_memcpy_d2h(orqcu_runtime* rt, void* dst, const void* src, size_t bytes) {
+    return guard([&] {
+        need_rt(rt);
+        if (!bytes) return;
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, rt->ctx.stream));
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+    });
+}
+
+int orqcu_keystream(orqcu_runtime* rt, int stream, uint64_t nonce0, size_t nbytes, void* out) {
+    return guard([&] {
+        need_rt(rt);
+        need(stream >= 0 && stream < orqcu::NSTREAMS, "bad stream id");
+        need(out != nullptr || nbytes == 0, "null output");
+        orqcu::launch_keystream(rt->ctx, stream, nonce0, out, nbytes);
+    });
+}
+
+int orqcu_secret_share(orqcu_runtime* rt, int arith, int width, size_t n, const void* data,
+                       int data_party, void* const shares[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh((const void* const*)shares, n, "null share pointer");
+        need(data != nullptr || n == 0, "null data");
+        orqcu::op_secret_share(rt->ctx, arith != 0, width, n, data, data_party, m3(shares));
+    });
+}
+
+int orqcu_public_share(orqcu_runtime* rt, int width, size_t n, const void* data, void* const shares[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh((const void* const*)shares, n, "null share pointer");
+        orqcu::op_public_share(rt->ctx, width, n, data, m3(shares));
+    });
+}
+
+int orqcu_open(orqcu_runtime* rt, int arith, int width, size_t n, const void* const shares[3], void* out) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh(shares, n, "null share pointer");
+        orqcu::op_open(rt->ctx, arith != 0, width, n, c3(shares), out);
+    });
+}
+
+static int binop(orqcu_runtime* rt, int kind, int width, size_t n, const void* const x[3],
+                 const void* const y[3], void* const z[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh(x, n, "null x");
+        need_sh(y, n, "null y");
+        need_sh((const void* const*)z, n, "null z");
+        switch (kind) {
+            case 0: orqcu::op_mult(rt->ctx, false, width, n, c3(x), c3(y), m3(z)); break;
+            case 1: orqcu::op_mult(rt->ctx, true, width, n, c3(x), c3(y), m3(z)); break;
+            case 2: orqcu::op_local(rt->ctx, 0, width, n, c3(x), c3(y), m3(z)); break;
+            case 3: orqcu::op_local(rt->ctx, 1, width, n, c3(x), c3(y), m3(z)); break;
+            case 4: orqcu::op_local(rt->ctx, 2, width, n, c3(x), c3(y), m3(z)); break;
+        }
+    });
+}
+
+int orqcu_and_b(orqcu_runtime* rt, int w, size_t n, const void* const x[3], const void* const y[3], void* const z[3]) {
+    return binop(rt, 0, w, n, x, y, z);
+}
+int orqcu_multiply_a(orqcu_runtime* rt, int w, size_t n, const void* const x[3], const void* const y[3], void* const z[3]) {
+    return binop(rt, 1, w, n, x, y, z);
+}
+int orqcu_xor_b(orqcu_runtime* rt, int w, size_t n, const void* const x[3], const void* const y[3], void* const z[3]) {
+    return binop(rt, 2, w, n, x, y, z);
+}
+int orqcu_add_a(orqcu_runtime* rt, int w, size_t n, const void* const x[3], const void* const y[3], void* const z[3]) {
+    return binop(rt, 3, w, n, x, y, z);
+}
+int orqcu_sub_a(orqcu_runtime* rt, int w, size_t n, const void* const x[3], const void* const y[3], void* const z[3]) {
+    return binop(rt, 4, w, n, x, y, z);
+}
+
+int orqcu_not_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh(x, n, "null x");
+        need_sh((const void* const*)y, n, "null y");
+        orqcu::op_not(rt->ctx, width, n, c3(x), m3(y));
+    });
+}
+
+int orqcu_b2a_bit(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh(x, n, "null x");
+        need_sh((const void* const*)y, n, "null y");
+        orqcu::op_b2a_bit(rt->ctx, width, n, c3(x), m3(y));
+    });
+}
+
+int orqcu_zero_share(orqcu_runtime* rt, int arith, int width, size_t n, void* const r[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh((const void* const*)r, n, "null r");
+        orqcu::op_zero_share(rt->ctx, arith != 0, width, n, m3(r));
+    });
+}
+
+int orqcu_reshare(orqcu_runtime* rt, int arith, int width, size_t n, int group, void* const s[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_w(width);
+        need_sh((const void* const*)s, n, "null shares");
+        orqcu::op_reshare(rt->ctx, arith != 0, width, n, group, m3(s));
+    });
+}
+
+int orqcu_reserve_permutations(orqcu_runtime* rt, size_t n, size_t count) {
+    return guard([&] {
+        need_rt(rt);
+        orqcu::reserve_perms(rt->ctx, n, count);
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+    });
+}
+
+int orqcu_next_permutation(orqcu_runtime* rt, size_t n, int32_t* const perm_dev[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(perm_dev != nullptr, "null output");
+        orqcu::ShardedPerm sp = orqcu::next_perm(rt->ctx, n);
+        for (int g = 0; g < 3; g++)
+            if (n)
+                ORQ_CUDA_CHECK(cudaMemcpyAsync(perm_dev[g], sp.perm[g], n * 4, cudaMemcpyDeviceToDevice,
+                                               rt->ctx.stream));
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+        rt->ctx.free_perm(sp);
+    });
+}
+
+int orqcu_shuffle(orqcu_runtime* rt, int arith, int width, size_t n, void* const s[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_sh((const void* const*)s, n, "null shares");
+        orqcu::op_shuffle(rt->ctx, arith != 0, width, n, m3(s));
+    });
+}
+
+int orqcu_apply_elementwise_perm(orqcu_runtime* rt, int x_arith, int x_width, size_t n,
+                                 void* const x[3], const void* const perm[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_sh((const void* const*)x, n, "null x");
+        need_sh(perm, n, "null perm");
+        orqcu::op_apply_elementwise(rt->ctx, x_arith != 0, x_width, n, m3(x), c3(perm));
+    });
+}
+
+int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int bits,
+                     int descending, void* const perm_out[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_sh((const void* const*)key, n, "null key");
+        need_sh((const void* const*)perm_out, n, "null perm_out");
+        orqcu::op_radix_sort(rt->ctx, key_width, n, m3(key), bits, descending != 0, m3(perm_out));
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,917 @@
+// perm.cu — sharded permutations: generation (Fisher–Yates from the group
+// PRGs, bit-exact with ORQ) and their oblivious application fused with the
+// group reshare.
+//
+// Generation restates gen_perm (include/core/random/permutations/
+// hm_sharded_permutation_generator.h:70-108): draws are u32 words of the group
+// stream taken from getNext buffers of 2^20 words (4 nonces each), reduced by
+// mask = 2^bit_width(n) - 1; draw values above n-1-i are rejected; the i-th
+// accepted value v gives swap(p[i], p[i+v]). A permutation starts on a fresh
+// buffer, so consecutive permutations of one group form a chain whose start
+// nonces depend on how many draws the previous one used.
+//
+// GPU design:
+//  * fy_gen  (all SMs but three): AES keystream of a window of buffers, drop
+//    draws with v >= n (they can never be accepted), compact the survivors of
+//    each 32768-draw tile in order, record a tile bitmap and the tile minimum.
+//  * fy_scan (one 1024-thread CTA per group): replays the sequential
+//    acceptance exactly over the survivors, 8192 at a time; a survivor is
+//    certainly accepted if v + (its index in the step) <= n-1-i, certainly
+//    rejected if v > n-1-i, and the rare ones in between are decided in order
+//    by one thread. Tiles whose minimum exceeds n-1-i are skipped.
+//    Window w+1 is generated while window w is scanned.
+//  * fy_finalize: turns the accepted offsets into the final permutation in
+//    parallel (see k_fy_final) and writes its inverse.
+#include <algorithm>
+#include <cstring>
+
+#include "launch.cuh"
+
+namespace orqcu {
+
+namespace {
+
+constexpr uint32_t kTileDraws = 32768;        // draws per tile
+constexpr uint32_t kTileBlocks = kTileDraws / 4;
+constexpr uint32_t kTilesPerRefill = (1u << 20) / kTileDraws;  // 32
+constexpr uint32_t kBitWords = kTileDraws / 32;                // 1024
+constexpr int kScanThreads = 1024;
+constexpr uint32_t kStep = 8192;  // survivors per scan step (8 per thread)
+
+struct FyState {
+    unsigned long long start_tile;  // absolute tile where the current permutation starts
+    uint32_t m;                     // index of the permutation being scanned
+    uint32_t i;                     // accepted so far
+    uint32_t done;
+    uint32_t pad;
+};
+
+struct FyGenArgs {
+    StreamArg st[3];  // nonce = chain start nonce + 4 * (window start buffer)
+    uint32_t n, mask, tiles;
+    uint32_t* surv;   // [3][tiles][kTileDraws]
+    uint32_t* cnt;    // [3][tiles]
+    uint32_t* tmin;   // [3][tiles]
+    uint32_t* bits;   // [3][tiles][kBitWords]
+    const FyState* state;
+};
+
+__global__ void __launch_bounds__(kAesThreads) k_fy_gen(FyGenArgs a) {
+    extern __shared__ uint32_t sm[];
+    __shared__ uint32_t red[33];
+    __shared__ uint32_t smin, sdone;
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    const uint32_t total = 3 * a.tiles;
+    for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const uint32_t g = item / a.tiles, tile = item % a.tiles;
+        // the scanner may be updating the flag concurrently: read it once per CTA
+        if (threadIdx.x == 0) sdone = *(volatile const uint32_t*)&a.state[g].done;
+        __syncthreads();
+        if (sdone) continue;
+        const size_t slot = (size_t)g * a.tiles + tile;
+        uint32_t* out = a.surv + slot * kTileDraws;
+        uint32_t* bw = a.bits + slot * kBitWords;
+        if (threadIdx.x == 0) smin = 0xffffffffu;
+        uint32_t base = 0, mymin = 0xffffffffu;
+        for (uint32_t q = 0; q < kTileBlocks / kAesThreads; q++) {
+            const uint32_t lb = q * kAesThreads + threadIdx.x;  // block within tile
+            const uint4 ks =
+                keystream_block(S, a.st[g], (unsigned long long)tile * kTileBlocks + lb);
+            const uint32_t v0 = ks.x & a.mask, v1 = ks.y & a.mask, v2 = ks.z & a.mask,
+                           v3 = ks.w & a.mask;
+            const uint32_t f = (v0 < a.n) | ((v1 < a.n) << 1) | ((v2 < a.n) << 2) | ((v3 < a.n) << 3);
+            const uint32_t c = __popc(f);
+            uint32_t tot;
+            const uint32_t off = block_excl_sum(c, red, tot);
+            uint32_t* o = out + base + off;
+            if (f & 1) { *o++ = v0; mymin = min(mymin, v0); }
+            if (f & 2) { *o++ = v1; mymin = min(mymin, v1); }
+            if (f & 4) { *o++ = v2; mymin = min(mymin, v2); }
+            if (f & 8) { *o++ = v3; mymin = min(mymin, v3); }
+            // survivor bitmap: 8 threads x 4 bits per 32-bit word
+            uint32_t word = f << ((threadIdx.x & 7) * 4);
+            word |= __shfl_xor_sync(0xffffffffu, word, 1);
+            word |= __shfl_xor_sync(0xffffffffu, word, 2);
+            word |= __shfl_xor_sync(0xffffffffu, word, 4);
+            if ((threadIdx.x & 7) == 0) bw[lb >> 3] = word;
+            base += tot;
+        }
+        atomicMin(&smin, mymin);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            a.cnt[slot] = base;
+            a.tmin[slot] = smin;
+        }
+        __syncthreads();
+    }
+}
+
+struct FyScanArgs {
+    uint32_t n, count, tiles;
+    unsigned long long win_tile0;  // absolute index of the window's first tile
+    const uint32_t* surv;
+    const uint32_t* cnt;
+    const uint32_t* tmin;
+    const uint32_t* bits;
+    FyState* state;        // [3]
+    uint32_t* acc;         // [3][count][n] accepted offsets v_i (swap with i + v_i)
+    uint32_t* refills;     // [3][count] getNext buffers used
+};
+
+// Position of the q-th set bit (0-based) of a tile bitmap.
+__device__ uint32_t nth_set_bit(const uint32_t* bw, uint32_t q, uint32_t* red) {
+    __shared__ uint32_t pos;
+    const uint32_t w = bw[threadIdx.x];  // kBitWords == blockDim.x
+    const uint32_t c = __popc(w);
+    uint32_t tot;
+    const uint32_t pre = block_excl_sum(c, red, tot);
+    if (q >= pre && q < pre + c) {
+        uint32_t r = q - pre, x = w;
+        for (uint32_t k = 0; k < r; k++) x &= x - 1;
+        pos = threadIdx.x * 32 + (__ffs(x) - 1);
+    }
+    __syncthreads();
+    const uint32_t p = pos;
+    __syncthreads();
+    return p;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
+    __shared__ uint32_t red[33];
+    __shared__ uint32_t s_i, s_m, s_done, s_last_q, s_nunc;
+    __shared__ unsigned long long s_start;
+    __shared__ uint32_t unc_q[kStep / 8];   // uncertain survivors of a step (capped)
+    __shared__ uint32_t unc_cp[kStep / 8];
+    __shared__ uint8_t unc_ok[kStep / 8];
+    const uint32_t g = blockIdx.x;
+    const uint32_t n = a.n;
+    if (threadIdx.x == 0) {
+        s_i = a.state[g].i;
+        s_m = a.state[g].m;
+        s_done = a.state[g].done;
+        s_start = a.state[g].start_tile;
+    }
+    __syncthreads();
+    for (uint32_t tile = 0; tile < a.tiles; tile++) {
+        if (s_done) break;
+        const unsigned long long abs_tile = a.win_tile0 + tile;
+        if (abs_tile < s_start) continue;
+        const size_t slot = (size_t)g * a.tiles + tile;
+        const uint32_t c = a.cnt[slot];
+        if (a.tmin[slot] > n - 1 - s_i) continue;
+        const uint32_t* sv = a.surv + slot * kTileDraws;
+        bool finished = false;
+        for (uint32_t sb = 0; sb < c && !finished; sb += kStep) {
+            const uint32_t i0 = s_i;
+            const long long T = (long long)n - 1 - i0;
+            uint32_t v[8];
+            uint32_t certain = 0, unc = 0;
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const uint32_t q = threadIdx.x * 8 + u;  // index within the step
+                v[u] = (sb + q < c) ? sv[sb + q] : 0xffffffffu;
+                const long long vv = v[u] == 0xffffffffu ? (1ll << 40) : (long long)v[u];
+                if (vv + q <= T) certain |= 1u << u;
+                else if (vv <= T) unc |= 1u << u;
+            }
+            uint32_t accept = certain;
+            const int any_unc = __syncthreads_or(unc != 0);
+            if (any_unc) {
+                // order the uncertain survivors and decide them one by one
+                uint32_t tot_c;
+                const uint32_t cpre = block_excl_sum(__popc(certain), red, tot_c);
+                uint32_t tot_u;
+                const uint32_t upre = block_excl_sum(__popc(unc), red, tot_u);
+                const uint32_t cap = kStep / 8;
+                {
+                    uint32_t k = upre, cc = cpre;
+                    for (int u = 0; u < 8; u++) {
+                        if ((unc >> u) & 1u) {
+                            if (k < cap) {
+                                unc_q[k] = threadIdx.x * 8 + u;
+                                unc_cp[k] = cc;
+                            }
+                            k++;
+                        }
+                        if ((certain >> u) & 1u) cc++;
+                    }
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    uint32_t uacc = 0;
+                    const uint32_t m = tot_u < cap ? tot_u : cap;
+                    for (uint32_t k = 0; k < m; k++) {
+                        const uint32_t q = unc_q[k];
+                        const uint32_t vv = sv[sb + q];
+                        const unsigned long long iat = (unsigned long long)i0 + unc_cp[k] + uacc;
+                        const bool ok = iat < n && (unsigned long long)vv <= (unsigned long long)n - 1 - iat;
+                        unc_ok[k] = ok;
+                        uacc += ok;
+                    }
+                    s_nunc = m;
+                }
+                __syncthreads();
+                if (tot_u > cap) {
+                    // More uncertain survivors than the list holds (only when n is
+                    // tiny): fall back to a fully sequential decision of this step.
+                    if (threadIdx.x == 0) s_nunc = 0xffffffffu;
+                }
+                __syncthreads();
+                if (s_nunc == 0xffffffffu) {
+                    __shared__ uint32_t seq_acc[kStep / 32];
+                    if (threadIdx.x < kStep / 32) seq_acc[threadIdx.x] = 0;
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        uint32_t ii = i0;
+                        const uint32_t lim = (c - sb) < kStep ? (c - sb) : kStep;
+                        for (uint32_t q = 0; q < lim && ii < n; q++) {
+                            const uint32_t vv = sv[sb + q];
+                            if (vv <= n - 1 - ii) {
+                                seq_acc[q >> 5] |= 1u << (q & 31);
+                                ii++;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                    accept = 0;
+                    for (int u = 0; u < 8; u++) {
+                        const uint32_t q = threadIdx.x * 8 + u;
+                        if ((seq_acc[q >> 5] >> (q & 31)) & 1u) accept |= 1u << u;
+                    }
+                } else {
+                    uint32_t k = upre;
+                    for (int u = 0; u < 8; u++)
+                        if ((unc >> u) & 1u) {
+                            if (unc_ok[k]) accept |= 1u << u;
+                            k++;
+                        }
+                }
+            }
+            uint32_t tot_a;
+            const uint32_t apre = block_excl_sum(__popc(accept), red, tot_a);
+            const uint32_t need = n - i0;
+            uint32_t* acc = a.acc + ((size_t)g * a.count + s_m) * (size_t)n;
+            uint32_t r = apre;
+            for (int u = 0; u < 8; u++) {
+                if ((accept >> u) & 1u) {
+                    if (r < need) {
+                        acc[i0 + r] = v[u];
+                        if (r == need - 1) s_last_q = sb + threadIdx.x * 8 + u;
+                    }
+                    r++;
+                }
+            }
+            __syncthreads();
+            if (tot_a >= need) {
+                // permutation complete: locate its last draw, count the buffers
+                const uint32_t p = nth_set_bit(a.bits + slot * kBitWords, s_last_q, red);
+                if (threadIdx.x == 0) {
+                    const unsigned long long kend =
+                        (abs_tile - s_start) * (unsigned long long)kTileDraws + p;
+                    const unsigned long long R = 1 + ((kend + 1) >> 20);
+                    a.refills[(size_t)g * a.count + s_m] = (uint32_t)R;
+                    s_start = (s_start / kTilesPerRefill + R) * kTilesPerRefill;
+                    s_m = s_m + 1;
+                    s_i = 0;
+                    if (s_m >= a.count) s_done = 1;
+                }
+                finished = true;
+            } else if (threadIdx.x == 0) {
+                s_i = i0 + tot_a;
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        a.state[g].i = s_i;
+        a.state[g].m = s_m;
+        a.state[g].done = s_done;
+        a.state[g].start_tile = s_start;
+    }
+}
+
+// ---- finalize: accepted offsets -> permutation -----------------------------
+// Step i swaps positions i and j_i = i + v_i (j_i >= i), so position i is final
+// after step i. Let A(k) be the value at position k when step k starts: A(k) =
+// A(parent(k)) where parent(k) is the last earlier step whose target was k, or
+// k itself when no earlier step touched k (identity start). Then
+//   p[i] = value at j_i just before step i
+//        = A(previous step that targeted j_i)  or  j_i if there is none,
+// and self-swaps (j_i = i) give p[i] = A(i). Parents come from an atomicMax
+// over targets, A from chasing parent links, the "previous step with the same
+// target" from a small bucket per target.
+struct FinArgs {
+    const uint32_t* acc;  // [P][n]
+    uint32_t n, P;
+    int32_t* par;         // [P][n]  last earlier step targeting k (-1)
+    uint32_t* cnt;        // [P][n]  non-self steps per target
+    uint32_t* off;        // [P][n]  bucket offsets (exclusive, per permutation)
+    uint32_t* fill;       // [P][n]
+    int32_t* bucket;      // [P][n]
+    int32_t* A;           // [P][n]
+    int32_t* const* perm_out;  // [P] -> n
+    int32_t* const* inv_out;   // [P] -> n
+};
+
+__global__ void k_fin_init(FinArgs a) {
+    const size_t tot = (size_t)a.P * a.n;
+    for (size_t t = gtid(); t < tot; t += gstride()) {
+        a.par[t] = -1;
+        a.cnt[t] = 0;
+        a.fill[t] = 0;
+    }
+}
+__global__ void k_fin_targets(FinArgs a) {
+    const size_t tot = (size_t)a.P * a.n;
+    for (size_t t = gtid(); t < tot; t += gstride()) {
+        const size_t pm = t / a.n;
+        const uint32_t i = (uint32_t)(t % a.n);
+        const uint32_t j = i + a.acc[t];
+        if (j != i) {
+            atomicMax(&a.par[pm * a.n + j], (int32_t)i);
+            atomicAdd(&a.cnt[pm * a.n + j], 1u);
+        }
+    }
+}
+// exclusive scan of cnt within each permutation (one CTA per permutation)
+__global__ void __launch_bounds__(1024) k_fin_scan(FinArgs a) {
+    __shared__ uint32_t red[33];
+    const size_t pm = blockIdx.x;
+    const uint32_t* c = a.cnt + pm * a.n;
+    uint32_t* o = a.off + pm * a.n;
+    uint32_t carry = 0;
+    for (uint32_t b0 = 0; b0 < a.n; b0 += 1024 * 4) {
+        uint32_t v[4], s = 0;
+        for (int u = 0; u < 4; u++) {
+            const uint32_t k = b0 + threadIdx.x * 4 + u;
+            v[u] = k < a.n ? c[k] : 0;
+            s += v[u];
+        }
+        uint32_t tot;
+        uint32_t pre = block_excl_sum(s, red, tot) + carry;
+        for (int u = 0; u < 4; u++) {
+            const uint32_t k = b0 + threadIdx.x * 4 + u;
+            if (k < a.n) o[k] = pre;
+            pre += v[u];
+        }
+        carry += tot;
+    }
+}
+__global__ void k_fin_place(FinArgs a) {
+    const size_t tot = (size_t)a.P * a.n;
+    for (size_t t = gtid(); t < tot; t += gstride()) {
+        const size_t pm = t / a.n;
+        const uint32_t i = (uint32_t)(t % a.n);
+        const uint32_t j = i + a.acc[t];
+        if (j != i) {
+            const uint32_t s = atomicAdd(&a.fill[pm * a.n + j], 1u);
+            a.bucket[pm * a.n + a.off[pm * a.n + j] + s] = (int32_t)i;
+        }
+    }
+}
+__global__ void k_fin_roots(FinArgs a) {
+    const size_t tot = (size_t)a.P * a.n;
+    for (size_t t = gtid(); t < tot; t += gstride()) {
+        const size_t pm = t / a.n;
+        const int32_t* par = a.par + pm * a.n;
+        int32_t k = (int32_t)(t % a.n);
+        int32_t p = par[k];
+        while (p >= 0) {
+            k = p;
+            p = par[k];
+        }
+        a.A[t] = k;
+    }
+}
+__global__ void k_fin_final(FinArgs a) {
+    const size_t tot = (size_t)a.P * a.n;
+    for (size_t t = gtid(); t < tot; t += gstride()) {
+        const size_t pm = t / a.n;
+        const uint32_t i = (uint32_t)(t % a.n);
+        const uint32_t j = i + a.acc[t];
+        const int32_t* A = a.A + pm * a.n;
+        int32_t val;
+        if (j == i) {
+            val = A[i];
+        } else {
+            const uint32_t o = a.off[pm * a.n + j], c = a.cnt[pm * a.n + j];
+            const int32_t* b = a.bucket + pm * a.n + o;
+            int32_t pred = -1;
+            for (uint32_t k = 0; k < c; k++) {
+                const int32_t s = b[k];
+                if (s < (int32_t)i && s > pred) pred = s;
+            }
+            val = pred >= 0 ? A[pred] : (int32_t)j;
+        }
+        a.perm_out[pm][i] = val;
+        a.inv_out[pm][val] = (int32_t)i;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Generate `count` sharded permutations of size n from the three 2-party group
+// streams, in ORQ's order: permutation-major, groups {0,1},{0,2},{1,2}
+// (generateBatch, hm_sharded_permutation_generator.h:178-194).
+void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>& out) {
+    out.clear();
+    if (count == 0) return;
+    if (n >= (1ull << 31)) throw std::invalid_argument("permutation size must be < 2^31");
+    out.resize(count);
+    for (auto& sp : out) {
+        sp.n = n;
+        for (int g = 0; g < 3; g++) {
+            sp.perm[g] = (int32_t*)c.alloc(std::max<size_t>(n, 1) * 4);
+            sp.inv[g] = (int32_t*)c.alloc(std::max<size_t>(n, 1) * 4);
+        }
+    }
+    if (n == 0) {
+        // gen_perm still draws one buffer (4 nonces) per permutation
+        for (int g = 0; g < 3; g++) c.nonce[G01 + g] += 4ull * count;
+        return;
+    }
+    int bitsw = 0;
+    while (bitsw < 64 && (n >> bitsw)) bitsw++;
+    const uint32_t mask = (uint32_t)((1ull << bitsw) - 1);
+
+    // window of buffers generated per pipeline step
+    const double M = (double)(1ull << bitsw);
+    double H = 0;
+    for (size_t k = 1; k <= std::min<size_t>(n, 1 << 16); k++) H += 1.0 / k;
+    if (n > (1u << 16)) H += std::log((double)n / (1 << 16));
+    const double per_perm = M * H / (double)(1 << 20) + 1.0;  // expected buffers
+    uint32_t W = (uint32_t)std::clamp(per_perm * count / 8.0, 2.0, 32.0);
+    const uint32_t tiles = W * kTilesPerRefill;
+
+    const size_t surv_b = (size_t)3 * tiles * kTileDraws * 4;
+    const size_t bits_b = (size_t)3 * tiles * kBitWords * 4;
+    const size_t small_b = (size_t)3 * tiles * 4;
+    Scratch surv0(c, surv_b), surv1(c, surv_b), bits0(c, bits_b), bits1(c, bits_b);
+    Scratch cnt0(c, small_b), cnt1(c, small_b), min0(c, small_b), min1(c, small_b);
+    Scratch state(c, 3 * sizeof(FyState));
+    Scratch acc(c, (size_t)3 * count * n * 4);
+    Scratch refills(c, (size_t)3 * count * 4);
+    ORQ_CUDA_CHECK(cudaMemsetAsync(state.p, 0, 3 * sizeof(FyState), c.stream));
+
+    cudaStream_t gs;
+    ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
+    cudaEvent_t ev_start, gen_done[2], scan_done[2];
+    ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
+    for (int k = 0; k < 2; k++) {
+        ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&gen_done[k], cudaEventDisableTiming));
+        ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&scan_done[k], cudaEventDisableTiming));
+    }
+    ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
+    ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
+
+    FyState* hstate = nullptr;
+    ORQ_CUDA_CHECK(cudaMallocHost(&hstate, 3 * sizeof(FyState)));
+    prep_aes_kernel(k_fy_gen);
+
+    const unsigned gen_grid = (unsigned)std::max(1, c.num_sms - 3);
+    uint32_t* survp[2] = {surv0.as<uint32_t>(), surv1.as<uint32_t>()};
+    uint32_t* bitsp[2] = {bits0.as<uint32_t>(), bits1.as<uint32_t>()};
+    uint32_t* cntp[2] = {cnt0.as<uint32_t>(), cnt1.as<uint32_t>()};
+    uint32_t* minp[2] = {min0.as<uint32_t>(), min1.as<uint32_t>()};
+
+    const unsigned long long limit_windows =
+        (unsigned long long)(count * (per_perm * 4.0 + 64.0) / W + 16);
+    auto launch_gen = [&](unsigned long long w) {
+        const int b = (int)(w & 1);
+        // buffer b was last read by the scanner of window w-2
+        if (w >= 2) ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, scan_done[b], 0));
+        FyGenArgs ga;
+        for (int g = 0; g < 3; g++) ga.st[g] = c.stream_arg(G01 + g, 4ull * W * w);
+        ga.n = (uint32_t)n;
+        ga.mask = mask;
+        ga.tiles = tiles;
+        ga.surv = survp[b];
+        ga.cnt = cntp[b];
+        ga.tmin = minp[b];
+        ga.bits = bitsp[b];
+        ga.state = state.as<FyState>();
+        k_fy_gen<<<gen_grid, kAesThreads, kAesSmemBytes, gs>>>(ga);
+        ORQ_CUDA_CHECK(cudaGetLastError());
+        ORQ_CUDA_CHECK(cudaEventRecord(gen_done[b], gs));
+        c.kernels_launched++;
+    };
+    launch_gen(0);
+    unsigned long long w = 0;
+    bool all_done = false;
+    while (!all_done) {
+        if (w > limit_windows)
+            throw std::runtime_error("permutation generation did not converge");
+        const int b = (int)(w & 1);
+        // scanner for window w
+        ORQ_CUDA_CHECK(cudaStreamWaitEvent(c.stream, gen_done[b], 0));
+        FyScanArgs sa;
+        sa.n = (uint32_t)n;
+        sa.count = (uint32_t)count;
+        sa.tiles = tiles;
+        sa.win_tile0 = (unsigned long long)w * tiles;
+        sa.surv = survp[b];
+        sa.cnt = cntp[b];
+        sa.tmin = minp[b];
+        sa.bits = bitsp[b];
+        sa.state = state.as<FyState>();
+        sa.acc = acc.as<uint32_t>();
+        sa.refills = refills.as<uint32_t>();
+        k_fy_scan<<<3, kScanThreads, 0, c.stream>>>(sa);
+        ORQ_CUDA_CHECK(cudaGetLastError());
+        ORQ_CUDA_CHECK(cudaEventRecord(scan_done[b], c.stream));
+        c.kernels_launched++;
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(hstate, state.p, 3 * sizeof(FyState),
+                                       cudaMemcpyDeviceToHost, c.stream));
+        // generate the next window while this one is scanned
+        launch_gen(w + 1);
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+        all_done = hstate[0].done && hstate[1].done && hstate[2].done;
+        w++;
+    }
+    ORQ_CUDA_CHECK(cudaStreamSynchronize(gs));
+
+    // nonce accounting: 4 nonces per getNext buffer
+    std::vector<uint32_t> hr(3 * count);
+    ORQ_CUDA_CHECK(cudaMemcpyAsync(hr.data(), refills.p, hr.size() * 4, cudaMemcpyDeviceToHost,
+                                   c.stream));
+    ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    for (int g = 0; g < 3; g++) {
+        unsigned long long used = 0;
+        for (size_t m = 0; m < count; m++) used += hr[g * count + m];
+        c.nonce[G01 + g] += 4ull * used;
+    }
+
+    // finalize, a few permutations at a time to bound scratch
+    const size_t per_batch = std::max<size_t>(1, std::min<size_t>(3 * count, (size_t)(1ull << 27) / std::max<size_t>(n, 1)));
+    for (size_t p0 = 0; p0 < 3 * count; p0 += per_batch) {
+        const size_t P = std::min(per_batch, 3 * count - p0);
+        const size_t el = P * n;
+        Scratch par(c, el * 4), cnt(c, el * 4), off(c, el * 4), fill(c, el * 4), bucket(c, el * 4),
+            A(c, el * 4), ptrs(c, 2 * P * sizeof(void*));
+        std::vector<int32_t*> hp(2 * P);
+        for (size_t k = 0; k < P; k++) {
+            // acc is laid out [group][perm]; permutation index pm = p0 + k
+            const size_t pm = p0 + k, g = pm / count, m = pm % count;
+            hp[k] = out[m].perm[g];
+            hp[P + k] = out[m].inv[g];
+        }
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(ptrs.p, hp.data(), hp.size() * sizeof(void*),
+                                       cudaMemcpyHostToDevice, c.stream));
+        FinArgs fa;
+        fa.acc = acc.as<uint32_t>() + p0 * n;
+        fa.n = (uint32_t)n;
+        fa.P = (uint32_t)P;
+        fa.par = par.as<int32_t>();
+        fa.cnt = cnt.as<uint32_t>();
+        fa.off = off.as<uint32_t>();
+        fa.fill = fill.as<uint32_t>();
+        fa.bucket = bucket.as<int32_t>();
+        fa.A = A.as<int32_t>();
+        fa.perm_out = ptrs.as<int32_t*>();
+        fa.inv_out = ptrs.as<int32_t*>() + P;
+        const unsigned gg = plain_grid(c, el);
+        k_fin_init<<<gg, 256, 0, c.stream>>>(fa);
+        k_fin_targets<<<gg, 256, 0, c.stream>>>(fa);
+        k_fin_scan<<<(unsigned)P, 1024, 0, c.stream>>>(fa);
+        k_fin_place<<<gg, 256, 0, c.stream>>>(fa);
+        k_fin_roots<<<gg, 256, 0, c.stream>>>(fa);
+        k_fin_final<<<gg, 256, 0, c.stream>>>(fa);
+        ORQ_CUDA_CHECK(cudaGetLastError());
+        c.kernels_launched += 6;
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // scratch reuse
+    }
+    cudaFreeHost(hstate);
+    cudaEventDestroy(ev_start);
+    for (int k = 0; k < 2; k++) {
+        cudaEventDestroy(gen_done[k]);
+        cudaEventDestroy(scan_done[k]);
+    }
+    cudaStreamDestroy(gs);
+}
+
+// PermutationManager::reserve (permutation_manager.h:102-181): keep a queue of
+// permutations of one size; a size change empties it.
+void reserve_perms(Ctx& c, size_t n, size_t count) {
+    if (!c.perm_queue.empty() && c.perm_queue_n != n) {
+        for (auto& sp : c.perm_queue) c.free_perm(sp);
+        c.perm_queue.clear();
+    }
+    c.perm_queue_n = n;
+    if (c.perm_queue.size() >= count) return;
+    std::vector<ShardedPerm> fresh;
+    gen_sharded_perms(c, n, count - c.perm_queue.size(), fresh);
+    for (auto& sp : fresh) c.perm_queue.push_back(sp);
+}
+
+// PermutationManager::getNext / getNextPair for 3PC: pop the queue, or
+// generate one on demand (hm generator getNext).
+ShardedPerm next_perm(Ctx& c, size_t n) {
+    if (!c.perm_queue.empty()) {
+        if (c.perm_queue_n != n) throw std::runtime_error("queued permutation has the wrong size");
+        ShardedPerm sp = c.perm_queue.front();
+        c.perm_queue.pop_front();
+        return sp;
+    }
+    std::vector<ShardedPerm> one;
+    gen_sharded_perms(c, n, 1, one);
+    return one[0];
+}
+
+// ---------------------------------------------------------------------------
+// Application of one group's local permutation fused with that group's
+// reshare, for up to two vectors that use the same permutation (ORQ applies
+// the data vector and the permutation vector in turn with the same sharded
+// permutation, shuffle.h:687-706). dst[k] = src[idx[k]] (+|^) r_j[k]:
+// idx = inverse permutation for local_apply_perm (scatter new[pi[i]] = x[i],
+// shuffle.h:113-133), idx = the permutation itself for
+// local_apply_inverse_perm (shuffle.h:250-270).
+//   MODE 0: store both results
+//   MODE 2: open the second vector into sigma and scatter the first by it
+//           (local_apply_perm of the opened permutation, shuffle.h:702-705)
+//   MODE 3: open the first vector into sigma (no stores)
+struct ApplyArgs {
+    const void* src1[3];
+    void* dst1[3];
+    const void* src2[3];
+    void* dst2[3];
+    const int32_t* idx;
+    StreamArg g1, g2;
+    unsigned long long ch1, ch2;
+    unsigned long long n;
+    int32_t* sigma;
+};
+
+template <int W>
+__device__ __forceinline__ void gather_elem(const void* src, int32_t k, uint8_t* dst) {
+    if constexpr (W == 4) {
+        *reinterpret_cast<uint32_t*>(dst) = __ldg(reinterpret_cast<const uint32_t*>(src) + k);
+    } else if constexpr (W == 8) {
+        *reinterpret_cast<uint2*>(dst) = __ldg(reinterpret_cast<const uint2*>(src) + k);
+    } else {
+        *reinterpret_cast<uint4*>(dst) = __ldg(reinterpret_cast<const uint4*>(src) + k);
+    }
+}
+template <int W>
+__device__ __forceinline__ void store_elem(void* dst, int32_t k, const uint8_t* v) {
+    if constexpr (W == 4) {
+        reinterpret_cast<uint32_t*>(dst)[k] = *reinterpret_cast<const uint32_t*>(v);
+    } else if constexpr (W == 8) {
+        reinterpret_cast<uint2*>(dst)[k] = *reinterpret_cast<const uint2*>(v);
+    } else {
+        reinterpret_cast<uint4*>(dst)[k] = *reinterpret_cast<const uint4*>(v);
+    }
+}
+
+// E elements per thread; E*W1 and E*W2 are multiples of 16 bytes.
+template <int W1, bool A1, int W2, bool A2, int MODE>
+__global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
+    constexpr int WMIN = (W2 && W2 < W1) ? W2 : W1;
+    constexpr int E = 16 / WMIN;
+    constexpr int B1 = E * W1 / 16;
+    constexpr int B2 = W2 ? E * W2 / 16 : 1;
+    extern __shared__ uint32_t sm[];
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    const unsigned long long units = ceil_div(a.n, E);
+    for (unsigned long long t = gtid(); t < units; t += gstride()) {
+        const unsigned long long k0 = t * E;
+        int32_t id[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) id[e] = (k0 + e < a.n) ? __ldg(a.idx + k0 + e) : 0;
+        // ---- vector 2 (the permutation vector in elementwise application)
+        uint32_t sig[E];
+        if constexpr (W2 != 0) {
+            uint4 v2[3][B2];
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+#pragma unroll
+                for (int e = 0; e < E; e++)
+                    if (k0 + e < a.n)
+                        gather_elem<W2>(a.src2[j], id[e], reinterpret_cast<uint8_t*>(&v2[j][0]) + e * W2);
+#pragma unroll
+            for (int bb = 0; bb < B2; bb++) {
+                const unsigned long long blk = t * B2 + bb;
+                StreamArg gs = a.g2;
+                const uint4 r0 = keystream_block(S, gs, blk);
+                gs.nonce += a.ch2;
+                const uint4 r1 = keystream_block(S, gs, blk);
+                uint4 r2;
+                if constexpr (A2) r2 = Ring<W2>::sub(Ring<W2>::sub(make_uint4(0, 0, 0, 0), r0), r1);
+                else r2 = r0 ^ r1;
+                v2[0][bb] = Share<W2, A2>::plus(v2[0][bb], r0);
+                v2[1][bb] = Share<W2, A2>::plus(v2[1][bb], r1);
+                v2[2][bb] = Share<W2, A2>::plus(v2[2][bb], r2);
+            }
+            if constexpr (MODE == 0) {
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+#pragma unroll
+                    for (int bb = 0; bb < B2; bb++)
+                        st16(a.dst2[j], t * B2 + bb, a.n * W2, v2[j][bb]);
+            } else if constexpr (MODE == 2) {
+                // open (W2 == 4): sigma = sum or xor of the three shares
+                uint4 o[B2];
+#pragma unroll
+                for (int bb = 0; bb < B2; bb++)
+                    o[bb] = Share<W2, A2>::plus(Share<W2, A2>::plus(v2[0][bb], v2[1][bb]), v2[2][bb]);
+#pragma unroll
+                for (int e = 0; e < E; e++) sig[e] = reinterpret_cast<const uint32_t*>(o)[e];
+            }
+        }
+        // ---- vector 1
+        uint4 v1[3][B1];
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                if (k0 + e < a.n)
+                    gather_elem<W1>(a.src1[j], id[e], reinterpret_cast<uint8_t*>(&v1[j][0]) + e * W1);
+#pragma unroll
+        for (int bb = 0; bb < B1; bb++) {
+            const unsigned long long blk = t * B1 + bb;
+            StreamArg gs = a.g1;
+            const uint4 r0 = keystream_block(S, gs, blk);
+            gs.nonce += a.ch1;
+            const uint4 r1 = keystream_block(S, gs, blk);
+            uint4 r2;
+            if constexpr (A1) r2 = Ring<W1>::sub(Ring<W1>::sub(make_uint4(0, 0, 0, 0), r0), r1);
+            else r2 = r0 ^ r1;
+            v1[0][bb] = Share<W1, A1>::plus(v1[0][bb], r0);
+            v1[1][bb] = Share<W1, A1>::plus(v1[1][bb], r1);
+            v1[2][bb] = Share<W1, A1>::plus(v1[2][bb], r2);
+        }
+        if constexpr (MODE == 0) {
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+#pragma unroll
+                for (int bb = 0; bb < B1; bb++) st16(a.dst1[j], t * B1 + bb, a.n * W1, v1[j][bb]);
+        } else if constexpr (MODE == 2) {
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+#pragma unroll
+                for (int e = 0; e < E; e++)
+                    if (k0 + e < a.n)
+                        store_elem<W1>(a.dst1[j], (int32_t)sig[e],
+                                       reinterpret_cast<const uint8_t*>(&v1[j][0]) + e * W1);
+        } else if constexpr (MODE == 3) {
+            uint4 o[B1];
+#pragma unroll
+            for (int bb = 0; bb < B1; bb++)
+                o[bb] = Share<W1, A1>::plus(Share<W1, A1>::plus(v1[0][bb], v1[1][bb]), v1[2][bb]);
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                if (k0 + e < a.n) a.sigma[k0 + e] = reinterpret_cast<const int32_t*>(o)[e];
+        }
+    }
+}
+
+namespace {
+
+template <int W1, bool A1, int W2, bool A2, int MODE>
+void launch_apply(Ctx& c, const ApplyArgs& a) {
+    constexpr int WMIN = (W2 && W2 < W1) ? W2 : W1;
+    constexpr int E = 16 / WMIN;
+    auto kern = k_apply<W1, A1, W2, A2, MODE>;
+    prep_aes_kernel(kern);
+    const unsigned long long units = ceil_div(a.n, E);
+    kern<<<aes_grid(c, units), kAesThreads, kAesSmemBytes, c.stream>>>(a);
+    ORQ_CUDA_CHECK(cudaGetLastError());
+    c.kernels_launched++;
+}
+
+// runtime dispatch over the (width, encoding) combinations used by the operators
+template <int MODE>
+void dispatch_apply(Ctx& c, int w1, bool a1, int w2, bool a2, const ApplyArgs& a) {
+#define ORQ_AP(W1v, A1v, W2v, A2v)                                      \
+    if (w1 == W1v && a1 == A1v && w2 == W2v && (W2v == 0 || a2 == A2v)) \
+        return launch_apply<W1v, A1v, W2v, A2v, MODE>(c, a);
+    ORQ_AP(4, false, 0, false)
+    ORQ_AP(4, true, 0, false)
+    ORQ_AP(8, false, 0, false)
+    ORQ_AP(8, true, 0, false)
+    ORQ_AP(16, false, 0, false)
+    ORQ_AP(16, true, 0, false)
+    ORQ_AP(16, false, 4, true)
+    ORQ_AP(16, false, 4, false)
+    ORQ_AP(8, false, 4, true)
+    ORQ_AP(8, true, 4, true)
+    ORQ_AP(8, false, 4, false)
+    ORQ_AP(8, true, 4, false)
+    ORQ_AP(4, true, 4, true)
+    ORQ_AP(4, false, 4, true)
+    ORQ_AP(4, true, 4, false)
+    ORQ_AP(4, false, 4, false)
+#undef ORQ_AP
+    throw std::invalid_argument("unsupported share width/encoding for permutation application");
+}
+
+}  // namespace
+
+// hm_oblivious_apply_sharded_perm / _inverse (shuffle.h:349-412) on one vector.
+void op_apply_sharded(Ctx& c, bool arith, int w, size_t n, Sh3 s, const ShardedPerm& sp,
+                      bool inverse) {
+    if (w != 4 && w != 8 && w != 16)
+        throw std::invalid_argument("permutation application supports 4, 8 and 16-byte shares");
+    const unsigned long long ch = chunks_of((unsigned long long)n * w);
+    if (n == 0) return;
+    Scratch tmp(c, 3 * n * (size_t)w);
+    void* other[3] = {tmp.as<uint8_t>(), tmp.as<uint8_t>() + n * (size_t)w,
+                      tmp.as<uint8_t>() + 2 * n * (size_t)w};
+    void* cur[3] = {s.p[0], s.p[1], s.p[2]};
+    for (int step = 0; step < 3; step++) {
+        const int g = inverse ? 2 - step : step;
+        ApplyArgs a{};
+        for (int j = 0; j < 3; j++) {
+            a.src1[j] = cur[j];
+            a.dst1[j] = other[j];
+        }
+        a.idx = inverse ? sp.perm[g] : sp.inv[g];
+        a.g1 = c.stream_arg(G01 + g);
+        a.ch1 = ch;
+        a.n = n;
+        dispatch_apply<0>(c, w, arith, 0, false, a);
+        c.nonce[G01 + g] += 2 * ch;
+        for (int j = 0; j < 3; j++) std::swap(cur[j], other[j]);
+    }
+    // three swaps leave the result in the scratch buffers
+    for (int j = 0; j < 3; j++)
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(s.p[j], cur[j], n * (size_t)w, cudaMemcpyDeviceToDevice, c.stream));
+}
+
+// oblivious_apply_elementwise_perm (shuffle.h:687-706): shuffle x and a copy
+// of the permutation with the same sharded permutation, open the shuffled
+// permutation and scatter x with it. Three fused kernels, one per group.
+void op_apply_elementwise(Ctx& c, bool x_arith, int xw, size_t n, Sh3 x, CSh3 perm) {
+    if (n == 0) {
+        ShardedPerm sp = next_perm(c, n);
+        c.free_perm(sp);
+        return;
+    }
+    ShardedPerm sp = next_perm(c, n);
+    const unsigned long long chx = chunks_of((unsigned long long)n * xw);
+    const unsigned long long chp = chunks_of((unsigned long long)n * 4);
+    Scratch xa(c, 3 * n * (size_t)xw), xb(c, 3 * n * (size_t)xw), pa(c, 3 * n * 4), pb(c, 3 * n * 4);
+    void* X[2][3];
+    void* Pp[2][3];
+    for (int j = 0; j < 3; j++) {
+        X[0][j] = xa.as<uint8_t>() + j * n * (size_t)xw;
+        X[1][j] = xb.as<uint8_t>() + j * n * (size_t)xw;
+        Pp[0][j] = pa.as<uint8_t>() + j * n * 4;
+        Pp[1][j] = pb.as<uint8_t>() + j * n * 4;
+    }
+    for (int g = 0; g < 3; g++) {
+        ApplyArgs a{};
+        for (int j = 0; j < 3; j++) {
+            a.src1[j] = g == 0 ? x.p[j] : X[(g - 1) & 1][j];
+            a.dst1[j] = g == 2 ? x.p[j] : X[g & 1][j];
+            a.src2[j] = g == 0 ? perm.p[j] : Pp[(g - 1) & 1][j];
+            a.dst2[j] = Pp[g & 1][j];
+        }
+        a.idx = sp.inv[g];
+        // per group stream: the x reshare first, then the permutation's
+        a.g1 = c.stream_arg(G01 + g);
+        a.g2 = c.stream_arg(G01 + g, 2 * chx);
+        a.ch1 = chx;
+        a.ch2 = chp;
+        a.n = n;
+        if (g < 2) dispatch_apply<0>(c, xw, x_arith, 4, true, a);
+        else dispatch_apply<2>(c, xw, x_arith, 4, true, a);
+        c.nonce[G01 + g] += 2 * chx + 2 * chp;
+    }
+    c.free_perm(sp);
+}
+
+// shuffle (shuffle.h:752-757)
+void op_shuffle(Ctx& c, bool arith, int w, size_t n, Sh3 s) {
+    ShardedPerm sp = next_perm(c, n);
+    op_apply_sharded(c, arith, w, n, s, sp, false);
+    c.free_perm(sp);
+}
+
+// local_apply_perm with a public permutation: dst[sigma[i]] = src[i]
+template <int W>
+__global__ void k_scatter(CSh3 src, Sh3 dst, const int32_t* sigma, unsigned long long n) {
+    for (unsigned long long i = gtid(); i < n; i += gstride()) {
+        const int32_t d = __ldg(sigma + i);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            uint8_t v[W];
+            gather_elem<W>(src.p[j], (int32_t)i, v);
+            store_elem<W>(dst.p[j], d, v);
+        }
+    }
+}
+void op_scatter(Ctx& c, int w, size_t n, CSh3 src, Sh3 dst, const int32_t* sigma) {
+    if (!n) return;
+    const unsigned g = plain_grid(c, n);
+    if (w == 4) k_scatter<4><<<g, 256, 0, c.stream>>>(src, dst, sigma, n);
+    else if (w == 8) k_scatter<8><<<g, 256, 0, c.stream>>>(src, dst, sigma, n);
+    else if (w == 16) k_scatter<16><<<g, 256, 0, c.stream>>>(src, dst, sigma, n);
+    else throw std::invalid_argument("scatter supports 4, 8, 16-byte shares");
+    ORQ_CUDA_CHECK(cudaGetLastError());
+    c.kernels_launched++;
+}
+
+}  // namespace orqcu

@@ -1,0 +1,193 @@
+// runtime.cu — context set-up: key schedule, AES tables, device buffer pool.
+#include <cstring>
+
+#include "runtime.h"
+
+namespace orqcu {
+
+// ---------------------------------------------------------------------------
+// Keys. The reference draws every AES-256 key from libsodium's keygen
+// (include/core/random/prg/prg_algorithm.h:192-197). Reproducible runs replace
+// that with SplitMix64 keyed by (seed, party, keygen-call index); the test shim
+// that builds the reference does the same, so identical seeds give identical
+// shares. Call order per party follows setup_random_generation
+// (include/backend/common/rand_setup.h:306-381) — see init_ctx_keys.
+static uint64_t splitmix64(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+void derive_key(uint64_t seed, int party, int call, uint8_t key[32]) {
+    uint64_t st = seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(party + 1)) ^
+                  (0xABC98388FB8FAC03ull * (uint64_t)(call + 1));
+    for (int i = 0; i < 4; i++) {
+        uint64_t v = splitmix64(st);
+        for (int b = 0; b < 8; b++) key[8 * i + b] = (uint8_t)(v >> (8 * b));
+    }
+}
+
+// AES (FIPS-197): S-box from the GF(2^8) inverse and affine map.
+static uint8_t gmul(uint8_t a, uint8_t b) {
+    uint8_t p = 0;
+    while (b) {
+        if (b & 1) p ^= a;
+        a = (uint8_t)((a << 1) ^ ((a & 0x80) ? 0x1B : 0));
+        b >>= 1;
+    }
+    return p;
+}
+static const uint8_t* sbox() {
+    static uint8_t s[256];
+    static bool ready = false;
+    if (!ready) {
+        for (int x = 0; x < 256; x++) {
+            uint8_t inv = 0;
+            for (int y = 1; x && y < 256; y++)
+                if (gmul((uint8_t)x, (uint8_t)y) == 1) {
+                    inv = (uint8_t)y;
+                    break;
+                }
+            uint8_t v = inv, r = inv;
+            for (int i = 0; i < 4; i++) {
+                r = (uint8_t)((r << 1) | (r >> 7));
+                v ^= r;
+            }
+            s[x] = v ^ 0x63;
+        }
+        ready = true;
+    }
+    return s;
+}
+
+void aes256_expand(const uint8_t key[32], uint32_t rk[60]) {
+    const uint8_t* S = sbox();
+    auto subw = [&](uint32_t w) {
+        return (uint32_t)S[w & 0xff] | ((uint32_t)S[(w >> 8) & 0xff] << 8) |
+               ((uint32_t)S[(w >> 16) & 0xff] << 16) | ((uint32_t)S[w >> 24] << 24);
+    };
+    for (int i = 0; i < 8; i++)
+        rk[i] = (uint32_t)key[4 * i] | ((uint32_t)key[4 * i + 1] << 8) |
+                ((uint32_t)key[4 * i + 2] << 16) | ((uint32_t)key[4 * i + 3] << 24);
+    uint8_t rcon = 1;
+    for (int i = 8; i < 60; i++) {
+        uint32_t t = rk[i - 1];
+        if (i % 8 == 0) {
+            t = subw((t >> 8) | (t << 24)) ^ rcon;
+            rcon = gmul(rcon, 2);
+        } else if (i % 8 == 4) {
+            t = subw(t);
+        }
+        rk[i] = rk[i - 8] ^ t;
+    }
+}
+
+// Which keygen call of which party keys each stream (rand_setup.h:21-146):
+// call 0 = local PRG; lowest member draws group keys in the order {0,1},{0,2},
+// {1,2},{0,1,2}; P0 draws a discarded duplicate everyone-group key; the last
+// call is the pairwise key of setup_3pc_common_prgs.
+void init_ctx_keys(Ctx& c, uint64_t seed) {
+    static const int who[NSTREAMS][2] = {{0, 5}, {1, 2}, {2, 1}, {0, 1}, {0, 2},
+                                         {1, 1}, {0, 3}, {0, 0}, {1, 0}, {2, 0}};
+    c.seed = seed;
+    for (int s = 0; s < NSTREAMS; s++) {
+        uint8_t key[32];
+        derive_key(seed, who[s][0], who[s][1], key);
+        aes256_expand(key, c.rk[s].k);
+        c.nonce[s] = 0;
+    }
+}
+
+static std::vector<AesTableUploader>& uploaders() {
+    static std::vector<AesTableUploader> v;
+    return v;
+}
+int register_aes_table_uploader(AesTableUploader f) {
+    uploaders().push_back(f);
+    return (int)uploaders().size();
+}
+
+void upload_aes_tables(int device) {
+    static bool done[64] = {false};
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (device >= 0 && device < 64 && done[device]) return;
+    const uint8_t* S = sbox();
+    uint32_t T[4 * 256];
+    for (int x = 0; x < 256; x++) {
+        const uint32_t s = S[x], s2 = gmul((uint8_t)s, 2), s3 = gmul((uint8_t)s, 3);
+        const uint32_t t0 = s2 | (s << 8) | (s << 16) | (s3 << 24);
+        T[x] = t0;
+        T[256 + x] = (t0 << 8) | (t0 >> 24);
+        T[512 + x] = (t0 << 16) | (t0 >> 16);
+        T[768 + x] = (t0 << 24) | (t0 >> 8);
+    }
+    for (AesTableUploader f : uploaders()) f(T);
+    if (device >= 0 && device < 64) done[device] = true;
+}
+
+// ---------------------------------------------------------------------------
+// Pool: size-bucketed reuse of device allocations (buckets are powers of two
+// above 1 MiB, 256-byte multiples below), so the per-round temporaries of a
+// sort do not go back to cudaMalloc.
+static size_t bucket(size_t bytes) {
+    if (bytes < 256) return 256;
+    if (bytes <= (1u << 20)) return (bytes + 255) & ~size_t(255);
+    size_t b = size_t(1) << 20;
+    while (b < bytes) b <<= 1;
+    return b;
+}
+
+void* Pool::get(size_t bytes) {
+    const size_t b = bucket(bytes);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.find(b);
+        if (it != free_.end()) {
+            void* p = it->second;
+            free_.erase(it);
+            live_[p] = b;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        trim();
+        ORQ_CUDA_CHECK(cudaMalloc(&p, b));
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    live_[p] = b;
+    return p;
+}
+
+void Pool::put(void* p) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = live_.find(p);
+    if (it == live_.end()) return;
+    free_.emplace(it->second, p);
+    live_.erase(it);
+}
+
+void Pool::trim() {
+    std::lock_guard<std::mutex> lk(mu_);
+    for (auto& kv : free_) cudaFree(kv.second);
+    free_.clear();
+}
+
+Pool::~Pool() {
+    for (auto& kv : free_) cudaFree(kv.second);
+    for (auto& kv : live_) cudaFree(kv.first);
+}
+
+void Ctx::free_perm(ShardedPerm& sp) {
+    for (int g = 0; g < 3; g++) {
+        release(sp.perm[g]);
+        release(sp.inv[g]);
+        sp.perm[g] = sp.inv[g] = nullptr;
+    }
+}
+
+}  // namespace orqcu

@@ -1,0 +1,137 @@
+// runtime.h — the single-process loopback runtime that stands in for ORQ's
+// RunTime + per-party protocol objects (include/backend/common/runtime.h,
+// include/core/protocols/replicated_3pc.h) on one GPU.
+//
+// One Ctx holds all three parties: the 10 AES streams of a 3PC worker
+// (3 pairwise, 4 group, 3 party-local; include/backend/common/rand_setup.h),
+// their nonce counters, a CUDA stream, a device buffer pool and the queue of
+// reserved sharded permutations (random/permutations/permutation_manager.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace orqcu {
+
+enum StreamId {
+    PAIR0 = 0,  // shared by P0/P1 (P0's local key): P0 get(+1), P1 get(-1)
+    PAIR1 = 1,
+    PAIR2 = 2,
+    G01 = 3,
+    G02 = 4,
+    G12 = 5,
+    G012 = 6,
+    LOCAL0 = 7,
+    LOCAL1 = 8,
+    LOCAL2 = 9,
+    NSTREAMS = 10
+};
+
+// Device allocation that returns to the pool when dropped.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+class Pool {
+   public:
+    void* get(size_t bytes);
+    void put(void* p);
+    void trim();
+    ~Pool();
+
+   private:
+    std::mutex mu_;
+    std::multimap<size_t, void*> free_;
+    std::map<void*, size_t> live_;
+};
+
+// A sharded permutation: one local permutation per 2-party group
+// ({0,1},{0,2},{1,2}), each with its inverse, all device-resident int32.
+struct ShardedPerm {
+    size_t n = 0;
+    int32_t* perm[3] = {nullptr, nullptr, nullptr};
+    int32_t* inv[3] = {nullptr, nullptr, nullptr};
+};
+
+struct Ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    uint64_t seed = 0;
+    AesRK rk[NSTREAMS];
+    unsigned long long nonce[NSTREAMS] = {0};
+    Pool pool;
+    std::deque<ShardedPerm> perm_queue;
+    size_t perm_queue_n = 0;
+    unsigned long long kernels_launched = 0;
+
+    StreamArg stream_arg(int s, unsigned long long extra_nonces = 0) const {
+        StreamArg a;
+        a.rk = rk[s];
+        a.nonce = nonce[s] + extra_nonces;
+        return a;
+    }
+    void* alloc(size_t bytes) { return pool.get(bytes); }
+    void release(void* p) {
+        if (p) pool.put(p);
+    }
+    void free_perm(ShardedPerm& sp);
+};
+
+// RAII scratch from the pool.
+struct Scratch {
+    Ctx* c;
+    void* p;
+    Scratch(Ctx& ctx, size_t bytes) : c(&ctx), p(ctx.alloc(bytes)) {}
+    ~Scratch() { c->release(p); }
+    template <typename T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+    Scratch(const Scratch&) = delete;
+    Scratch& operator=(const Scratch&) = delete;
+};
+
+// host-side key derivation (identical to the test shim / restatement)
+void derive_key(uint64_t seed, int party, int call, uint8_t key[32]);
+void aes256_expand(const uint8_t key[32], uint32_t rk[60]);
+void init_ctx_keys(Ctx& c, uint64_t seed);
+void upload_aes_tables(int device);
+
+// ---- primitives (prims.cu) ----
+void launch_keystream(Ctx& c, int stream_id, unsigned long long nonce0, void* out, size_t nbytes);
+void op_secret_share(Ctx& c, bool arith, int w, size_t n, const void* data_dev, int party, Sh3 s);
+void op_public_share(Ctx& c, int w, size_t n, const void* data_dev, Sh3 s);
+void op_open(Ctx& c, bool arith, int w, size_t n, CSh3 s, void* out_dev);
+void op_mult(Ctx& c, bool arith, int w, size_t n, CSh3 x, CSh3 y, Sh3 z);
+void op_local(Ctx& c, int op, int w, size_t n, CSh3 x, CSh3 y, Sh3 z);  // 0 xor,1 add,2 sub
+void op_not(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
+void op_b2a_bit(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
+void op_zero_share(Ctx& c, bool arith, int w, size_t n, Sh3 r);
+void op_reshare(Ctx& c, bool arith, int w, size_t n, int group, Sh3 s);
+
+// ---- permutations (perm.cu) ----
+void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>& out);
+void reserve_perms(Ctx& c, size_t n, size_t count);
+ShardedPerm next_perm(Ctx& c, size_t n);
+// y = local permutation of x under one group's permutation followed by that
+// group's reshare; idx gives dst[k] = src[idx[k]].
+void op_apply_sharded(Ctx& c, bool arith, int w, size_t n, Sh3 s, const ShardedPerm& sp,
+                      bool inverse);
+void op_apply_elementwise(Ctx& c, bool x_arith, int xw, size_t n, Sh3 x, CSh3 perm /*int32 A*/);
+void op_scatter(Ctx& c, int w, size_t n, CSh3 src, Sh3 dst, const int32_t* sigma);
+void op_shuffle(Ctx& c, bool arith, int w, size_t n, Sh3 s);
+
+// ---- sorting (radix.cu) ----
+void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out /*int32*/);
+
+}  // namespace orqcu

@@ -1,0 +1,93 @@
+"""Generate the golden fixtures from the reference itself.
+
+Runs ORQ's own code (oracle/_ref/ref_driver, built by `make -C oracle ref`
+from the reference headers with the deterministic libsodium shim) as three
+local party processes and stores each dumped share array as the three
+distinct shares S0, S1, S2:
+
+  ref_golden.npz    small cases, full arrays
+  ref_digests.json  large cases, SHA-256 of every share array
+  aes_gcm_kat.json  AES-256-GCM keystream known answers from Python
+                    `cryptography` (FIPS-197 / SP 800-38D)
+
+Usage: python tests/golden/make_golden.py   (needs the reference tree; run in
+the build container, not at test time)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import run_ref  # noqa: E402
+
+# (tag, op, n, data_seed, shim_seed, bits, full arrays?)
+CASES = [
+    ("prims_n1000", "prims", 1000, 7, 1, 40, True),
+    ("prims_n1", "prims", 1, 11, 2, 40, True),
+    ("prims_n300000", "prims", 300000, 7, 1, 40, False),
+    ("radix_n1000_b40", "radix", 1000, 7, 3, 40, True),
+    ("radix_n513_b8", "radix", 513, 7, 3, 8, True),
+    ("radix_n64_b64", "radix", 64, 5, 4, 64, True),
+    ("radix_n20000_b40", "radix", 20000, 9, 5, 40, False),
+    ("shuffle_n1000", "shuffle", 1000, 7, 6, 40, True),
+]
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def aes_kat():
+    from cryptography.hazmat.primitives.ciphers.aead import AESGCM
+
+    out = []
+    rng = np.random.default_rng(2024)
+    for nonce0, nbytes in ((0, 48), (5, (1 << 20) + 37), (2**33 + 7, 4096)):
+        key = rng.integers(0, 256, 32, dtype=np.uint8).tobytes()
+        ks = b""
+        off, nonce = 0, nonce0
+        while off < nbytes:
+            ln = min(1 << 20, nbytes - off)
+            iv = nonce.to_bytes(8, "little") + b"\0\0\0\0"
+            ks += AESGCM(key).encrypt(iv, b"\0" * ln, None)[:ln]
+            off += ln
+            nonce += 1
+        out.append({"key": key.hex(), "nonce0": nonce0, "nbytes": nbytes,
+                    "head": ks[:64].hex(), "sha256": hashlib.sha256(ks).hexdigest()})
+    return out
+
+
+def main():
+    arrays = {}
+    digests = {}
+    for tag, op, n, dseed, sseed, bits, full in CASES:
+        dumps, _ = run_ref.run(op, n, dseed, shim_seed=sseed, bits=bits)
+        meta = {"op": op, "n": n, "data_seed": dseed, "shim_seed": sseed, "bits": bits}
+        digests[tag] = {"meta": meta, "arrays": {}}
+        for name in dumps[0]:
+            if name.startswith("open_") or "open" in name:
+                S = [dumps[0][name][0]]
+            else:
+                S = run_ref.distinct_shares(dumps, name)
+            stacked = np.stack(S)
+            digests[tag]["arrays"][name] = [digest(s) for s in S]
+            if full:
+                arrays[f"{tag}/{name}"] = stacked
+        print(tag, "ok", flush=True)
+    np.savez_compressed(os.path.join(HERE, "ref_golden.npz"), **arrays)
+    with open(os.path.join(HERE, "ref_digests.json"), "w") as f:
+        json.dump(digests, f, indent=1, sort_keys=True)
+    with open(os.path.join(HERE, "aes_gcm_kat.json"), "w") as f:
+        json.dump(aes_kat(), f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,145 @@
+"""Replays of the call sequences in oracle/ref_driver.cpp on a backend.
+
+Both the C restatement (OracleBackend) and the GPU runtime (GpuBackend)
+expose the same small interface; every function returns the three distinct
+share arrays as a (3, n) numpy array so results can be compared with the
+reference's golden dumps and with each other.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle.oracle import Oracle, splitmix64_fast
+
+_U = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}
+
+
+class OracleBackend:
+    def __init__(self, seed):
+        self.o = Oracle(seed)
+
+    def share(self, data, arith, party):
+        return self.o.secret_share(data, arith, party)
+
+    def and_b(self, x, y):
+        return self.o.and_b(x, y)
+
+    def xor_b(self, x, y):
+        return self.o.xor_b(x, y)
+
+    def mul_a(self, x, y):
+        return self.o.mul_a(x, y)
+
+    def add_a(self, x, y):
+        return self.o.add_a(x, y)
+
+    def b2a_bit(self, x):
+        return self.o.b2a_bit(x)
+
+    def open(self, x, arith):
+        return self.o.open(x, arith)
+
+    def np(self, x):
+        return np.stack(x)
+
+    def radix(self, key, bits, payloads):
+        perm = self.o.radix_sort(key, bits, payloads)
+        return perm
+
+
+class GpuBackend:
+    def __init__(self, seed, device=0):
+        import orq_b200 as orq
+
+        self.orq = orq
+        self.rt = orq.Runtime(seed=seed, device=device)
+
+    def share(self, data, arith, party):
+        return (self.rt.secret_share_a if arith else self.rt.secret_share_b)(data, party)
+
+    def and_b(self, x, y):
+        return x & y
+
+    def xor_b(self, x, y):
+        return x ^ y
+
+    def mul_a(self, x, y):
+        return x * y
+
+    def add_a(self, x, y):
+        return x + y
+
+    def b2a_bit(self, x):
+        return x.b2a_bit()
+
+    def open(self, x, arith):
+        return x.open().cpu().numpy()
+
+    def np(self, x):
+        a = x.shares.cpu().numpy()
+        return a.view(_U[a.dtype.itemsize]) if a.ndim == 2 else a
+
+    def radix(self, key, bits, payloads):
+        perm = self.orq.radix_sort(key, self.orq.ASC, bits)
+        for p in payloads:
+            self.orq.oblivious_apply_elementwise_perm(p, perm)
+        return perm
+
+
+def prim_inputs(n, seed, dt):
+    st = splitmix64_fast(seed, 2 * n)
+    return st[:n].astype(dt), st[n:].astype(dt)
+
+
+def replay_prims(be, n, seed):
+    """run_prims<int32>, <int64>, <int8> of ref_driver.cpp, in order."""
+    out = {}
+    for tag, dt, s in (("w4_", np.uint32, seed), ("w8_", np.uint64, seed + 1), ("w1_", np.uint8, seed + 2)):
+        x, y = prim_inputs(n, s, dt)
+        xb = be.share(x, False, 0)
+        yb = be.share(y, False, 1)
+        out[tag + "xb"] = be.np(xb)
+        out[tag + "yb"] = be.np(yb)
+        zb = be.and_b(xb, yb)
+        out[tag + "and"] = be.np(zb)
+        out[tag + "xor"] = be.np(be.xor_b(xb, yb))
+        xa = be.share(x, True, 2)
+        ya = be.share(y, True, 0)
+        out[tag + "xa"] = be.np(xa)
+        out[tag + "ya"] = be.np(ya)
+        za = be.mul_a(xa, ya)
+        out[tag + "mul"] = be.np(za)
+        out[tag + "add"] = be.np(be.add_a(xa, ya))
+        ba = be.b2a_bit(xb)
+        out[tag + "b2a"] = be.np(ba)
+        out[tag + "open_and"] = be.open(zb, False)[None]
+        out[tag + "open_mul"] = be.open(za, True)[None]
+        out[tag + "open_b2a"] = be.open(ba, True)[None]
+    return out
+
+
+def radix_inputs(n, seed, bits):
+    st = splitmix64_fast(seed, 3 * n)
+    km = np.uint64((1 << bits) - 1) if bits < 64 else np.uint64(2**64 - 1)
+    return st[:n] & km, st[n:2 * n] & np.uint64(0xFFFFFFFF), st[2 * n:] & np.uint64(0xFFFFFFFF)
+
+
+def replay_radix(be, n, seed, bits):
+    """The "radix" op of ref_driver.cpp: radix_sort(key, ASC, bits) then the
+    permutation applied to two A-shared int64 payloads."""
+    key, p1, p2 = radix_inputs(n, seed, bits)
+    kb = be.share(key, False, 0)
+    a1 = be.share(p1, True, 0)
+    a2 = be.share(p2, True, 0)
+    perm = be.radix(kb, bits, [a1, a2])
+    out = {"key": be.np(kb), "pay1": be.np(a1), "pay2": be.np(a2), "perm": be.np(perm)}
+    out["open_key"] = be.open(kb, False)[None]
+    out["open_pay1"] = be.open(a1, True)[None]
+    out["open_pay2"] = be.open(a2, True)[None]
+    return out, (key, p1, p2)
+
+
+def same(a, b):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    return a.shape == b.shape and a.tobytes() == b.tobytes()

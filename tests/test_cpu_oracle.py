@@ -1,0 +1,92 @@
+"""The C restatement (oracle/) against the reference's own outputs.
+
+Golden vectors come from ORQ's code run as three party processes
+(tests/golden/make_golden.py); the AES keystream against Python
+`cryptography` known answers.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from replay import OracleBackend, replay_prims, replay_radix, same
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_aes_gcm_keystream_kat(oracle_lib, aes_kat):
+    from oracle.oracle import Oracle
+
+    o = Oracle(0)
+    lib = o.lib
+    import ctypes
+
+    for case in aes_kat:
+        key = bytes.fromhex(case["key"])
+        rk = (ctypes.c_uint32 * 60)()
+        lib.oro_aes256_expand(key, rk)
+        buf = np.zeros(case["nbytes"], dtype=np.uint8)
+        lib.oro_keystream(rk, ctypes.c_uint64(case["nonce0"]), buf.ctypes.data_as(ctypes.c_void_p),
+                          ctypes.c_size_t(case["nbytes"]))
+        assert buf[:64].tobytes().hex() == case["head"]
+        assert hashlib.sha256(buf.tobytes()).hexdigest() == case["sha256"]
+
+
+def test_fips197_aes256_vector(oracle_lib):
+    import ctypes
+
+    from oracle.oracle import Oracle
+
+    lib = Oracle(0).lib
+    rk = (ctypes.c_uint32 * 60)()
+    lib.oro_aes256_expand(bytes(range(32)), rk)
+    out = ctypes.create_string_buffer(16)
+    lib.oro_aes256_encrypt(rk, bytes.fromhex("00112233445566778899aabbccddeeff"), out)
+    assert out.raw.hex() == "8ea2b7ca516745bfeafc49904b496089"  # FIPS-197 C.3
+
+
+@pytest.mark.parametrize("tag,n,seed,shim", [("prims_n1000", 1000, 7, 1), ("prims_n1", 1, 11, 2)])
+def test_prims_match_reference_shares(oracle_lib, golden, tag, n, seed, shim):
+    out = replay_prims(OracleBackend(shim), n, seed)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+def test_prims_large_match_reference_digests(oracle_lib, digests):
+    d = digests["prims_n300000"]
+    m = d["meta"]
+    out = replay_prims(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag", ["radix_n1000_b40", "radix_n513_b8", "radix_n64_b64"])
+def test_radix_matches_reference_shares(oracle_lib, golden, digests, tag):
+    m = digests[tag]["meta"]
+    out, (key, p1, p2) = replay_radix(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"])
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    # and the plaintext semantics: stable sort on the signed key
+    order = np.argsort(key.view(np.int64), kind="stable")
+    assert same(out["open_key"][0], key[order])
+    assert same(out["open_pay1"][0], p1[order])
+
+
+def test_radix_large_matches_reference_digests(oracle_lib, digests):
+    d = digests["radix_n20000_b40"]
+    m = d["meta"]
+    out, _ = replay_radix(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+def test_gen_perm_is_a_permutation(oracle_lib):
+    from oracle.oracle import G01, Oracle
+
+    o = Oracle(5)
+    for n in (0, 1, 2, 3, 100, 1024, 4097):
+        p, draws = o.gen_perm(G01, n)
+        assert sorted(p.tolist()) == list(range(n))
+        assert draws >= n
