@@ -63,13 +63,21 @@ const char* orqcu_last_error(void);
  * parties: keys for the 10 streams, nonces at 0. device = CUDA ordinal. */
 int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out);
 int orqcu_runtime_destroy(orqcu_runtime* rt);
-/* Run subsequent work on an existing cudaStream_t (NULL = the runtime's own). */
+/* Run subsequent work on an existing cudaStream_t; NULL selects the CUDA
+ * default stream (as in the CUDA runtime API). */
 int orqcu_runtime_set_stream(orqcu_runtime* rt, void* cuda_stream);
 int orqcu_synchronize(orqcu_runtime* rt);
 /* Nonce counter of a PRG stream (AESPRGAlgorithm::nonce, prg_algorithm.h:208). */
 int orqcu_get_nonce(orqcu_runtime* rt, int stream, uint64_t* nonce);
 /* Number of kernels this runtime has launched. */
 int orqcu_kernels_launched(orqcu_runtime* rt, uint64_t* count);
+
+/* Per-kernel timing, the device counterpart of ORQ's thread instrumentation
+ * (include/profiling/thread_profiling.h:227-280): when enabled, every launch is
+ * bracketed by CUDA events on its stream. The report (and reset) gives one line
+ * per kernel class: "name launches total_ms algorithmic_bytes aes_blocks". */
+int orqcu_profile_enable(orqcu_runtime* rt, int on);
+int orqcu_profile_report(orqcu_runtime* rt, char* buf, size_t len);
 
 /* device memory helpers */
 int orqcu_malloc(orqcu_runtime* rt, size_t bytes, void** dptr);

@@ -64,6 +64,8 @@ int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out) {
         ORQ_CUDA_CHECK(cudaDeviceGetAttribute(&rt->ctx.num_sms, cudaDevAttrMultiProcessorCount, device));
         ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&rt->ctx.stream, cudaStreamNonBlocking));
         rt->ctx.owns_stream = true;
+        ORQ_CUDA_CHECK(cudaMalloc(&rt->ctx.d_err, sizeof(int)));
+        ORQ_CUDA_CHECK(cudaMemset(rt->ctx.d_err, 0, sizeof(int)));
         orqcu::init_ctx_keys(rt->ctx, seed);
         orqcu::upload_aes_tables(device);
         *out = rt;
@@ -78,6 +80,7 @@ int orqcu_runtime_destroy(orqcu_runtime* rt) {
         for (auto& sp : rt->ctx.perm_queue) rt->ctx.free_perm(sp);
         rt->ctx.perm_queue.clear();
         if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
+        if (rt->ctx.d_err) cudaFree(rt->ctx.d_err);
         delete rt;
     });
 }
@@ -86,18 +89,9 @@ int orqcu_runtime_set_stream(orqcu_runtime* rt, void* s) {
     return guard([&] {
         need_rt(rt);
         cudaSetDevice(rt->ctx.device);
-        if (s == nullptr) {
-            if (!rt->ctx.owns_stream) {
-                ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&rt->ctx.stream, cudaStreamNonBlocking));
-                rt->ctx.owns_stream = true;
-            }
-            return;
-        }
-        if (rt->ctx.owns_stream) {
-            ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
-            cudaStreamDestroy(rt->ctx.stream);
-        }
-        rt->ctx.stream = (cudaStream_t)s;
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+        if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
+        rt->ctx.stream = (cudaStream_t)s;  // NULL = the CUDA default stream
         rt->ctx.owns_stream = false;
     });
 }
@@ -106,6 +100,7 @@ int orqcu_synchronize(orqcu_runtime* rt) {
     return guard([&] {
         need_rt(rt);
         ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+        rt->ctx.check_device_error();
     });
 }
 
@@ -122,6 +117,32 @@ int orqcu_kernels_launched(orqcu_runtime* rt, uint64_t* count) {
         need_rt(rt);
         need(count != nullptr, "null output");
         *count = rt->ctx.kernels_launched;
+    });
+}
+
+int orqcu_profile_enable(orqcu_runtime* rt, int on) {
+    return guard([&] {
+        need_rt(rt);
+        rt->ctx.prof_collect();
+        rt->ctx.profiling = on != 0;
+    });
+}
+
+int orqcu_profile_report(orqcu_runtime* rt, char* buf, size_t len) {
+    return guard([&] {
+        need_rt(rt);
+        need(buf != nullptr && len > 0, "null buffer");
+        rt->ctx.prof_collect();
+        std::string out;
+        for (auto& kv : rt->ctx.prof_agg) {
+            char line[256];
+            snprintf(line, sizeof(line), "%s %llu %.6f %.0f %.0f\n", kv.first.c_str(),
+                     kv.second.launches, kv.second.ms, kv.second.bytes, kv.second.aes_blocks);
+            out += line;
+        }
+        rt->ctx.prof_agg.clear();
+        need(out.size() < len, "report buffer too small");
+        std::memcpy(buf, out.c_str(), out.size() + 1);
     });
 }
 
@@ -313,7 +334,7 @@ int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key
         need_sh((const void* const*)key, n, "null key");
         need_sh((const void* const*)perm_out, n, "null perm_out");
         orqcu::op_radix_sort(rt->ctx, key_width, n, m3(key), bits, descending != 0, m3(perm_out));
-        ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
+        rt->ctx.check_device_error();
     });
 }
 

@@ -30,9 +30,13 @@ inline void prep_aes_kernel(K kern) {
                                         kAesSmemBytes));
 }
 
+// Launch an AES kernel over `units` thread work items; name/bytes/blocks feed
+// the optional per-kernel profile.
 template <typename K, typename... Args>
-inline void launch_aes(Ctx& c, K kern, unsigned long long units, Args... args) {
+inline void launch_aes(Ctx& c, const char* name, double bytes, double aes_blocks, K kern,
+                       unsigned long long units, Args... args) {
     prep_aes_kernel(kern);
+    ProfScope ps(c, name, bytes, aes_blocks);
     kern<<<aes_grid(c, units), kAesThreads, kAesSmemBytes, c.stream>>>(args...);
     ORQ_CUDA_CHECK(cudaGetLastError());
     c.kernels_launched++;

@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
     __shared__ uint32_t red[33];
     __shared__ uint32_t s_i, s_m, s_done, s_last_q, s_nunc;
     __shared__ unsigned long long s_start;
-    __shared__ uint32_t unc_q[kStep / 8];   // uncertain survivors of a step (capped)
+    __shared__ uint32_t unc_v[kStep / 8];   // uncertain survivors of a step (capped)
     __shared__ uint32_t unc_cp[kStep / 8];
     __shared__ uint8_t unc_ok[kStep / 8];
     const uint32_t g = blockIdx.x;
@@ -166,14 +166,28 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
             const uint32_t i0 = s_i;
             const long long T = (long long)n - 1 - i0;
             uint32_t v[8];
-            uint32_t certain = 0, unc = 0;
+            uint32_t cand = 0;  // not certainly rejected: v <= T
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const uint32_t q = threadIdx.x * 8 + u;  // index within the step
                 v[u] = (sb + q < c) ? sv[sb + q] : 0xffffffffu;
-                const long long vv = v[u] == 0xffffffffu ? (1ll << 40) : (long long)v[u];
-                if (vv + q <= T) certain |= 1u << u;
-                else if (vv <= T) unc |= 1u << u;
+                if (v[u] != 0xffffffffu && (long long)v[u] <= T) cand |= 1u << u;
+            }
+            // Only candidates can advance i, so at candidate u at most
+            // (candidates before u) acceptances have happened: v <= T - that
+            // makes u certainly accepted.
+            uint32_t tot_cand;
+            const uint32_t cpre_cand = block_excl_sum(__popc(cand), red, tot_cand);
+            uint32_t certain = 0, unc = 0;
+            {
+                uint32_t before = cpre_cand;
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    if ((cand >> u) & 1u) {
+                        if ((long long)v[u] + before <= T) certain |= 1u << u;
+                        else unc |= 1u << u;
+                        before++;
+                    }
             }
             uint32_t accept = certain;
             const int any_unc = __syncthreads_or(unc != 0);
@@ -189,7 +203,7 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
                     for (int u = 0; u < 8; u++) {
                         if ((unc >> u) & 1u) {
                             if (k < cap) {
-                                unc_q[k] = threadIdx.x * 8 + u;
+                                unc_v[k] = v[u];
                                 unc_cp[k] = cc;
                             }
                             k++;
@@ -199,34 +213,33 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
                 }
                 __syncthreads();
                 if (threadIdx.x == 0) {
-                    uint32_t uacc = 0;
-                    const uint32_t m = tot_u < cap ? tot_u : cap;
-                    for (uint32_t k = 0; k < m; k++) {
-                        const uint32_t q = unc_q[k];
-                        const uint32_t vv = sv[sb + q];
-                        const unsigned long long iat = (unsigned long long)i0 + unc_cp[k] + uacc;
-                        const bool ok = iat < n && (unsigned long long)vv <= (unsigned long long)n - 1 - iat;
-                        unc_ok[k] = ok;
-                        uacc += ok;
+                    if (tot_u > cap) {
+                        s_nunc = 0xffffffffu;  // too many: decide the whole step in order
+                    } else {
+                        uint32_t uacc = 0;
+                        for (uint32_t k = 0; k < tot_u; k++) {
+                            const unsigned long long iat = (unsigned long long)i0 + unc_cp[k] + uacc;
+                            const bool ok = iat < n && (unsigned long long)unc_v[k] <=
+                                                           (unsigned long long)n - 1 - iat;
+                            unc_ok[k] = ok;
+                            uacc += ok;
+                        }
+                        s_nunc = tot_u;
                     }
-                    s_nunc = m;
-                }
-                __syncthreads();
-                if (tot_u > cap) {
-                    // More uncertain survivors than the list holds (only when n is
-                    // tiny): fall back to a fully sequential decision of this step.
-                    if (threadIdx.x == 0) s_nunc = 0xffffffffu;
                 }
                 __syncthreads();
                 if (s_nunc == 0xffffffffu) {
                     __shared__ uint32_t seq_acc[kStep / 32];
+                    __shared__ uint32_t seq_v[kStep];
                     if (threadIdx.x < kStep / 32) seq_acc[threadIdx.x] = 0;
+#pragma unroll
+                    for (int u = 0; u < 8; u++) seq_v[threadIdx.x * 8 + u] = v[u];
                     __syncthreads();
                     if (threadIdx.x == 0) {
                         uint32_t ii = i0;
                         const uint32_t lim = (c - sb) < kStep ? (c - sb) : kStep;
                         for (uint32_t q = 0; q < lim && ii < n; q++) {
-                            const uint32_t vv = sv[sb + q];
+                            const uint32_t vv = seq_v[q];
                             if (vv <= n - 1 - ii) {
                                 seq_acc[q >> 5] |= 1u << (q & 31);
                                 ii++;
@@ -312,7 +325,19 @@ struct FinArgs {
     int32_t* A;           // [P][n]
     int32_t* const* perm_out;  // [P] -> n
     int32_t* const* inv_out;   // [P] -> n
+    int* err;
 };
+
+// target of step i; an out-of-range offset (never produced by a correct scan)
+// is flagged and treated as a self-swap so no access leaves the arrays
+__device__ __forceinline__ uint32_t fin_target(const FinArgs& a, size_t t, uint32_t i) {
+    const unsigned long long j = (unsigned long long)i + a.acc[t];
+    if (j >= a.n) {
+        atomicOr(a.err, 1);
+        return i;
+    }
+    return (uint32_t)j;
+}
 
 __global__ void k_fin_init(FinArgs a) {
     const size_t tot = (size_t)a.P * a.n;
@@ -327,7 +352,7 @@ __global__ void k_fin_targets(FinArgs a) {
     for (size_t t = gtid(); t < tot; t += gstride()) {
         const size_t pm = t / a.n;
         const uint32_t i = (uint32_t)(t % a.n);
-        const uint32_t j = i + a.acc[t];
+        const uint32_t j = fin_target(a, t, i);
         if (j != i) {
             atomicMax(&a.par[pm * a.n + j], (int32_t)i);
             atomicAdd(&a.cnt[pm * a.n + j], 1u);
@@ -363,10 +388,12 @@ __global__ void k_fin_place(FinArgs a) {
     for (size_t t = gtid(); t < tot; t += gstride()) {
         const size_t pm = t / a.n;
         const uint32_t i = (uint32_t)(t % a.n);
-        const uint32_t j = i + a.acc[t];
+        const uint32_t j = fin_target(a, t, i);
         if (j != i) {
             const uint32_t s = atomicAdd(&a.fill[pm * a.n + j], 1u);
-            a.bucket[pm * a.n + a.off[pm * a.n + j] + s] = (int32_t)i;
+            const unsigned long long slot = (unsigned long long)a.off[pm * a.n + j] + s;
+            if (slot < a.n) a.bucket[pm * a.n + slot] = (int32_t)i;
+            else atomicOr(a.err, 2);
         }
     }
 }
@@ -389,13 +416,14 @@ __global__ void k_fin_final(FinArgs a) {
     for (size_t t = gtid(); t < tot; t += gstride()) {
         const size_t pm = t / a.n;
         const uint32_t i = (uint32_t)(t % a.n);
-        const uint32_t j = i + a.acc[t];
+        const uint32_t j = fin_target(a, t, i);
         const int32_t* A = a.A + pm * a.n;
         int32_t val;
         if (j == i) {
             val = A[i];
         } else {
-            const uint32_t o = a.off[pm * a.n + j], c = a.cnt[pm * a.n + j];
+            const uint32_t o = a.off[pm * a.n + j];
+            const uint32_t c = min(a.cnt[pm * a.n + j], a.n - min(o, a.n));
             const int32_t* b = a.bucket + pm * a.n + o;
             int32_t pred = -1;
             for (uint32_t k = 0; k < c; k++) {
@@ -403,6 +431,10 @@ __global__ void k_fin_final(FinArgs a) {
                 if (s < (int32_t)i && s > pred) pred = s;
             }
             val = pred >= 0 ? A[pred] : (int32_t)j;
+        }
+        if ((uint32_t)val >= a.n) {
+            atomicOr(a.err, 4);
+            val = (int32_t)i;
         }
         a.perm_out[pm][i] = val;
         a.inv_out[pm][val] = (int32_t)i;
@@ -492,7 +524,10 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         ga.tmin = minp[b];
         ga.bits = bitsp[b];
         ga.state = state.as<FyState>();
-        k_fy_gen<<<gen_grid, kAesThreads, kAesSmemBytes, gs>>>(ga);
+        {
+            ProfScope ps(c, "fy_gen", 0.0, 3.0 * tiles * kTileBlocks, gs);
+            k_fy_gen<<<gen_grid, kAesThreads, kAesSmemBytes, gs>>>(ga);
+        }
         ORQ_CUDA_CHECK(cudaGetLastError());
         ORQ_CUDA_CHECK(cudaEventRecord(gen_done[b], gs));
         c.kernels_launched++;
@@ -518,7 +553,10 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         sa.state = state.as<FyState>();
         sa.acc = acc.as<uint32_t>();
         sa.refills = refills.as<uint32_t>();
-        k_fy_scan<<<3, kScanThreads, 0, c.stream>>>(sa);
+        {
+            ProfScope ps(c, "fy_scan", 0.0);
+            k_fy_scan<<<3, kScanThreads, 0, c.stream>>>(sa);
+        }
         ORQ_CUDA_CHECK(cudaGetLastError());
         ORQ_CUDA_CHECK(cudaEventRecord(scan_done[b], c.stream));
         c.kernels_launched++;
@@ -571,7 +609,9 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         fa.A = A.as<int32_t>();
         fa.perm_out = ptrs.as<int32_t*>();
         fa.inv_out = ptrs.as<int32_t*>() + P;
+        fa.err = c.d_err;
         const unsigned gg = plain_grid(c, el);
+        ProfScope ps(c, "fy_finalize", 0.0);
         k_fin_init<<<gg, 256, 0, c.stream>>>(fa);
         k_fin_targets<<<gg, 256, 0, c.stream>>>(fa);
         k_fin_scan<<<(unsigned)P, 1024, 0, c.stream>>>(fa);
@@ -582,6 +622,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         c.kernels_launched += 6;
         ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // scratch reuse
     }
+    c.check_device_error();
     cudaFreeHost(hstate);
     cudaEventDestroy(ev_start);
     for (int k = 0; k < 2; k++) {
@@ -641,6 +682,7 @@ struct ApplyArgs {
     unsigned long long ch1, ch2;
     unsigned long long n;
     int32_t* sigma;
+    int* err;
 };
 
 template <int W>
@@ -752,9 +794,15 @@ __global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
             for (int j = 0; j < 3; j++)
 #pragma unroll
                 for (int e = 0; e < E; e++)
-                    if (k0 + e < a.n)
-                        store_elem<W1>(a.dst1[j], (int32_t)sig[e],
-                                       reinterpret_cast<const uint8_t*>(&v1[j][0]) + e * W1);
+                    if (k0 + e < a.n) {
+                        // sigma is an opened permutation; a value outside [0, n)
+                        // means corrupted shares: flag it, skip the store
+                        if ((unsigned long long)sig[e] < a.n)
+                            store_elem<W1>(a.dst1[j], (int32_t)sig[e],
+                                           reinterpret_cast<const uint8_t*>(&v1[j][0]) + e * W1);
+                        else
+                            atomicOr(a.err, 8);
+                    }
         } else if constexpr (MODE == 3) {
             uint4 o[B1];
 #pragma unroll
@@ -776,6 +824,11 @@ void launch_apply(Ctx& c, const ApplyArgs& a) {
     auto kern = k_apply<W1, A1, W2, A2, MODE>;
     prep_aes_kernel(kern);
     const unsigned long long units = ceil_div(a.n, E);
+    // idx + gathered shares + written shares (the second vector is only read
+    // when its result is opened instead of stored)
+    const double by = (double)a.n * (4.0 + 6.0 * W1 + (W2 ? (MODE == 0 ? 6.0 : 3.0) * W2 : 0.0));
+    const double bl = 2.0 * ((double)ceil_div(a.n * W1, 16) + (W2 ? (double)ceil_div(a.n * W2, 16) : 0.0));
+    ProfScope ps(c, "apply_group", by, bl);
     kern<<<aes_grid(c, units), kAesThreads, kAesSmemBytes, c.stream>>>(a);
     ORQ_CUDA_CHECK(cudaGetLastError());
     c.kernels_launched++;
@@ -870,6 +923,7 @@ void op_apply_elementwise(Ctx& c, bool x_arith, int xw, size_t n, Sh3 x, CSh3 pe
             a.dst2[j] = Pp[g & 1][j];
         }
         a.idx = sp.inv[g];
+        a.err = c.d_err;
         // per group stream: the x reshare first, then the permutation's
         a.g1 = c.stream_arg(G01 + g);
         a.g2 = c.stream_arg(G01 + g, 2 * chx);
@@ -892,9 +946,13 @@ void op_shuffle(Ctx& c, bool arith, int w, size_t n, Sh3 s) {
 
 // local_apply_perm with a public permutation: dst[sigma[i]] = src[i]
 template <int W>
-__global__ void k_scatter(CSh3 src, Sh3 dst, const int32_t* sigma, unsigned long long n) {
+__global__ void k_scatter(CSh3 src, Sh3 dst, const int32_t* sigma, unsigned long long n, int* err) {
     for (unsigned long long i = gtid(); i < n; i += gstride()) {
         const int32_t d = __ldg(sigma + i);
+        if ((unsigned long long)(uint32_t)d >= n) {
+            atomicOr(err, 8);
+            continue;
+        }
 #pragma unroll
         for (int j = 0; j < 3; j++) {
             uint8_t v[W];
@@ -906,9 +964,9 @@ __global__ void k_scatter(CSh3 src, Sh3 dst, const int32_t* sigma, unsigned long
 void op_scatter(Ctx& c, int w, size_t n, CSh3 src, Sh3 dst, const int32_t* sigma) {
     if (!n) return;
     const unsigned g = plain_grid(c, n);
-    if (w == 4) k_scatter<4><<<g, 256, 0, c.stream>>>(src, dst, sigma, n);
-    else if (w == 8) k_scatter<8><<<g, 256, 0, c.stream>>>(src, dst, sigma, n);
-    else if (w == 16) k_scatter<16><<<g, 256, 0, c.stream>>>(src, dst, sigma, n);
+    if (w == 4) k_scatter<4><<<g, 256, 0, c.stream>>>(src, dst, sigma, n, c.d_err);
+    else if (w == 8) k_scatter<8><<<g, 256, 0, c.stream>>>(src, dst, sigma, n, c.d_err);
+    else if (w == 16) k_scatter<16><<<g, 256, 0, c.stream>>>(src, dst, sigma, n, c.d_err);
     else throw std::invalid_argument("scatter supports 4, 8, 16-byte shares");
     ORQ_CUDA_CHECK(cudaGetLastError());
     c.kernels_launched++;

@@ -237,7 +237,8 @@ void launch_keystream(Ctx& c, int stream_id, unsigned long long nonce0, void* ou
     st.rk = c.rk[stream_id];
     st.nonce = nonce0;
     if (!nbytes) return;
-    launch_aes(c, k_keystream, ceil_div(nbytes, 16), st, (uint8_t*)out, (unsigned long long)nbytes);
+    launch_aes(c, "keystream", (double)nbytes, (double)ceil_div(nbytes, 16), k_keystream,
+               ceil_div(nbytes, 16), st, (uint8_t*)out, (unsigned long long)nbytes);
 }
 
 void op_secret_share(Ctx& c, bool arith, int w, size_t n, const void* data, int party, Sh3 s) {
@@ -249,10 +250,11 @@ void op_secret_share(Ctx& c, bool arith, int w, size_t n, const void* data, int 
         void* b = s.p[(party + 1) % 3];
         void* d = s.p[(party + 2) % 3];
         ORQ_DISPATCH_W(w, {
+            const double by = 4.0 * nb, bl = 2.0 * ceil_div(nb, 16);
             if (arith)
-                launch_aes(c, k_share<W, true>, ceil_div(nb, 16), (const uint8_t*)data, a, b, d, st, ch, nb);
+                launch_aes(c, "secret_share", by, bl, k_share<W, true>, ceil_div(nb, 16), (const uint8_t*)data, a, b, d, st, ch, nb);
             else
-                launch_aes(c, k_share<W, false>, ceil_div(nb, 16), (const uint8_t*)data, a, b, d, st, ch, nb);
+                launch_aes(c, "secret_share", by, bl, k_share<W, false>, ceil_div(nb, 16), (const uint8_t*)data, a, b, d, st, ch, nb);
         });
     }
     c.nonce[LOCAL0 + party] += 2 * ch;
@@ -270,6 +272,7 @@ void op_public_share(Ctx& c, int w, size_t n, const void* data, Sh3 s) {
 void op_open(Ctx& c, bool arith, int w, size_t n, CSh3 s, void* out) {
     const unsigned long long nb = (unsigned long long)n * w;
     if (!nb) return;
+    ProfScope ps(c, "open", 4.0 * nb);
     ORQ_DISPATCH_W(w, {
         if (arith)
             k_open<W, true><<<plain_grid(c, ceil_div(nb, 16)), 256, 0, c.stream>>>(s.p[0], s.p[1], s.p[2], out, nb);
@@ -292,8 +295,9 @@ void op_mult(Ctx& c, bool arith, int w, size_t n, CSh3 x, CSh3 y, Sh3 z) {
     a.nbytes = nb;
     if (nb) {
         ORQ_DISPATCH_W(w, {
-            if (arith) launch_aes(c, k_mult<W, true>, ceil_div(nb, 16), a);
-            else launch_aes(c, k_mult<W, false>, ceil_div(nb, 16), a);
+            const double by = 9.0 * nb, bl = 3.0 * ceil_div(nb, 16);
+            if (arith) launch_aes(c, "multiply_a", by, bl, k_mult<W, true>, ceil_div(nb, 16), a);
+            else launch_aes(c, "and_b", by, bl, k_mult<W, false>, ceil_div(nb, 16), a);
         });
     }
     for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += ch;
@@ -310,6 +314,7 @@ void op_local(Ctx& c, int op, int w, size_t n, CSh3 x, CSh3 y, Sh3 z) {
     }
     a.nbytes = nb;
     const unsigned g = plain_grid(c, ceil_div(nb, 16));
+    ProfScope ps(c, "local", 9.0 * nb);
     ORQ_DISPATCH_W(w, {
         if (op == 0) k_local<W, 0><<<g, 256, 0, c.stream>>>(a);
         else if (op == 1) k_local<W, 1><<<g, 256, 0, c.stream>>>(a);
@@ -348,7 +353,7 @@ void op_b2a_bit(Ctx& c, int w, size_t n, CSh3 x, Sh3 y) {
     a.chunks = ch;
     a.nbytes = nb;
     if (nb) {
-        ORQ_DISPATCH_W(w, { launch_aes(c, k_b2a<W>, ceil_div(nb, 16), a); });
+        ORQ_DISPATCH_W(w, { launch_aes(c, "b2a_bit", 6.0 * nb, 9.0 * ceil_div(nb, 16), k_b2a<W>, ceil_div(nb, 16), a); });
     }
     for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += 3 * ch;
 }
@@ -358,8 +363,9 @@ void op_zero_share(Ctx& c, bool arith, int w, size_t n, Sh3 r) {
     if (nb) {
         StreamArg p0 = c.stream_arg(PAIR0), p1 = c.stream_arg(PAIR1), p2 = c.stream_arg(PAIR2);
         ORQ_DISPATCH_W(w, {
-            if (arith) launch_aes(c, k_zero<W, true>, ceil_div(nb, 16), r.p[0], r.p[1], r.p[2], p0, p1, p2, nb);
-            else launch_aes(c, k_zero<W, false>, ceil_div(nb, 16), r.p[0], r.p[1], r.p[2], p0, p1, p2, nb);
+            const double by = 3.0 * nb, bl = 3.0 * ceil_div(nb, 16);
+            if (arith) launch_aes(c, "zero_share", by, bl, k_zero<W, true>, ceil_div(nb, 16), r.p[0], r.p[1], r.p[2], p0, p1, p2, nb);
+            else launch_aes(c, "zero_share", by, bl, k_zero<W, false>, ceil_div(nb, 16), r.p[0], r.p[1], r.p[2], p0, p1, p2, nb);
         });
     }
     for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += ch;
@@ -371,8 +377,9 @@ void op_reshare(Ctx& c, bool arith, int w, size_t n, int group, Sh3 s) {
     StreamArg g = c.stream_arg(G01 + group);
     if (nb) {
         ORQ_DISPATCH_W(w, {
-            if (arith) launch_aes(c, k_reshare<W, true>, ceil_div(nb, 16), s.p[0], s.p[1], s.p[2], g, ch, nb);
-            else launch_aes(c, k_reshare<W, false>, ceil_div(nb, 16), s.p[0], s.p[1], s.p[2], g, ch, nb);
+            const double by = 6.0 * nb, bl = 2.0 * ceil_div(nb, 16);
+            if (arith) launch_aes(c, "reshare", by, bl, k_reshare<W, true>, ceil_div(nb, 16), s.p[0], s.p[1], s.p[2], g, ch, nb);
+            else launch_aes(c, "reshare", by, bl, k_reshare<W, false>, ceil_div(nb, 16), s.p[0], s.p[1], s.p[2], g, ch, nb);
         });
     }
     c.nonce[G01 + group] += 2 * ch;

@@ -306,8 +306,9 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
             ba.n = n;
             ba.shift = 32 + b;
             ba.invert = (full_width && b == bits - 1) ? 1u : 0u;
-            if (PW == 16) launch_aes(c, k_radix_b2a<16>, ceil_div(n, 4), ba);
-            else launch_aes(c, k_radix_b2a<8>, ceil_div(n, 4), ba);
+            const double by = 24.0 * n, bl = 9.0 * ceil_div(n, 4);
+            if (PW == 16) launch_aes(c, "radix_bit_b2a", by, bl, k_radix_b2a<16>, ceil_div(n, 4), ba);
+            else launch_aes(c, "radix_bit_b2a", by, bl, k_radix_b2a<8>, ceil_div(n, 4), ba);
         }
         for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += 3 * ch4;
 
@@ -321,9 +322,12 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
             sa.n = n;
             sa.tiles = tiles;
             const dim3 grid(std::min<uint32_t>(tiles, (uint32_t)c.num_sms * 8), 3);
-            k_scan_up<<<grid, 256, 0, c.stream>>>(sa);
-            k_scan_mid<<<3, 1024, 0, c.stream>>>(sa);
-            k_scan_down<<<grid, 256, 0, c.stream>>>(sa);
+            {
+                ProfScope ps(c, "radix_scan", 72.0 * n);
+                k_scan_up<<<grid, 256, 0, c.stream>>>(sa);
+                k_scan_mid<<<3, 1024, 0, c.stream>>>(sa);
+                k_scan_down<<<grid, 256, 0, c.stream>>>(sa);
+            }
             ORQ_CUDA_CHECK(cudaGetLastError());
             c.kernels_launched += 3;
 
@@ -335,7 +339,7 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
                 pa.pair[j] = c.stream_arg(PAIR0 + j);
             }
             pa.n = n;
-            launch_aes(c, k_radix_perm, ceil_div(n, 4), pa);
+            launch_aes(c, "radix_perm_mul", 48.0 * n, 3.0 * ceil_div(n, 4), k_radix_perm, ceil_div(n, 4), pa);
         }
         for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += ch4;
 

@@ -182,6 +182,49 @@ Pool::~Pool() {
     for (auto& kv : live_) cudaFree(kv.first);
 }
 
+void Ctx::check_device_error() {
+    if (!d_err) return;
+    int h = 0;
+    ORQ_CUDA_CHECK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ORQ_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (h) {
+        ORQ_CUDA_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+        throw std::runtime_error("out-of-range index in a permutation (code " + std::to_string(h) + ")");
+    }
+}
+
+ProfScope::ProfScope(Ctx& ctx, const char* name, double bytes, double aes_blocks, cudaStream_t st)
+    : c(&ctx), s(st ? st : ctx.stream), on(ctx.profiling) {
+    if (!on) return;
+    ev.name = name;
+    ev.bytes = bytes;
+    ev.aes_blocks = aes_blocks;
+    ORQ_CUDA_CHECK(cudaEventCreate(&ev.a));
+    ORQ_CUDA_CHECK(cudaEventCreate(&ev.b));
+    ORQ_CUDA_CHECK(cudaEventRecord(ev.a, s));
+}
+ProfScope::~ProfScope() {
+    if (!on) return;
+    cudaEventRecord(ev.b, s);
+    c->prof_pending.push_back(ev);
+}
+
+void Ctx::prof_collect() {
+    for (auto& e : prof_pending) {
+        float ms = 0;
+        ORQ_CUDA_CHECK(cudaEventSynchronize(e.b));
+        ORQ_CUDA_CHECK(cudaEventElapsedTime(&ms, e.a, e.b));
+        auto& g = prof_agg[e.name];
+        g.launches++;
+        g.ms += ms;
+        g.bytes += e.bytes;
+        g.aes_blocks += e.aes_blocks;
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    prof_pending.clear();
+}
+
 void Ctx::free_perm(ShardedPerm& sp) {
     for (int g = 0; g < 3; g++) {
         release(sp.perm[g]);

@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <deque>
 #include <map>
+#include <string>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -61,6 +62,20 @@ struct ShardedPerm {
     int32_t* inv[3] = {nullptr, nullptr, nullptr};
 };
 
+// Per-launch timing records (enabled on demand): CUDA events around a launch on
+// the stream it runs on, aggregated per kernel class with the launch's
+// algorithmic bytes (distinct share arrays read once + outputs written once)
+// and the AES-256 blocks it computes.
+struct ProfEvent {
+    std::string name;
+    cudaEvent_t a, b;
+    double bytes, aes_blocks;
+};
+struct ProfAgg {
+    unsigned long long launches = 0;
+    double ms = 0, bytes = 0, aes_blocks = 0;
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -73,6 +88,14 @@ struct Ctx {
     std::deque<ShardedPerm> perm_queue;
     size_t perm_queue_n = 0;
     unsigned long long kernels_launched = 0;
+    // device word set by kernels that meet an out-of-range data-dependent index
+    // (they skip the access); checked at the synchronous points.
+    int* d_err = nullptr;
+    void check_device_error();
+    bool profiling = false;
+    std::vector<ProfEvent> prof_pending;
+    std::map<std::string, ProfAgg> prof_agg;
+    void prof_collect();
 
     StreamArg stream_arg(int s, unsigned long long extra_nonces = 0) const {
         StreamArg a;
@@ -99,6 +122,18 @@ struct Scratch {
     }
     Scratch(const Scratch&) = delete;
     Scratch& operator=(const Scratch&) = delete;
+};
+
+struct ProfScope {
+    Ctx* c;
+    cudaStream_t s;
+    ProfEvent ev;
+    bool on;
+    ProfScope(Ctx& ctx, const char* name, double bytes, double aes_blocks = 0,
+              cudaStream_t st = nullptr);
+    ~ProfScope();
+    ProfScope(const ProfScope&) = delete;
+    ProfScope& operator=(const ProfScope&) = delete;
 };
 
 // host-side key derivation (identical to the test shim / restatement)
