@@ -23,6 +23,10 @@
 //  * fy_finalize: turns the accepted offsets into the final permutation in
 //    parallel (see k_fy_final) and writes its inverse.
 #include <algorithm>
+#include <array>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "launch.cuh"
@@ -34,9 +38,21 @@ namespace {
 constexpr uint32_t kTileDraws = 32768;        // draws per tile
 constexpr uint32_t kTileBlocks = kTileDraws / 4;
 constexpr uint32_t kTilesPerRefill = (1u << 20) / kTileDraws;  // 32
-constexpr uint32_t kBitWords = kTileDraws / 32;                // 1024
+constexpr int kGenThreads = 512;
+constexpr int kBlocksPerThread = kTileBlocks / kGenThreads;     // 16 blocks = 64 draws
+constexpr int kMaxLevels = 16;
 constexpr int kScanThreads = 1024;
-constexpr uint32_t kStep = 8192;  // survivors per scan step (8 per thread)
+constexpr uint32_t kStep = 8192;  // entries per scan step (8 per thread)
+constexpr uint32_t kMaxWindowTiles = 1024;
+
+// Level L of a tile keeps, in draw order, the draws with v < n >> 2L (level 0:
+// every draw that can ever be accepted). Entries are (position << 32) | v.
+__host__ __device__ inline uint32_t level_threshold(uint32_t n, int L) { return n >> (2 * L); }
+__host__ inline uint32_t level_capacity(int L) {
+    // twice the largest expected count (mask >= n) plus slack; overflow is
+    // reported as an error, never truncated silently
+    return L == 0 ? kTileDraws : ((kTileDraws >> (2 * L)) * 2 + 256);
+}
 
 struct FyState {
     unsigned long long start_tile;  // absolute tile where the current permutation starts
@@ -46,20 +62,27 @@ struct FyState {
     uint32_t pad;
 };
 
+struct FyLayout {
+    uint32_t nl;               // levels in use
+    uint32_t off[kMaxLevels];  // entry offset of each level list inside a tile slot
+    uint32_t cap[kMaxLevels];
+    uint32_t slot;             // entries per tile slot
+};
+
 struct FyGenArgs {
     StreamArg st[3];  // nonce = chain start nonce + 4 * (window start buffer)
     uint32_t n, mask, tiles;
-    uint32_t* surv;   // [3][tiles][kTileDraws]
-    uint32_t* cnt;    // [3][tiles]
-    uint32_t* tmin;   // [3][tiles]
-    uint32_t* bits;   // [3][tiles][kBitWords]
+    FyLayout lay;
+    unsigned long long* ents;  // [3][tiles][slot]
+    uint32_t* cnt;             // [3][tiles][kMaxLevels]
     const FyState* state;
+    int* err;
 };
 
-__global__ void __launch_bounds__(kAesThreads) k_fy_gen(FyGenArgs a) {
+__global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
     extern __shared__ uint32_t sm[];
     __shared__ uint32_t red[33];
-    __shared__ uint32_t smin, sdone;
+    __shared__ uint32_t sdone;
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const uint32_t total = 3 * a.tiles;
@@ -69,39 +92,47 @@ __global__ void __launch_bounds__(kAesThreads) k_fy_gen(FyGenArgs a) {
         if (threadIdx.x == 0) sdone = *(volatile const uint32_t*)&a.state[g].done;
         __syncthreads();
         if (sdone) continue;
-        const size_t slot = (size_t)g * a.tiles + tile;
-        uint32_t* out = a.surv + slot * kTileDraws;
-        uint32_t* bw = a.bits + slot * kBitWords;
-        if (threadIdx.x == 0) smin = 0xffffffffu;
-        uint32_t base = 0, mymin = 0xffffffffu;
-        for (uint32_t q = 0; q < kTileBlocks / kAesThreads; q++) {
-            const uint32_t lb = q * kAesThreads + threadIdx.x;  // block within tile
-            const uint4 ks =
-                keystream_block(S, a.st[g], (unsigned long long)tile * kTileBlocks + lb);
-            const uint32_t v0 = ks.x & a.mask, v1 = ks.y & a.mask, v2 = ks.z & a.mask,
-                           v3 = ks.w & a.mask;
-            const uint32_t f = (v0 < a.n) | ((v1 < a.n) << 1) | ((v2 < a.n) << 2) | ((v3 < a.n) << 3);
-            const uint32_t c = __popc(f);
-            uint32_t tot;
-            const uint32_t off = block_excl_sum(c, red, tot);
-            uint32_t* o = out + base + off;
-            if (f & 1) { *o++ = v0; mymin = min(mymin, v0); }
-            if (f & 2) { *o++ = v1; mymin = min(mymin, v1); }
-            if (f & 4) { *o++ = v2; mymin = min(mymin, v2); }
-            if (f & 8) { *o++ = v3; mymin = min(mymin, v3); }
-            // survivor bitmap: 8 threads x 4 bits per 32-bit word
-            uint32_t word = f << ((threadIdx.x & 7) * 4);
-            word |= __shfl_xor_sync(0xffffffffu, word, 1);
-            word |= __shfl_xor_sync(0xffffffffu, word, 2);
-            word |= __shfl_xor_sync(0xffffffffu, word, 4);
-            if ((threadIdx.x & 7) == 0) bw[lb >> 3] = word;
-            base += tot;
+        // this thread's 64 consecutive draws of the tile
+        uint32_t v[4 * kBlocksPerThread];
+        const unsigned long long b0 =
+            (unsigned long long)tile * kTileBlocks + (unsigned long long)threadIdx.x * kBlocksPerThread;
+#pragma unroll
+        for (int b = 0; b < kBlocksPerThread; b++) {
+            const uint4 ks = keystream_block(S, a.st[g], b0 + b);
+            v[4 * b + 0] = ks.x & a.mask;
+            v[4 * b + 1] = ks.y & a.mask;
+            v[4 * b + 2] = ks.z & a.mask;
+            v[4 * b + 3] = ks.w & a.mask;
         }
-        atomicMin(&smin, mymin);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            a.cnt[slot] = base;
-            a.tmin[slot] = smin;
+        const size_t slot = (size_t)g * a.tiles + tile;
+        unsigned long long* out = a.ents + slot * a.lay.slot;
+        const uint32_t pos0 = threadIdx.x * 4 * kBlocksPerThread;
+        // two levels per block-wide scan (16-bit fields; totals <= 32768)
+        for (uint32_t L = 0; L < a.lay.nl; L += 2) {
+            const uint32_t t0 = level_threshold(a.n, L);
+            const uint32_t t1 = L + 1 < a.lay.nl ? level_threshold(a.n, L + 1) : 0u;
+            uint32_t c0 = 0, c1 = 0;
+#pragma unroll
+            for (int k = 0; k < 4 * kBlocksPerThread; k++) {
+                c0 += v[k] < t0;
+                c1 += v[k] < t1;
+            }
+            uint32_t tot;
+            const uint32_t pre = block_excl_sum(c0 | (c1 << 16), red, tot);
+            for (int h = 0; h < 2 && L + h < a.lay.nl; h++) {
+                const uint32_t Lh = L + h, th = h ? t1 : t0;
+                uint32_t o = h ? (pre >> 16) : (pre & 0xffffu);
+                const uint32_t tt = h ? (tot >> 16) : (tot & 0xffffu);
+                if (tt > a.lay.cap[Lh]) {
+                    if (threadIdx.x == 0) atomicOr(a.err, 16);
+                    continue;
+                }
+                unsigned long long* ol = out + a.lay.off[Lh];
+#pragma unroll
+                for (int k = 0; k < 4 * kBlocksPerThread; k++)
+                    if (v[k] < th) ol[o++] = ((unsigned long long)(pos0 + k) << 32) | v[k];
+                if (threadIdx.x == 0) a.cnt[slot * kMaxLevels + Lh] = tt;
+            }
         }
         __syncthreads();
     }
@@ -110,197 +141,258 @@ __global__ void __launch_bounds__(kAesThreads) k_fy_gen(FyGenArgs a) {
 struct FyScanArgs {
     uint32_t n, count, tiles;
     unsigned long long win_tile0;  // absolute index of the window's first tile
-    const uint32_t* surv;
+    FyLayout lay;
+    const unsigned long long* ents;
     const uint32_t* cnt;
-    const uint32_t* tmin;
-    const uint32_t* bits;
-    FyState* state;        // [3]
-    uint32_t* acc;         // [3][count][n] accepted offsets v_i (swap with i + v_i)
-    uint32_t* refills;     // [3][count] getNext buffers used
+    FyState* state;     // [3]
+    uint32_t* acc;      // [3][count][n] accepted offsets v_i (swap with i + v_i)
+    uint32_t* refills;  // [3][count] getNext buffers used
+    unsigned long long* stats;  // optional [3][8] diagnostic counters (ORQ_FY_STATS)
 };
 
-// Position of the q-th set bit (0-based) of a tile bitmap.
-__device__ uint32_t nth_set_bit(const uint32_t* bw, uint32_t q, uint32_t* red) {
-    __shared__ uint32_t pos;
-    const uint32_t w = bw[threadIdx.x];  // kBitWords == blockDim.x
-    const uint32_t c = __popc(w);
-    uint32_t tot;
-    const uint32_t pre = block_excl_sum(c, red, tot);
-    if (q >= pre && q < pre + c) {
-        uint32_t r = q - pre, x = w;
-        for (uint32_t k = 0; k < r; k++) x &= x - 1;
-        pos = threadIdx.x * 32 + (__ffs(x) - 1);
+// first index in P[0..m] with P[idx] > e, minus one (P non-decreasing, P[0] = 0)
+__device__ __forceinline__ uint32_t tile_of(const uint32_t* P, uint32_t m, uint32_t e) {
+    uint32_t lo = 0, hi = m;  // invariant: P[lo] <= e, answer in [lo, hi)
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (P[mid] <= e) lo = mid;
+        else hi = mid;
     }
-    __syncthreads();
-    const uint32_t p = pos;
-    __syncthreads();
-    return p;
+    return lo;
+}
+
+// entries per step at level L: the index bound makes ~S^2 / (2 n/4^L)
+// entries uncertain, kept near 128 per step
+__device__ __forceinline__ uint32_t step_entries(uint32_t n, uint32_t L) {
+    const unsigned long long t = level_threshold(n, L);
+    uint32_t s = kStep;
+    while (s > 256 && (unsigned long long)s * s > 256ull * t) s >>= 1;
+    return s;
+}
+
+// entries [e0, e0+cs) of the window's level lists (8 per thread)
+__device__ __forceinline__ void load_step(const uint32_t* P, uint32_t tiles,
+                                          const unsigned long long* E, uint32_t slot, uint32_t off,
+                                          uint32_t e0, uint32_t cs, uint32_t v[8], uint32_t et[8],
+                                          uint32_t ep[8]) {
+    const uint32_t my0 = e0 + threadIdx.x * 8;
+    uint32_t t = my0 < e0 + cs ? tile_of(P, tiles, my0) : 0u;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        const uint32_t q = threadIdx.x * 8 + u;
+        v[u] = 0xffffffffu;
+        et[u] = 0;
+        ep[u] = 0;
+        if (q < cs) {
+            while (P[t + 1] <= e0 + q) t++;
+            const unsigned long long ent = E[(size_t)t * slot + off + (e0 + q - P[t])];
+            v[u] = (uint32_t)ent;
+            ep[u] = (uint32_t)(ent >> 32);
+            et[u] = t;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
     __shared__ uint32_t red[33];
-    __shared__ uint32_t s_i, s_m, s_done, s_last_q, s_nunc;
-    __shared__ unsigned long long s_start;
-    __shared__ uint32_t unc_v[kStep / 8];   // uncertain survivors of a step (capped)
-    __shared__ uint32_t unc_cp[kStep / 8];
+    __shared__ uint32_t P[kMaxWindowTiles + 1];  // prefix of level-L counts over the window
+    __shared__ uint32_t s_last_tile, s_last_pos, s_uacc_total, s_seq;
+    __shared__ uint32_t unc_v[kStep / 8];      // uncertain entries of a step, in order
+    __shared__ uint32_t unc_cp[kStep / 8];     // certain accepts before each
+    __shared__ uint32_t unc_pre[kStep / 8 + 1];  // uncertain accepted before each (exclusive)
     __shared__ uint8_t unc_ok[kStep / 8];
     const uint32_t g = blockIdx.x;
     const uint32_t n = a.n;
-    if (threadIdx.x == 0) {
-        s_i = a.state[g].i;
-        s_m = a.state[g].m;
-        s_done = a.state[g].done;
-        s_start = a.state[g].start_tile;
-    }
-    __syncthreads();
-    for (uint32_t tile = 0; tile < a.tiles; tile++) {
-        if (s_done) break;
-        const unsigned long long abs_tile = a.win_tile0 + tile;
-        if (abs_tile < s_start) continue;
-        const size_t slot = (size_t)g * a.tiles + tile;
-        const uint32_t c = a.cnt[slot];
-        if (a.tmin[slot] > n - 1 - s_i) continue;
-        const uint32_t* sv = a.surv + slot * kTileDraws;
-        bool finished = false;
-        for (uint32_t sb = 0; sb < c && !finished; sb += kStep) {
-            const uint32_t i0 = s_i;
-            const long long T = (long long)n - 1 - i0;
-            uint32_t v[8];
-            uint32_t cand = 0;  // not certainly rejected: v <= T
-#pragma unroll
-            for (int u = 0; u < 8; u++) {
-                const uint32_t q = threadIdx.x * 8 + u;  // index within the step
-                v[u] = (sb + q < c) ? sv[sb + q] : 0xffffffffu;
-                if (v[u] != 0xffffffffu && (long long)v[u] <= T) cand |= 1u << u;
+    const uint32_t tiles = a.tiles;
+    // scan state, identical in every thread
+    uint32_t i = a.state[g].i, m = a.state[g].m, done = a.state[g].done;
+    unsigned long long start = a.state[g].start_tile;
+    uint32_t tau = 0, ix = 0, L = 0, Lp = 0xffffffffu;
+    const unsigned long long* E = a.ents + (size_t)g * tiles * a.lay.slot;
+    const uint32_t* C = a.cnt + (size_t)g * tiles * kMaxLevels;
+    unsigned long long st_steps = 0, st_unc_steps = 0, st_seq = 0, st_ent = 0, st_unc = 0,
+                       st_cyc_load = 0, st_cyc_unc = 0, st_cyc_all = 0;
+    const unsigned long long t_begin = clock64();
+    for (int guard = 0; guard < (1 << 24) && !done; guard++) {
+        // never look before the current permutation's first tile
+        if (a.win_tile0 + tau < start) {
+            const unsigned long long d = start - a.win_tile0;
+            tau = d > tiles ? tiles : (uint32_t)d;
+            ix = 0;
+        }
+        if (tau >= tiles) break;
+        const uint32_t T = n - 1 - i;
+        // sparsest level still holding every candidate v <= T
+        uint32_t want = 0;
+        while (want + 1 < a.lay.nl && T < level_threshold(n, want + 1)) want++;
+        if (ix == 0) L = want;  // levels change only at tile starts
+        if (L != Lp) {
+            uint32_t tot;
+            const uint32_t c = threadIdx.x < tiles ? C[threadIdx.x * kMaxLevels + L] : 0u;
+            const uint32_t pre = block_excl_sum(c, red, tot);
+            if (threadIdx.x < tiles) P[threadIdx.x] = pre;
+            if (threadIdx.x == 0) P[tiles] = tot;
+            __syncthreads();
+            Lp = L;
+        }
+        const uint32_t e0 = P[tau] + ix;
+        const uint32_t eend = (ix != 0 && want != L) ? P[tau + 1] : P[tiles];
+        if (e0 >= eend) {
+            if (eend == P[tiles]) tau = tiles;
+            else {
+                tau++;
+                ix = 0;
             }
-            // Only candidates can advance i, so at candidate u at most
-            // (candidates before u) acceptances have happened: v <= T - that
-            // makes u certainly accepted.
-            uint32_t tot_cand;
-            const uint32_t cpre_cand = block_excl_sum(__popc(cand), red, tot_cand);
-            uint32_t certain = 0, unc = 0;
-            {
-                uint32_t before = cpre_cand;
+            continue;
+        }
+        const uint32_t cs = min(step_entries(n, L), eend - e0);
+        const unsigned long long t_l0 = clock64();
+        uint32_t v[8], etile[8], epos[8];
+        load_step(P, tiles, E, a.lay.slot, a.lay.off[L], e0, cs, v, etile, epos);
+        uint32_t certain = 0, unc = 0;
 #pragma unroll
-                for (int u = 0; u < 8; u++)
-                    if ((cand >> u) & 1u) {
-                        if ((long long)v[u] + before <= T) certain |= 1u << u;
-                        else unc |= 1u << u;
-                        before++;
-                    }
+        for (int u = 0; u < 8; u++) {
+            const uint32_t q = threadIdx.x * 8 + u;  // index within the step
+            if (q < cs) {
+                // at most q acceptances precede entry q in this step
+                if ((unsigned long long)v[u] + q <= T) certain |= 1u << u;
+                else if (v[u] <= T) unc |= 1u << u;
             }
-            uint32_t accept = certain;
-            const int any_unc = __syncthreads_or(unc != 0);
-            if (any_unc) {
-                // order the uncertain survivors and decide them one by one
-                uint32_t tot_c;
-                const uint32_t cpre = block_excl_sum(__popc(certain), red, tot_c);
-                uint32_t tot_u;
-                const uint32_t upre = block_excl_sum(__popc(unc), red, tot_u);
-                const uint32_t cap = kStep / 8;
-                {
-                    uint32_t k = upre, cc = cpre;
-                    for (int u = 0; u < 8; u++) {
-                        if ((unc >> u) & 1u) {
-                            if (k < cap) {
-                                unc_v[k] = v[u];
-                                unc_cp[k] = cc;
-                            }
-                            k++;
-                        }
-                        if ((certain >> u) & 1u) cc++;
+        }
+        uint32_t tot;
+        const uint32_t pre = block_excl_sum(__popc(certain) | (__popc(unc) << 16), red, tot);
+        const uint32_t cpre = pre & 0xffffu, upre = pre >> 16;
+        const uint32_t tot_c = tot & 0xffffu, tot_u = tot >> 16;
+        st_steps++;
+        st_ent += cs;
+        st_cyc_load += clock64() - t_l0;
+        uint32_t accept = certain, tot_a = tot_c;
+        uint32_t rank_base = cpre;  // accepted entries of earlier threads
+        if (tot_u) {
+            const unsigned long long t_u0 = clock64();
+            st_unc_steps++;
+            st_unc += tot_u;
+            const uint32_t cap = kStep / 8;
+            if (tot_u <= cap) {
+                uint32_t k = upre, cc = cpre;
+                for (int u = 0; u < 8; u++) {
+                    if ((unc >> u) & 1u) {
+                        unc_v[k] = v[u];
+                        unc_cp[k] = cc;
+                        k++;
                     }
+                    if ((certain >> u) & 1u) cc++;
                 }
                 __syncthreads();
                 if (threadIdx.x == 0) {
-                    if (tot_u > cap) {
-                        s_nunc = 0xffffffffu;  // too many: decide the whole step in order
-                    } else {
-                        uint32_t uacc = 0;
-                        for (uint32_t k = 0; k < tot_u; k++) {
-                            const unsigned long long iat = (unsigned long long)i0 + unc_cp[k] + uacc;
-                            const bool ok = iat < n && (unsigned long long)unc_v[k] <=
-                                                           (unsigned long long)n - 1 - iat;
-                            unc_ok[k] = ok;
-                            uacc += ok;
-                        }
-                        s_nunc = tot_u;
+                    uint32_t uacc = 0;
+                    for (uint32_t k2 = 0; k2 < tot_u; k2++) {
+                        unc_pre[k2] = uacc;
+                        const unsigned long long iat = (unsigned long long)i + unc_cp[k2] + uacc;
+                        const bool ok = iat < n && (unsigned long long)unc_v[k2] <= (unsigned long long)n - 1 - iat;
+                        unc_ok[k2] = ok;
+                        uacc += ok;
                     }
+                    unc_pre[tot_u] = uacc;
+                    s_uacc_total = uacc;
                 }
                 __syncthreads();
-                if (s_nunc == 0xffffffffu) {
-                    __shared__ uint32_t seq_acc[kStep / 32];
-                    __shared__ uint32_t seq_v[kStep];
-                    if (threadIdx.x < kStep / 32) seq_acc[threadIdx.x] = 0;
+                uint32_t k2 = upre;
+                rank_base = cpre + unc_pre[upre];
+                for (int u = 0; u < 8; u++)
+                    if ((unc >> u) & 1u) {
+                        if (unc_ok[k2]) accept |= 1u << u;
+                        k2++;
+                    }
+                tot_a = tot_c + s_uacc_total;
+            } else {
+                // too many to list: decide the whole step in order
+                __shared__ uint32_t seq_acc[kStep / 32];
+                extern __shared__ uint32_t seq_v[];  // kStep words of dynamic shared memory
+                if (threadIdx.x < kStep / 32) seq_acc[threadIdx.x] = 0;
 #pragma unroll
-                    for (int u = 0; u < 8; u++) seq_v[threadIdx.x * 8 + u] = v[u];
-                    __syncthreads();
-                    if (threadIdx.x == 0) {
-                        uint32_t ii = i0;
-                        const uint32_t lim = (c - sb) < kStep ? (c - sb) : kStep;
-                        for (uint32_t q = 0; q < lim && ii < n; q++) {
-                            const uint32_t vv = seq_v[q];
-                            if (vv <= n - 1 - ii) {
-                                seq_acc[q >> 5] |= 1u << (q & 31);
-                                ii++;
-                            }
+                for (int u = 0; u < 8; u++) seq_v[threadIdx.x * 8 + u] = v[u];
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    uint32_t ii = i;
+                    for (uint32_t q = 0; q < cs && ii < n; q++)
+                        if (seq_v[q] <= n - 1 - ii) {
+                            seq_acc[q >> 5] |= 1u << (q & 31);
+                            ii++;
                         }
-                    }
-                    __syncthreads();
-                    accept = 0;
-                    for (int u = 0; u < 8; u++) {
-                        const uint32_t q = threadIdx.x * 8 + u;
-                        if ((seq_acc[q >> 5] >> (q & 31)) & 1u) accept |= 1u << u;
-                    }
-                } else {
-                    uint32_t k = upre;
-                    for (int u = 0; u < 8; u++)
-                        if ((unc >> u) & 1u) {
-                            if (unc_ok[k]) accept |= 1u << u;
-                            k++;
-                        }
+                    s_seq = ii - i;
                 }
+                __syncthreads();
+                accept = 0;
+                for (int u = 0; u < 8; u++) {
+                    const uint32_t q = threadIdx.x * 8 + u;
+                    if ((seq_acc[q >> 5] >> (q & 31)) & 1u) accept |= 1u << u;
+                }
+                uint32_t t2;
+                rank_base = block_excl_sum(__popc(accept), red, t2);
+                tot_a = t2;
+                st_seq++;
             }
-            uint32_t tot_a;
-            const uint32_t apre = block_excl_sum(__popc(accept), red, tot_a);
-            const uint32_t need = n - i0;
-            uint32_t* acc = a.acc + ((size_t)g * a.count + s_m) * (size_t)n;
-            uint32_t r = apre;
-            for (int u = 0; u < 8; u++) {
+            st_cyc_unc += clock64() - t_u0;
+        }
+        const uint32_t need = n - i;
+        uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
+        {
+            uint32_t r = rank_base;
+            for (int u = 0; u < 8; u++)
                 if ((accept >> u) & 1u) {
                     if (r < need) {
-                        acc[i0 + r] = v[u];
-                        if (r == need - 1) s_last_q = sb + threadIdx.x * 8 + u;
+                        acc[i + r] = v[u];
+                        if (r == need - 1) {
+                            s_last_tile = etile[u];
+                            s_last_pos = epos[u];
+                        }
                     }
                     r++;
                 }
-            }
+        }
+        if (tot_a >= need) {
             __syncthreads();
-            if (tot_a >= need) {
-                // permutation complete: locate its last draw, count the buffers
-                const uint32_t p = nth_set_bit(a.bits + slot * kBitWords, s_last_q, red);
-                if (threadIdx.x == 0) {
-                    const unsigned long long kend =
-                        (abs_tile - s_start) * (unsigned long long)kTileDraws + p;
-                    const unsigned long long R = 1 + ((kend + 1) >> 20);
-                    a.refills[(size_t)g * a.count + s_m] = (uint32_t)R;
-                    s_start = (s_start / kTilesPerRefill + R) * kTilesPerRefill;
-                    s_m = s_m + 1;
-                    s_i = 0;
-                    if (s_m >= a.count) s_done = 1;
-                }
-                finished = true;
-            } else if (threadIdx.x == 0) {
-                s_i = i0 + tot_a;
-            }
+            // permutation complete: count the getNext buffers it used
+            const unsigned long long kend =
+                (a.win_tile0 + s_last_tile - start) * (unsigned long long)kTileDraws + s_last_pos;
+            const unsigned long long R = 1 + ((kend + 1) >> 20);
+            if (threadIdx.x == 0) a.refills[(size_t)g * a.count + m] = (uint32_t)R;
+            start = (start / kTilesPerRefill + R) * kTilesPerRefill;
+            m++;
+            i = 0;
+            ix = 0;
+            if (m >= a.count) done = 1;
             __syncthreads();
+        } else {
+            i += tot_a;
+            const uint32_t enew = e0 + cs;
+            if (enew >= P[tiles]) {
+                tau = tiles;
+                ix = 0;
+            } else {
+                tau = tile_of(P, tiles, enew);
+                ix = enew - P[tau];
+            }
         }
     }
     if (threadIdx.x == 0) {
-        a.state[g].i = s_i;
-        a.state[g].m = s_m;
-        a.state[g].done = s_done;
-        a.state[g].start_tile = s_start;
+        a.state[g].i = i;
+        a.state[g].m = m;
+        a.state[g].done = done;
+        a.state[g].start_tile = start;
+        if (a.stats) {
+            st_cyc_all = clock64() - t_begin;
+            unsigned long long* st = a.stats + g * 8;
+            st[0] += st_steps;
+            st[1] += st_unc_steps;
+            st[2] += st_seq;
+            st[3] += st_ent;
+            st[4] += st_unc;
+            st[5] += st_cyc_load;
+            st[6] += st_cyc_unc;
+            st[7] += st_cyc_all;
+        }
     }
 }
 
@@ -474,21 +566,39 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     for (size_t k = 1; k <= std::min<size_t>(n, 1 << 16); k++) H += 1.0 / k;
     if (n > (1u << 16)) H += std::log((double)n / (1 << 16));
     const double per_perm = M * H / (double)(1 << 20) + 1.0;  // expected buffers
-    uint32_t W = (uint32_t)std::clamp(per_perm * count / 8.0, 2.0, 32.0);
+    uint32_t W = (uint32_t)std::clamp(per_perm * count / 8.0, 2.0, (double)(kMaxWindowTiles / kTilesPerRefill));
     const uint32_t tiles = W * kTilesPerRefill;
 
-    const size_t surv_b = (size_t)3 * tiles * kTileDraws * 4;
-    const size_t bits_b = (size_t)3 * tiles * kBitWords * 4;
-    const size_t small_b = (size_t)3 * tiles * 4;
-    Scratch surv0(c, surv_b), surv1(c, surv_b), bits0(c, bits_b), bits1(c, bits_b);
-    Scratch cnt0(c, small_b), cnt1(c, small_b), min0(c, small_b), min1(c, small_b);
+    FyLayout lay{};
+    {
+        uint32_t nl = 0;
+        while (nl < (uint32_t)kMaxLevels && level_threshold((uint32_t)n, nl) >= 1) nl++;
+        lay.nl = nl;
+        uint32_t o = 0;
+        for (uint32_t L = 0; L < nl; L++) {
+            lay.off[L] = o;
+            lay.cap[L] = level_capacity(L);
+            o += lay.cap[L];
+        }
+        lay.slot = o;
+    }
+    const size_t ents_b = (size_t)3 * tiles * lay.slot * 8;
+    const size_t cnt_b = (size_t)3 * tiles * kMaxLevels * 4;
+    Scratch ents0(c, ents_b), ents1(c, ents_b), cnt0(c, cnt_b), cnt1(c, cnt_b);
     Scratch state(c, 3 * sizeof(FyState));
     Scratch acc(c, (size_t)3 * count * n * 4);
     Scratch refills(c, (size_t)3 * count * 4);
     ORQ_CUDA_CHECK(cudaMemsetAsync(state.p, 0, 3 * sizeof(FyState), c.stream));
+    const bool want_stats = std::getenv("ORQ_FY_STATS") != nullptr;
+    const auto t_start = std::chrono::steady_clock::now();
+    Scratch stats(c, 3 * 8 * 8);
+    if (want_stats) ORQ_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 3 * 8 * 8, c.stream));
 
-    cudaStream_t gs;
+    // generator and scanner run on private non-blocking streams so they overlap
+    // whatever the caller's stream is (the legacy default stream included)
+    cudaStream_t gs, ss;
     ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
+    ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking));
     cudaEvent_t ev_start, gen_done[2], scan_done[2];
     ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
     for (int k = 0; k < 2; k++) {
@@ -497,19 +607,29 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     }
     ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
     ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
+    ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss, ev_start, 0));
 
     FyState* hstate = nullptr;
     ORQ_CUDA_CHECK(cudaMallocHost(&hstate, 3 * sizeof(FyState)));
     prep_aes_kernel(k_fy_gen);
+    ORQ_CUDA_CHECK(cudaFuncSetAttribute(k_fy_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, kStep * 4));
 
     const unsigned gen_grid = (unsigned)std::max(1, c.num_sms - 3);
-    uint32_t* survp[2] = {surv0.as<uint32_t>(), surv1.as<uint32_t>()};
-    uint32_t* bitsp[2] = {bits0.as<uint32_t>(), bits1.as<uint32_t>()};
+    unsigned long long* entsp[2] = {ents0.as<unsigned long long>(), ents1.as<unsigned long long>()};
     uint32_t* cntp[2] = {cnt0.as<uint32_t>(), cnt1.as<uint32_t>()};
-    uint32_t* minp[2] = {min0.as<uint32_t>(), min1.as<uint32_t>()};
 
     const unsigned long long limit_windows =
         (unsigned long long)(count * (per_perm * 4.0 + 64.0) / W + 16);
+    std::vector<cudaEvent_t> tl;  // stats mode: [gen start, gen end, scan start, scan end] per window
+    auto tl_event = [&](cudaStream_t st) -> int {
+        if (!want_stats) return -1;
+        cudaEvent_t e;
+        ORQ_CUDA_CHECK(cudaEventCreate(&e));
+        ORQ_CUDA_CHECK(cudaEventRecord(e, st));
+        tl.push_back(e);
+        return (int)tl.size() - 1;
+    };
+    std::vector<std::array<int, 4>> tl_idx;
     auto launch_gen = [&](unsigned long long w) {
         const int b = (int)(w & 1);
         // buffer b was last read by the scanner of window w-2
@@ -519,15 +639,18 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         ga.n = (uint32_t)n;
         ga.mask = mask;
         ga.tiles = tiles;
-        ga.surv = survp[b];
+        ga.lay = lay;
+        ga.ents = entsp[b];
         ga.cnt = cntp[b];
-        ga.tmin = minp[b];
-        ga.bits = bitsp[b];
         ga.state = state.as<FyState>();
+        ga.err = c.d_err;
+        if (tl_idx.size() <= w) tl_idx.resize(w + 1, {-1, -1, -1, -1});
+        tl_idx[w][0] = tl_event(gs);
         {
             ProfScope ps(c, "fy_gen", 0.0, 3.0 * tiles * kTileBlocks, gs);
-            k_fy_gen<<<gen_grid, kAesThreads, kAesSmemBytes, gs>>>(ga);
+            k_fy_gen<<<gen_grid, kGenThreads, kAesSmemBytes, gs>>>(ga);
         }
+        tl_idx[w][1] = tl_event(gs);
         ORQ_CUDA_CHECK(cudaGetLastError());
         ORQ_CUDA_CHECK(cudaEventRecord(gen_done[b], gs));
         c.kernels_launched++;
@@ -539,36 +662,39 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         if (w > limit_windows)
             throw std::runtime_error("permutation generation did not converge");
         const int b = (int)(w & 1);
-        // scanner for window w
-        ORQ_CUDA_CHECK(cudaStreamWaitEvent(c.stream, gen_done[b], 0));
+        ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss, gen_done[b], 0));
         FyScanArgs sa;
         sa.n = (uint32_t)n;
         sa.count = (uint32_t)count;
         sa.tiles = tiles;
         sa.win_tile0 = (unsigned long long)w * tiles;
-        sa.surv = survp[b];
+        sa.lay = lay;
+        sa.ents = entsp[b];
         sa.cnt = cntp[b];
-        sa.tmin = minp[b];
-        sa.bits = bitsp[b];
         sa.state = state.as<FyState>();
         sa.acc = acc.as<uint32_t>();
         sa.refills = refills.as<uint32_t>();
+        sa.stats = want_stats ? stats.as<unsigned long long>() : nullptr;
+        if (tl_idx.size() <= w) tl_idx.resize(w + 1, {-1, -1, -1, -1});
+        tl_idx[w][2] = tl_event(ss);
         {
-            ProfScope ps(c, "fy_scan", 0.0);
-            k_fy_scan<<<3, kScanThreads, 0, c.stream>>>(sa);
+            ProfScope ps(c, "fy_scan", 0.0, 0.0, ss);
+            k_fy_scan<<<3, kScanThreads, kStep * 4, ss>>>(sa);
         }
+        tl_idx[w][3] = tl_event(ss);
         ORQ_CUDA_CHECK(cudaGetLastError());
-        ORQ_CUDA_CHECK(cudaEventRecord(scan_done[b], c.stream));
+        ORQ_CUDA_CHECK(cudaEventRecord(scan_done[b], ss));
         c.kernels_launched++;
         ORQ_CUDA_CHECK(cudaMemcpyAsync(hstate, state.p, 3 * sizeof(FyState),
-                                       cudaMemcpyDeviceToHost, c.stream));
+                                       cudaMemcpyDeviceToHost, ss));
         // generate the next window while this one is scanned
         launch_gen(w + 1);
-        ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(ss));
         all_done = hstate[0].done && hstate[1].done && hstate[2].done;
         w++;
     }
     ORQ_CUDA_CHECK(cudaStreamSynchronize(gs));
+    ORQ_CUDA_CHECK(cudaStreamSynchronize(ss));
 
     // nonce accounting: 4 nonces per getNext buffer
     std::vector<uint32_t> hr(3 * count);
@@ -579,6 +705,27 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         unsigned long long used = 0;
         for (size_t m = 0; m < count; m++) used += hr[g * count + m];
         c.nonce[G01 + g] += 4ull * used;
+    }
+    if (want_stats) {
+        std::fprintf(stderr, "[fy] windows %llu of %u buffers, %.3f ms\n", w, W,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+        for (size_t k = 0; k < tl_idx.size() && k < 6; k++) {
+            float g0 = 0, g1 = 0, s0 = 0, s1 = 0;
+            if (tl_idx[k][0] >= 0) cudaEventElapsedTime(&g0, tl[0], tl[tl_idx[k][0]]);
+            if (tl_idx[k][1] >= 0) cudaEventElapsedTime(&g1, tl[0], tl[tl_idx[k][1]]);
+            if (tl_idx[k][2] >= 0) cudaEventElapsedTime(&s0, tl[0], tl[tl_idx[k][2]]);
+            if (tl_idx[k][3] >= 0) cudaEventElapsedTime(&s1, tl[0], tl[tl_idx[k][3]]);
+            std::fprintf(stderr, "[fy] window %zu: gen %.3f-%.3f scan %.3f-%.3f ms\n", k, g0, g1, s0, s1);
+        }
+        for (auto e : tl) cudaEventDestroy(e);
+        unsigned long long hs[24];
+        ORQ_CUDA_CHECK(cudaMemcpy(hs, stats.p, sizeof(hs), cudaMemcpyDeviceToHost));
+        for (int g = 0; g < 3; g++)
+            std::fprintf(stderr,
+                         "[fy] n=%zu perms=%zu windows=%llu group %d: steps %llu unc_steps %llu seq %llu "
+                         "entries %llu unc %llu cyc_load %llu cyc_unc %llu cyc_all %llu\n",
+                         n, count, w, g, hs[g * 8], hs[g * 8 + 1], hs[g * 8 + 2], hs[g * 8 + 3],
+                         hs[g * 8 + 4], hs[g * 8 + 5], hs[g * 8 + 6], hs[g * 8 + 7]);
     }
 
     // finalize, a few permutations at a time to bound scratch
@@ -630,6 +777,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         cudaEventDestroy(scan_done[k]);
     }
     cudaStreamDestroy(gs);
+    cudaStreamDestroy(ss);
 }
 
 // PermutationManager::reserve (permutation_manager.h:102-181): keep a queue of
