@@ -123,6 +123,10 @@ int orqcu_zero_share(orqcu_runtime* rt, int arith, int width, size_t n, void* co
 int orqcu_reshare(orqcu_runtime* rt, int arith, int width, size_t n, int group,
                   void* const shares[3]);
 
+/* SharedVector::prefix_sum (shared_vector.h:249): in-place inclusive scan of
+ * each share array mod 2^(8*width); width 4 or 8. Local (no randomness). */
+int orqcu_prefix_sum_a(orqcu_runtime* rt, int width, size_t n, void* const shares[3]);
+
 /* PermutationManager::reserve (permutation_manager.h:102-181): generate
  * `count` sharded permutations of size n ahead of use. Synchronous. */
 int orqcu_reserve_permutations(orqcu_runtime* rt, size_t n, size_t count);

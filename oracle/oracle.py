@@ -156,3 +156,7 @@ class Oracle:
         w = s[0].dtype.itemsize
         self.lib.oro_shuffle(ctypes.byref(self.ctx), int(arith), w, ctypes.c_size_t(len(s[0])),
                              self._ptrs(s))
+
+    def prefix_sum(self, s):
+        w = s[0].dtype.itemsize
+        self.lib.oro_prefix_sum(w, ctypes.c_size_t(len(s[0])), self._ptrs(s))

@@ -683,3 +683,15 @@ void oro_shuffle(oro_ctx* c, int arith, int w, size_t n, void* s[3]) {
     apply_sharded(c, arith, w, n, s, &sp);
     sperm_free(&sp);
 }
+
+/* SharedVector::prefix_sum (containers/shared_vector.h:249): inclusive scan
+ * of each share array, mod 2^(8w). */
+void oro_prefix_sum(int w, size_t n, void* s[3]) {
+    for (int j = 0; j < 3; j++) {
+        u128 acc = 0;
+        for (size_t i = 0; i < n; i++) {
+            acc += ld(s[j], i, w);
+            st(s[j], i, w, acc);
+        }
+    }
+}

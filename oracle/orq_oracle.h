@@ -86,6 +86,7 @@ void oro_zero_share(oro_ctx* c, int arith, int w, size_t n, void* r[3]);
  * Returns the number of u32 draws consumed. */
 uint64_t oro_gen_perm(oro_ctx* c, int stream, int32_t* perm, size_t n);
 void oro_shuffle(oro_ctx* c, int arith, int w, size_t n, void* s[3]);
+void oro_prefix_sum(int w, size_t n, void* s[3]);
 
 /* radix_sort(v, ASC|DESC, bits) on an int32/int64 B-shared key followed by
  * oblivious_apply_elementwise_perm of each A-shared payload (64-bit) with the

@@ -300,6 +300,12 @@ class ASharedVector(SharedVector):
         return self._ibin(o, self.rt.lib.orqcu_sub_a)
 
 
+def prefix_sum(v: ASharedVector):
+    """SharedVector::prefix_sum (shared_vector.h:249): in-place inclusive scan."""
+    rt = v.rt
+    _check(rt.lib.orqcu_prefix_sum_a(rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares)))
+
+
 class ElementwisePermutation(ASharedVector):
     """A-shared int32 destination indices (core/containers/permutation.h)."""
 

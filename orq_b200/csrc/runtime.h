@@ -166,6 +166,11 @@ void op_apply_elementwise(Ctx& c, bool x_arith, int xw, size_t n, Sh3 x, CSh3 pe
 void op_scatter(Ctx& c, int w, size_t n, CSh3 src, Sh3 dst, const int32_t* sigma);
 void op_shuffle(Ctx& c, bool arith, int w, size_t n, Sh3 s);
 
+// ---- prefix sum of arithmetic shares (scan.cu) ----
+uint32_t prefix_sum_tiles(size_t n);
+void op_prefix_sum_into(Ctx& c, int w, size_t n, Sh3 s, void* tsum);
+void op_prefix_sum(Ctx& c, int w, size_t n, Sh3 s);
+
 // ---- sorting (radix.cu) ----
 void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out /*int32*/);
 

@@ -152,3 +152,21 @@ def test_radix_full_size_properties(orq):
     assert same(out["open_pay2"][0], p2[order])
     perm = out["perm"].astype(np.uint64).sum(0) & np.uint64(0xFFFFFFFF)
     assert same(np.sort(perm), np.arange(n, dtype=np.uint64))
+
+
+@pytest.mark.parametrize("w", [4, 8])
+@pytest.mark.parametrize("n", [1, 4095, 4096, 4097, (1 << 20) + 3])
+def test_prefix_sum_matches_restatement(orq, w, n):
+    from oracle.oracle import Oracle
+
+    rt = orq.Runtime(seed=8)
+    o = Oracle(8)
+    dt = {4: np.uint32, 8: np.uint64}[w]
+    data = np.arange(n, dtype=dt) * dt(2654435761)
+    v = rt.secret_share_a(data, 0)
+    s = o.secret_share(data, True, 0)
+    orq.prefix_sum(v)
+    o.prefix_sum(s)
+    assert same(v.shares.cpu().numpy().view(dt), np.stack(s))
+    with np.errstate(over="ignore"):
+        assert same(v.open().cpu().numpy().view(dt), np.cumsum(data, dtype=dt))
