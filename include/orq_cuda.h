@@ -126,6 +126,18 @@ int orqcu_reshare(orqcu_runtime* rt, int arith, int width, size_t n, int group,
 /* SharedVector::prefix_sum (shared_vector.h:249): in-place inclusive scan of
  * each share array mod 2^(8*width); width 4 or 8. Local (no randomness). */
 int orqcu_prefix_sum_a(orqcu_runtime* rt, int width, size_t n, void* const shares[3]);
+/* The same prefix sum for callers that cannot allocate device memory when they
+ * call: a host program that has already reserved the GPU's memory for its own
+ * pool, or a service loop that cannot afford cudaMalloc's device-wide
+ * synchronisation while other work runs. It has no counterpart in the
+ * reference. Its scratch (the tile sums) is a fixed 384 KiB array in the
+ * library, held on every GPU that loads it until the process exits, so n is
+ * limited to 2^26 elements (larger n returns ORQCU_EINVAL and touches nothing).
+ * The first call on a device looks up the array's device address, so make
+ * that first call before any stream capture. All calls share the array: calls
+ * that overlap on the GPU (on any streams) race and must be serialised. No
+ * cudaMalloc, cudaFree or other allocating routine is called. */
+int orqcu_prefix_sum_a_noalloc(orqcu_runtime* rt, int width, size_t n, void* const shares[3]);
 
 /* PermutationManager::reserve (permutation_manager.h:102-181): generate
  * `count` sharded permutations of size n ahead of use. Synchronous. */

@@ -296,6 +296,16 @@ int orqcu_prefix_sum_a(orqcu_runtime* rt, int width, size_t n, void* const share
     });
 }
 
+int orqcu_prefix_sum_a_noalloc(orqcu_runtime* rt, int width, size_t n, void* const shares[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "prefix sum supports 4 and 8-byte shares");
+        need_sh((const void* const*)shares, n, "null shares");
+        ORQ_CUDA_CHECK(cudaSetDevice(rt->ctx.device));
+        orqcu::op_prefix_sum_noalloc(rt->ctx, width, n, m3(shares));
+    });
+}
+
 int orqcu_reserve_permutations(orqcu_runtime* rt, size_t n, size_t count) {
     return guard([&] {
         need_rt(rt);

@@ -170,6 +170,7 @@ void op_shuffle(Ctx& c, bool arith, int w, size_t n, Sh3 s);
 uint32_t prefix_sum_tiles(size_t n);
 void op_prefix_sum_into(Ctx& c, int w, size_t n, Sh3 s, void* tsum);
 void op_prefix_sum(Ctx& c, int w, size_t n, Sh3 s);
+void op_prefix_sum_noalloc(Ctx& c, int w, size_t n, Sh3 s);
 
 // ---- sorting (radix.cu) ----
 void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out /*int32*/);

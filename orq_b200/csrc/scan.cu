@@ -5,6 +5,9 @@
 // in loopback that is an inclusive scan mod 2^(8W) of each distinct share array
 // S[0], S[1], S[2]. Reduce-then-scan over 4096-element tiles: per-tile sums,
 // a scan of the tile sums per share, then each tile rescanned with its offset.
+#include <memory>
+#include <mutex>
+
 #include "launch.cuh"
 
 namespace orqcu {
@@ -104,14 +107,15 @@ __global__ void __launch_bounds__(kThreads) k_down(ScanArgs3<T> a) {
 }
 
 template <typename T>
-void run_scan(Ctx& c, size_t n, Sh3 s, T* tsum, uint32_t tiles) {
+void run_scan(Ctx& c, size_t n, Sh3 s, T* tsum, uint32_t tiles, bool profile = true) {
     ScanArgs3<T> a;
     for (int j = 0; j < 3; j++) a.s[j] = reinterpret_cast<T*>(s.p[j]);
     a.tsum = tsum;
     a.n = n;
     a.tiles = tiles;
     const dim3 grid(std::min<uint32_t>(tiles, (uint32_t)c.num_sms * 8), 3);
-    ProfScope ps(c, "prefix_sum", 3.0 * 3.0 * n * sizeof(T));
+    std::unique_ptr<ProfScope> ps;
+    if (profile) ps.reset(new ProfScope(c, "prefix_sum", 3.0 * 3.0 * n * sizeof(T)));
     k_up<T><<<grid, kThreads, 0, c.stream>>>(a);
     k_mid<T><<<3, 1024, 0, c.stream>>>(a);
     k_down<T><<<grid, kThreads, 0, c.stream>>>(a);
@@ -130,6 +134,52 @@ void op_prefix_sum_into(Ctx& c, int w, size_t n, Sh3 s, void* tsum) {
     if (w == 4) run_scan<uint32_t>(c, n, s, reinterpret_cast<uint32_t*>(tsum), tiles);
     else if (w == 8) run_scan<unsigned long long>(c, n, s, reinterpret_cast<unsigned long long*>(tsum), tiles);
     else throw std::invalid_argument("prefix sum supports 4 and 8-byte shares");
+}
+
+// ---------------------------------------------------------------------------
+// Prefix sum without any device allocation.
+//
+// Some callers cannot allocate device memory at the moment they call us: a
+// host program that reserved the GPU's memory up front for its own pool (so a
+// cudaMalloc would fail or break its budget), or a service loop that must not
+// pay cudaMalloc's implicit device-wide synchronisation while other requests
+// are running. For them the tile sums live in this fixed array instead of the
+// runtime's pool. It holds 3 x 16384 tile sums of 8 bytes (384 KiB per device,
+// kept until the process exits), which limits a call to 2^26 elements. Every
+// call reuses the same array, so two such calls must not run at the same time
+// on the GPU (different streams included): their tile sums would mix. Each
+// call writes every tile sum it reads, so nothing needs clearing between calls.
+constexpr size_t kNoAllocMaxElems = size_t(1) << 26;
+constexpr size_t kNoAllocTiles = kNoAllocMaxElems / kTile;
+static __device__ __align__(256) unsigned long long g_noalloc_tsum[3 * kNoAllocTiles];
+
+// Device address of g_noalloc_tsum on `device`, looked up once per device with
+// that device current (host code may not pass the symbol itself to a kernel).
+static void* noalloc_scratch(int device) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static void* ptrs[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device ordinal out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    if (ptrs[device]) return ptrs[device];
+    int cur = -1;
+    ORQ_CUDA_CHECK(cudaGetDevice(&cur));
+    if (cur != device) throw std::runtime_error("the runtime's device is not the current device");
+    void* p = nullptr;
+    ORQ_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_tsum));
+    ptrs[device] = p;
+    return p;
+}
+
+void op_prefix_sum_noalloc(Ctx& c, int w, size_t n, Sh3 s) {
+    if (w != 4 && w != 8) throw std::invalid_argument("prefix sum supports 4 and 8-byte shares");
+    if (n > kNoAllocMaxElems)
+        throw std::invalid_argument("orqcu_prefix_sum_a_noalloc handles at most 2^26 elements per call");
+    if (n == 0) return;
+    void* ts = noalloc_scratch(c.device);
+    const uint32_t tiles = prefix_sum_tiles(n);
+    if (w == 4) run_scan<uint32_t>(c, n, s, reinterpret_cast<uint32_t*>(ts), tiles, false);
+    else run_scan<unsigned long long>(c, n, s, reinterpret_cast<unsigned long long*>(ts), tiles, false);
 }
 
 void op_prefix_sum(Ctx& c, int w, size_t n, Sh3 s) {
