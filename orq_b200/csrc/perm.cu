@@ -73,16 +73,20 @@ struct FyGenArgs {
     StreamArg st[3];  // nonce = chain start nonce + 4 * (window start buffer)
     uint32_t n, mask, tiles;
     FyLayout lay;
-    unsigned long long* ents;  // [3][tiles][slot]
-    uint32_t* cnt;             // [3][tiles][kMaxLevels]
+    uint32_t* ev;   // [3][tiles][slot] entry values v
+    uint32_t* ep;   // [3][tiles][slot] entry positions within the tile
+    uint32_t* cnt;  // [3][tiles][kMaxLevels]
     const FyState* state;
     int* err;
 };
+
+constexpr int kHalfBlocks = kBlocksPerThread / 2;  // blocks per thread per half tile
 
 __global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
     extern __shared__ uint32_t sm[];
     __shared__ uint32_t red[33];
     __shared__ uint32_t sdone;
+    __shared__ uint32_t sbase[kMaxLevels];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const uint32_t total = 3 * a.tiles;
@@ -90,50 +94,68 @@ __global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
         const uint32_t g = item / a.tiles, tile = item % a.tiles;
         // the scanner may be updating the flag concurrently: read it once per CTA
         if (threadIdx.x == 0) sdone = *(volatile const uint32_t*)&a.state[g].done;
+        if (threadIdx.x < kMaxLevels) sbase[threadIdx.x] = 0;
         __syncthreads();
         if (sdone) continue;
-        // this thread's 64 consecutive draws of the tile
-        uint32_t v[4 * kBlocksPerThread];
-        const unsigned long long b0 =
-            (unsigned long long)tile * kTileBlocks + (unsigned long long)threadIdx.x * kBlocksPerThread;
-#pragma unroll
-        for (int b = 0; b < kBlocksPerThread; b++) {
-            const uint4 ks = keystream_block(S, a.st[g], b0 + b);
-            v[4 * b + 0] = ks.x & a.mask;
-            v[4 * b + 1] = ks.y & a.mask;
-            v[4 * b + 2] = ks.z & a.mask;
-            v[4 * b + 3] = ks.w & a.mask;
-        }
         const size_t slot = (size_t)g * a.tiles + tile;
-        unsigned long long* out = a.ents + slot * a.lay.slot;
-        const uint32_t pos0 = threadIdx.x * 4 * kBlocksPerThread;
-        // two levels per block-wide scan (16-bit fields; totals <= 32768)
-        for (uint32_t L = 0; L < a.lay.nl; L += 2) {
-            const uint32_t t0 = level_threshold(a.n, L);
-            const uint32_t t1 = L + 1 < a.lay.nl ? level_threshold(a.n, L + 1) : 0u;
-            uint32_t c0 = 0, c1 = 0;
+        uint32_t* ov = a.ev + slot * a.lay.slot;
+        uint32_t* op = a.ep + slot * a.lay.slot;
+        for (int half = 0; half < 2; half++) {
+            // this thread's 32 consecutive draws of the half tile
+            uint32_t v[4 * kHalfBlocks];
+            const uint32_t blk0 = half * (kTileBlocks / 2) + threadIdx.x * kHalfBlocks;
 #pragma unroll
-            for (int k = 0; k < 4 * kBlocksPerThread; k++) {
-                c0 += v[k] < t0;
-                c1 += v[k] < t1;
+            for (int b = 0; b < kHalfBlocks; b++) {
+                const uint4 ks = keystream_block(S, a.st[g], (unsigned long long)tile * kTileBlocks + blk0 + b);
+                v[4 * b + 0] = ks.x & a.mask;
+                v[4 * b + 1] = ks.y & a.mask;
+                v[4 * b + 2] = ks.z & a.mask;
+                v[4 * b + 3] = ks.w & a.mask;
             }
-            uint32_t tot;
-            const uint32_t pre = block_excl_sum(c0 | (c1 << 16), red, tot);
-            for (int h = 0; h < 2 && L + h < a.lay.nl; h++) {
-                const uint32_t Lh = L + h, th = h ? t1 : t0;
-                uint32_t o = h ? (pre >> 16) : (pre & 0xffffu);
-                const uint32_t tt = h ? (tot >> 16) : (tot & 0xffffu);
-                if (tt > a.lay.cap[Lh]) {
-                    if (threadIdx.x == 0) atomicOr(a.err, 16);
-                    continue;
-                }
-                unsigned long long* ol = out + a.lay.off[Lh];
+            const uint32_t pos0 = blk0 * 4;
+            // two levels per block-wide scan (16-bit fields; half-tile totals <= 16384)
+            for (uint32_t L = 0; L < a.lay.nl; L += 2) {
+                const uint32_t t0 = level_threshold(a.n, L);
+                const uint32_t t1 = L + 1 < a.lay.nl ? level_threshold(a.n, L + 1) : 0u;
+                uint32_t c0 = 0, c1 = 0;
 #pragma unroll
-                for (int k = 0; k < 4 * kBlocksPerThread; k++)
-                    if (v[k] < th) ol[o++] = ((unsigned long long)(pos0 + k) << 32) | v[k];
-                if (threadIdx.x == 0) a.cnt[slot * kMaxLevels + Lh] = tt;
+                for (int k = 0; k < 4 * kHalfBlocks; k++) {
+                    c0 += v[k] < t0;
+                    c1 += v[k] < t1;
+                }
+                uint32_t tot;
+                const uint32_t pre = block_excl_sum(c0 | (c1 << 16), red, tot);
+                for (int h = 0; h < 2 && L + h < a.lay.nl; h++) {
+                    const uint32_t Lh = L + h, th = h ? t1 : t0;
+                    const uint32_t base = sbase[Lh];
+                    uint32_t o = base + (h ? (pre >> 16) : (pre & 0xffffu));
+                    const uint32_t tt = h ? (tot >> 16) : (tot & 0xffffu);
+                    if (base + tt > a.lay.cap[Lh]) {
+                        if (threadIdx.x == 0) atomicOr(a.err, 16);
+                        continue;
+                    }
+                    uint32_t* olv = ov + a.lay.off[Lh];
+                    uint32_t* olp = op + a.lay.off[Lh];
+#pragma unroll
+                    for (int k = 0; k < 4 * kHalfBlocks; k++)
+                        if (v[k] < th) {
+                            olv[o] = v[k];
+                            olp[o] = pos0 + k;
+                            o++;
+                        }
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    sbase[L] += tot & 0xffffu;
+                    if (L + 1 < a.lay.nl) sbase[L + 1] += tot >> 16;
+                }
+                __syncthreads();
             }
         }
+        // an overflowing level was flagged above; its count is clamped so the
+        // scanner never reads past the level's list
+        if (threadIdx.x < a.lay.nl)
+            a.cnt[slot * kMaxLevels + threadIdx.x] = min(sbase[threadIdx.x], a.lay.cap[threadIdx.x]);
         __syncthreads();
     }
 }
@@ -142,7 +164,8 @@ struct FyScanArgs {
     uint32_t n, count, tiles;
     unsigned long long win_tile0;  // absolute index of the window's first tile
     FyLayout lay;
-    const unsigned long long* ents;
+    const uint32_t* ev;
+    const uint32_t* ep;
     const uint32_t* cnt;
     FyState* state;     // [3]
     uint32_t* acc;      // [3][count][n] accepted offsets v_i (swap with i + v_i)
@@ -150,65 +173,60 @@ struct FyScanArgs {
     unsigned long long* stats;  // optional [3][8] diagnostic counters (ORQ_FY_STATS)
 };
 
-// first index in P[0..m] with P[idx] > e, minus one (P non-decreasing, P[0] = 0)
-__device__ __forceinline__ uint32_t tile_of(const uint32_t* P, uint32_t m, uint32_t e) {
-    uint32_t lo = 0, hi = m;  // invariant: P[lo] <= e, answer in [lo, hi)
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
+
+// ---------------------------------------------------------------------------
+// The scanner. One 1024-thread CTA per group replays the acceptance of its
+// chain exactly. A step takes the next cs entries (<= 32768) of the current
+// level, staged through shared memory with coalesced loads; thread t then owns
+// entries [32t, 32t+32). Level 1: entry q is certainly accepted if
+// v + q <= T (at most q acceptances precede it), certainly rejected if v > T,
+// otherwise uncertain. Level 2 (warp 0, 32 uncertain entries at a time):
+// with c = certain accepts before an uncertain entry and a = uncertain accepts
+// before it, it is accepted iff a <= T - c - v ("slack"); lane j of a chunk is
+// certain if slack >= a_chunk + j, rejected if slack < a_chunk, and only the
+// rest is decided lane by lane. One packed block scan per step gives ranks.
+constexpr uint32_t kMaxStepEntries = 32768;
+constexpr int kPerThread = kMaxStepEntries / kScanThreads;  // 32
+constexpr uint32_t kUncCap = 2048;
+constexpr size_t kScanSmem = (kMaxStepEntries + kMaxStepEntries / 32) * 4;  // padded staging
+
+__device__ __forceinline__ uint32_t pad_idx(uint32_t q) { return q + (q >> 5); }
+
+// entries per step at level L: uncertain entries of a step are about
+// cs^2 / (2 n/4^L); keep that near 512
+__device__ __forceinline__ uint32_t step_entries(uint32_t n, uint32_t L) {
+    const unsigned long long t = level_threshold(n, L);
+    uint32_t s = kMaxStepEntries;
+    while (s > 1024 && (unsigned long long)s * s > 1024ull * t) s >>= 1;
+    return s;
+}
+
+// tile holding entry e, searching P[lo..hi] (P[lo] <= e < P[hi+1])
+__device__ __forceinline__ uint32_t tile_in(const uint32_t* P, uint32_t lo, uint32_t hi, uint32_t e) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
         if (P[mid] <= e) lo = mid;
-        else hi = mid;
+        else hi = mid - 1;
     }
     return lo;
 }
 
-// entries per step at level L: the index bound makes ~S^2 / (2 n/4^L)
-// entries uncertain, kept near 128 per step
-__device__ __forceinline__ uint32_t step_entries(uint32_t n, uint32_t L) {
-    const unsigned long long t = level_threshold(n, L);
-    uint32_t s = kStep;
-    while (s > 256 && (unsigned long long)s * s > 256ull * t) s >>= 1;
-    return s;
-}
-
-// entries [e0, e0+cs) of the window's level lists (8 per thread)
-__device__ __forceinline__ void load_step(const uint32_t* P, uint32_t tiles,
-                                          const unsigned long long* E, uint32_t slot, uint32_t off,
-                                          uint32_t e0, uint32_t cs, uint32_t v[8], uint32_t et[8],
-                                          uint32_t ep[8]) {
-    const uint32_t my0 = e0 + threadIdx.x * 8;
-    uint32_t t = my0 < e0 + cs ? tile_of(P, tiles, my0) : 0u;
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-        const uint32_t q = threadIdx.x * 8 + u;
-        v[u] = 0xffffffffu;
-        et[u] = 0;
-        ep[u] = 0;
-        if (q < cs) {
-            while (P[t + 1] <= e0 + q) t++;
-            const unsigned long long ent = E[(size_t)t * slot + off + (e0 + q - P[t])];
-            v[u] = (uint32_t)ent;
-            ep[u] = (uint32_t)(ent >> 32);
-            et[u] = t;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
+__global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
+    extern __shared__ uint32_t sv[];  // staged entry values, padded
     __shared__ uint32_t red[33];
     __shared__ uint32_t P[kMaxWindowTiles + 1];  // prefix of level-L counts over the window
-    __shared__ uint32_t s_last_tile, s_last_pos, s_uacc_total, s_seq;
-    __shared__ uint32_t unc_v[kStep / 8];      // uncertain entries of a step, in order
-    __shared__ uint32_t unc_cp[kStep / 8];     // certain accepts before each
-    __shared__ uint32_t unc_pre[kStep / 8 + 1];  // uncertain accepted before each (exclusive)
-    __shared__ uint8_t unc_ok[kStep / 8];
+    __shared__ uint32_t unc_v[kUncCap], unc_cp[kUncCap], unc_pre[kUncCap + 1];
+    __shared__ uint32_t s_last_q, s_uacc;
     const uint32_t g = blockIdx.x;
     const uint32_t n = a.n;
     const uint32_t tiles = a.tiles;
+    const int lane = threadIdx.x & 31;
     // scan state, identical in every thread
     uint32_t i = a.state[g].i, m = a.state[g].m, done = a.state[g].done;
     unsigned long long start = a.state[g].start_tile;
     uint32_t tau = 0, ix = 0, L = 0, Lp = 0xffffffffu;
-    const unsigned long long* E = a.ents + (size_t)g * tiles * a.lay.slot;
+    const uint32_t* EV = a.ev + (size_t)g * tiles * a.lay.slot;
+    const uint32_t* EP = a.ep + (size_t)g * tiles * a.lay.slot;
     const uint32_t* C = a.cnt + (size_t)g * tiles * kMaxLevels;
     unsigned long long st_steps = 0, st_unc_steps = 0, st_seq = 0, st_ent = 0, st_unc = 0,
                        st_cyc_load = 0, st_cyc_unc = 0, st_cyc_all = 0;
@@ -247,16 +265,41 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
         }
         const uint32_t cs = min(step_entries(n, L), eend - e0);
         const unsigned long long t_l0 = clock64();
-        uint32_t v[8], etile[8], epos[8];
-        load_step(P, tiles, E, a.lay.slot, a.lay.off[L], e0, cs, v, etile, epos);
-        uint32_t certain = 0, unc = 0;
+        // ---- stage entry values (coalesced: consecutive threads, consecutive
+        // entries); each lane walks its tile cursor forward, no searches
+        {
+            const size_t off = a.lay.off[L];
+            uint32_t t = tau;
+            uint32_t vals[kPerThread];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const uint32_t q = threadIdx.x * 8 + u;  // index within the step
-            if (q < cs) {
-                // at most q acceptances precede entry q in this step
-                if ((unsigned long long)v[u] + q <= T) certain |= 1u << u;
-                else if (v[u] <= T) unc |= 1u << u;
+            for (int u = 0; u < kPerThread; u++) {
+                const uint32_t q = u * kScanThreads + threadIdx.x;
+                vals[u] = 0;
+                if (q < cs) {
+                    const uint32_t e = e0 + q;
+                    while (P[t + 1] <= e) t++;
+                    vals[u] = __ldg(EV + (size_t)t * a.lay.slot + off + (e - P[t]));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kPerThread; u++) {
+                const uint32_t q = u * kScanThreads + threadIdx.x;
+                if (q < cs) sv[pad_idx(q)] = vals[u];
+            }
+        }
+        __syncthreads();
+        // ---- level 1
+        uint32_t certain = 0, unc = 0;
+        {
+            const uint32_t q0 = threadIdx.x * kPerThread;
+#pragma unroll
+            for (int u = 0; u < kPerThread; u++) {
+                const uint32_t q = q0 + u;
+                if (q < cs) {
+                    const uint32_t v = sv[pad_idx(q)];
+                    if ((unsigned long long)v + q <= T) certain |= 1u << u;
+                    else if (v <= T) unc |= 1u << u;
+                }
             }
         }
         uint32_t tot;
@@ -266,68 +309,87 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
         st_steps++;
         st_ent += cs;
         st_cyc_load += clock64() - t_l0;
-        uint32_t accept = certain, tot_a = tot_c;
-        uint32_t rank_base = cpre;  // accepted entries of earlier threads
+        uint32_t accept = certain, tot_a = tot_c, rank_base = cpre;
         if (tot_u) {
             const unsigned long long t_u0 = clock64();
             st_unc_steps++;
             st_unc += tot_u;
-            const uint32_t cap = kStep / 8;
-            if (tot_u <= cap) {
+            const bool listed = tot_u <= kUncCap;
+            if (listed) {
                 uint32_t k = upre, cc = cpre;
-                for (int u = 0; u < 8; u++) {
+                const uint32_t q0 = threadIdx.x * kPerThread;
+                for (int u = 0; u < kPerThread; u++) {
                     if ((unc >> u) & 1u) {
-                        unc_v[k] = v[u];
+                        unc_v[k] = sv[pad_idx(q0 + u)];
                         unc_cp[k] = cc;
                         k++;
                     }
                     if ((certain >> u) & 1u) cc++;
                 }
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    uint32_t uacc = 0;
-                    for (uint32_t k2 = 0; k2 < tot_u; k2++) {
-                        unc_pre[k2] = uacc;
-                        const unsigned long long iat = (unsigned long long)i + unc_cp[k2] + uacc;
-                        const bool ok = iat < n && (unsigned long long)unc_v[k2] <= (unsigned long long)n - 1 - iat;
-                        unc_ok[k2] = ok;
-                        uacc += ok;
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                // level 2 over the listed uncertain entries, or (too many) over
+                // every entry of the step in order with no certain ones
+                const uint32_t cnt = listed ? tot_u : cs;
+                uint32_t acc_so_far = 0;
+                for (uint32_t base = 0; base < cnt; base += 32) {
+                    const uint32_t k = base + lane;
+                    const bool valid = k < cnt;
+                    long long slack = -1;
+                    if (valid) {
+                        const uint32_t v = listed ? unc_v[k] : sv[pad_idx(k)];
+                        const uint32_t cp = listed ? unc_cp[k] : 0u;
+                        slack = (long long)T - cp - v;
                     }
-                    unc_pre[tot_u] = uacc;
-                    s_uacc_total = uacc;
-                }
-                __syncthreads();
-                uint32_t k2 = upre;
-                rank_base = cpre + unc_pre[upre];
-                for (int u = 0; u < 8; u++)
-                    if ((unc >> u) & 1u) {
-                        if (unc_ok[k2]) accept |= 1u << u;
-                        k2++;
-                    }
-                tot_a = tot_c + s_uacc_total;
-            } else {
-                // too many to list: decide the whole step in order
-                __shared__ uint32_t seq_acc[kStep / 32];
-                extern __shared__ uint32_t seq_v[];  // kStep words of dynamic shared memory
-                if (threadIdx.x < kStep / 32) seq_acc[threadIdx.x] = 0;
-#pragma unroll
-                for (int u = 0; u < 8; u++) seq_v[threadIdx.x * 8 + u] = v[u];
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    uint32_t ii = i;
-                    for (uint32_t q = 0; q < cs && ii < n; q++)
-                        if (seq_v[q] <= n - 1 - ii) {
-                            seq_acc[q >> 5] |= 1u << (q & 31);
-                            ii++;
+                    const bool cert = valid && slack >= (long long)acc_so_far + lane;
+                    const bool und = valid && !cert && slack >= (long long)acc_so_far;
+                    uint32_t okmask = __ballot_sync(0xffffffffu, cert);
+                    const uint32_t undmask = __ballot_sync(0xffffffffu, und);
+                    if (undmask) {
+                        // decide the chunk lane by lane
+                        okmask = 0;
+                        uint32_t cur = acc_so_far;
+                        for (int j = 0; j < 32; j++) {
+                            const long long sj = __shfl_sync(0xffffffffu, slack, j);
+                            if (base + j < cnt && sj >= (long long)cur) {
+                                okmask |= 1u << j;
+                                cur++;
+                            }
                         }
-                    s_seq = ii - i;
+                    }
+                    if (valid) {
+                        const uint32_t before = acc_so_far + __popc(okmask & ((1u << lane) - 1u));
+                        if (listed) {
+                            unc_pre[k] = before;
+                            unc_cp[k] = (okmask >> lane) & 1u;  // reuse as the decision
+                        } else {
+                            sv[pad_idx(k)] = ((okmask >> lane) & 1u) ? sv[pad_idx(k)] : 0xffffffffu;
+                        }
+                    }
+                    acc_so_far += __popc(okmask);
                 }
-                __syncthreads();
+                if (lane == 0) {
+                    if (listed) unc_pre[tot_u] = acc_so_far;
+                    s_uacc = acc_so_far;
+                }
+            }
+            __syncthreads();
+            if (listed) {
+                uint32_t k = upre;
+                rank_base = cpre + unc_pre[upre];
+                for (int u = 0; u < kPerThread; u++)
+                    if ((unc >> u) & 1u) {
+                        if (unc_cp[k]) accept |= 1u << u;
+                        k++;
+                    }
+                tot_a = tot_c + s_uacc;
+            } else {
+                // every accepted entry kept its value, rejected ones became ~0
                 accept = 0;
-                for (int u = 0; u < 8; u++) {
-                    const uint32_t q = threadIdx.x * 8 + u;
-                    if ((seq_acc[q >> 5] >> (q & 31)) & 1u) accept |= 1u << u;
-                }
+                const uint32_t q0 = threadIdx.x * kPerThread;
+                for (int u = 0; u < kPerThread; u++)
+                    if (q0 + u < cs && sv[pad_idx(q0 + u)] != 0xffffffffu) accept |= 1u << u;
                 uint32_t t2;
                 rank_base = block_excl_sum(__popc(accept), red, t2);
                 tot_a = t2;
@@ -339,23 +401,24 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
         uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
         {
             uint32_t r = rank_base;
-            for (int u = 0; u < 8; u++)
+            const uint32_t q0 = threadIdx.x * kPerThread;
+            for (int u = 0; u < kPerThread; u++)
                 if ((accept >> u) & 1u) {
                     if (r < need) {
-                        acc[i + r] = v[u];
-                        if (r == need - 1) {
-                            s_last_tile = etile[u];
-                            s_last_pos = epos[u];
-                        }
+                        acc[i + r] = sv[pad_idx(q0 + u)];
+                        if (r == need - 1) s_last_q = q0 + u;
                     }
                     r++;
                 }
         }
         if (tot_a >= need) {
             __syncthreads();
-            // permutation complete: count the getNext buffers it used
+            // permutation complete: locate its last draw, count the getNext buffers
+            const uint32_t e = e0 + s_last_q;
+            const uint32_t t = tile_in(P, tau, tiles - 1, e);
+            const uint32_t pos = EP[(size_t)t * a.lay.slot + a.lay.off[L] + (e - P[t])];
             const unsigned long long kend =
-                (a.win_tile0 + s_last_tile - start) * (unsigned long long)kTileDraws + s_last_pos;
+                (a.win_tile0 + t - start) * (unsigned long long)kTileDraws + pos;
             const unsigned long long R = 1 + ((kend + 1) >> 20);
             if (threadIdx.x == 0) a.refills[(size_t)g * a.count + m] = (uint32_t)R;
             start = (start / kTilesPerRefill + R) * kTilesPerRefill;
@@ -363,7 +426,6 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
             i = 0;
             ix = 0;
             if (m >= a.count) done = 1;
-            __syncthreads();
         } else {
             i += tot_a;
             const uint32_t enew = e0 + cs;
@@ -371,10 +433,11 @@ __global__ void __launch_bounds__(kScanThreads) k_fy_scan(FyScanArgs a) {
                 tau = tiles;
                 ix = 0;
             } else {
-                tau = tile_of(P, tiles, enew);
+                tau = tile_in(P, tau, tiles - 1, enew);
                 ix = enew - P[tau];
             }
         }
+        __syncthreads();  // sv and the lists are reused by the next step
     }
     if (threadIdx.x == 0) {
         a.state[g].i = i;
@@ -582,9 +645,10 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         }
         lay.slot = o;
     }
-    const size_t ents_b = (size_t)3 * tiles * lay.slot * 8;
+    const size_t ents_b = (size_t)3 * tiles * lay.slot * 4;
     const size_t cnt_b = (size_t)3 * tiles * kMaxLevels * 4;
-    Scratch ents0(c, ents_b), ents1(c, ents_b), cnt0(c, cnt_b), cnt1(c, cnt_b);
+    Scratch ev0(c, ents_b), ev1(c, ents_b), ep0(c, ents_b), ep1(c, ents_b), cnt0(c, cnt_b),
+        cnt1(c, cnt_b);
     Scratch state(c, 3 * sizeof(FyState));
     Scratch acc(c, (size_t)3 * count * n * 4);
     Scratch refills(c, (size_t)3 * count * 4);
@@ -612,10 +676,11 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     FyState* hstate = nullptr;
     ORQ_CUDA_CHECK(cudaMallocHost(&hstate, 3 * sizeof(FyState)));
     prep_aes_kernel(k_fy_gen);
-    ORQ_CUDA_CHECK(cudaFuncSetAttribute(k_fy_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, kStep * 4));
+    ORQ_CUDA_CHECK(cudaFuncSetAttribute(k_fy_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem));
 
     const unsigned gen_grid = (unsigned)std::max(1, c.num_sms - 3);
-    unsigned long long* entsp[2] = {ents0.as<unsigned long long>(), ents1.as<unsigned long long>()};
+    uint32_t* evp[2] = {ev0.as<uint32_t>(), ev1.as<uint32_t>()};
+    uint32_t* epp[2] = {ep0.as<uint32_t>(), ep1.as<uint32_t>()};
     uint32_t* cntp[2] = {cnt0.as<uint32_t>(), cnt1.as<uint32_t>()};
 
     const unsigned long long limit_windows =
@@ -640,7 +705,8 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         ga.mask = mask;
         ga.tiles = tiles;
         ga.lay = lay;
-        ga.ents = entsp[b];
+        ga.ev = evp[b];
+        ga.ep = epp[b];
         ga.cnt = cntp[b];
         ga.state = state.as<FyState>();
         ga.err = c.d_err;
@@ -669,7 +735,8 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         sa.tiles = tiles;
         sa.win_tile0 = (unsigned long long)w * tiles;
         sa.lay = lay;
-        sa.ents = entsp[b];
+        sa.ev = evp[b];
+        sa.ep = epp[b];
         sa.cnt = cntp[b];
         sa.state = state.as<FyState>();
         sa.acc = acc.as<uint32_t>();
@@ -679,7 +746,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         tl_idx[w][2] = tl_event(ss);
         {
             ProfScope ps(c, "fy_scan", 0.0, 0.0, ss);
-            k_fy_scan<<<3, kScanThreads, kStep * 4, ss>>>(sa);
+            k_fy_scan<<<3, kScanThreads, kScanSmem, ss>>>(sa);
         }
         tl_idx[w][3] = tl_event(ss);
         ORQ_CUDA_CHECK(cudaGetLastError());
