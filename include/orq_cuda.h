@@ -158,6 +158,18 @@ int orqcu_apply_elementwise_perm(orqcu_runtime* rt, int x_arith, int x_width, si
 int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int bits,
                      int descending, void* const perm_out[3]);
 
+/* BSharedVector::_compare (circuits.h:231-295, bit_same at
+ * b_shared_vector.h:164-178): eq = (x == y), gt = (x > y) in the signed order,
+ * both as B-shared single bits (LSB of each share). width 4 or 8. One fused
+ * launch: log2(8*width)+1 AND rounds on every pair and the packed sign fix-up. */
+int orqcu_compare_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                    const void* const y[3], void* const eq[3], void* const gt[3]);
+/* bitonic_sort (sorting.h:266-353) of one B-shared key column in place, in the
+ * signed order; n a power of two, width 4 or 8. One launch per network stage
+ * (compare + two multiplexes, operators/common.h:20-28). */
+int orqcu_bitonic_sort(orqcu_runtime* rt, int width, size_t n, void* const key[3],
+                       int descending);
+
 #ifdef __cplusplus
 }
 #endif

@@ -160,3 +160,16 @@ class Oracle:
     def prefix_sum(self, s):
         w = s[0].dtype.itemsize
         self.lib.oro_prefix_sum(w, ctypes.c_size_t(len(s[0])), self._ptrs(s))
+
+    def compare(self, x, y):
+        w = x[0].dtype.itemsize
+        n = len(x[0])
+        eq, gt = self.new(n, w), self.new(n, w)
+        self.lib.oro_compare(ctypes.byref(self.ctx), w, ctypes.c_size_t(n), self._ptrs(x), self._ptrs(y),
+                             self._ptrs(eq), self._ptrs(gt))
+        return eq, gt
+
+    def bitonic_sort(self, key, desc=False):
+        w = key[0].dtype.itemsize
+        self.lib.oro_bitonic_sort(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(key[0])), self._ptrs(key),
+                                  int(desc))

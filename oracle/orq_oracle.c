@@ -695,3 +695,199 @@ void oro_prefix_sum(int w, size_t n, void* s[3]) {
         }
     }
 }
+
+/* ------------------------------------------------------------------------- */
+/* Compare circuit and bitonic sort on B-shared int32/int64 keys. */
+
+/* arithmetic right shift of a w-byte two's-complement value */
+static u128 ashr(u128 v, int w, int s) {
+    return (u128)(((__int128)sext(v, w)) >> s);
+}
+static u128 wmask(int w) { return w == 16 ? ~(u128)0 : (((u128)1 << (8 * w)) - 1); }
+
+/* BSharedVector::_compare (operators/circuits.h:231-295) with bit_same
+ * (containers/b_shared_vector.h:164-178), for m pairs of w-byte keys; xa[j][p]
+ * plays `this`. eq and gt come out masked to their LSB (one call sequence:
+ * log2(8w) ANDs, gt &= this, and the packed OR on ceil(m/8w) words). */
+static void compare_pairs(oro_ctx* c, int w, size_t m, u128* const xa[3], u128* const ya[3],
+                          u128* eq[3], u128* gt[3]) {
+    const int B = 8 * w;
+    int L = 0;
+    while ((1 << L) < B) L++; /* bit_width(B - 1) */
+    const u128 M = wmask(w);
+    void* S[3];
+    void* Tm[3];
+    for (int j = 0; j < 3; j++) {
+        S[j] = xalloc(m * (size_t)w);
+        Tm[j] = xalloc(m * (size_t)w);
+        for (size_t p = 0; p < m; p++) st(S[j], p, w, ~(xa[j][p] ^ ya[j][p]) & M);
+    }
+    for (int lev = 0; lev < L; lev++) {
+        for (int j = 0; j < 3; j++)
+            for (size_t p = 0; p < m; p++) st(Tm[j], p, w, ashr(ld(S[j], p, w), w, 1 << lev) & M);
+        oro_and_b(c, w, m, S, Tm, S);
+    }
+    /* gt = ((eq >> 1) ^ eq) & this, then parity of every share */
+    void* G[3];
+    void* X[3];
+    for (int j = 0; j < 3; j++) {
+        G[j] = xalloc(m * (size_t)w);
+        X[j] = xalloc(m * (size_t)w);
+        for (size_t p = 0; p < m; p++) {
+            u128 e = ld(S[j], p, w);
+            st(G[j], p, w, (ashr(e, w, 1) ^ e) & M);
+            st(X[j], p, w, xa[j][p]);
+        }
+    }
+    oro_and_b(c, w, m, G, X, G);
+    /* sign fix-up on packed bits */
+    const size_t cw = m / B + (m % B > 0);
+    void* s1[3];
+    void* s2[3];
+    void* r[3];
+    for (int j = 0; j < 3; j++) {
+        s1[j] = xalloc(cw * (size_t)w);
+        s2[j] = xalloc(cw * (size_t)w);
+        r[j] = xalloc(cw * (size_t)w);
+        for (size_t word = 0; word < cw; word++) {
+            u128 a = 0, b = 0, e = 0;
+            for (int k = 0; k < B && word * B + k < m; k++) {
+                size_t p = word * B + k;
+                u128 gv = ld(G[j], p, w);
+                int par = 0;
+                for (int bit = 0; bit < B; bit++) par ^= (int)((gv >> bit) & 1);
+                a |= ((xa[j][p] >> (B - 1)) & 1) << k;
+                b |= ((ya[j][p] >> (B - 1)) & 1) << k;
+                e |= (u128)par << k;
+            }
+            /* r ^= s2 ; s2 ^= s1 ; then s2 |= r as ~(~s2 & ~r) */
+            e ^= b;
+            b ^= a;
+            st(s1[j], word, w, a);
+            st(s2[j], word, w, ~b & M);
+            st(r[j], word, w, ~e & M);
+        }
+    }
+    oro_and_b(c, w, cw, s2, r, s2);
+    for (int j = 0; j < 3; j++) {
+        for (size_t word = 0; word < cw; word++) {
+            u128 o = ~ld(s2[j], word, w) & M;
+            st(s1[j], word, w, ld(s1[j], word, w) ^ o);
+        }
+        for (size_t p = 0; p < m; p++) {
+            eq[j][p] = ld(S[j], p, w) & 1;
+            gt[j][p] = (ld(s1[j], p / B, w) >> (p % B)) & 1;
+        }
+        free(S[j]);
+        free(Tm[j]);
+        free(G[j]);
+        free(X[j]);
+        free(s1[j]);
+        free(s2[j]);
+        free(r[j]);
+    }
+}
+
+void oro_compare(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* eq[3],
+                 void* gt[3]) {
+    u128* xa[3];
+    u128* ya[3];
+    u128* e[3];
+    u128* g[3];
+    for (int j = 0; j < 3; j++) {
+        xa[j] = (u128*)xalloc(n * 16);
+        ya[j] = (u128*)xalloc(n * 16);
+        e[j] = (u128*)xalloc(n * 16);
+        g[j] = (u128*)xalloc(n * 16);
+        for (size_t p = 0; p < n; p++) {
+            xa[j][p] = ld(x[j], p, w);
+            ya[j][p] = ld(y[j], p, w);
+        }
+    }
+    compare_pairs(c, w, n, xa, ya, e, g);
+    for (int j = 0; j < 3; j++) {
+        for (size_t p = 0; p < n; p++) {
+            st(eq[j], p, w, e[j][p]);
+            st(gt[j], p, w, g[j][p]);
+        }
+        free(xa[j]);
+        free(ya[j]);
+        free(e[j]);
+        free(g[j]);
+    }
+}
+
+/* bitonic_sort (operators/sorting.h:266-353,394-399) of one B-shared key
+ * column: stage (i, j) with h = 2^(i-j) compares x[c*h+k] = c*2h+k with
+ * y = c*2h+2h-1-k (j == 0, the reversed subset) or c*2h+h+k, then swaps with
+ * two multiplexes (operators/common.h:20-28). */
+void oro_bitonic_sort(oro_ctx* c, int w, size_t n, void* key[3], int desc) {
+    if (n < 2) return;
+    int rounds = 0;
+    while (((size_t)1 << rounds) < n) rounds++;
+    const size_t m = n / 2;
+    const u128 M = wmask(w);
+    u128* xa[3];
+    u128* ya[3];
+    u128* e[3];
+    u128* g[3];
+    size_t* xi = (size_t*)xalloc(m * sizeof(size_t));
+    size_t* yi = (size_t*)xalloc(m * sizeof(size_t));
+    for (int j = 0; j < 3; j++) {
+        xa[j] = (u128*)xalloc(m * 16);
+        ya[j] = (u128*)xalloc(m * 16);
+        e[j] = (u128*)xalloc(m * 16);
+        g[j] = (u128*)xalloc(m * 16);
+    }
+    void* E[3];
+    void* D[3];
+    void* Z[3];
+    for (int j = 0; j < 3; j++) {
+        E[j] = xalloc(m * (size_t)w);
+        D[j] = xalloc(m * (size_t)w);
+        Z[j] = xalloc(m * (size_t)w);
+    }
+    for (int i = 0; i < rounds; i++) {
+        for (int jj = 0; jj <= i; jj++) {
+            const size_t h = (size_t)1 << (i - jj);
+            for (size_t p = 0; p < m; p++) {
+                size_t cb = p / h, k = p % h;
+                xi[p] = cb * 2 * h + k;
+                yi[p] = jj == 0 ? cb * 2 * h + 2 * h - 1 - k : cb * 2 * h + h + k;
+            }
+            for (int j = 0; j < 3; j++)
+                for (size_t p = 0; p < m; p++) {
+                    xa[j][p] = ld(key[j], xi[p], w);
+                    ya[j][p] = ld(key[j], yi[p], w);
+                }
+            /* ASC: x > y ; DESC: y > x (compare_rows, sorting.h:80-108) */
+            if (desc)
+                compare_pairs(c, w, m, ya, xa, e, g);
+            else
+                compare_pairs(c, w, m, xa, ya, e, g);
+            /* tmp = multiplex(b, x, y) = x ^ (ext(b) & (y ^ x)) ; y' = y ^ (ext(b) & (x ^ y)) */
+            for (int j = 0; j < 3; j++)
+                for (size_t p = 0; p < m; p++) {
+                    st(E[j], p, w, (g[j][p] & 1) ? M : 0);
+                    st(D[j], p, w, (xa[j][p] ^ ya[j][p]) & M);
+                }
+            oro_and_b(c, w, m, E, D, Z);
+            for (int j = 0; j < 3; j++)
+                for (size_t p = 0; p < m; p++) st(key[j], xi[p], w, xa[j][p] ^ ld(Z[j], p, w));
+            oro_and_b(c, w, m, E, D, Z);
+            for (int j = 0; j < 3; j++)
+                for (size_t p = 0; p < m; p++) st(key[j], yi[p], w, ya[j][p] ^ ld(Z[j], p, w));
+        }
+    }
+    for (int j = 0; j < 3; j++) {
+        free(xa[j]);
+        free(ya[j]);
+        free(e[j]);
+        free(g[j]);
+        free(E[j]);
+        free(D[j]);
+        free(Z[j]);
+    }
+    free(xi);
+    free(yi);
+}

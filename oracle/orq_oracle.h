@@ -97,6 +97,14 @@ void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int de
                     int npayload, void** payloads /* npayload x 3 pointers, int64 */,
                     int32_t* perm_out[3]);
 
+/* BSharedVector::_compare (circuits.h:231-295) of int32/int64 B-shared keys:
+ * eq = (x == y), gt = (x > y) signed, each as B-shared bits in the LSB. */
+void oro_compare(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* eq[3],
+                 void* gt[3]);
+/* bitonic_sort (sorting.h:266-353) of one B-shared int32/int64 key column in
+ * place; n a power of two. */
+void oro_bitonic_sort(oro_ctx* c, int w, size_t n, void* key[3], int desc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -149,6 +149,55 @@ int main(int argc, char** argv) {
             d.plain("open_pay1", o1);
             d.plain("open_pay2", o2);
         }
+    } else if (op == "bitonic32" || op == "bitonic64" || op == "bitonic32_desc" ||
+               op == "bitonic_time") {
+        // bitonic_sort(key) of one B-shared column (n a power of two), keys
+        // uniform over all bits (sorted in the signed order)
+        uint64_t st = seed;
+        const bool desc = op == "bitonic32_desc";
+        const auto order = desc ? orq::operators::SortOrder::DESC : orq::operators::SortOrder::ASC;
+        if (op == "bitonic64") {
+            auto key = gen<int64_t>(n, st, ~0ull);
+            BSharedVector<int64_t> kb = secret_share_b(key, 0);
+            orq::operators::bitonic_sort(kb, order);
+            d.shares("key", kb);
+            auto o = kb.open();
+            d.plain("open_key", o);
+        } else {
+            auto key = gen<int32_t>(n, st, ~0ull);
+            BSharedVector<int32_t> kb = secret_share_b(key, 0);
+            t0 = std::chrono::steady_clock::now();
+            orq::operators::bitonic_sort(kb, order);
+            secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (op != "bitonic_time") {
+                d.shares("key", kb);
+                auto o = kb.open();
+                d.plain("open_key", o);
+            }
+        }
+    } else if (op == "compare32" || op == "compare64") {
+        // BSharedVector::_compare of x vs y; a quarter of the pairs are equal
+        uint64_t st = seed;
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            auto x = gen<T>(n, st, ~0ull);
+            auto y = gen<T>(n, st, ~0ull);
+            for (size_t i = 0; i < n; i += 4) y[i] = x[i];
+            BSharedVector<T> xb = secret_share_b(x, 0);
+            BSharedVector<T> yb = secret_share_b(y, 1);
+            BSharedVector<T> eq(n), gt(n);
+            xb._compare(yb, eq, gt);
+            d.shares("xb", xb);
+            d.shares("yb", yb);
+            d.shares("eq", eq);
+            d.shares("gt", gt);
+            auto oe = eq.open();
+            auto og = gt.open();
+            d.plain("open_eq", oe);
+            d.plain("open_gt", og);
+        };
+        if (op == "compare32") run(int32_t{});
+        else run(int64_t{});
     } else if (op == "shuffle") {
         uint64_t st = seed;
         auto x = gen<int32_t>(n, st, ~0ull);

@@ -276,6 +276,25 @@ class BSharedVector(SharedVector):
                                          _p3(self.shares), _p3(z)))
         return ASharedVector(self.rt, z)
 
+    def _compare(self, other: "BSharedVector"):
+        """BSharedVector::_compare (circuits.h:231-295): (eq, gt) as B-shared
+        bits, self vs other in the signed order."""
+        if other.size() != self.size() or other.width != self.width:
+            raise ValueError("size/width mismatch")
+        eq = self.rt._alloc(self.size(), self.width)
+        gt = self.rt._alloc(self.size(), self.width)
+        _check(self.rt.lib.orqcu_compare_b(self.rt.h, self.width, ctypes.c_size_t(self.size()),
+                                           _p3(self.shares), _p3(other.shares), _p3(eq), _p3(gt)))
+        return BSharedVector(self.rt, eq), BSharedVector(self.rt, gt)
+
+    def __gt__(self, other: "BSharedVector") -> "BSharedVector":
+        """operator> (b_shared_vector.h:538-545)."""
+        return self._compare(other)[1]
+
+    def __lt__(self, other: "BSharedVector") -> "BSharedVector":
+        """operator< (b_shared_vector.h:556-558): other > self."""
+        return other._compare(self)[1]
+
 
 class ASharedVector(SharedVector):
     """Arithmetic shares mod 2^(8w) (core/containers/a_shared_vector.h)."""
@@ -330,6 +349,14 @@ def oblivious_apply_elementwise_perm(x: SharedVector, perm: ASharedVector):
     _check(rt.lib.orqcu_apply_elementwise_perm(rt.h, int(x.arith), x.width,
                                                ctypes.c_size_t(x.size()), _p3(x.shares),
                                                _p3(perm.shares)))
+
+
+def bitonic_sort(v: BSharedVector, order: int = ASC):
+    """orq::operators::bitonic_sort (sorting.h:266-353) of one key column, in
+    place; the size must be a power of two."""
+    rt = v.rt
+    _check(rt.lib.orqcu_bitonic_sort(rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares),
+                                     int(order == DESC)))
 
 
 def radix_sort(v: BSharedVector, order: int = ASC, bits: int | None = None) -> ElementwisePermutation:

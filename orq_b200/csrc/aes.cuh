@@ -38,10 +38,27 @@ constexpr int kAesSmemBytes = 2 * 256 * 256;  // 4 tables x 256 entries x 32 lan
 // uploader per unit and the runtime fills every copy once per device.
 static __device__ uint32_t g_aes_T[4 * 256];
 
+// The 32 lane copies of one entry are 128 contiguous bytes; a thread writes 4
+// of them with one 128-bit store, so a quarter-warp store phase covers one
+// 128-byte row (conflict-free) and each global word is read by 8 threads.
 __device__ __forceinline__ void aes_stage_tables(uint32_t* sm) {
-    for (int idx = threadIdx.x; idx < 4 * 256 * 32; idx += blockDim.x) {
-        const int l = idx & 31, x = (idx >> 5) & 255, t = idx >> 13;
-        sm[(t >> 1) * 16384 + x * 64 + (t & 1) * 32 + l] = g_aes_T[t * 256 + x];
+    constexpr int kStores = 4 * 256 * 8;
+    for (int base = 0; base < kStores; base += 16 * blockDim.x) {
+        uint32_t v[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int idx = base + u * blockDim.x + threadIdx.x;
+            v[u] = idx < kStores ? __ldg(&g_aes_T[idx >> 3]) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int idx = base + u * blockDim.x + threadIdx.x;
+            if (idx < kStores) {
+                const int e = idx >> 3, t = e >> 8, x = e & 255;
+                reinterpret_cast<uint4*>(sm + (t >> 1) * 16384 + x * 64 + (t & 1) * 32)[idx & 7] =
+                    make_uint4(v[u], v[u], v[u], v[u]);
+            }
+        }
     }
     __syncthreads();
 }

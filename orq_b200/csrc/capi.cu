@@ -357,4 +357,28 @@ int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key
     });
 }
 
+int orqcu_compare_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                    const void* const y[3], void* const eq[3], void* const gt[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "compare supports 4 and 8-byte keys");
+        need_sh(x, n, "null x");
+        need_sh(y, n, "null y");
+        need_sh((const void* const*)eq, n, "null eq");
+        need_sh((const void* const*)gt, n, "null gt");
+        orqcu::op_compare(rt->ctx, width, n, c3(x), c3(y), m3(eq), m3(gt));
+    });
+}
+
+int orqcu_bitonic_sort(orqcu_runtime* rt, int width, size_t n, void* const key[3],
+                       int descending) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "bitonic sort supports 4 and 8-byte keys");
+        need((n & (n - 1)) == 0, "bitonic sort needs a power-of-two size");
+        need_sh((const void* const*)key, n, "null key");
+        orqcu::op_bitonic_sort(rt->ctx, width, n, m3(key), descending != 0);
+    });
+}
+
 }  // extern "C"

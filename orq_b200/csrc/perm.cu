@@ -83,7 +83,7 @@ struct FyGenArgs {
 constexpr int kHalfBlocks = kBlocksPerThread / 2;  // blocks per thread per half tile
 
 __global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t red[33];
     __shared__ uint32_t sdone;
     __shared__ uint32_t sbase[kMaxLevels];
@@ -928,7 +928,7 @@ __global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
     constexpr int E = 16 / WMIN;
     constexpr int B1 = E * W1 / 16;
     constexpr int B2 = W2 ? E * W2 / 16 : 1;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const unsigned long long units = ceil_div(a.n, E);

@@ -25,7 +25,7 @@ __device__ __forceinline__ uint4 lsb_mask() {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kAesThreads) k_keystream(StreamArg st, uint8_t* out,
                                                            unsigned long long nbytes) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const unsigned long long nblk = ceil_div(nbytes, 16);
@@ -39,7 +39,7 @@ template <int W, bool ARITH>
 __global__ void __launch_bounds__(kAesThreads)
     k_share(const uint8_t* data, void* s1, void* s2, void* s3, StreamArg st,
             unsigned long long chunks, unsigned long long nbytes) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     StreamArg st2 = st;
@@ -69,7 +69,7 @@ struct MultArgs {
 template <int W, bool ARITH>
 __global__ void __launch_bounds__(kAesThreads) k_mult(MultArgs a) {
     using Sh = Share<W, ARITH>;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const unsigned long long nblk = ceil_div(a.nbytes, 16);
@@ -109,7 +109,7 @@ struct B2AArgs {
 template <int W>
 __global__ void __launch_bounds__(kAesThreads) k_b2a(B2AArgs a) {
     using R = Ring<W>;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const uint4 one = lsb_mask<W>();
@@ -154,7 +154,7 @@ template <int W, bool ARITH>
 __global__ void __launch_bounds__(kAesThreads)
     k_reshare(void* s0, void* s1, void* s2, StreamArg g, unsigned long long chunks,
               unsigned long long nbytes) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     StreamArg g2 = g;
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kAesThreads)
     k_zero(void* r0o, void* r1o, void* r2o, StreamArg p0, StreamArg p1, StreamArg p2,
            unsigned long long nbytes) {
     using Sh = Share<W, ARITH>;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const unsigned long long nblk = ceil_div(nbytes, 16);

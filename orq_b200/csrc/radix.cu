@@ -38,7 +38,7 @@ struct RadixB2AArgs {
 template <int PW>
 __global__ void __launch_bounds__(kAesThreads) k_radix_b2a(RadixB2AArgs a) {
     using R = Ring<4>;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const unsigned long long units = ceil_div(a.n, 4);
@@ -174,7 +174,7 @@ struct PermMulArgs {
 // s1 -= s0 ; f1 *= s1 (multiply_a) ; s0 += f1  (radixsort.h:183-185)
 __global__ void __launch_bounds__(kAesThreads) k_radix_perm(PermMulArgs a) {
     using R = Ring<4>;
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const unsigned long long units = ceil_div(a.n, 4), nbytes = a.n * 4;

@@ -175,4 +175,8 @@ void op_prefix_sum_noalloc(Ctx& c, int w, size_t n, Sh3 s);
 // ---- sorting (radix.cu) ----
 void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out /*int32*/);
 
+// ---- compare circuit and bitonic sort (cmp.cu) ----
+void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt);
+void op_bitonic_sort(Ctx& c, int w, size_t n, Sh3 key, bool desc);
+
 }  // namespace orqcu

@@ -38,6 +38,13 @@ CASES = [
     ("radix_n64_b64", "radix", 64, 5, 4, 64, True),
     ("radix_n20000_b40", "radix", 20000, 9, 5, 40, False),
     ("shuffle_n1000", "shuffle", 1000, 7, 6, 40, True),
+    ("compare32_n1000", "compare32", 1000, 7, 2, 32, True),
+    ("compare64_n333", "compare64", 333, 8, 3, 64, True),
+    ("compare32_n100000", "compare32", 100000, 9, 4, 32, False),
+    ("bitonic32_n256", "bitonic32", 256, 7, 2, 32, True),
+    ("bitonic64_n64", "bitonic64", 64, 5, 3, 64, True),
+    ("bitonic32_desc_n128", "bitonic32_desc", 128, 6, 4, 32, True),
+    ("bitonic32_n4096", "bitonic32", 4096, 10, 5, 32, False),
 ]
 
 

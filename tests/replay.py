@@ -46,6 +46,12 @@ class OracleBackend:
         perm = self.o.radix_sort(key, bits, payloads)
         return perm
 
+    def compare(self, x, y):
+        return self.o.compare(x, y)
+
+    def bitonic(self, key, desc):
+        self.o.bitonic_sort(key, desc)
+
 
 class GpuBackend:
     def __init__(self, seed, device=0):
@@ -84,6 +90,12 @@ class GpuBackend:
         for p in payloads:
             self.orq.oblivious_apply_elementwise_perm(p, perm)
         return perm
+
+    def compare(self, x, y):
+        return x._compare(y)
+
+    def bitonic(self, key, desc):
+        self.orq.bitonic_sort(key, self.orq.DESC if desc else self.orq.ASC)
 
 
 def prim_inputs(n, seed, dt):
@@ -137,6 +149,34 @@ def replay_radix(be, n, seed, bits):
     out["open_pay1"] = be.open(a1, True)[None]
     out["open_pay2"] = be.open(a2, True)[None]
     return out, (key, p1, p2)
+
+
+def compare_inputs(n, seed, dt):
+    """x, y uniform over all bits; every fourth pair equal."""
+    x, y = prim_inputs(n, seed, dt)
+    y[::4] = x[::4]
+    return x, y
+
+
+def replay_compare(be, n, seed, w):
+    """The "compare32"/"compare64" op of ref_driver.cpp: x._compare(y)."""
+    x, y = compare_inputs(n, seed, _U[w])
+    xb = be.share(x, False, 0)
+    yb = be.share(y, False, 1)
+    eq, gt = be.compare(xb, yb)
+    out = {"xb": be.np(xb), "yb": be.np(yb), "eq": be.np(eq), "gt": be.np(gt)}
+    out["open_eq"] = be.open(eq, False)[None]
+    out["open_gt"] = be.open(gt, False)[None]
+    return out, (x, y)
+
+
+def replay_bitonic(be, n, seed, w, desc=False):
+    """The "bitonic32"/"bitonic64"/"bitonic32_desc" ops of ref_driver.cpp."""
+    key = splitmix64_fast(seed, n).astype(_U[w])
+    kb = be.share(key, False, 0)
+    be.bitonic(kb, desc)
+    out = {"key": be.np(kb), "open_key": be.open(kb, False)[None]}
+    return out, key
 
 
 def same(a, b):

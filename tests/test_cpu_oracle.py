@@ -9,7 +9,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from replay import OracleBackend, replay_prims, replay_radix, same
+from replay import OracleBackend, replay_bitonic, replay_compare, replay_prims, replay_radix, same
 
 
 def sha(a):
@@ -90,3 +90,42 @@ def test_gen_perm_is_a_permutation(oracle_lib):
         p, draws = o.gen_perm(G01, n)
         assert sorted(p.tolist()) == list(range(n))
         assert draws >= n
+
+
+@pytest.mark.parametrize("tag,w", [("compare32_n1000", 4), ("compare64_n333", 8)])
+def test_compare_matches_reference_shares(oracle_lib, golden, digests, tag, w):
+    m = digests[tag]["meta"]
+    out, (x, y) = replay_compare(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    sd = {4: np.int32, 8: np.int64}[w]
+    assert np.array_equal(out["open_eq"][0], (x == y).astype(x.dtype))
+    assert np.array_equal(out["open_gt"][0], (x.view(sd) > y.view(sd)).astype(x.dtype))
+
+
+def test_compare_large_matches_reference_digests(oracle_lib, digests):
+    d = digests["compare32_n100000"]
+    m = d["meta"]
+    out, _ = replay_compare(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 4)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag,w,desc", [("bitonic32_n256", 4, False), ("bitonic64_n64", 8, False),
+                                        ("bitonic32_desc_n128", 4, True)])
+def test_bitonic_matches_reference_shares(oracle_lib, golden, digests, tag, w, desc):
+    m = digests[tag]["meta"]
+    out, key = replay_bitonic(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], w, desc)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    sd = {4: np.int32, 8: np.int64}[w]
+    want = np.sort(key.view(sd))
+    assert same(out["open_key"][0].view(sd), want[::-1] if desc else want)
+
+
+def test_bitonic_large_matches_reference_digests(oracle_lib, digests):
+    d = digests["bitonic32_n4096"]
+    m = d["meta"]
+    out, _ = replay_bitonic(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 4)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name

@@ -8,7 +8,8 @@ import hashlib
 import numpy as np
 import pytest
 
-from replay import GpuBackend, OracleBackend, radix_inputs, replay_prims, replay_radix, same
+from replay import (GpuBackend, OracleBackend, radix_inputs, replay_bitonic, replay_compare,
+                    replay_prims, replay_radix, same)
 
 pytestmark = pytest.mark.gpu
 
@@ -170,3 +171,110 @@ def test_prefix_sum_matches_restatement(orq, w, n):
     assert same(v.shares.cpu().numpy().view(dt), np.stack(s))
     with np.errstate(over="ignore"):
         assert same(v.open().cpu().numpy().view(dt), np.cumsum(data, dtype=dt))
+
+
+@pytest.mark.parametrize("tag,w", [("compare32_n1000", 4), ("compare64_n333", 8)])
+def test_compare_matches_reference_shares(orq, golden, digests, tag, w):
+    m = digests[tag]["meta"]
+    out, _ = replay_compare(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+def test_compare_large_matches_reference_digests(orq, digests):
+    d = digests["compare32_n100000"]
+    m = d["meta"]
+    out, _ = replay_compare(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], 4)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("w", [4, 8])
+@pytest.mark.parametrize("n", [1, 31, 32, 33, 64, 65, 383, 385, 4097, 300001])
+def test_compare_matches_restatement(orq, w, n):
+    """ragged warps and packed words, and draws of more than one 1 MiB chunk"""
+    gpu, (x, y) = replay_compare(GpuBackend(41), n, 5, w)
+    cpu, _ = replay_compare(OracleBackend(41), n, 5, w)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), (n, w, k)
+    sd = {4: np.int32, 8: np.int64}[w]
+    assert np.array_equal(gpu["open_gt"][0], (x.view(sd) > y.view(sd)).astype(x.dtype))
+
+
+@pytest.mark.parametrize("tag,w,desc", [("bitonic32_n256", 4, False), ("bitonic64_n64", 8, False),
+                                        ("bitonic32_desc_n128", 4, True)])
+def test_bitonic_matches_reference_shares(orq, golden, digests, tag, w, desc):
+    m = digests[tag]["meta"]
+    out, _ = replay_bitonic(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], w, desc)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+def test_bitonic_large_matches_reference_digests(orq, digests):
+    d = digests["bitonic32_n4096"]
+    m = d["meta"]
+    out, _ = replay_bitonic(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], 4)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("w", [4, 8])
+@pytest.mark.parametrize("desc", [False, True])
+@pytest.mark.parametrize("n", [1, 2, 4, 64, 128, 1024, 1 << 16])
+def test_bitonic_matches_restatement(orq, w, desc, n):
+    gpu, key = replay_bitonic(GpuBackend(43), n, 6, w, desc)
+    cpu, _ = replay_bitonic(OracleBackend(43), n, 6, w, desc)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), (n, w, desc, k)
+
+
+def test_bitonic_full_size_properties(orq):
+    """2^20 int32 keys: opened output is the sorted input (signed order)."""
+    n = 1 << 20
+    out, key = replay_bitonic(GpuBackend(7), n, 3, 4)
+    assert same(out["open_key"][0].view(np.int32), np.sort(key.view(np.int32)))
+
+
+def test_bitonic_rejects_non_power_of_two(orq):
+    rt = orq.Runtime(seed=1)
+    v = rt.secret_share_b(np.arange(3, dtype=np.uint32), 0)
+    with pytest.raises(orq.OrqError):
+        orq.bitonic_sort(v)
+
+
+def test_bitonic_known_answers(orq):
+    """the sort vectors of the reference's own bitonic test (int keys)"""
+    rt = orq.Runtime(seed=2)
+    v = rt.secret_share_b(np.array([0, 5, 4, 7, -1, -2, 8, 1], dtype=np.int32), 0)
+    orq.bitonic_sort(v)
+    assert v.open().cpu().numpy().tolist() == [-2, -1, 0, 1, 4, 5, 7, 8]
+    orq.bitonic_sort(v, orq.DESC)
+    assert v.open().cpu().numpy().tolist() == [8, 7, 5, 4, 1, 0, -1, -2]
+    imax = 2**31 - 1
+    for big in (imax // 2, imax // 2 + 1):
+        x = np.array([0, big, -1, 42, 87, 100, -444, -13], dtype=np.int32)
+        v = rt.secret_share_b(x, 0)
+        orq.bitonic_sort(v)
+        assert v.open().cpu().numpy().tolist() == sorted(x.tolist())
+
+
+def test_compare_known_answers(orq):
+    """the comparison vectors of the reference's own bitonic test"""
+    rt = orq.Runtime(seed=3)
+    a = np.array([111, -14, 0, -156, 2**31 - 1, 18], dtype=np.int32)
+    b = np.array([98, -4, 0, 2847, -2**31, -4491], dtype=np.int32)
+    va, vb = rt.secret_share_b(a, 0), rt.secret_share_b(b, 0)
+    eq, gt = va._compare(vb)
+    assert eq.open().cpu().numpy().tolist() == (a == b).astype(int).tolist()
+    assert gt.open().cpu().numpy().tolist() == (a > b).astype(int).tolist()
+    assert (va < vb).open().cpu().numpy().tolist() == (a < b).astype(int).tolist()
+
+
+def test_bitonic_2p16_seed1(orq):
+    """2^16 keys drawn from seed 1 over all 32 bits, ascending; the opened
+    output equals the plaintext sorted in the keys' (signed int) order, and the
+    shares equal the restatement's."""
+    gpu, key = replay_bitonic(GpuBackend(1), 1 << 16, 1, 4)
+    assert same(gpu["open_key"][0].view(np.int32), np.sort(key.view(np.int32)))
+    cpu, _ = replay_bitonic(OracleBackend(1), 1 << 16, 1, 4)
+    assert same(gpu["key"], cpu["key"])
