@@ -38,6 +38,11 @@ WORKLOAD = ("3PC oblivious shuffle-based radix sort, 2^22 rows, uint64 key unifo
 # T-table AES-256: 16 shared-memory lookups per round x 14 rounds (+4 in the
 # last) = 228 LDS per block at one warp-wide LDS per clock per SM.
 AES_LDS_PER_BLOCK = 228
+# DRAM traffic of the dominant k_apply instance (padded 16-byte key + int32
+# permutation, one group), dram__bytes_read.sum + dram__bytes_write.sum from
+# one ncu capture at 2^21 rows (profiles/radix_sort_2p22.md): 729 MB, scaled
+# per row to the benchmarked size.
+APPLY_TRAFFIC_BYTES_PER_ROW = 729.0e6 / (1 << 21)
 
 
 def load_peaks():
@@ -232,7 +237,7 @@ def run_orq(args, rank, world, local_rank):
     return ms, launches, prof, clk, e2e, ok
 
 
-def roofline(prof, steps):
+def roofline(prof, steps, n):
     hbm, sm_mhz, src = load_peaks()
     # dominant kernel by device time among the ones accounted in bytes
     mem = {k: v for k, v in prof.items() if v["bytes"] > 0}
@@ -243,7 +248,9 @@ def roofline(prof, steps):
         per_launch_ms = v["ms"] / v["launches"]
         ach = (v["bytes"] / v["launches"]) / (per_launch_ms / 1e3) / 1e9
         out["roofline"] = {"bound": "hbm", "kernel": name, "achieved": round(ach, 1), "peak": hbm,
-                           "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": None,
+                           "unit": "GB/s", "frac": round(ach / hbm, 4),
+                           "traffic": (round(APPLY_TRAFFIC_BYTES_PER_ROW * n) if name == "apply_group" else None),
+                           "traffic_note": "bytes per launch of the key-apply instance, ncu at 2^21 rows scaled by rows",
                            "peak_source": src, "launches_per_step": v["launches"] / steps,
                            "avg_launch_ms": round(per_launch_ms, 4)}
     aes = {k: v for k, v in prof.items() if v["aes_blocks"] > 0}
@@ -328,7 +335,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": config,
         "correct": ok, "gpu_launches": launches, "clocks": clk,
     }
-    line.update(roofline(prof, args.steps))
+    line.update(roofline(prof, args.steps, args.n))
     if e2e:
         line["e2e"] = e2e
     if not args.no_cpu_baseline and world == 1:

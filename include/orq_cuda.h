@@ -170,6 +170,35 @@ int orqcu_compare_b(orqcu_runtime* rt, int width, size_t n, const void* const x[
 int orqcu_bitonic_sort(orqcu_runtime* rt, int width, size_t n, void* const key[3],
                        int descending);
 
+/* Aggregation functions (aggregation.h:27-140). */
+enum {
+    ORQCU_AGG_SUM = 0,    /* arithmetic: a + g*b */
+    ORQCU_AGG_COUNT = 1,  /* arithmetic: sum over ones (or b2a_bit(sel) inside joins) */
+    ORQCU_AGG_COPY = 2,   /* arithmetic or boolean: multiplex(g, a, b) */
+    ORQCU_AGG_VALID = 3,  /* boolean: multiplex(g, a, a & b) */
+    ORQCU_AGG_BIT_OR = 4, /* boolean: a | (ext(g) & b) */
+    ORQCU_AGG_MIN = 5,
+    ORQCU_AGG_MAX = 6
+};
+/* One aggregation: input column, output column (3 share pointers each), and
+ * the function. The output is overwritten (out = in first, as the reference). */
+typedef struct {
+    const void* in[3];
+    void* out[3];
+    int func;
+} orqcu_agg_spec;
+/* orq::aggregators::aggregate (aggregation.h:167-346): the odd-even
+ * aggregation network over n rows (a power of two) of width-byte shares (4 or
+ * 8). keys: nkeys B-shared key columns, 3 pointers each (keys[3*j+p]); b_specs
+ * are boolean aggregations (copy, valid, bit_or), a_specs arithmetic ones
+ * (sum, count, copy); reverse selects Direction::Reverse; sel (3 pointers, or
+ * NULL) is the table-id column that restricts non-copy aggregations to rows of
+ * the same table. One fused launch per network level; at most 4 keys and 8
+ * specs of each kind. min/max return ORQCU_EINVAL on the device path. */
+int orqcu_aggregate(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* keys,
+                    int nb, const orqcu_agg_spec* b_specs, int na, const orqcu_agg_spec* a_specs,
+                    int reverse, const void* const* sel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,10 @@ def splitmix64_fast(seed: int, n: int) -> np.ndarray:
         return z ^ (z >> np.uint64(31))
 
 
+# aggregation function codes (orq_oracle.h)
+AGG_SUM, AGG_COUNT, AGG_COPY, AGG_VALID, AGG_BIT_OR, AGG_MIN, AGG_MAX = range(7)
+
+
 class _Ctx(ctypes.Structure):
     _fields_ = [("rk", (ctypes.c_uint32 * 60) * 10), ("nonce", ctypes.c_uint64 * 10)]
 
@@ -168,6 +172,23 @@ class Oracle:
         self.lib.oro_compare(ctypes.byref(self.ctx), w, ctypes.c_size_t(n), self._ptrs(x), self._ptrs(y),
                              self._ptrs(eq), self._ptrs(gt))
         return eq, gt
+
+    def aggregate(self, keys, b_specs, a_specs, reverse=False, sel=None):
+        """orq::aggregators::aggregate; specs are (input shares, function code);
+        returns the output shares of the boolean and arithmetic specs."""
+        w = (keys[0] if keys else (b_specs or a_specs)[0][0])[0].dtype.itemsize
+        n = len((keys[0] if keys else (b_specs or a_specs)[0][0])[0])
+        flat = lambda arrs: (ctypes.c_void_p * max(1, 3 * len(arrs)))(
+            *[x.ctypes.data for a in arrs for x in a])
+        b_out = [self.new(n, w) for _ in b_specs]
+        a_out = [self.new(n, w) for _ in a_specs]
+        bf = (ctypes.c_int * max(1, len(b_specs)))(*[f for _, f in b_specs])
+        af = (ctypes.c_int * max(1, len(a_specs)))(*[f for _, f in a_specs])
+        self.lib.oro_aggregate(ctypes.byref(self.ctx), w, ctypes.c_size_t(n), len(keys), flat(keys),
+                               len(b_specs), flat([i for i, _ in b_specs]), flat(b_out), bf,
+                               len(a_specs), flat([i for i, _ in a_specs]), flat(a_out), af,
+                               int(reverse), self._ptrs(sel) if sel is not None else None)
+        return b_out, a_out
 
     def bitonic_sort(self, key, desc=False):
         w = key[0].dtype.itemsize

@@ -7,6 +7,7 @@
  */
 #include "orq_oracle.h"
 
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #if defined(__x86_64__)
@@ -890,4 +891,255 @@ void oro_bitonic_sort(oro_ctx* c, int w, size_t n, void* key[3], int desc) {
     }
     free(xi);
     free(yi);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Aggregation network (operators/aggregation.h:27-140,167-346). */
+
+static void** sl3(void* const s[3], size_t off, int w, void* out[3]) {
+    for (int j = 0; j < 3; j++) out[j] = (uint8_t*)s[j] + off * (size_t)w;
+    return out;
+}
+static void alloc3(void* v[3], size_t n, int w) {
+    for (int j = 0; j < 3; j++) v[j] = xalloc(n * (size_t)w + 16);
+}
+static void free3(void* v[3]) {
+    for (int j = 0; j < 3; j++) free(v[j]);
+}
+static void copy3(void* dst[3], void* const src[3], size_t n, int w) {
+    for (int j = 0; j < 3; j++) memmove(dst[j], src[j], n * (size_t)w);
+}
+/* public constant 1 repeated (public_share: S0 = 1, S1 = S2 = 0) */
+static void one3(void* v[3], size_t n, int w) {
+    for (size_t i = 0; i < n; i++) {
+        st(v[0], i, w, 1);
+        st(v[1], i, w, 0);
+        st(v[2], i, w, 0);
+    }
+}
+/* extend_lsb: every share becomes -(s & 1) */
+static void ext3(void* dst[3], void* const src[3], size_t n, int w) {
+    for (int j = 0; j < 3; j++)
+        for (size_t i = 0; i < n; i++) st(dst[j], i, w, (ld(src[j], i, w) & 1) ? ~(u128)0 : 0);
+}
+static void not3(void* v[3], size_t n, int w) {
+    for (int j = 0; j < 3; j++)
+        for (size_t i = 0; i < n; i++) st(v[j], i, w, ~ld(v[j], i, w));
+}
+static void mask3(void* v[3], size_t n, int w, u128 m) {
+    for (int j = 0; j < 3; j++)
+        for (size_t i = 0; i < n; i++) st(v[j], i, w, ld(v[j], i, w) & m);
+}
+/* operator== : bit_same then mask(1) (b_shared_vector.h:164-178,493-504) */
+static void eq3(oro_ctx* c, int w, size_t m, void* const x[3], void* const y[3], void* out[3]) {
+    const int B = 8 * w;
+    int L = 0;
+    while ((1 << L) < B) L++;
+    const u128 M = wmask(w);
+    void* T[3];
+    alloc3(T, m, w);
+    for (int j = 0; j < 3; j++)
+        for (size_t p = 0; p < m; p++) st(out[j], p, w, ~(ld(x[j], p, w) ^ ld(y[j], p, w)) & M);
+    for (int lev = 0; lev < L; lev++) {
+        for (int j = 0; j < 3; j++)
+            for (size_t p = 0; p < m; p++) st(T[j], p, w, ashr(ld(out[j], p, w), w, 1 << lev) & M);
+        oro_and_b(c, w, m, out, T, out);
+    }
+    mask3(out, m, w, 1);
+    free3(T);
+}
+/* multiplex(sel, a, b) = a ^ (ext(sel) & (b ^ a)) (operators/common.h:20-28) */
+static void mux_b(oro_ctx* c, int w, size_t m, void* const sel[3], void* const a[3],
+                  void* const b[3], void* res[3]) {
+    void* E[3];
+    void* D[3];
+    alloc3(E, m, w);
+    alloc3(D, m, w);
+    ext3(E, sel, m, w);
+    oro_xor_b(w, m, b, a, D);
+    oro_and_b(c, w, m, E, D, D);
+    oro_xor_b(w, m, a, D, res);
+    free3(E);
+    free3(D);
+}
+
+/* func(g, a, b) for the boolean aggregations; writes the new a to res */
+static void agg_b(oro_ctx* c, int func, int w, size_t m, void* const g[3], void* const a[3],
+                  void* const b[3], void* res[3]) {
+    void* t[3];
+    alloc3(t, m, w);
+    switch (func) {
+        case ORO_AGG_COPY:
+            mux_b(c, w, m, g, a, b, res);
+            break;
+        case ORO_AGG_VALID: /* agg = a & b ; a = multiplex(g, a, agg) */
+            oro_and_b(c, w, m, a, b, t);
+            mux_b(c, w, m, g, a, t, res);
+            break;
+        case ORO_AGG_BIT_OR: { /* a | (ext(g) & b), | = ~(~a & ~x) */
+            void* na[3];
+            alloc3(na, m, w);
+            ext3(t, g, m, w);
+            oro_and_b(c, w, m, t, b, t);
+            copy3(na, a, m, w);
+            not3(na, m, w);
+            not3(t, m, w);
+            oro_and_b(c, w, m, na, t, res);
+            not3(res, m, w);
+            free3(na);
+            break;
+        }
+        case ORO_AGG_MAX:
+        case ORO_AGG_MIN: { /* bg = b > a (! for min); a = mux(g, a, mux(bg, a, b)) */
+            void* eq[3];
+            void* gt[3];
+            alloc3(eq, m, w);
+            alloc3(gt, m, w);
+            oro_compare(c, w, m, b, a, eq, gt);
+            if (func == ORO_AGG_MIN)
+                for (int j = 0; j < 3; j++)
+                    for (size_t i = 0; i < m; i++) st(gt[j], i, w, (ld(gt[j], i, w) & 1) ^ 1);
+            mux_b(c, w, m, gt, a, b, t);
+            mux_b(c, w, m, g, a, t, res);
+            free3(eq);
+            free3(gt);
+            break;
+        }
+        default:
+            fprintf(stderr, "oro_aggregate: bad boolean aggregation %d\n", func);
+            abort();
+    }
+    free3(t);
+}
+
+/* func(g, a, b) for the arithmetic aggregations: sum/count a + g*b, copy
+ * a + g*(b - a) */
+static void agg_a(oro_ctx* c, int func, int w, size_t m, void* const g[3], void* const a[3],
+                  void* const b[3], void* res[3]) {
+    void* t[3];
+    alloc3(t, m, w);
+    if (func == ORO_AGG_COPY) {
+        oro_sub_a(w, m, b, a, t);
+        oro_mul_a(c, w, m, g, t, t);
+    } else {
+        oro_mul_a(c, w, m, g, b, t);
+    }
+    oro_add_a(w, m, a, t, res);
+    free3(t);
+}
+
+void oro_aggregate(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, int nb,
+                   void* const* b_in, void* const* b_out, const int* b_func, int na,
+                   void* const* a_in, void* const* a_out, const int* a_func, int reverse,
+                   void* const* sel) {
+    int a_copy = 0, a_noncopy = 0, b_copy = 0, b_noncopy = 0;
+    (void)b_copy;
+    for (int s = 0; s < na; s++) {
+        void* out[3] = {a_out[3 * s], a_out[3 * s + 1], a_out[3 * s + 2]};
+        if (a_func[s] == ORO_AGG_COUNT) {
+            if (sel) oro_b2a_bit(c, w, n, sel, out);
+            else one3(out, n, w);
+        } else {
+            void* in[3] = {a_in[3 * s], a_in[3 * s + 1], a_in[3 * s + 2]};
+            copy3(out, in, n, w);
+        }
+        if (a_func[s] == ORO_AGG_COPY) a_copy = 1;
+        else a_noncopy = 1;
+    }
+    for (int s = 0; s < nb; s++) {
+        void* out[3] = {b_out[3 * s], b_out[3 * s + 1], b_out[3 * s + 2]};
+        void* in[3] = {b_in[3 * s], b_in[3 * s + 1], b_in[3 * s + 2]};
+        copy3(out, in, n, w);
+        if (b_func[s] == ORO_AGG_COPY) b_copy = 1;
+        else b_noncopy = 1;
+    }
+    int log_size = 0;
+    while (((size_t)2 << log_size) <= n) log_size++;
+    for (int i = 1; i <= log_size; i++) {
+        size_t d = n >> i;
+        if (reverse) d = n >> (log_size - i + 1);
+        const size_t dr = n - d;
+        void *G[3], *JG[3], *GA[3], *JGA[3], *X[3], *Y[3], *R[3], *E[3];
+        alloc3(G, dr, w);
+        alloc3(JG, dr, w);
+        alloc3(GA, dr, w);
+        alloc3(JGA, dr, w);
+        alloc3(X, dr, w);
+        alloc3(Y, dr, w);
+        alloc3(R, dr, w);
+        alloc3(E, dr, w);
+        if (nkeys == 0) {
+            one3(G, dr, w);
+            one3(GA, dr, w);
+        } else {
+            for (int k = 0; k < nkeys; k++) {
+                void* kk[3] = {keys[3 * k], keys[3 * k + 1], keys[3 * k + 2]};
+                void *lo[3], *hi[3];
+                sl3(kk, 0, w, lo);
+                sl3(kk, d, w, hi);
+                if (k == 0) {
+                    eq3(c, w, dr, lo, hi, G);
+                } else {
+                    eq3(c, w, dr, lo, hi, E);
+                    oro_and_b(c, w, dr, G, E, G);
+                }
+            }
+            for (int j = 0; j < 3; j++) memset(GA[j], 0, dr * (size_t)w);
+        }
+        copy3(JG, G, dr, w);
+        copy3(JGA, GA, dr, w);
+        if (sel && (a_noncopy || b_noncopy)) {
+            void *lo[3], *hi[3];
+            sl3(sel, 0, w, lo);
+            sl3(sel, d, w, hi);
+            oro_xor_b(w, dr, hi, lo, E);
+            not3(E, dr, w);
+            oro_and_b(c, w, dr, G, E, G);
+        }
+        mask3(G, dr, w, 1);
+        for (int s = 0; s < nb; s++) {
+            void* out[3] = {b_out[3 * s], b_out[3 * s + 1], b_out[3 * s + 2]};
+            void *lo[3], *hi[3];
+            sl3(out, 0, w, lo);
+            sl3(out, d, w, hi);
+            copy3(X, lo, dr, w);
+            copy3(Y, hi, dr, w);
+            void** g = b_func[s] == ORO_AGG_COPY ? JG : G;
+            if (reverse) {
+                agg_b(c, b_func[s], w, dr, g, Y, X, R);
+                copy3(hi, R, dr, w);
+            } else {
+                agg_b(c, b_func[s], w, dr, g, X, Y, R);
+                copy3(lo, R, dr, w);
+            }
+        }
+        if (nkeys > 0 && na > 0) {
+            if (a_noncopy) oro_b2a_bit(c, w, dr, G, GA);
+            if (a_copy) oro_b2a_bit(c, w, dr, JG, JGA);
+        }
+        for (int s = 0; s < na; s++) {
+            void* out[3] = {a_out[3 * s], a_out[3 * s + 1], a_out[3 * s + 2]};
+            void *lo[3], *hi[3];
+            sl3(out, 0, w, lo);
+            sl3(out, d, w, hi);
+            copy3(X, lo, dr, w);
+            copy3(Y, hi, dr, w);
+            void** g = a_func[s] == ORO_AGG_COPY ? JGA : GA;
+            if (reverse) {
+                agg_a(c, a_func[s], w, dr, g, Y, X, R);
+                copy3(hi, R, dr, w);
+            } else {
+                agg_a(c, a_func[s], w, dr, g, X, Y, R);
+                copy3(lo, R, dr, w);
+            }
+        }
+        free3(G);
+        free3(JG);
+        free3(GA);
+        free3(JGA);
+        free3(X);
+        free3(Y);
+        free3(R);
+        free3(E);
+    }
 }

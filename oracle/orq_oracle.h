@@ -105,6 +105,18 @@ void oro_compare(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3]
  * place; n a power of two. */
 void oro_bitonic_sort(oro_ctx* c, int w, size_t n, void* key[3], int desc);
 
+/* aggregation functions (operators/aggregation.h:27-140) */
+enum { ORO_AGG_SUM = 0, ORO_AGG_COUNT = 1, ORO_AGG_COPY = 2, ORO_AGG_VALID = 3, ORO_AGG_BIT_OR = 4,
+       ORO_AGG_MIN = 5, ORO_AGG_MAX = 6 };
+/* orq::aggregators::aggregate (aggregation.h:167-346) over n (a power of two)
+ * rows of w-byte shares: keys are nkeys B-shared columns (3 pointers each),
+ * b_in/b_out/b_func the boolean specs (copy/valid/bit_or/min/max), a_in/a_out/
+ * a_func the arithmetic specs (sum/count/copy); sel (3 pointers) or NULL. */
+void oro_aggregate(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, int nb,
+                   void* const* b_in, void* const* b_out, const int* b_func, int na,
+                   void* const* a_in, void* const* a_out, const int* a_func, int reverse,
+                   void* const* sel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,7 @@
 // usage: ref_driver <threads> <p_factor> <batch> <op> <n> <data_seed> <outdir> [bits]
 //   threads=1 and batch=-1 give one protocol call per runtime operation, the
 //   schedule the device runtime reproduces.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -198,6 +199,66 @@ int main(int argc, char** argv) {
         };
         if (op == "compare32") run(int32_t{});
         else run(int64_t{});
+    } else if (op == "agg_fwd" || op == "agg_rev" || op == "agg_nokey") {
+        // orq::aggregators::aggregate over n (power of two) int64 rows.
+        // key0: sorted, values in [0, n/4]; key1 (agg_rev): sorted within
+        // key0 runs, values in {0, 1}; sel (agg_rev): random table-id bits.
+        // A specs: sum, count, copy; B specs: copy, valid, bit_or, max, min.
+        using B = BSharedVector<int64_t>;
+        using A = ASharedVector<int64_t>;
+        namespace ag = orq::aggregators;
+        uint64_t st = seed;
+        std::vector<std::pair<int64_t, int64_t>> kv(n);
+        for (size_t i = 0; i < n; i++)
+            kv[i] = {(int64_t)(sm64(st) % (n / 4 + 1)), (int64_t)(sm64(st) & 1)};
+        std::sort(kv.begin(), kv.end());
+        orq::Vector<int64_t> k0(n), k1(n);
+        for (size_t i = 0; i < n; i++) {
+            k0[i] = kv[i].first;
+            k1[i] = kv[i].second;
+        }
+        auto va1 = gen<int64_t>(n, st, 0xffffffffull);
+        auto va3 = gen<int64_t>(n, st, 0xffffffffull);
+        auto vb1 = gen<int64_t>(n, st, ~0ull);
+        auto vb2 = gen<int64_t>(n, st, 1);
+        auto vb3 = gen<int64_t>(n, st, ~0ull);
+        auto vb4 = gen<int64_t>(n, st, ~0ull);
+        auto vb5 = gen<int64_t>(n, st, ~0ull);
+        auto sv = gen<int64_t>(n, st, 1);
+        std::vector<B> keys;
+        if (op != "agg_nokey") keys.push_back(secret_share_b(k0, 0));
+        if (op == "agg_rev") keys.push_back(secret_share_b(k1, 0));
+        A a1 = secret_share_a(va1, 0), a3 = secret_share_a(va3, 0);
+        B b1 = secret_share_b(vb1, 0), b2 = secret_share_b(vb2, 0), b3 = secret_share_b(vb3, 0);
+        B b4 = secret_share_b(vb4, 0), b5 = secret_share_b(vb5, 0);
+        B sel = secret_share_b(sv, 0);
+        A o1(n), o2(n), o3(n);
+        B q1(n), q2(n), q3(n), q4(n), q5(n);
+        std::vector<std::tuple<B, B, void (*)(const B&, B&, const B&)>> bs = {
+            {b1, q1, &ag::copy<B>}, {b2, q2, &ag::valid<B>}, {b3, q3, &ag::bit_or<B>},
+            {b4, q4, &ag::max<B>}, {b5, q5, &ag::min<B>}};
+        std::vector<std::tuple<A, A, void (*)(const A&, A&, const A&)>> as = {
+            {a1, o1, &ag::sum<A>}, {a1, o2, &ag::count<A>}, {a3, o3, &ag::copy<A>}};
+        if (op == "agg_nokey") {
+            bs.erase(bs.begin() + 1, bs.end());
+            as.erase(as.begin() + 1, as.end());
+        }
+        if (op == "agg_rev")
+            ag::aggregate(keys, bs, as, ag::Direction::Reverse, std::optional<B>(sel));
+        else
+            ag::aggregate(keys, bs, as, ag::Direction::Forward);
+        d.shares("o1", o1);
+        d.shares("q1", q1);
+        if (op != "agg_nokey") {
+            d.shares("o2", o2);
+            d.shares("o3", o3);
+            d.shares("q2", q2);
+            d.shares("q3", q3);
+            d.shares("q4", q4);
+            d.shares("q5", q5);
+        }
+        auto x1 = o1.open();
+        d.plain("open_o1", x1);
     } else if (op == "shuffle") {
         uint64_t st = seed;
         auto x = gen<int32_t>(n, st, ~0ull);

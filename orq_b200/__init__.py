@@ -359,6 +359,46 @@ def bitonic_sort(v: BSharedVector, order: int = ASC):
                                      int(order == DESC)))
 
 
+class aggregators:
+    """Aggregation functions of orq::aggregators (aggregation.h:27-140), as the
+    codes orqcu_aggregate takes."""
+    sum, count, copy, valid, bit_or, min, max = range(7)
+
+
+class Direction:
+    Forward, Reverse = 0, 1
+
+
+class _AggSpec(ctypes.Structure):
+    _fields_ = [("inp", ctypes.c_void_p * 3), ("out", ctypes.c_void_p * 3), ("func", ctypes.c_int)]
+
+
+def aggregate(keys, agg_spec_b, agg_spec_a, direction: int = Direction.Forward, sel=None):
+    """orq::aggregators::aggregate (aggregation.h:167-346). keys: list of
+    BSharedVector; agg_spec_b / agg_spec_a: lists of (input, output, function)
+    with BSharedVector / ASharedVector columns; sel: optional BSharedVector
+    (table id) restricting non-copy aggregations to rows of one table. The
+    outputs are overwritten in place."""
+    first = keys[0] if keys else (agg_spec_b or agg_spec_a)[0][1]
+    rt, n, w = first.rt, first.size(), first.width
+    kp = (ctypes.c_void_p * max(1, 3 * len(keys)))(*[k.shares[j].data_ptr() for k in keys for j in range(3)])
+
+    def specs(lst):
+        arr = (_AggSpec * max(1, len(lst)))()
+        for i, (inp, out, f) in enumerate(lst):
+            src = inp if inp is not None else out
+            for j in range(3):
+                arr[i].inp[j] = src.shares[j].data_ptr()
+                arr[i].out[j] = out.shares[j].data_ptr()
+            arr[i].func = int(f)
+        return arr
+
+    sp = _p3(sel.shares) if sel is not None else None
+    _check(rt.lib.orqcu_aggregate(rt.h, w, ctypes.c_size_t(n), len(keys), kp, len(agg_spec_b),
+                                  specs(agg_spec_b), len(agg_spec_a), specs(agg_spec_a),
+                                  int(direction == Direction.Reverse), sp))
+
+
 def radix_sort(v: BSharedVector, order: int = ASC, bits: int | None = None) -> ElementwisePermutation:
     """orq::operators::radix_sort (radixsort.h:205-229): sorts v in place and
     returns the A-shared sorting permutation."""

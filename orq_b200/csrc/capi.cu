@@ -381,4 +381,30 @@ int orqcu_bitonic_sort(orqcu_runtime* rt, int width, size_t n, void* const key[3
     });
 }
 
+int orqcu_aggregate(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* keys,
+                    int nb, const orqcu_agg_spec* b_specs, int na, const orqcu_agg_spec* a_specs,
+                    int reverse, const void* const* sel) {
+    static_assert(sizeof(orqcu_agg_spec) == sizeof(orqcu::AggSpec), "agg spec layout");
+    return guard([&] {
+        need_rt(rt);
+        need(nkeys >= 0 && nb >= 0 && na >= 0, "negative column count");
+        need(nkeys == 0 || keys != nullptr, "null keys");
+        need(nb == 0 || b_specs != nullptr, "null boolean specs");
+        need(na == 0 || a_specs != nullptr, "null arithmetic specs");
+        for (int j = 0; j < nkeys; j++) need_sh(keys + 3 * j, n, "null key share");
+        for (int s = 0; s < nb; s++) {
+            need_sh(b_specs[s].in, n, "null spec input");
+            need_sh((const void* const*)b_specs[s].out, n, "null spec output");
+        }
+        for (int s = 0; s < na; s++) {
+            if (a_specs[s].func != ORQCU_AGG_COUNT) need_sh(a_specs[s].in, n, "null spec input");
+            need_sh((const void* const*)a_specs[s].out, n, "null spec output");
+        }
+        if (sel) need_sh(sel, n, "null sel share");
+        orqcu::op_aggregate(rt->ctx, width, n, nkeys, keys, nb,
+                            reinterpret_cast<const orqcu::AggSpec*>(b_specs), na,
+                            reinterpret_cast<const orqcu::AggSpec*>(a_specs), reverse != 0, sel);
+    });
+}
+
 }  // extern "C"

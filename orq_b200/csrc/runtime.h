@@ -179,4 +179,14 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
 void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt);
 void op_bitonic_sort(Ctx& c, int w, size_t n, Sh3 key, bool desc);
 
+// ---- aggregation network (agg.cu) ----
+enum AggFunc { AGG_SUM = 0, AGG_COUNT = 1, AGG_COPY = 2, AGG_VALID = 3, AGG_BIT_OR = 4, AGG_MIN = 5, AGG_MAX = 6 };
+struct AggSpec {  // same layout as orqcu_agg_spec
+    const void* in[3];
+    void* out[3];
+    int func;
+};
+void op_aggregate(Ctx& c, int w, size_t n, int nkeys, const void* const* keys, int nb,
+                  const AggSpec* bs, int na, const AggSpec* as, bool reverse, const void* const* sel);
+
 }  // namespace orqcu

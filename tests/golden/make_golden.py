@@ -45,6 +45,11 @@ CASES = [
     ("bitonic64_n64", "bitonic64", 64, 5, 3, 64, True),
     ("bitonic32_desc_n128", "bitonic32_desc", 128, 6, 4, 32, True),
     ("bitonic32_n4096", "bitonic32", 4096, 10, 5, 32, False),
+    ("agg_fwd_n256", "agg_fwd", 256, 7, 2, 64, True),
+    ("agg_rev_n128", "agg_rev", 128, 8, 3, 64, True),
+    ("agg_nokey_n64", "agg_nokey", 64, 9, 4, 64, True),
+    ("agg_fwd_n4096", "agg_fwd", 4096, 11, 5, 64, False),
+    ("agg_rev_n4096", "agg_rev", 4096, 12, 6, 64, False),
 ]
 
 

@@ -49,6 +49,9 @@ class OracleBackend:
     def compare(self, x, y):
         return self.o.compare(x, y)
 
+    def aggregate(self, keys, bs, as_, reverse, sel):
+        return self.o.aggregate(keys, bs, as_, reverse, sel)
+
     def bitonic(self, key, desc):
         self.o.bitonic_sort(key, desc)
 
@@ -93,6 +96,16 @@ class GpuBackend:
 
     def compare(self, x, y):
         return x._compare(y)
+
+    def aggregate(self, keys, bs, as_, reverse, sel):
+        orq, rt = self.orq, self.rt
+        n = len((keys[0] if keys else (bs or as_)[0][0]))
+        bo = [orq.BSharedVector(rt, rt._alloc(n, x.width)) for x, _ in bs]
+        ao = [orq.ASharedVector(rt, rt._alloc(n, x.width)) for x, _ in as_]
+        orq.aggregate(keys, [(x, o, f) for (x, f), o in zip(bs, bo)],
+                      [(x, o, f) for (x, f), o in zip(as_, ao)],
+                      orq.Direction.Reverse if reverse else orq.Direction.Forward, sel)
+        return bo, ao
 
     def bitonic(self, key, desc):
         self.orq.bitonic_sort(key, self.orq.DESC if desc else self.orq.ASC)
@@ -177,6 +190,50 @@ def replay_bitonic(be, n, seed, w, desc=False):
     be.bitonic(kb, desc)
     out = {"key": be.np(kb), "open_key": be.open(kb, False)[None]}
     return out, key
+
+
+# aggregation function codes (the reference's aggregators, in this order)
+SUM, COUNT, COPY, VALID, BIT_OR, MIN, MAX = range(7)
+
+
+def agg_inputs(n, seed):
+    """Inputs of the "agg_*" ops of ref_driver.cpp: key0 sorted in [0, n/4],
+    key1 sorted within key0 runs, then A and B value columns and sel bits."""
+    st = splitmix64_fast(seed, 10 * n)
+    f = st[0:2 * n:2] % np.uint64(n // 4 + 1)
+    s2 = st[1:2 * n:2] & np.uint64(1)
+    order = np.lexsort((s2, f))
+    r = st[2 * n:]
+    cols = [r[i * n:(i + 1) * n] for i in range(8)]
+    m32 = np.uint64(0xFFFFFFFF)
+    return {"k0": f[order], "k1": s2[order], "va1": cols[0] & m32, "va3": cols[1] & m32,
+            "vb1": cols[2], "vb2": cols[3] & np.uint64(1), "vb3": cols[4], "vb4": cols[5],
+            "vb5": cols[6], "sel": cols[7] & np.uint64(1)}
+
+
+def replay_agg(be, op, n, seed):
+    """The "agg_fwd" / "agg_rev" / "agg_nokey" ops of ref_driver.cpp."""
+    x = agg_inputs(n, seed)
+    keys = []
+    if op != "agg_nokey":
+        keys.append(be.share(x["k0"], False, 0))
+    if op == "agg_rev":
+        keys.append(be.share(x["k1"], False, 0))
+    a1 = be.share(x["va1"], True, 0)
+    a3 = be.share(x["va3"], True, 0)
+    b = [be.share(x[k], False, 0) for k in ("vb1", "vb2", "vb3", "vb4", "vb5")]
+    sel = be.share(x["sel"], False, 0)
+    bs = [(b[0], COPY), (b[1], VALID), (b[2], BIT_OR), (b[3], MAX), (b[4], MIN)]
+    as_ = [(a1, SUM), (a1, COUNT), (a3, COPY)]
+    if op == "agg_nokey":
+        bs, as_ = bs[:1], as_[:1]
+    bo, ao = be.aggregate(keys, bs, as_, op == "agg_rev", sel if op == "agg_rev" else None)
+    out = {"o1": be.np(ao[0]), "q1": be.np(bo[0])}
+    if op != "agg_nokey":
+        out.update({"o2": be.np(ao[1]), "o3": be.np(ao[2]), "q2": be.np(bo[1]), "q3": be.np(bo[2]),
+                    "q4": be.np(bo[3]), "q5": be.np(bo[4])})
+    out["open_o1"] = be.open(ao[0], True)[None]
+    return out, x
 
 
 def same(a, b):

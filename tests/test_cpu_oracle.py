@@ -9,7 +9,8 @@ import hashlib
 import numpy as np
 import pytest
 
-from replay import OracleBackend, replay_bitonic, replay_compare, replay_prims, replay_radix, same
+from replay import (OracleBackend, replay_agg, replay_bitonic, replay_compare, replay_prims,
+                    replay_radix, same)
 
 
 def sha(a):
@@ -129,3 +130,33 @@ def test_bitonic_large_matches_reference_digests(oracle_lib, digests):
     out, _ = replay_bitonic(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 4)
     for name, arr in out.items():
         assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag,op", [("agg_fwd_n256", "agg_fwd"), ("agg_rev_n128", "agg_rev"),
+                                    ("agg_nokey_n64", "agg_nokey")])
+def test_aggregate_matches_reference_shares(oracle_lib, golden, digests, tag, op):
+    m = digests[tag]["meta"]
+    out, x = replay_agg(OracleBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+@pytest.mark.parametrize("tag,op", [("agg_fwd_n4096", "agg_fwd"), ("agg_rev_n4096", "agg_rev")])
+def test_aggregate_large_matches_reference_digests(oracle_lib, digests, tag, op):
+    d = digests[tag]
+    m = d["meta"]
+    out, _ = replay_agg(OracleBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+def test_aggregate_forward_sum_is_group_total(oracle_lib):
+    """plaintext meaning: after the forward network the first row of every
+    key group holds the group's sum"""
+    n = 512
+    out, x = replay_agg(OracleBackend(3), "agg_fwd", n, 5)
+    k0, v = x["k0"], x["va1"]
+    o1 = out["open_o1"][0]
+    heads = np.nonzero(np.r_[True, k0[1:] != k0[:-1]])[0]
+    for h in heads:
+        assert int(o1[h]) == int(v[k0 == k0[h]].sum())

@@ -8,8 +8,8 @@ import hashlib
 import numpy as np
 import pytest
 
-from replay import (GpuBackend, OracleBackend, radix_inputs, replay_bitonic, replay_compare,
-                    replay_prims, replay_radix, same)
+from replay import (GpuBackend, OracleBackend, radix_inputs, replay_agg, replay_bitonic,
+                    replay_compare, replay_prims, replay_radix, same)
 
 pytestmark = pytest.mark.gpu
 
@@ -278,3 +278,41 @@ def test_bitonic_2p16_seed1(orq):
     assert same(gpu["open_key"][0].view(np.int32), np.sort(key.view(np.int32)))
     cpu, _ = replay_bitonic(OracleBackend(1), 1 << 16, 1, 4)
     assert same(gpu["key"], cpu["key"])
+
+
+@pytest.mark.parametrize("tag,op", [("agg_fwd_n256", "agg_fwd"), ("agg_rev_n128", "agg_rev"),
+                                    ("agg_nokey_n64", "agg_nokey")])
+def test_aggregate_matches_reference_shares(orq, golden, digests, tag, op):
+    m = digests[tag]["meta"]
+    out, _ = replay_agg(GpuBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+@pytest.mark.parametrize("tag,op", [("agg_fwd_n4096", "agg_fwd"), ("agg_rev_n4096", "agg_rev")])
+def test_aggregate_large_matches_reference_digests(orq, digests, tag, op):
+    d = digests[tag]
+    m = d["meta"]
+    out, _ = replay_agg(GpuBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("op,n", [(op, n) for op in ("agg_fwd", "agg_rev", "agg_nokey")
+                                  for n in (1, 2, 8, 1 << 15)]
+                         + [("agg_nokey", 1 << 18), ("agg_fwd", 1 << 18)])
+def test_aggregate_matches_restatement(orq, op, n):
+    """sizes from one row to levels whose draws cross the 1 MiB nonce chunk"""
+    gpu, _ = replay_agg(GpuBackend(51), op, n, 9)
+    cpu, _ = replay_agg(OracleBackend(51), op, n, 9)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), (op, n, k)
+
+
+def test_aggregate_rejects_bad_sizes(orq):
+    rt = orq.Runtime(seed=1)
+    v = rt.secret_share_a(np.arange(3, dtype=np.uint64), 0)
+    k = rt.secret_share_b(np.arange(3, dtype=np.uint64), 0)
+    o = orq.ASharedVector(rt, rt._alloc(3, 8))
+    with pytest.raises(orq.OrqError):
+        orq.aggregate([k], [], [(v, o, orq.aggregators.sum)])
