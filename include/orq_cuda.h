@@ -199,6 +199,26 @@ int orqcu_aggregate(orqcu_runtime* rt, int width, size_t n, int nkeys, const voi
                     int nb, const orqcu_agg_spec* b_specs, int na, const orqcu_agg_spec* a_specs,
                     int reverse, const void* const* sel);
 
+/* compose_permutations (shuffle.h:717-743) of two A-shared int32 elementwise
+ * permutations of n rows: rho <- rho * sigma (sort by sigma's order, then
+ * rho's). sigma is consumed (left shuffled). Synchronous. */
+int orqcu_compose_permutations(orqcu_runtime* rt, size_t n, void* const sigma[3],
+                               void* const rho[3]);
+/* table_sort (sorting.h:509-612) with SortingProtocol::RADIXSORT over n rows
+ * of width-byte columns (4 or 8): ncols B-shared key columns (cols[3*k+p]),
+ * each ascending or descending and sorted on 1 bit (single_bit, e.g. valid
+ * and table-id columns) or on its full width; na A-shared and nb B-shared
+ * data columns are permuted along. Reserves its permutations up front like
+ * the reference. Synchronous. */
+int orqcu_table_sort(orqcu_runtime* rt, int width, size_t n, int ncols, void* const* cols,
+                     const int* descending, const int* single_bit, int na, void* const* data_a,
+                     int nb, void* const* data_b);
+/* distinct (distinct.h:20-53): res[0] = 1 and res[i] = 1 where row i differs
+ * from row i-1 in any of the nkeys B-shared key columns (keys[3*k+p]); one
+ * fused launch. */
+int orqcu_distinct(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* keys,
+                   void* const res[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -190,6 +190,31 @@ class Oracle:
                                int(reverse), self._ptrs(sel) if sel is not None else None)
         return b_out, a_out
 
+    def compose_permutations(self, sigma, rho):
+        """rho <- compose(sigma, rho); sigma is consumed."""
+        self.lib.oro_compose_permutations(ctypes.byref(self.ctx), ctypes.c_size_t(len(rho[0])),
+                                          self._ptrs(sigma), self._ptrs(rho))
+        return rho
+
+    def table_sort(self, cols, desc, single_bit, data_a=(), data_b=()):
+        """operators::table_sort (radix protocol); every column sorted in place."""
+        w = cols[0][0].dtype.itemsize
+        flat = lambda arrs: (ctypes.c_void_p * max(1, 3 * len(arrs)))(
+            *[x.ctypes.data for a in arrs for x in a])
+        self.lib.oro_table_sort(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(cols[0][0])), len(cols),
+                                flat(cols), (ctypes.c_int * len(cols))(*[int(d) for d in desc]),
+                                (ctypes.c_int * len(cols))(*[int(b) for b in single_bit]),
+                                len(data_a), flat(data_a), len(data_b), flat(data_b))
+
+    def distinct(self, keys):
+        w = keys[0][0].dtype.itemsize
+        n = len(keys[0][0])
+        res = self.new(n, w)
+        flat = (ctypes.c_void_p * (3 * len(keys)))(*[x.ctypes.data for a in keys for x in a])
+        self.lib.oro_distinct(ctypes.byref(self.ctx), w, ctypes.c_size_t(n), len(keys), flat,
+                              self._ptrs(res))
+        return res
+
     def bitonic_sort(self, key, desc=False):
         w = key[0].dtype.itemsize
         self.lib.oro_bitonic_sort(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(key[0])), self._ptrs(key),

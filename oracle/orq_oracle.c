@@ -531,9 +531,21 @@ static void apply_elementwise(oro_ctx* c, pqueue* pq, int x_arith, int w, size_t
 /* radix_sort (operators/radixsort.h:116-229) with pad_input/remove_padding
  * (operators/sorting.h:405-495) and ElementwisePermutation::b2a/invert
  * (containers/permutation.h:205-258). */
+static void radix_sort_pq(oro_ctx* c, pqueue* pqp, int kw, size_t n, void* key[3], int bits,
+                          int desc, int npayload, void** payloads, int32_t* perm_out[3]);
+
 void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int desc,
                     int npayload, void** payloads, int32_t* perm_out[3]) {
     pqueue pq = {0};
+    radix_sort_pq(c, &pq, kw, n, key, bits, desc, npayload, payloads, perm_out);
+    while (pq.head < pq.tail) sperm_free(&pq.q[pq.head++]);
+    free(pq.q);
+}
+
+/* radix_sort with the caller's PermutationManager queue */
+static void radix_sort_pq(oro_ctx* c, pqueue* pqp, int kw, size_t n, void* key[3], int bits,
+                          int desc, int npayload, void** payloads, int32_t* perm_out[3]) {
+#define pq (*pqp)
     const int pw = (kw == 8) ? 16 : 8; /* PadWidth: int64 -> int128, else int64 */
     const int full_width = (kw * 8 == bits);
     void* P[3];
@@ -672,8 +684,7 @@ void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int de
         free(t[j]);
         free(pm[j]);
     }
-    while (pq.head < pq.tail) sperm_free(&pq.q[pq.head++]);
-    free(pq.q);
+#undef pq
 }
 
 /* shuffle (operators/shuffle.h:752-757): one on-demand sharded permutation
@@ -1142,4 +1153,119 @@ void oro_aggregate(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, in
         free3(R);
         free3(E);
     }
+}
+
+
+/* ------------------------------------------------------------------------- */
+/* Permutation composition, table sort and distinct. */
+
+/* compose_permutations (operators/shuffle.h:717-743): pi from the queue;
+ * sigma' = pi(sigma) (sharded apply, sigma modified), opened; rho gathered
+ * by it (local_apply_inverse_perm), then pi undone on rho. Result in rho. */
+static void compose_pq(oro_ctx* c, pqueue* pq, size_t n, int32_t* sigma[3], int32_t* rho[3]) {
+    sperm sp = pq_next(c, pq, n);
+    apply_sharded(c, 1, 4, n, (void**)sigma, &sp);
+    int32_t* opened = (int32_t*)xalloc(n * 4 + 4);
+    oro_open(1, 4, n, (void* const*)sigma, opened);
+    for (int j = 0; j < 3; j++) gather(4, n, rho[j], opened);
+    apply_inverse_sharded(c, 1, 4, n, (void**)rho, &sp);
+    sperm_free(&sp);
+    free(opened);
+}
+
+void oro_compose_permutations(oro_ctx* c, size_t n, int32_t* sigma[3], int32_t* rho[3]) {
+    pqueue pq = {0};
+    compose_pq(c, &pq, n, sigma, rho);
+    free(pq.q);
+}
+
+/* table_sort (operators/sorting.h:509-612) with SortingProtocol::RADIXSORT:
+ * reserve every permutation up front, sort the last key column, then each
+ * earlier column after applying the running permutation to it, composing the
+ * permutations; finally apply the total permutation to the key columns, the
+ * arithmetic data columns and the boolean data columns, in that order. */
+void oro_table_sort(oro_ctx* c, int w, size_t n, int ncols, void* const* cols, const int* desc,
+                    const int* single_bit, int na, void* const* data_a, int nb,
+                    void* const* data_b) {
+    int ns = 0;
+    for (int k = 0; k < ncols; k++) ns += single_bit[k] != 0;
+    const int nk = ncols - ns, nc = na + nb, L = 8 * w;
+    const size_t perms = (size_t)(nk + ns - 1) + (size_t)(nk + ns);
+    const size_t pairs = (size_t)(4 * ns + 3 * nk + nc - 1) + (size_t)nk * L;
+    pqueue pq = {0};
+    pq_reserve(c, &pq, n, perms + pairs);
+    void* orig[3];
+    alloc3(orig, n, w);
+    int32_t* sp[3];
+    int32_t* np_[3];
+    for (int j = 0; j < 3; j++) {
+        sp[j] = (int32_t*)xalloc(n * 4 + 4);
+        np_[j] = (int32_t*)xalloc(n * 4 + 4);
+    }
+    int C = ncols - 1;
+    {
+        void* col[3] = {cols[3 * C], cols[3 * C + 1], cols[3 * C + 2]};
+        copy3(orig, col, n, w);
+        radix_sort_pq(c, &pq, w, n, col, single_bit[C] ? 1 : L, desc[C], 0, NULL, sp);
+        copy3(col, orig, n, w);
+    }
+    for (C--; C >= 0; C--) {
+        void* col[3] = {cols[3 * C], cols[3 * C + 1], cols[3 * C + 2]};
+        copy3(orig, col, n, w);
+        apply_elementwise(c, &pq, 0, w, n, col, sp);
+        radix_sort_pq(c, &pq, w, n, col, single_bit[C] ? 1 : L, desc[C], 0, NULL, np_);
+        copy3(col, orig, n, w);
+        compose_pq(c, &pq, n, sp, np_);
+        for (int j = 0; j < 3; j++) {
+            int32_t* t = sp[j];
+            sp[j] = np_[j];
+            np_[j] = t;
+        }
+    }
+    for (int k = 0; k < ncols; k++) {
+        void* col[3] = {cols[3 * k], cols[3 * k + 1], cols[3 * k + 2]};
+        apply_elementwise(c, &pq, 0, w, n, col, sp);
+    }
+    for (int k = 0; k < na; k++) {
+        void* col[3] = {data_a[3 * k], data_a[3 * k + 1], data_a[3 * k + 2]};
+        apply_elementwise(c, &pq, 1, w, n, col, sp);
+    }
+    for (int k = 0; k < nb; k++) {
+        void* col[3] = {data_b[3 * k], data_b[3 * k + 1], data_b[3 * k + 2]};
+        apply_elementwise(c, &pq, 0, w, n, col, sp);
+    }
+    free3(orig);
+    for (int j = 0; j < 3; j++) {
+        free(sp[j]);
+        free(np_[j]);
+    }
+    while (pq.head < pq.tail) sperm_free(&pq.q[pq.head++]);
+    free(pq.q);
+}
+
+/* distinct (operators/distinct.h:20-53): res = 0; res[0] = public 1; for
+ * every key, res[1:] |= (key[:-1] != key[1:]) where != is !(bit_same & 1)
+ * and |= is ~(~res & ~x) (b_shared_vector.h:450-455). */
+void oro_distinct(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, void* res[3]) {
+    for (int j = 0; j < 3; j++) memset(res[j], 0, n * (size_t)w);
+    if (n == 0) return;
+    st(res[0], 0, w, 1);
+    const size_t m = n - 1;
+    void *E[3], *R[3];
+    alloc3(E, m, w);
+    sl3(res, 1, w, R);
+    for (int k = 0; k < nkeys; k++) {
+        void* kk[3] = {keys[3 * k], keys[3 * k + 1], keys[3 * k + 2]};
+        void *lo[3], *hi[3];
+        sl3(kk, 0, w, lo);
+        sl3(kk, 1, w, hi);
+        eq3(c, w, m, lo, hi, E);
+        for (int j = 0; j < 3; j++)
+            for (size_t i = 0; i < m; i++) st(E[j], i, w, (ld(E[j], i, w) & 1) ^ 1);
+        not3(R, m, w);
+        not3(E, m, w);
+        oro_and_b(c, w, m, R, E, R);
+        not3(R, m, w);
+    }
+    free3(E);
 }

@@ -117,6 +117,19 @@ void oro_aggregate(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, in
                    void* const* a_in, void* const* a_out, const int* a_func, int reverse,
                    void* const* sel);
 
+/* compose_permutations (shuffle.h:717-743) of two A-shared int32 elementwise
+ * permutations; sigma is consumed, the result is written to rho. */
+void oro_compose_permutations(oro_ctx* c, size_t n, int32_t* sigma[3], int32_t* rho[3]);
+/* table_sort (sorting.h:509-612) with the radix sort protocol: ncols key
+ * columns (3 pointers each) with per-column order and single-bit flags, then
+ * na arithmetic and nb boolean data columns permuted along. */
+void oro_table_sort(oro_ctx* c, int w, size_t n, int ncols, void* const* cols, const int* desc,
+                    const int* single_bit, int na, void* const* data_a, int nb,
+                    void* const* data_b);
+/* distinct (distinct.h:20-53): res marks the first row of every run of equal
+ * keys (adjacent rows only). */
+void oro_distinct(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, void* res[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -119,7 +119,88 @@ int main(int argc, char** argv) {
         run_prims<int32_t>(n, seed, d, "w4_");
         run_prims<int64_t>(n, seed + 1, d, "w8_");
         run_prims<int8_t>(n, seed + 2, d, "w1_");
-    } else if (op == "radix" || op == "radix_time") {
+    } else if (op == "join_agg") {
+        // The relational pipeline on small tables: A(n rows) = {[K] pk (a
+        // Fisher-Yates permutation of 0..n-1), [G] group (0..4), V value
+        // (< 10^6)}; B(2n rows) = {[K] fk (uniform over pk), Q quantity
+        // (1..50)}. J = A.inner_join(B, [K], copy [G] and V); J.VQ = V*Q;
+        // J.aggregate([G], sum VQ, count CNT). Every column of J is dumped.
+        uint64_t st = seed;
+        const size_t na = n, nb = 2 * n;
+        orq::Vector<int64_t> pk(na), g(na), v(na), fk(nb), q(nb);
+        for (size_t i = 0; i < na; i++) pk[i] = (int64_t)i;
+        for (size_t i = na; i-- > 1;) {
+            size_t j = sm64(st) % (i + 1);
+            std::swap(pk[i], pk[j]);
+        }
+        for (size_t i = 0; i < na; i++) g[i] = (int64_t)(sm64(st) % 5);
+        for (size_t i = 0; i < na; i++) v[i] = (int64_t)(sm64(st) % 1000000);
+        for (size_t i = 0; i < nb; i++) fk[i] = (int64_t)(sm64(st) % na);
+        for (size_t i = 0; i < nb; i++) q[i] = (int64_t)(1 + sm64(st) % 50);
+        std::vector<orq::Vector<int64_t>> ca = {pk, g, v};
+        std::vector<orq::Vector<int64_t>> cb = {fk, q};
+        EncodedTable<int64_t> A = secret_share(ca, {"[K]", "[G]", "V"});
+        EncodedTable<int64_t> B = secret_share(cb, {"[K]", "Q"});
+        auto J = A.inner_join(B, {"[K]"}, {{"[G]", "[G]", copy<BSharedVector<int64_t>>},
+                                           {"V", "V", copy<ASharedVector<int64_t>>}});
+        J.addColumns(std::vector<std::string>{"VQ", "CNT"});
+        J["VQ"] = J["V"] * J["Q"];
+        J.aggregate({"[G]"}, {{"VQ", "VQ", sum<ASharedVector<int64_t>>},
+                              {"CNT", "CNT", count<ASharedVector<int64_t>>}});
+        for (auto& name : J.getColumnNames()) {
+            if (EncodedTable<int64_t>::isBShared(name)) {
+                auto c = J.asBSharedVector(name);
+                d.shares(name, c);
+            } else {
+                auto c = J.asASharedVector(name);
+                d.shares(name, c);
+            }
+        }
+        auto T = J.open_with_schema();
+        for (size_t k = 0; k < T.second.size(); k++) d.plain("open_" + T.second[k], T.first[k]);
+    } else if (op == "tsort" || op == "distinct") {
+        // tsort: operators::table_sort with the radix protocol on three key
+        // columns [bit ASC, small-int DESC, bit ASC] plus one A and one B data
+        // column. distinct: operators::distinct over two sorted key columns.
+        using B = BSharedVector<int64_t>;
+        using A = ASharedVector<int64_t>;
+        uint64_t st = seed;
+        auto v0 = gen<int64_t>(n, st, 1);
+        auto v1 = gen<int64_t>(n, st, 7);
+        auto v2 = gen<int64_t>(n, st, 1);
+        auto va = gen<int64_t>(n, st, 0xffffffffull);
+        auto vb = gen<int64_t>(n, st, ~0ull);
+        B b0 = secret_share_b(v0, 0), b1 = secret_share_b(v1, 0), b2 = secret_share_b(v2, 0);
+        A a0 = secret_share_a(va, 0);
+        B b3 = secret_share_b(vb, 0);
+        if (op == "tsort") {
+            std::vector<B*> cols = {&b0, &b1, &b2};
+            std::vector<A*> da = {&a0};
+            std::vector<B*> db = {&b3};
+            orq::operators::table_sort(cols, da, db,
+                                       {orq::operators::SortOrder::ASC, orq::operators::SortOrder::DESC,
+                                        orq::operators::SortOrder::ASC},
+                                       {true, false, true}, orq::SortingProtocol::RADIXSORT);
+            d.shares("c0", b0);
+            d.shares("c1", b1);
+            d.shares("c2", b2);
+            d.shares("da", a0);
+            d.shares("db", b3);
+            auto o0 = b0.open(), o1 = b1.open(), o2 = b2.open();
+            auto oa = a0.open();
+            d.plain("open_c0", o0);
+            d.plain("open_c1", o1);
+            d.plain("open_c2", o2);
+            d.plain("open_da", oa);
+        } else {
+            std::vector<B*> keys = {&b0, &b1};
+            B res(n);
+            orq::operators::distinct(keys, &res);
+            d.shares("res", res);
+            auto o = res.open();
+            d.plain("open_res", o);
+        }
+    } else if (op == "radix" || op == "radix_time" || op == "radix_desc") {
         // radix_sort(key, ASC, bits) then apply the permutation to two
         // A-shared payloads (key uniform in [0, 2^bits), payloads u32).
         uint64_t st = seed;
@@ -131,11 +212,13 @@ int main(int argc, char** argv) {
         ASharedVector<int64_t> a1 = secret_share_a(p1, 0);
         ASharedVector<int64_t> a2 = secret_share_a(p2, 0);
         t0 = std::chrono::steady_clock::now();
-        auto perm = orq::operators::radix_sort(kb, orq::operators::SortOrder::ASC, bits);
+        auto perm = orq::operators::radix_sort(
+            kb, op == "radix_desc" ? orq::operators::SortOrder::DESC : orq::operators::SortOrder::ASC,
+            bits);
         orq::operators::oblivious_apply_elementwise_perm(a1, perm);
         orq::operators::oblivious_apply_elementwise_perm(a2, perm);
         secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        if (op == "radix") {
+        if (op != "radix_time") {
             d.shares("key", kb);
             d.shares("pay1", a1);
             d.shares("pay2", a2);
@@ -145,7 +228,7 @@ int main(int argc, char** argv) {
         auto ko = kb.open();
         auto o1 = a1.open();
         auto o2 = a2.open();
-        if (op == "radix") {
+        if (op != "radix_time") {
             d.plain("open_key", ko);
             d.plain("open_pay1", o1);
             d.plain("open_pay2", o2);

@@ -399,6 +399,41 @@ def aggregate(keys, agg_spec_b, agg_spec_a, direction: int = Direction.Forward, 
                                   int(direction == Direction.Reverse), sp))
 
 
+def _flat(vecs):
+    return (ctypes.c_void_p * max(1, 3 * len(vecs)))(*[v.shares[j].data_ptr() for v in vecs for j in range(3)])
+
+
+def compose_permutations(sigma: ASharedVector, rho: ASharedVector) -> ASharedVector:
+    """orq::operators::compose_permutations (shuffle.h:717-743); sigma is
+    consumed, rho is updated in place and returned."""
+    rt = rho.rt
+    _check(rt.lib.orqcu_compose_permutations(rt.h, ctypes.c_size_t(rho.size()), _p3(sigma.shares),
+                                             _p3(rho.shares)))
+    return rho
+
+
+def table_sort(columns, data_a=(), data_b=(), order=None, single_bit=None):
+    """orq::operators::table_sort (sorting.h:509-612) with the radix sort
+    protocol: columns are B-shared key columns (most significant first), each
+    sorted ASC/DESC per `order`, on one bit where `single_bit` says so; data
+    columns are permuted along. Everything is updated in place."""
+    rt, n, w = columns[0].rt, columns[0].size(), columns[0].width
+    order = order or [ASC] * len(columns)
+    single_bit = single_bit or [False] * len(columns)
+    _check(rt.lib.orqcu_table_sort(rt.h, w, ctypes.c_size_t(n), len(columns), _flat(columns),
+                                   (ctypes.c_int * len(columns))(*[int(o == DESC) for o in order]),
+                                   (ctypes.c_int * len(columns))(*[int(bool(b)) for b in single_bit]),
+                                   len(data_a), _flat(data_a), len(data_b), _flat(data_b)))
+
+
+def distinct(keys) -> BSharedVector:
+    """orq::operators::distinct (distinct.h:20-53) over adjacent rows."""
+    rt, n, w = keys[0].rt, keys[0].size(), keys[0].width
+    res = rt._alloc(n, w)
+    _check(rt.lib.orqcu_distinct(rt.h, w, ctypes.c_size_t(n), len(keys), _flat(keys), _p3(res)))
+    return BSharedVector(rt, res)
+
+
 def radix_sort(v: BSharedVector, order: int = ASC, bits: int | None = None) -> ElementwisePermutation:
     """orq::operators::radix_sort (radixsort.h:205-229): sorts v in place and
     returns the A-shared sorting permutation."""

@@ -1,6 +1,7 @@
 // capi.cu — extern "C" entry points (include/orq_cuda.h).
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/orq_cuda.h"
 #include "runtime.h"
@@ -404,6 +405,59 @@ int orqcu_aggregate(orqcu_runtime* rt, int width, size_t n, int nkeys, const voi
         orqcu::op_aggregate(rt->ctx, width, n, nkeys, keys, nb,
                             reinterpret_cast<const orqcu::AggSpec*>(b_specs), na,
                             reinterpret_cast<const orqcu::AggSpec*>(a_specs), reverse != 0, sel);
+    });
+}
+
+int orqcu_compose_permutations(orqcu_runtime* rt, size_t n, void* const sigma[3],
+                               void* const rho[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need_sh((const void* const*)sigma, n, "null sigma");
+        need_sh((const void* const*)rho, n, "null rho");
+        orqcu::op_compose(rt->ctx, n, m3(sigma), m3(rho));
+        rt->ctx.check_device_error();
+    });
+}
+
+int orqcu_table_sort(orqcu_runtime* rt, int width, size_t n, int ncols, void* const* cols,
+                     const int* descending, const int* single_bit, int na, void* const* data_a,
+                     int nb, void* const* data_b) {
+    return guard([&] {
+        need_rt(rt);
+        need(ncols >= 1 && cols && descending && single_bit, "table sort needs key columns");
+        need(na >= 0 && nb >= 0 && (na == 0 || data_a) && (nb == 0 || data_b), "bad data columns");
+        need(n < (1ull << 31), "table sort supports n < 2^31");
+        std::vector<orqcu::Sh3> k(ncols), a(na), b(nb);
+        for (int i = 0; i < ncols; i++) {
+            need_sh((const void* const*)cols + 3 * i, n, "null key column");
+            k[i] = m3(cols + 3 * i);
+        }
+        for (int i = 0; i < na; i++) {
+            need_sh((const void* const*)data_a + 3 * i, n, "null data column");
+            a[i] = m3(data_a + 3 * i);
+        }
+        for (int i = 0; i < nb; i++) {
+            need_sh((const void* const*)data_b + 3 * i, n, "null data column");
+            b[i] = m3(data_b + 3 * i);
+        }
+        orqcu::op_table_sort(rt->ctx, width, n, ncols, k.data(), descending, single_bit, na, a.data(),
+                             nb, b.data());
+        rt->ctx.check_device_error();
+    });
+}
+
+int orqcu_distinct(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* keys,
+                   void* const res[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(nkeys >= 1 && keys, "distinct needs key columns");
+        std::vector<orqcu::CSh3> k(nkeys);
+        for (int i = 0; i < nkeys; i++) {
+            need_sh(keys + 3 * i, n, "null key column");
+            k[i] = c3(keys + 3 * i);
+        }
+        need_sh((const void* const*)res, n, "null res");
+        orqcu::op_distinct(rt->ctx, width, n, nkeys, k.data(), m3(res));
     });
 }
 

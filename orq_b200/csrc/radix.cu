@@ -210,19 +210,22 @@ __global__ void __launch_bounds__(kAesThreads) k_radix_perm(PermMulArgs a) {
 
 // pad_input (sorting.h:431-462): (v << 32) | index, index public-shared into
 // S0 only (P0 and P2 hold it); v is sign-extended to the padded width.
+// Descending (reverse_order): the index is -1-i and the padded vector is
+// reversed, so row i lands at position n-1-i.
 template <int KW, int PW>
-__global__ void k_pad(CSh3 key, Sh3 P, unsigned long long n) {
-    for (unsigned long long i = gtid(); i < n; i += gstride()) {
+__global__ void k_pad(CSh3 key, Sh3 P, unsigned long long n, int desc) {
+    for (unsigned long long i0 = gtid(); i0 < n; i0 += gstride()) {
+        const unsigned long long i = desc ? n - 1 - i0 : i0;  // destination
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            const uint32_t idx = j == 0 ? (uint32_t)i : 0u;
+            const uint32_t idx = j == 0 ? (desc ? (uint32_t)(-1ll - (long long)i0) : (uint32_t)i0) : 0u;
             if constexpr (KW == 8) {
-                const long long v = reinterpret_cast<const long long*>(key.p[j])[i];
+                const long long v = reinterpret_cast<const long long*>(key.p[j])[i0];
                 const unsigned long long lo = ((unsigned long long)v << 32) | idx;
                 const unsigned long long hi = (unsigned long long)(v >> 32);  // sign fill
                 reinterpret_cast<uint4*>(P.p[j])[i] = mk4(lo, hi);
             } else {
-                const int v = reinterpret_cast<const int*>(key.p[j])[i];
+                const int v = reinterpret_cast<const int*>(key.p[j])[i0];
                 const unsigned long long p = ((unsigned long long)(long long)v << 32) | idx;
                 reinterpret_cast<unsigned long long*>(P.p[j])[i] = p;
             }
@@ -232,18 +235,20 @@ __global__ void k_pad(CSh3 key, Sh3 P, unsigned long long n) {
 
 // remove_padding (sorting.h:475-495): low 32 bits -> B-shared permutation,
 // arithmetic shift by 32 -> the key.
+// Descending: the padded vector is reversed back first (row i reads n-1-i).
 template <int KW, int PW>
-__global__ void k_unpad(CSh3 P, Sh3 key, Sh3 perm, unsigned long long n) {
+__global__ void k_unpad(CSh3 P, Sh3 key, Sh3 perm, unsigned long long n, int desc) {
     for (unsigned long long i = gtid(); i < n; i += gstride()) {
+        const unsigned long long src = desc ? n - 1 - i : i;
 #pragma unroll
         for (int j = 0; j < 3; j++) {
             if constexpr (PW == 16) {
-                const uint4 v = reinterpret_cast<const uint4*>(P.p[j])[i];
+                const uint4 v = reinterpret_cast<const uint4*>(P.p[j])[src];
                 reinterpret_cast<uint32_t*>(perm.p[j])[i] = v.x;
                 const unsigned long long k = (unsigned long long)v.y | ((unsigned long long)v.z << 32);
                 reinterpret_cast<unsigned long long*>(key.p[j])[i] = k;
             } else {
-                const unsigned long long v = reinterpret_cast<const unsigned long long*>(P.p[j])[i];
+                const unsigned long long v = reinterpret_cast<const unsigned long long*>(P.p[j])[src];
                 reinterpret_cast<uint32_t*>(perm.p[j])[i] = (uint32_t)v;
                 reinterpret_cast<uint32_t*>(key.p[j])[i] = (uint32_t)(v >> 32);
             }
@@ -255,12 +260,20 @@ __global__ void k_iota(int32_t* out, unsigned long long n) {
     for (unsigned long long i = gtid(); i < n; i += gstride()) out[i] = (int32_t)i;
 }
 
+// public_share of the constant -1 (S0 = -1, S1 = S2 = 0)
+__global__ void k_minus_one(Sh3 m, unsigned long long n) {
+    for (unsigned long long i = gtid(); i < n; i += gstride()) {
+        reinterpret_cast<int32_t*>(m.p[0])[i] = -1;
+        reinterpret_cast<int32_t*>(m.p[1])[i] = 0;
+        reinterpret_cast<int32_t*>(m.p[2])[i] = 0;
+    }
+}
+
 }  // namespace
 
 void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out) {
     if (kw != 4 && kw != 8) throw std::invalid_argument("radix sort keys must be int32 or int64");
     if (bits < 1 || bits > kw * 8) throw std::invalid_argument("bits out of range");
-    if (desc) throw std::invalid_argument("descending radix sort is not supported yet");
     if (n >= (1ull << 31)) throw std::invalid_argument("radix sort supports n < 2^31");
     const int PW = kw == 8 ? 16 : 8;
     const bool full_width = (kw * 8 == bits);
@@ -274,8 +287,8 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
     const unsigned pg = plain_grid(c, n);
     if (n) {
         CSh3 k{{key.p[0], key.p[1], key.p[2]}};
-        if (kw == 8) k_pad<8, 16><<<pg, 256, 0, c.stream>>>(k, P, n);
-        else k_pad<4, 8><<<pg, 256, 0, c.stream>>>(k, P, n);
+        if (kw == 8) k_pad<8, 16><<<pg, 256, 0, c.stream>>>(k, P, n, desc);
+        else k_pad<4, 8><<<pg, 256, 0, c.stream>>>(k, P, n, desc);
         ORQ_CUDA_CHECK(cudaGetLastError());
         c.kernels_launched++;
     }
@@ -353,8 +366,8 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
     for (int j = 0; j < 3; j++) PM.p[j] = pm.as<uint8_t>() + j * n1 * 4;
     if (n) {
         CSh3 Pc{{P.p[0], P.p[1], P.p[2]}};
-        if (kw == 8) k_unpad<8, 16><<<pg, 256, 0, c.stream>>>(Pc, key, PM, n);
-        else k_unpad<4, 8><<<pg, 256, 0, c.stream>>>(Pc, key, PM, n);
+        if (kw == 8) k_unpad<8, 16><<<pg, 256, 0, c.stream>>>(Pc, key, PM, n, desc);
+        else k_unpad<4, 8><<<pg, 256, 0, c.stream>>>(Pc, key, PM, n, desc);
         ORQ_CUDA_CHECK(cudaGetLastError());
         c.kernels_launched++;
     }
@@ -375,6 +388,21 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
         op_public_share(c, 4, n, sig.p, PM);
         op_apply_sharded(c, true, 4, n, PM, sp, true);
         c.free_perm(sp);
+    }
+    // negate (permutation.h:268-280) for descending sorts: v *= -1 (a
+    // multiply_a with the public -1), v += -1
+    if (desc) {
+        Scratch mb(c, 3 * n1 * 4);
+        Sh3 M1;
+        for (int j = 0; j < 3; j++) M1.p[j] = mb.as<uint8_t>() + j * n1 * 4;
+        if (n) {
+            k_minus_one<<<pg, 256, 0, c.stream>>>(M1, n);
+            ORQ_CUDA_CHECK(cudaGetLastError());
+            c.kernels_launched++;
+        }
+        const CSh3 m1c{{M1.p[0], M1.p[1], M1.p[2]}};
+        op_mult(c, true, 4, n, CSh3{{PM.p[0], PM.p[1], PM.p[2]}}, m1c, PM);
+        op_local(c, 1, 4, n, CSh3{{PM.p[0], PM.p[1], PM.p[2]}}, m1c, PM);
     }
     // invert (permutation.h:205-213): apply the permutation to a public identity
     {

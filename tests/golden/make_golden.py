@@ -50,6 +50,14 @@ CASES = [
     ("agg_nokey_n64", "agg_nokey", 64, 9, 4, 64, True),
     ("agg_fwd_n4096", "agg_fwd", 4096, 11, 5, 64, False),
     ("agg_rev_n4096", "agg_rev", 4096, 12, 6, 64, False),
+    ("radix_desc_n100_b40", "radix_desc", 100, 7, 3, 40, True),
+    ("radix_desc_n64_b64", "radix_desc", 64, 7, 3, 64, True),
+    ("radix_n33_b1", "radix", 33, 7, 3, 1, True),
+    ("radix_desc_n3000_b16", "radix_desc", 3000, 8, 4, 16, False),
+    ("tsort_n64", "tsort", 64, 5, 4, 64, True),
+    ("tsort_n200", "tsort", 200, 6, 5, 64, False),
+    ("distinct_n64", "distinct", 64, 5, 4, 64, True),
+    ("distinct_n5000", "distinct", 5000, 6, 5, 64, False),
 ]
 
 

@@ -42,9 +42,15 @@ class OracleBackend:
     def np(self, x):
         return np.stack(x)
 
-    def radix(self, key, bits, payloads):
-        perm = self.o.radix_sort(key, bits, payloads)
+    def radix(self, key, bits, payloads, desc=False):
+        perm = self.o.radix_sort(key, bits, payloads, desc=desc)
         return perm
+
+    def table_sort(self, cols, desc, single_bit, data_a, data_b):
+        self.o.table_sort(cols, desc, single_bit, data_a, data_b)
+
+    def distinct(self, keys):
+        return self.o.distinct(keys)
 
     def compare(self, x, y):
         return self.o.compare(x, y)
@@ -88,11 +94,18 @@ class GpuBackend:
         a = x.shares.cpu().numpy()
         return a.view(_U[a.dtype.itemsize]) if a.ndim == 2 else a
 
-    def radix(self, key, bits, payloads):
-        perm = self.orq.radix_sort(key, self.orq.ASC, bits)
+    def radix(self, key, bits, payloads, desc=False):
+        perm = self.orq.radix_sort(key, self.orq.DESC if desc else self.orq.ASC, bits)
         for p in payloads:
             self.orq.oblivious_apply_elementwise_perm(p, perm)
         return perm
+
+    def table_sort(self, cols, desc, single_bit, data_a, data_b):
+        o = self.orq
+        o.table_sort(cols, data_a, data_b, [o.DESC if d else o.ASC for d in desc], single_bit)
+
+    def distinct(self, keys):
+        return self.orq.distinct(keys)
 
     def compare(self, x, y):
         return x._compare(y)
@@ -149,14 +162,14 @@ def radix_inputs(n, seed, bits):
     return st[:n] & km, st[n:2 * n] & np.uint64(0xFFFFFFFF), st[2 * n:] & np.uint64(0xFFFFFFFF)
 
 
-def replay_radix(be, n, seed, bits):
-    """The "radix" op of ref_driver.cpp: radix_sort(key, ASC, bits) then the
-    permutation applied to two A-shared int64 payloads."""
+def replay_radix(be, n, seed, bits, desc=False):
+    """The "radix" ("radix_desc") op of ref_driver.cpp: radix_sort(key, ASC
+    (DESC), bits) then the permutation applied to two A-shared int64 payloads."""
     key, p1, p2 = radix_inputs(n, seed, bits)
     kb = be.share(key, False, 0)
     a1 = be.share(p1, True, 0)
     a2 = be.share(p2, True, 0)
-    perm = be.radix(kb, bits, [a1, a2])
+    perm = be.radix(kb, bits, [a1, a2], desc)
     out = {"key": be.np(kb), "pay1": be.np(a1), "pay2": be.np(a2), "perm": be.np(perm)}
     out["open_key"] = be.open(kb, False)[None]
     out["open_pay1"] = be.open(a1, True)[None]
@@ -234,6 +247,35 @@ def replay_agg(be, op, n, seed):
                     "q4": be.np(bo[3]), "q5": be.np(bo[4])})
     out["open_o1"] = be.open(ao[0], True)[None]
     return out, x
+
+
+def tsort_inputs(n, seed):
+    """Inputs of the "tsort"/"distinct" ops: bit, 3-bit, bit key columns, then
+    a u32 A column and a full-width B column."""
+    st = splitmix64_fast(seed, 5 * n)
+    one = np.uint64(1)
+    return (st[:n] & one, st[n:2 * n] & np.uint64(7), st[2 * n:3 * n] & one,
+            st[3 * n:4 * n] & np.uint64(0xFFFFFFFF), st[4 * n:])
+
+
+def replay_tsort(be, op, n, seed):
+    """The "tsort" op (table_sort on [bit ASC, 3-bit DESC, bit ASC] with one A
+    and one B data column) or the "distinct" op (distinct on the first two
+    key columns) of ref_driver.cpp."""
+    v0, v1, v2, va, vb = tsort_inputs(n, seed)
+    b0, b1, b2 = (be.share(v, False, 0) for v in (v0, v1, v2))
+    a0 = be.share(va, True, 0)
+    b3 = be.share(vb, False, 0)
+    if op == "tsort":
+        be.table_sort([b0, b1, b2], [False, True, False], [True, False, True], [a0], [b3])
+        out = {"c0": be.np(b0), "c1": be.np(b1), "c2": be.np(b2), "da": be.np(a0), "db": be.np(b3)}
+        for k, v in (("c0", b0), ("c1", b1), ("c2", b2)):
+            out["open_" + k] = be.open(v, False)[None]
+        out["open_da"] = be.open(a0, True)[None]
+    else:
+        r = be.distinct([b0, b1])
+        out = {"res": be.np(r), "open_res": be.open(r, False)[None]}
+    return out, (v0, v1, v2, va, vb)
 
 
 def same(a, b):

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from replay import (OracleBackend, replay_agg, replay_bitonic, replay_compare, replay_prims,
-                    replay_radix, same)
+                    replay_radix, replay_tsort, same)
 
 
 def sha(a):
@@ -160,3 +160,46 @@ def test_aggregate_forward_sum_is_group_total(oracle_lib):
     heads = np.nonzero(np.r_[True, k0[1:] != k0[:-1]])[0]
     for h in heads:
         assert int(o1[h]) == int(v[k0 == k0[h]].sum())
+
+
+@pytest.mark.parametrize("tag,desc", [("radix_desc_n100_b40", True), ("radix_desc_n64_b64", True),
+                                      ("radix_n33_b1", False)])
+def test_radix_desc_and_single_bit_match_reference_shares(oracle_lib, golden, digests, tag, desc):
+    m = digests[tag]["meta"]
+    out, (key, _, _) = replay_radix(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], desc)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+def test_radix_desc_large_matches_reference_digests(oracle_lib, digests):
+    d = digests["radix_desc_n3000_b16"]
+    m = d["meta"]
+    out, _ = replay_radix(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], True)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag,op", [("tsort_n64", "tsort"), ("distinct_n64", "distinct")])
+def test_table_sort_and_distinct_match_reference_shares(oracle_lib, golden, digests, tag, op):
+    m = digests[tag]["meta"]
+    out, _ = replay_tsort(OracleBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+@pytest.mark.parametrize("tag,op", [("tsort_n200", "tsort"), ("distinct_n5000", "distinct")])
+def test_table_sort_and_distinct_large_match_reference_digests(oracle_lib, digests, tag, op):
+    d = digests[tag]
+    m = d["meta"]
+    out, _ = replay_tsort(OracleBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+def test_table_sort_plaintext_order(oracle_lib):
+    """rows ordered by (c0 asc, c1 desc, c2 asc), stable, data carried"""
+    n = 128
+    out, (v0, v1, v2, va, vb) = replay_tsort(OracleBackend(9), "tsort", n, 4)
+    order = sorted(range(n), key=lambda i: (int(v0[i]), -int(v1[i]), int(v2[i])))
+    assert out["open_c1"][0].tolist() == [int(v1[i]) for i in order]
+    assert sorted(out["open_da"][0].tolist()) == sorted(int(x) for x in va)

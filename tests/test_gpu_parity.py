@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from replay import (GpuBackend, OracleBackend, radix_inputs, replay_agg, replay_bitonic,
-                    replay_compare, replay_prims, replay_radix, same)
+                    replay_compare, replay_prims, replay_radix, replay_tsort, same)
 
 pytestmark = pytest.mark.gpu
 
@@ -316,3 +316,54 @@ def test_aggregate_rejects_bad_sizes(orq):
     o = orq.ASharedVector(rt, rt._alloc(3, 8))
     with pytest.raises(orq.OrqError):
         orq.aggregate([k], [], [(v, o, orq.aggregators.sum)])
+
+
+@pytest.mark.parametrize("tag,desc", [("radix_desc_n100_b40", True), ("radix_desc_n64_b64", True),
+                                      ("radix_n33_b1", False)])
+def test_radix_desc_and_single_bit_match_reference_shares(orq, golden, digests, tag, desc):
+    m = digests[tag]["meta"]
+    out, _ = replay_radix(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], desc)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+def test_radix_desc_large_matches_reference_digests(orq, digests):
+    d = digests["radix_desc_n3000_b16"]
+    m = d["meta"]
+    out, _ = replay_radix(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], True)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag,op", [("tsort_n64", "tsort"), ("distinct_n64", "distinct")])
+def test_table_sort_and_distinct_match_reference_shares(orq, golden, digests, tag, op):
+    m = digests[tag]["meta"]
+    out, _ = replay_tsort(GpuBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+@pytest.mark.parametrize("tag,op", [("tsort_n200", "tsort"), ("distinct_n5000", "distinct")])
+def test_table_sort_and_distinct_large_match_reference_digests(orq, digests, tag, op):
+    d = digests[tag]
+    m = d["meta"]
+    out, _ = replay_tsort(GpuBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("op,n", [("tsort", 1), ("tsort", 2), ("tsort", 1000), ("distinct", 1),
+                                  ("distinct", 2), ("distinct", 33), ("distinct", 300001)])
+def test_table_sort_and_distinct_match_restatement(orq, op, n):
+    gpu, _ = replay_tsort(GpuBackend(61), op, n, 3)
+    cpu, _ = replay_tsort(OracleBackend(61), op, n, 3)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), (op, n, k)
+
+
+@pytest.mark.parametrize("n,bits", [(1, 40), (1000, 40), (4097, 64), (777, 1)])
+def test_radix_desc_matches_restatement(orq, n, bits):
+    gpu, (key, _, _) = replay_radix(GpuBackend(33), n, 19, bits, True)
+    cpu, _ = replay_radix(OracleBackend(33), n, 19, bits, True)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), (n, bits, k)
