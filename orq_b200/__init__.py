@@ -263,6 +263,10 @@ class BSharedVector(SharedVector):
     def __ixor__(self, o):
         return self._ibin(o, self.rt.lib.orqcu_xor_b)
 
+    def __or__(self, o):
+        """operator| (b_shared_vector.h:438-441): ~(~a & ~b)."""
+        return ~((~self) & (~o))
+
     def __invert__(self):
         z = self.rt._alloc(self.size(), self.width)
         _check(self.rt.lib.orqcu_not_b(self.rt.h, self.width, ctypes.c_size_t(self.size()),

@@ -58,6 +58,8 @@ CASES = [
     ("tsort_n200", "tsort", 200, 6, 5, 64, False),
     ("distinct_n64", "distinct", 64, 5, 4, 64, True),
     ("distinct_n5000", "distinct", 5000, 6, 5, 64, False),
+    ("join_agg_n16", "join_agg", 16, 7, 2, 64, True),
+    ("join_agg_n300", "join_agg", 300, 8, 3, 64, False),
 ]
 
 

@@ -278,6 +278,53 @@ def replay_tsort(be, op, n, seed):
     return out, (v0, v1, v2, va, vb)
 
 
+def join_inputs(n, seed):
+    """Inputs of the "join_agg" op of ref_driver.cpp: A has n rows (pk a
+    Fisher-Yates permutation, group 0..4, value < 10^6), B has 2n rows (fk
+    uniform over pk, quantity 1..50)."""
+    na, nb = n, 2 * n
+    st = splitmix64_fast(seed, (na - 1) + 2 * na + 2 * nb)
+    pk = np.arange(na, dtype=np.int64)
+    k = 0
+    for i in range(na - 1, 0, -1):
+        j = int(st[k] % np.uint64(i + 1))
+        k += 1
+        pk[i], pk[j] = pk[j], pk[i]
+    g = (st[k:k + na] % np.uint64(5)).astype(np.int64)
+    k += na
+    v = (st[k:k + na] % np.uint64(1000000)).astype(np.int64)
+    k += na
+    fk = (st[k:k + nb] % np.uint64(na)).astype(np.int64)
+    k += nb
+    q = (1 + st[k:k + nb] % np.uint64(50)).astype(np.int64)
+    return pk, g, v, fk, q
+
+
+def run_join_agg(rt, pk, g, v, fk, q):
+    """The relational pipeline of the "join_agg" op on the device:
+    A.inner_join(B, [K], copy [G], V); VQ = V*Q; aggregate by [G] (sum, count)."""
+    from orq_b200 import aggregators as ag
+    from orq_b200.table import EncodedTable
+
+    A = EncodedTable.secret_share(rt, [pk, g, v], ["[K]", "[G]", "V"])
+    B = EncodedTable.secret_share(rt, [fk, q], ["[K]", "Q"])
+    J = A.inner_join(B, ["[K]"], [("[G]", "[G]", ag.copy), ("V", "V", ag.copy)])
+    J.addColumns(["VQ", "CNT"])
+    J["VQ"] = J["V"] * J["Q"]
+    J.aggregate(["[G]"], [("VQ", "VQ", ag.sum), ("CNT", "CNT", ag.count)])
+    return J
+
+
+def replay_join(n, seed, shim_seed):
+    be = GpuBackend(shim_seed)
+    J = run_join_agg(be.rt, *join_inputs(n, seed))
+    out = {k: be.np(J[k]) for k in J.getColumnNames()}
+    data, names = J.open_with_schema()
+    for d, nm in zip(data, names):
+        out["open_" + nm] = d.view(np.uint64)[None]
+    return out
+
+
 def same(a, b):
     a = np.ascontiguousarray(a)
     b = np.ascontiguousarray(b)

@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 from replay import (GpuBackend, OracleBackend, radix_inputs, replay_agg, replay_bitonic,
-                    replay_compare, replay_prims, replay_radix, replay_tsort, same)
+                    replay_compare, replay_join, replay_prims, replay_radix, replay_tsort,
+                    same)
 
 pytestmark = pytest.mark.gpu
 
@@ -367,3 +368,20 @@ def test_radix_desc_matches_restatement(orq, n, bits):
     cpu, _ = replay_radix(OracleBackend(33), n, 19, bits, True)
     for k in gpu:
         assert same(gpu[k], cpu[k]), (n, bits, k)
+
+
+def test_join_aggregate_matches_reference_shares(orq, golden, digests):
+    """EncodedTable inner_join + column product + group-by aggregate: every
+    column's shares (valid and invalid rows) equal the reference's"""
+    m = digests["join_agg_n16"]["meta"]
+    out = replay_join(m["n"], m["data_seed"], m["shim_seed"])
+    for name in digests["join_agg_n16"]["arrays"]:
+        assert same(out[name], golden[f"join_agg_n16/{name}"]), name
+
+
+def test_join_aggregate_large_matches_reference_digests(orq, digests):
+    d = digests["join_agg_n300"]
+    m = d["meta"]
+    out = replay_join(m["n"], m["data_seed"], m["shim_seed"])
+    for name, arr in d["arrays"].items():
+        assert [sha(a) for a in out[name]] == arr, name
