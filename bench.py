@@ -1,21 +1,27 @@
 #!/usr/bin/env python
-"""bench.py — 3PC oblivious radix sort on B200 (ORQ's shuffle-based radix sort).
+"""bench.py — ORQ's 3PC oblivious operators on B200.
 
-Workload (per GPU): 2^22 rows, uint64 key uniform in [0, 2^40) boolean-shared,
-two uint32 payload columns arithmetic-shared mod 2^64, seed 7; one step =
-radix_sort(key, ASC, 40) followed by oblivious_apply_elementwise_perm of both
-payloads, including the Fisher–Yates generation of the 44 sharded
-permutations it consumes (ORQ reserves them inside radix_sort).
+Default workload (the headline, per GPU): 2^22 rows, uint64 key uniform in
+[0, 2^40) boolean-shared, two uint32 payload columns arithmetic-shared mod
+2^64, seed 7; one step = radix_sort(key, ASC, 40) followed by
+oblivious_apply_elementwise_perm of both payloads, including the
+Fisher–Yates generation of the 44 sharded permutations it consumes (ORQ
+reserves them inside radix_sort).
+
+Other workloads (--workload): bitonic (2^16 int32 keys, seed 1), join (A
+2^22 rows inner-join B 2^24 rows, product, group-by sum/count), batch (512
+ragged sorts through the batched path) and serve (continuous batching loop
+with p50/p99 latency).
 
   value  device-resident rows/s: shares already in HBM, CUDA events on the
-         runtime's stream around K steps (each step re-copies the unsorted
-         shares), max over ranks.
-  e2e    the same through the C ABI with host buffers: pinned plaintext
-         H2D, secret sharing, sort + payload applies, open, D2H.
+         runtime's stream around each of K steps (each step re-copies the
+         input shares), max over ranks.
+  e2e    the same through the public API with host buffers: pinned plaintext
+         H2D, secret sharing, the operators, open, D2H.
   --impl reference   ORQ's own CPU code (oracle/_ref/ref_driver: three party
          processes over its socket communicator) on a bounded sample.
 
-Multi-GPU: independent replicas (each rank sorts its own 2^22 rows; weak
+Multi-GPU: independent replicas (each rank runs its own workload; weak
 scaling, no collective on the data path).
 """
 from __future__ import annotations
@@ -38,6 +44,7 @@ WORKLOAD = ("3PC oblivious shuffle-based radix sort, 2^22 rows, uint64 key unifo
 # T-table AES-256: 16 shared-memory lookups per round x 14 rounds (+4 in the
 # last) = 228 LDS per block at one warp-wide LDS per clock per SM.
 AES_LDS_PER_BLOCK = 228
+DEFAULT_N = 1 << 22
 # DRAM traffic of the dominant k_apply instance (padded 16-byte key + int32
 # permutation, one group), dram__bytes_read.sum + dram__bytes_write.sum from
 # one ncu capture at 2^21 rows (profiles/radix_sort_2p22.md): 729 MB, scaled
@@ -121,10 +128,278 @@ def parse_profile(text):
     return out
 
 
+class RadixWorkload:
+    """Config 2 (the headline): radix_sort(key, ASC, 40) of 2^22 rows plus two
+    payload applies."""
+
+    name = "radix"
+
+    def __init__(self, args, seed):
+        self.n, self.bits, self.seed = args.n, args.bits, seed
+        self.units = self.n
+        self.flush_l2 = False  # 302 MB of shares per step, larger than L2
+        self.config = {"workload": WORKLOAD, "rows_per_gpu": self.n, "key_bits": self.bits, "payloads": 2,
+                       "l2": "inputs larger than L2 (302 MB of shares per GPU)", "seed": 7}
+
+    def setup(self, rt, orq):
+        import numpy as np
+
+        self.orq, self.rt, self.np = orq, rt, np
+        self.key, self.p1, self.p2 = gen_inputs(self.n, self.seed, self.bits)
+        self.kb = rt.secret_share_b(self.key, 0)
+        self.a1 = rt.secret_share_a(self.p1, 0)
+        self.a2 = rt.secret_share_a(self.p2, 0)
+        self.orig = [self.kb.shares.clone(), self.a1.shares.clone(), self.a2.shares.clone()]
+
+    def step(self):
+        orq = self.orq
+        self.kb.shares.copy_(self.orig[0])
+        self.a1.shares.copy_(self.orig[1])
+        self.a2.shares.copy_(self.orig[2])
+        perm = orq.radix_sort(self.kb, orq.ASC, self.bits)
+        orq.oblivious_apply_elementwise_perm(self.a1, perm)
+        orq.oblivious_apply_elementwise_perm(self.a2, perm)
+
+    def check(self):
+        np = self.np
+        ko = self.kb.open().cpu().numpy().view(np.uint64)
+        return bool(np.all(ko[1:] >= ko[:-1])) and np.array_equal(np.sort(self.key), ko)
+
+    def e2e_setup(self, dev):
+        import torch
+
+        np, n = self.np, self.n
+        self.pin = [torch.from_numpy(a.view(np.int64)).pin_memory() for a in (self.key, self.p1, self.p2)]
+        self.outs = [torch.empty(n, dtype=torch.int64).pin_memory() for _ in range(3)]
+        self.dbuf = [torch.empty(n, dtype=torch.int64, device=dev) for _ in range(3)]
+        self.h2d = self.d2h = 3 * n * 8
+
+    def e2e_step(self):
+        orq, rt = self.orq, self.rt
+        for h, d in zip(self.pin, self.dbuf):
+            d.copy_(h, non_blocking=True)
+        k = rt.secret_share_b(self.dbuf[0], 0)
+        x1 = rt.secret_share_a(self.dbuf[1], 0)
+        x2 = rt.secret_share_a(self.dbuf[2], 0)
+        perm = orq.radix_sort(k, orq.ASC, self.bits)
+        orq.oblivious_apply_elementwise_perm(x1, perm)
+        orq.oblivious_apply_elementwise_perm(x2, perm)
+        for v, o in zip((k, x1, x2), self.outs):
+            o.copy_(v.open(), non_blocking=True)
+
+    def e2e_check(self):
+        return bool(self.np.array_equal(self.outs[0].numpy().view(self.np.uint64), self.np.sort(self.key)))
+
+    def cpu_reference(self, sample, threads):
+        sec = run_ref_seconds("radix_time", sample, 7, self.bits, threads)
+        return sample / sec, sec, (f"n={sample} rows of the same distributions (bounded sample of the 2^22 "
+                              f"workload), ORQ's own radix_sort + 2 payload applies, 3 party processes x "
+                              f"{threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
+
+
+class BitonicWorkload:
+    """Config 1: bitonic_sort of 2^16 int32 keys drawn over all 32 bits from
+    seed 1, ascending (the reference's CPU configuration, on the GPU here)."""
+
+    name = "bitonic"
+
+    def __init__(self, args, seed):
+        self.n = args.n if args.n != DEFAULT_N else 1 << 16
+        self.seed = 1 + (seed - 7)
+        self.units = self.n
+        self.flush_l2 = True  # 786 KB of shares: L2 is flushed between steps
+        self.config = {"workload": f"3PC bitonic sort, {self.n} int32 keys B-shared, uniform over 32 bits, "
+                                   "seed 1, ascending", "rows_per_gpu": self.n,
+                       "l2": "L2 flushed (256 MB write) between timed steps", "seed": 1}
+
+    def setup(self, rt, orq):
+        import numpy as np
+
+        self.orq, self.rt, self.np = orq, rt, np
+        self.key = splitmix(self.seed, self.n).astype(np.uint32)
+        self.kb = rt.secret_share_b(self.key.view(np.int32), 0)
+        self.orig = self.kb.shares.clone()
+
+    def step(self):
+        self.kb.shares.copy_(self.orig)
+        self.orq.bitonic_sort(self.kb, self.orq.ASC)
+
+    def check(self):
+        np = self.np
+        ko = self.kb.open().cpu().numpy().view(np.int32)
+        return bool(np.array_equal(np.sort(self.key.view(np.int32)), ko))
+
+    def e2e_setup(self, dev):
+        import torch
+
+        np, n = self.np, self.n
+        self.pin = torch.from_numpy(self.key.view(np.int32).copy()).pin_memory()
+        self.out = torch.empty(n, dtype=torch.int32).pin_memory()
+        self.dbuf = torch.empty(n, dtype=torch.int32, device=dev)
+        self.h2d = self.d2h = n * 4
+
+    def e2e_step(self):
+        self.dbuf.copy_(self.pin, non_blocking=True)
+        k = self.rt.secret_share_b(self.dbuf, 0)
+        self.orq.bitonic_sort(k, self.orq.ASC)
+        self.out.copy_(k.open(), non_blocking=True)
+
+    def e2e_check(self):
+        np = self.np
+        return bool(np.array_equal(self.out.numpy(), np.sort(self.key.view(np.int32))))
+
+    def cpu_reference(self, sample, threads):
+        n = self.n
+        sec = run_ref_seconds("bitonic_time", n, self.seed, 32, threads)
+        return n / sec, sec, (f"the full workload (n={n}), ORQ's own bitonic_sort, 3 party processes x "
+                         f"{threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
+
+
+def zipf_keys(u, s=1.1, m=10000):
+    """Zipf(s) over m values by inverse CDF of u in [0, 1)."""
+    import numpy as np
+
+    w = 1.0 / np.arange(1, m + 1, dtype=np.float64) ** s
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    return np.minimum(np.searchsorted(cdf, u, side="right"), m - 1).astype(np.int64)
+
+
+def gen_join(seed, na, nb):
+    """Config 3 tables: A (pk = seeded Fisher-Yates permutation of 0..na-1,
+    group Zipf s=1.1 over 10^4 values, value uniform [0, 10^6)); B (fk uniform
+    over A.pk, quantity uniform [1, 50])."""
+    import numpy as np
+
+    st = splitmix(seed, 2 * na + 2 * nb)
+    pk = np.random.Generator(np.random.PCG64(seed)).permutation(na).astype(np.int64)
+    u = (st[:na] >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+    g = zipf_keys(u)
+    v = (st[na:2 * na] % np.uint64(1000000)).astype(np.int64)
+    fk = (st[2 * na:2 * na + nb] % np.uint64(na)).astype(np.int64)
+    q = (1 + st[2 * na + nb:] % np.uint64(50)).astype(np.int64)
+    return pk, g, v, fk, q
+
+
+def join_expected(pk, g, v, fk, q):
+    """SELECT g, SUM(value*qty), COUNT(*) FROM A JOIN B ON pk = fk GROUP BY g."""
+    import numpy as np
+
+    gv = np.empty(len(pk), dtype=np.int64)
+    vv = np.empty(len(pk), dtype=np.int64)
+    gv[pk] = g
+    vv[pk] = v
+    gb, vb = gv[fk], vv[fk] * q
+    keys = np.unique(gb)
+    sums = np.bincount(np.searchsorted(keys, gb), weights=None, minlength=len(keys))
+    tot = np.zeros(len(keys), dtype=np.int64)
+    np.add.at(tot, np.searchsorted(keys, gb), vb)
+    return keys, tot, sums.astype(np.int64)
+
+
+class JoinWorkload:
+    """Config 3: A (2^22 rows) inner-join B (2^24 rows) on pk = fk, copying
+    the group key and value; VQ = value * quantity; group-by SUM(VQ), COUNT."""
+
+    name = "join"
+
+    def __init__(self, args, seed):
+        self.na = args.na
+        self.nb = 4 * self.na
+        self.seed = seed
+        self.units = self.na + self.nb
+        self.flush_l2 = False
+        self.config = {"workload": f"3PC PK-FK join + group-by: A {self.na} rows (pk perm, Zipf(1.1, 10^4) "
+                                   f"group, value U[0,10^6)), B {self.nb} rows (fk U over pk, qty U[1,50]); "
+                                   "inner_join copy g, value; vq = value*qty; aggregate by g: sum(vq), count",
+                       "rows_per_gpu": self.units, "l2": "inputs larger than L2", "seed": seed}
+
+    def setup(self, rt, orq):
+        import numpy as np
+
+        from orq_b200.table import EncodedTable
+
+        self.orq, self.rt, self.np, self.ET = orq, rt, np, EncodedTable
+        self.data = gen_join(self.seed, self.na, self.nb)
+        pk, g, v, fk, q = self.data
+        self.A0 = EncodedTable.secret_share(rt, [pk, g, v], ["[K]", "[G]", "V"])
+        self.B0 = EncodedTable.secret_share(rt, [fk, q], ["[K]", "Q"])
+
+    def _copy(self, t):
+        cols = {k: type(t[k])(self.rt, t[k].shares.clone()) for k in t.getColumnNames()}
+        return self.ET(self.rt, cols, t.rows)
+
+    def _pipeline(self, A, B):
+        ag = self.orq.aggregators
+        J = A.inner_join(B, ["[K]"], [("[G]", "[G]", ag.copy), ("V", "V", ag.copy)])
+        J.addColumns(["VQ", "CNT"])
+        J["VQ"] = J["V"] * J["Q"]
+        J.aggregate(["[G]"], [("VQ", "VQ", ag.sum), ("CNT", "CNT", ag.count)])
+        return J
+
+    def step(self):
+        self.J = self._pipeline(self._copy(self.A0), self._copy(self.B0))
+
+    def _check_table(self, cols, names):
+        np = self.np
+        keys, tot, cnt = join_expected(*self.data)
+        d = dict(zip(names, cols))
+        order = np.argsort(d["[G]"], kind="stable")
+        return (np.array_equal(d["[G]"][order], keys) and np.array_equal(d["VQ"][order], tot)
+                and np.array_equal(d["CNT"][order], cnt))
+
+    def check(self):
+        cols, names = self.J.open_with_schema()
+        return bool(self._check_table([c.view(self.np.int64) for c in cols], names))
+
+    def e2e_setup(self, dev):
+        import torch
+
+        np = self.np
+        self.pin = [torch.from_numpy(a).pin_memory() for a in self.data]
+        self.dbuf = [torch.empty(len(a), dtype=torch.int64, device=dev) for a in self.data]
+        self.h2d = 8 * (3 * self.na + 2 * self.nb)
+
+    def e2e_step(self):
+        import torch
+
+        for h, d in zip(self.pin, self.dbuf):
+            d.copy_(h, non_blocking=True)
+        rt, ET = self.rt, self.ET
+        A = ET(rt, {"[K]": rt.secret_share_b(self.dbuf[0], 0), "[G]": rt.secret_share_b(self.dbuf[1], 0),
+                    "V": rt.secret_share_a(self.dbuf[2], 0)}, self.na)
+        B = ET(rt, {"[K]": rt.secret_share_b(self.dbuf[3], 0), "Q": rt.secret_share_a(self.dbuf[4], 0)}, self.nb)
+        J = self._pipeline(A, B)
+        # open every column (the result table) and copy it to pinned host memory
+        names = J.getColumnNames()
+        opened = [J[k].open() for k in names]
+        self.e2e_out = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in opened]
+        for h, o in zip(self.e2e_out, opened):
+            h.copy_(o, non_blocking=True)
+        self.e2e_names = names
+        self.d2h = sum(o.numel() * o.element_size() for o in opened)
+
+    def e2e_check(self):
+        np = self.np
+        d = dict(zip(self.e2e_names, [o.numpy().view(np.int64) for o in self.e2e_out]))
+        keep = d.pop("[##V]") != 0
+        names = list(d)
+        return bool(self._check_table([d[k][keep] for k in names], names))
+
+    def cpu_reference(self, sample, threads):
+        na = max(64, sample)
+        sec = run_ref_seconds("join_time", na, self.seed, 64, threads)
+        return 5 * na / sec, sec, (f"A={na}, B={4 * na} rows of the same distributions (bounded sample), ORQ's "
+                              f"own inner_join + product + aggregate (radix sort protocol), 3 party processes "
+                              f"x {threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
+
+
+WORKLOADS = {"radix": RadixWorkload, "bitonic": BitonicWorkload, "join": JoinWorkload}
+
+
 def run_orq(args, rank, world, local_rank):
     import ctypes
 
-    import numpy as np
     import torch
 
     import orq_b200 as orq
@@ -143,28 +418,15 @@ def run_orq(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
-    n, bits = args.n, args.bits
+    wl = WORKLOADS[args.workload](args, 7 + rank)
     rt = orq.Runtime(seed=7 + rank, device=local_rank)
-    key, p1, p2 = gen_inputs(n, 7 + rank, bits)
-    kb = rt.secret_share_b(key, 0)
-    a1 = rt.secret_share_a(p1, 0)
-    a2 = rt.secret_share_a(p2, 0)
-    orig = [kb.shares.clone(), a1.shares.clone(), a2.shares.clone()]
-
-    def step():
-        kb.shares.copy_(orig[0])
-        a1.shares.copy_(orig[1])
-        a2.shares.copy_(orig[2])
-        perm = orq.radix_sort(kb, orq.ASC, bits)
-        orq.oblivious_apply_elementwise_perm(a1, perm)
-        orq.oblivious_apply_elementwise_perm(a2, perm)
+    wl.setup(rt, orq)
+    flush = torch.empty(1 << 26, dtype=torch.float32, device=dev) if wl.flush_l2 else None
 
     for _ in range(args.warmup):
-        step()
+        wl.step()
     torch.cuda.synchronize()
-    # correctness of the last warm-up step (opened, size-independent checks)
-    ko = kb.open().cpu().numpy().view(np.uint64)
-    ok = bool(np.all(ko[1:] >= ko[:-1])) and np.array_equal(np.sort(key), ko)
+    ok = wl.check()
 
     clocks = ClockSampler(local_rank)
     _lib = rt.lib
@@ -173,16 +435,20 @@ def run_orq(args, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record()
+    evs = []
     for _ in range(args.steps):
-        step()
-    ev1.record()
+        if flush is not None:
+            flush.fill_(1.0)  # write 256 MB: evicts L2 between timed steps
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        wl.step()
+        e1.record()
+        evs.append((e0, e1))
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier()
-    ms = ev0.elapsed_time(ev1)
+    ms = sum(a.elapsed_time(b) for a, b in evs)
     launches = rt.kernels_launched() - k0
     buf = ctypes.create_string_buffer(1 << 16)
     orq._check(_lib.orqcu_profile_report(rt.h, buf, ctypes.c_size_t(len(buf))))
@@ -193,26 +459,11 @@ def run_orq(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
 
-    # ---- e2e through the C ABI with host buffers --------------------------
+    # ---- e2e through the public API with host buffers ----------------------
     e2e = None
     if not args.no_e2e:
-        pin = [torch.from_numpy(a.view(np.int64)).pin_memory() for a in (key, p1, p2)]
-        outs = [torch.empty(n, dtype=torch.int64).pin_memory() for _ in range(3)]
-        dbuf = [torch.empty(n, dtype=torch.int64, device=dev) for _ in range(3)]
-
-        def e2e_step():
-            for h, d in zip(pin, dbuf):
-                d.copy_(h, non_blocking=True)
-            k = rt.secret_share_b(dbuf[0], 0)
-            x1 = rt.secret_share_a(dbuf[1], 0)
-            x2 = rt.secret_share_a(dbuf[2], 0)
-            perm = orq.radix_sort(k, orq.ASC, bits)
-            orq.oblivious_apply_elementwise_perm(x1, perm)
-            orq.oblivious_apply_elementwise_perm(x2, perm)
-            for v, o in zip((k, x1, x2), outs):
-                o.copy_(v.open(), non_blocking=True)
-
-        e2e_step()
+        wl.e2e_setup(dev)
+        wl.e2e_step()
         torch.cuda.synchronize()
         ke = max(1, min(args.steps, 3))
         barrier()
@@ -220,7 +471,7 @@ def run_orq(args, rank, world, local_rank):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(ke):
-            e2e_step()
+            wl.e2e_step()
         e1.record()
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
@@ -228,13 +479,12 @@ def run_orq(args, rank, world, local_rank):
             t = torch.tensor([ems], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
-        ok = ok and bool(np.array_equal(outs[0].numpy().view(np.uint64), np.sort(key)))
-        e2e = {"value": world * n * ke / (ems / 1e3), "unit": "rows/s",
-               "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 3 * n * 8,
-               "ms_per_step": ems / ke}
+        ok = ok and wl.e2e_check()
+        e2e = {"value": world * wl.units * ke / (ems / 1e3), "unit": "rows/s",
+               "h2d_bytes_per_step": wl.h2d, "d2h_bytes_per_step": wl.d2h, "ms_per_step": ems / ke}
     if dist is not None:
         dist.destroy_process_group()
-    return ms, launches, prof, clk, e2e, ok
+    return wl, ms, launches, prof, clk, e2e, ok
 
 
 def roofline(prof, steps, n):
@@ -249,7 +499,8 @@ def roofline(prof, steps, n):
         ach = (v["bytes"] / v["launches"]) / (per_launch_ms / 1e3) / 1e9
         out["roofline"] = {"bound": "hbm", "kernel": name, "achieved": round(ach, 1), "peak": hbm,
                            "unit": "GB/s", "frac": round(ach / hbm, 4),
-                           "traffic": (round(APPLY_TRAFFIC_BYTES_PER_ROW * n) if name == "apply_group" else None),
+                           "traffic": (round(APPLY_TRAFFIC_BYTES_PER_ROW * n)
+                                       if name == "apply_group" and n else None),
                            "traffic_note": "bytes per launch of the key-apply instance, ncu at 2^21 rows scaled by rows",
                            "peak_source": src, "launches_per_step": v["launches"] / steps,
                            "avg_launch_ms": round(per_launch_ms, 4)}
@@ -270,13 +521,13 @@ def roofline(prof, steps, n):
     return out
 
 
-def cpu_reference(n_sample, bits, threads, timeout=900):
-    """ORQ's own CPU radix sort on the host (three party processes)."""
+def run_ref_seconds(op, n, seed, bits, threads, timeout=1800):
+    """ORQ's own CPU code for one op (oracle/_ref/ref_driver, three party
+    processes); returns the seconds it reports for the timed region."""
     from oracle import run_ref
 
     t0 = time.time()
-    _, out = run_ref.run("radix_time", n_sample, 7, shim_seed=7, bits=bits, threads=threads,
-                         timeout=timeout)
+    _, out = run_ref.run(op, n, seed, shim_seed=7, bits=bits, threads=threads, timeout=timeout)
     wall = time.time() - t0
     sec = None
     for line in out.splitlines():
@@ -285,39 +536,52 @@ def cpu_reference(n_sample, bits, threads, timeout=900):
     return sec if sec else wall
 
 
+def splitmix(seed, n):
+    """SplitMix64 outputs for state seed (Steele, Lea, Flood, OOPSLA 2014)."""
+    import numpy as np
+
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + np.arange(1, n + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="orq", choices=["orq", "reference"])
-    ap.add_argument("--n", type=int, default=1 << 22)
+    ap.add_argument("--workload", default="radix", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=DEFAULT_N)
+    ap.add_argument("--na", type=int, default=1 << 22, help="join: rows of A (B has 4x)")
     ap.add_argument("--bits", type=int, default=40)
     ap.add_argument("--cpu-sample", type=int, default=1 << 17)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload == "join" and args.cpu_sample == 1 << 17:
+        args.cpu_sample = 1 << 11
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     nproc = os.cpu_count() or 1
-    config = {"workload": WORKLOAD, "rows_per_gpu": args.n, "key_bits": args.bits, "payloads": 2,
-              "parallelism": f"replicas x{args.gpus}", "l2": "inputs larger than L2 (302 MB of shares per GPU)",
-              "seed": 7}
 
     if args.impl == "reference":
         if rank != 0:
             return
+        wl = WORKLOADS[args.workload](args, 7)
+        config = dict(wl.config, parallelism=f"replicas x{args.gpus}")
         threads = max(1, nproc // 3)
         for _ in range(args.warmup):
-            cpu_reference(args.cpu_sample, args.bits, threads)
-        secs = [cpu_reference(args.cpu_sample, args.bits, threads) for _ in range(args.steps)]
-        v = args.cpu_sample / statistics.mean(secs)
-        sample = (f"n={args.cpu_sample} rows of the same distributions per step (bounded sample of the "
-                  f"2^22 workload), 3 party processes x {threads} worker threads, batch -1, NoCopy sockets")
+            wl.cpu_reference(args.cpu_sample, threads)
+        runs = [wl.cpu_reference(args.cpu_sample, threads) for _ in range(args.steps)]
+        v = statistics.mean(r[0] for r in runs)
+        sample = runs[0][2]
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": "rows/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(secs),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(r[1] for r in runs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic", "config": config,
             "cpu_baseline": {"value": v, "unit": "rows/s", "cores": 3 * threads, "kind": "reference",
@@ -325,26 +589,24 @@ def main():
             "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
-    ms, launches, prof, clk, e2e, ok = run_orq(args, rank, world, local_rank)
+    wl, ms, launches, prof, clk, e2e, ok = run_orq(args, rank, world, local_rank)
     if rank != 0:
         return
-    value = world * args.n * args.steps / (ms / 1e3)
+    config = dict(wl.config, parallelism=f"replicas x{world}")
+    value = world * wl.units * args.steps / (ms / 1e3)
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": config,
         "correct": ok, "gpu_launches": launches, "clocks": clk,
     }
-    line.update(roofline(prof, args.steps, args.n))
+    line.update(roofline(prof, args.steps, wl.units if wl.name == "radix" else None))
     if e2e:
         line["e2e"] = e2e
     if not args.no_cpu_baseline and world == 1:
-        sec = cpu_reference(args.cpu_sample, args.bits, 1)
-        line["cpu_baseline"] = {"value": args.cpu_sample / sec, "unit": "rows/s", "cores": 3,
-                                "kind": "reference",
-                                "sample": f"n={args.cpu_sample} rows, same distributions, ORQ's own "
-                                          "radix_sort + 2 payload applies, 3 party processes x 1 thread, "
-                                          "batch -1, NoCopy sockets over 127.0.0.1"}
+        v, _, sample = wl.cpu_reference(args.cpu_sample, 1)
+        line["cpu_baseline"] = {"value": v, "unit": "rows/s", "cores": 3, "kind": "reference",
+                                "sample": sample}
     print(json.dumps(line))
 
 

@@ -11,6 +11,7 @@
 //   schedule the device runtime reproduces.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -119,6 +120,40 @@ int main(int argc, char** argv) {
         run_prims<int32_t>(n, seed, d, "w4_");
         run_prims<int64_t>(n, seed + 1, d, "w8_");
         run_prims<int8_t>(n, seed + 2, d, "w1_");
+    } else if (op == "join_time") {
+        // Timing only: the relational pipeline of join_agg on n A rows and 4n B
+        // rows with the distributions of the 2^22 x 2^24 configuration (group
+        // key Zipf s=1.1 over 10^4 values by inverse CDF).
+        uint64_t st = seed;
+        const size_t na = n, nb = 4 * n;
+        std::vector<double> cdf(10000);
+        double acc = 0;
+        for (int k = 0; k < 10000; k++) cdf[k] = (acc += 1.0 / std::pow(k + 1.0, 1.1));
+        for (auto& c : cdf) c /= acc;
+        orq::Vector<int64_t> pk(na), g(na), v(na), fk(nb), q(nb);
+        for (size_t i = 0; i < na; i++) pk[i] = (int64_t)i;
+        for (size_t i = na; i-- > 1;) std::swap(pk[i], pk[sm64(st) % (i + 1)]);
+        for (size_t i = 0; i < na; i++) {
+            double u = (double)(sm64(st) >> 11) * (1.0 / 9007199254740992.0);
+            size_t k = std::upper_bound(cdf.begin(), cdf.end(), u) - cdf.begin();
+            g[i] = (int64_t)std::min<size_t>(k, 9999);
+        }
+        for (size_t i = 0; i < na; i++) v[i] = (int64_t)(sm64(st) % 1000000);
+        for (size_t i = 0; i < nb; i++) fk[i] = (int64_t)(sm64(st) % na);
+        for (size_t i = 0; i < nb; i++) q[i] = (int64_t)(1 + sm64(st) % 50);
+        std::vector<orq::Vector<int64_t>> ca = {pk, g, v};
+        std::vector<orq::Vector<int64_t>> cb = {fk, q};
+        EncodedTable<int64_t> A = secret_share(ca, {"[K]", "[G]", "V"});
+        EncodedTable<int64_t> B = secret_share(cb, {"[K]", "Q"});
+        t0 = std::chrono::steady_clock::now();
+        auto J = A.inner_join(B, {"[K]"}, {{"[G]", "[G]", copy<BSharedVector<int64_t>>},
+                                           {"V", "V", copy<ASharedVector<int64_t>>}});
+        J.addColumns(std::vector<std::string>{"VQ", "CNT"});
+        J["VQ"] = J["V"] * J["Q"];
+        J.aggregate({"[G]"}, {{"VQ", "VQ", sum<ASharedVector<int64_t>>},
+                              {"CNT", "CNT", count<ASharedVector<int64_t>>}});
+        secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        auto T = J.open_with_schema();
     } else if (op == "join_agg") {
         // The relational pipeline on small tables: A(n rows) = {[K] pk (a
         // Fisher-Yates permutation of 0..n-1), [G] group (0..4), V value

@@ -385,3 +385,33 @@ def test_join_aggregate_large_matches_reference_digests(orq, digests):
     out = replay_join(m["n"], m["data_seed"], m["shim_seed"])
     for name, arr in d["arrays"].items():
         assert [sha(a) for a in out[name]] == arr, name
+
+
+def _sqlite_join_groupby(pk, g, v, fk, q):
+    import sqlite3
+
+    con = sqlite3.connect(":memory:")
+    con.execute("CREATE TABLE A (pk INTEGER PRIMARY KEY, g INTEGER, value INTEGER)")
+    con.execute("CREATE TABLE B (fk INTEGER, qty INTEGER)")
+    con.executemany("INSERT INTO A VALUES (?, ?, ?)", zip(pk.tolist(), g.tolist(), v.tolist()))
+    con.executemany("INSERT INTO B VALUES (?, ?)", zip(fk.tolist(), q.tolist()))
+    rows = con.execute("SELECT g, SUM(value * qty), COUNT(*) FROM A JOIN B ON A.pk = B.fk "
+                       "GROUP BY g ORDER BY g").fetchall()
+    return [tuple(r) for r in rows]
+
+
+@pytest.mark.parametrize("na", [1 << 10, 1 << 13])
+def test_join_groupby_config3_distributions_vs_sqlite(orq, na):
+    """the 2^22 x 2^24 join + group-by at reduced size with the same
+    distributions (pk permutation, Zipf(1.1) groups over 10^4 values): the
+    opened result equals sqlite's on the plaintext"""
+    from bench import gen_join
+    from replay import run_join_agg
+
+    data = gen_join(11, na, 4 * na)
+    rt = orq.Runtime(seed=5)
+    J = run_join_agg(rt, *data)
+    cols, names = J.open_with_schema()
+    d = dict(zip(names, [c.view(np.int64) for c in cols]))
+    got = sorted(zip(d["[G]"].tolist(), d["VQ"].tolist(), d["CNT"].tolist()))
+    assert got == _sqlite_join_groupby(*data)
