@@ -219,6 +219,17 @@ int orqcu_table_sort(orqcu_runtime* rt, int width, size_t n, int ncols, void* co
 int orqcu_distinct(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* keys,
                    void* const res[3]);
 
+/* Batched bitonic_sort: `count` independent B-shared key columns of
+ * power-of-two sizes n[i] (keys[3*i+p]), each ascending or descending. The
+ * shares produced are exactly those of `count` orqcu_bitonic_sort calls in
+ * list order. Execution is batched: one persistent launch per network round
+ * walks a ragged work list of every column that still has a stage, the
+ * threads per CTA are autotuned once per size class, and with use_graph the
+ * rounds are captured once per batch shape into a CUDA graph that later calls
+ * replay. No reference counterpart: ORQ sorts one vector per call. */
+int orqcu_bitonic_sort_batch(orqcu_runtime* rt, int width, int count, const size_t* n,
+                             void* const* keys, const int* descending, int use_graph);
+
 #ifdef __cplusplus
 }
 #endif

@@ -438,6 +438,20 @@ def distinct(keys) -> BSharedVector:
     return BSharedVector(rt, res)
 
 
+def bitonic_sort_batch(vectors, order=ASC, use_graph: bool = True):
+    """Batched bitonic_sort of many independent key columns (power-of-two
+    sizes, same width), in place: the shares equal those of calling
+    bitonic_sort on each column in list order. `order` is one order or a list."""
+    if not vectors:
+        return
+    rt, w = vectors[0].rt, vectors[0].width
+    orders = order if isinstance(order, (list, tuple)) else [order] * len(vectors)
+    ns = (ctypes.c_size_t * len(vectors))(*[v.size() for v in vectors])
+    _check(rt.lib.orqcu_bitonic_sort_batch(rt.h, w, len(vectors), ns, _flat(vectors),
+                                           (ctypes.c_int * len(vectors))(*[int(o == DESC) for o in orders]),
+                                           int(bool(use_graph))))
+
+
 def radix_sort(v: BSharedVector, order: int = ASC, bits: int | None = None) -> ElementwisePermutation:
     """orq::operators::radix_sort (radixsort.h:205-229): sorts v in place and
     returns the A-shared sorting permutation."""

@@ -110,6 +110,17 @@ __device__ __forceinline__ void aes256_encrypt(const AesSmem& S, const AesRK& rk
     s3 = n3 ^ rk.k[59];
 }
 
+// Keystream block `blk` of a draw that starts at nonce `nonce0` of the stream
+// keyed by rk.
+__device__ __forceinline__ uint4 keystream_block_n(const AesSmem& S, const AesRK& rk,
+                                                   unsigned long long nonce0, unsigned long long blk) {
+    const unsigned long long nonce = nonce0 + (blk >> 16);
+    uint32_t s0 = (uint32_t)nonce, s1 = (uint32_t)(nonce >> 32), s2 = 0u;
+    uint32_t s3 = __byte_perm((uint32_t)(blk & 0xffffu) + 2u, 0, 0x0123);
+    aes256_encrypt(S, rk, s0, s1, s2, s3);
+    return make_uint4(s0, s1, s2, s3);
+}
+
 // Keystream block `blk` (16-byte unit) of a draw that starts at nonce `nonce0`.
 __device__ __forceinline__ uint4 keystream_block(const AesSmem& S, const StreamArg& st,
                                                  unsigned long long blk) {

@@ -80,6 +80,7 @@ int orqcu_runtime_destroy(orqcu_runtime* rt) {
         cudaStreamSynchronize(rt->ctx.stream);
         for (auto& sp : rt->ctx.perm_queue) rt->ctx.free_perm(sp);
         rt->ctx.perm_queue.clear();
+        rt->ctx.release_graphs();
         if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
         if (rt->ctx.d_err) cudaFree(rt->ctx.d_err);
         delete rt;
@@ -458,6 +459,23 @@ int orqcu_distinct(orqcu_runtime* rt, int width, size_t n, int nkeys, const void
         }
         need_sh((const void* const*)res, n, "null res");
         orqcu::op_distinct(rt->ctx, width, n, nkeys, k.data(), m3(res));
+    });
+}
+
+int orqcu_bitonic_sort_batch(orqcu_runtime* rt, int width, int count, const size_t* n,
+                             void* const* keys, const int* descending, int use_graph) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "bitonic sort supports 4 and 8-byte keys");
+        need(count >= 0 && (count == 0 || (n && keys && descending)), "bad batch");
+        std::vector<orqcu::Sh3> k(count);
+        for (int i = 0; i < count; i++) {
+            need((n[i] & (n[i] - 1)) == 0, "bitonic sort needs power-of-two sizes");
+            need(n[i] < (1ull << 32), "bitonic batch items must have fewer than 2^32 rows");
+            need_sh((const void* const*)keys + 3 * i, n[i], "null key share");
+            k[i] = m3(keys + 3 * i);
+        }
+        orqcu::op_bitonic_sort_batch(rt->ctx, width, count, n, k.data(), descending, use_graph != 0);
     });
 }
 

@@ -13,7 +13,10 @@
 // zero-sharing keystream of all its rounds into shared memory (every AES block
 // once), then each thread runs the circuit in registers. The packed fix-up
 // (a bit transpose of 8W consecutive pairs) is a warp ballot.
+#include <cstring>
+#include <string>
 #include <type_traits>
+#include <vector>
 
 #include "launch.cuh"
 
@@ -23,9 +26,10 @@ namespace {
 
 // Threads (= pairs) per CTA iteration. The AES tables take 128 KiB of shared
 // memory, so one CTA runs per SM; the per-warp keystream buffers take the rest
-// (3 KiB per warp for int32 stages, 6.75 KiB for int64).
+// (3 KiB per warp for int32 stages, 6.75 KiB for int64; 512 threads keep the
+// int32 tile within 128 registers a thread).
 template <int W>
-constexpr int cmp_threads() { return W == 4 ? 768 : 448; }
+constexpr int cmp_threads() { return W == 4 ? 512 : 448; }
 
 template <typename T>
 struct CmpArgs {
@@ -60,25 +64,22 @@ __device__ __forceinline__ void and3(const T x[3], const T y[3], const T k[3], T
     }
 }
 
-template <typename T, int MODE>  // MODE 0: bitonic stage, MODE 1: compare
-__global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_cmp(CmpArgs<T> a) {
+// One CTA tile of a bitonic stage (MODE 0) or of a compare (MODE 1): the
+// pairs [base, base + blockDim.x).
+template <typename T, int MODE>
+__device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&pairs)[3],
+                                         const unsigned long long (&nonce)[3], unsigned long long base,
+                                         const AesSmem& S, uint32_t* ksw,
+                                         uint32_t (*ksp)[3][4], uint32_t (*ballots)[3][3]) {
     constexpr int W = sizeof(T);
-    constexpr int kCmpThreads = cmp_threads<W>();
     constexpr int B = 8 * W;               // pairs per packed word
     constexpr int L = (W == 4) ? 5 : 6;    // bit_same rounds
     constexpr int NFULL = MODE == 0 ? L + 3 : L + 1;
     constexpr int WORDS = 32 * W / 4;      // keystream words per call and stream per warp
     constexpr int NB = 32 * W / 16;        // AES blocks per call and stream per warp
-    extern __shared__ __align__(16) uint32_t sm[];
-    uint32_t* ksw = sm + kAesSmemBytes / 4;  // [warp][call][stream][WORDS]
-    __shared__ uint32_t ksp[kCmpThreads / 32][3][4];      // packed call block per warp
-    __shared__ uint32_t ballots[kCmpThreads / 32][3][3];  // [warp][s1,s2,r][share]
-    aes_stage_tables(sm);
-    const AesSmem S(sm);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t* myks = ksw + (size_t)warp * NFULL * 3 * WORDS;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < a.m;
-         base += (unsigned long long)gridDim.x * blockDim.x) {
+    {
         const unsigned long long p0w = base + warp * 32;  // this warp's first pair
         const unsigned long long p = p0w + lane;
         const bool valid = p < a.m;
@@ -107,9 +108,7 @@ __global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_cmp(CmpArgs<T> 
             const int call = idx / (3 * NB), q = (idx / NB) % 3, b = idx % NB;
             unsigned long long off = (unsigned long long)call * a.C;
             if (call > L) off = (unsigned long long)(L + 1) * a.C + a.Cp + (unsigned long long)(call - L - 1) * a.C;
-            StreamArg st = a.pair[q];
-            st.nonce += off;
-            const uint4 ks = keystream_block(S, st, p0w * W / 16 + b);
+            const uint4 ks = keystream_block_n(S, pairs[q].rk, nonce[q] + off, p0w * W / 16 + b);
             uint32_t* o = myks + (call * 3 + q) * WORDS + b * 4;
             o[0] = ks.x;
             o[1] = ks.y;
@@ -119,9 +118,9 @@ __global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_cmp(CmpArgs<T> 
         if (lane < 3) {
             // the packed AND: word c = pair / B covers pairs [cB, cB+B)
             const unsigned long long c = p0w / B;
-            StreamArg st = a.pair[lane];
-            st.nonce += (unsigned long long)(L + 1) * a.C;
-            const uint4 ks = keystream_block(S, st, c * W / 16);
+            const unsigned long long nl = lane == 0 ? nonce[0] : (lane == 1 ? nonce[1] : nonce[2]);
+            const uint4 ks = keystream_block_n(S, pairs[lane].rk, nl + (unsigned long long)(L + 1) * a.C,
+                                               c * W / 16);
             ksp[warp][lane][0] = ks.x;
             ksp[warp][lane][1] = ks.y;
             ksp[warp][lane][2] = ks.z;
@@ -257,7 +256,78 @@ __global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_cmp(CmpArgs<T> 
                     a.key[j][yi] = Y[j] ^ Z[j];
                 }
         }
-        __syncthreads();  // keystream buffers are rewritten by the next iteration
+        __syncthreads();  // keystream buffers are rewritten by the next tile
+    }
+}
+
+template <typename T, int MODE>  // MODE 0: bitonic stage, MODE 1: compare
+__global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_cmp(CmpArgs<T> a) {
+    constexpr int kCmpThreads = cmp_threads<sizeof(T)>();
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t ksp[kCmpThreads / 32][3][4];      // packed call block per warp
+    __shared__ uint32_t ballots[kCmpThreads / 32][3][3];  // [warp][s1,s2,r][share]
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    const unsigned long long nonce[3] = {a.pair[0].nonce, a.pair[1].nonce, a.pair[2].nonce};
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < a.m;
+         base += (unsigned long long)gridDim.x * blockDim.x)
+        cmp_tile<T, MODE>(a, a.pair, nonce, base, S, sm + kAesSmemBytes / 4, ksp, ballots);
+}
+
+// ---- batched bitonic sorting -------------------------------------------------
+// Many independent sorts advance one network stage per launch ("round"): a
+// round's work list holds (item, first pair) tiles of every item that still
+// has a stage; stage r has the same (box size, reversal) for every item, and
+// item i's nonces at stage r are its base plus r times its per-stage use, so
+// the shares equal those of sequential plain calls in list order.
+struct CmpBatchItem {
+    void* key[3];
+    unsigned long long m;          // pairs (n / 2)
+    unsigned long long nonce0[3];  // PAIR nonces at the item's first stage
+    unsigned long long C, Cp;      // nonces per full / packed AND call
+    int stages;
+    int desc;
+};
+
+template <typename T>
+struct CmpBatchArgs {
+    CmpArgs<T> proto;  // keys of the PAIR streams
+    const CmpBatchItem* items;
+    const uint2* work;  // (item, first pair) per tile
+    unsigned nwork;
+    int round, hs, first;
+};
+
+// at most 512 threads per CTA (the item bookkeeping needs registers)
+template <int W>
+constexpr int batch_max_threads() { return W == 4 ? 512 : 448; }
+
+template <typename T>
+__global__ void __launch_bounds__(batch_max_threads<sizeof(T)>(), 1) k_cmp_batch(CmpBatchArgs<T> ba) {
+    constexpr int W = sizeof(T);
+    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int kCmpThreads = batch_max_threads<W>();
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t ksp[kCmpThreads / 32][3][4];
+    __shared__ uint32_t ballots[kCmpThreads / 32][3][3];
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    for (unsigned w = blockIdx.x; w < ba.nwork; w += gridDim.x) {
+        const uint2 wk = ba.work[w];
+        const CmpBatchItem& it = ba.items[wk.x];
+        CmpArgs<T> a;  // the stream keys stay in the kernel parameters (ba.proto)
+        unsigned long long nonce[3];
+        for (int j = 0; j < 3; j++) {
+            a.key[j] = (T*)it.key[j];
+            nonce[j] = it.nonce0[j] + (unsigned long long)ba.round * ((L + 3) * it.C + it.Cp);
+        }
+        a.m = it.m;
+        a.C = it.C;
+        a.Cp = it.Cp;
+        a.hs = ba.hs;
+        a.first = ba.first;
+        a.desc = it.desc;
+        cmp_tile<T, 0>(a, ba.proto.pair, nonce, wk.y, S, sm + kAesSmemBytes / 4, ksp, ballots);
     }
 }
 
@@ -328,6 +398,238 @@ void bitonic_t(Ctx& c, size_t n, Sh3 key, bool desc) {
         }
 }
 
+// stage r of a bitonic network: round i with i(i+1)/2 <= r, substage jj
+void stage_of(int r, int& hs, int& first) {
+    int i = 0;
+    while ((i + 1) * (i + 2) / 2 <= r) i++;
+    const int jj = r - i * (i + 1) / 2;
+    hs = i - jj;
+    first = jj == 0;
+}
+
+template <typename T>
+void build_items(Ctx& c, int count, const size_t* n, const Sh3* keys, const int* desc,
+                 std::vector<CmpBatchItem>& items, unsigned long long advance[1], int& rounds) {
+    constexpr int W = sizeof(T);
+    constexpr int L = (W == 4) ? 5 : 6;
+    items.resize(count);
+    unsigned long long off = 0;
+    rounds = 0;
+    for (int i = 0; i < count; i++) {
+        CmpBatchItem& it = items[i];
+        int k = 0;
+        while (((size_t)1 << k) < n[i]) k++;
+        it.m = n[i] / 2;
+        it.C = chunks_of(it.m * W);
+        it.Cp = chunks_of(ceil_div(it.m, 8ull * W) * W);
+        it.stages = n[i] < 2 ? 0 : k * (k + 1) / 2;
+        it.desc = desc[i];
+        for (int j = 0; j < 3; j++) {
+            it.key[j] = keys[i].p[j];
+            it.nonce0[j] = c.nonce[PAIR0 + j] + off;
+        }
+        off += (unsigned long long)it.stages * ((L + 3) * it.C + it.Cp);
+        rounds = std::max(rounds, it.stages);
+    }
+    advance[0] = off;
+}
+
+void build_work(const std::vector<CmpBatchItem>& items, int rounds, int nt, std::vector<uint2>& work,
+                std::vector<size_t>& round_off) {
+    work.clear();
+    round_off.assign(rounds + 1, 0);
+    for (int r = 0; r < rounds; r++) {
+        round_off[r] = work.size();
+        for (size_t i = 0; i < items.size(); i++) {
+            if (items[i].stages <= r) continue;
+            for (unsigned long long p = 0; p < items[i].m; p += nt) work.push_back(make_uint2((unsigned)i, (unsigned)p));
+        }
+    }
+    round_off[rounds] = work.size();
+}
+
+template <typename T>
+size_t batch_smem(int nt) {
+    constexpr int W = sizeof(T);
+    constexpr int L = (W == 4) ? 5 : 6;
+    return kAesSmemBytes + (size_t)(nt / 32) * (L + 3) * 3 * (32 * W / 4) * 4;
+}
+
+template <typename T>
+CmpArgs<T> batch_proto(Ctx& c) {
+    CmpArgs<T> p{};
+    for (int q = 0; q < 3; q++) p.pair[q] = c.stream_arg(PAIR0 + q);
+    return p;
+}
+
+template <typename T>
+void launch_rounds(Ctx& c, cudaStream_t st, const CmpArgs<T>& proto, const CmpBatchItem* items_dev,
+                   const uint2* work_dev, const std::vector<size_t>& round_off, int rounds, int nt,
+                   bool profile) {
+    auto kern = k_cmp_batch<T>;
+    ORQ_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)batch_smem<T>(batch_max_threads<sizeof(T)>())));
+    for (int r = 0; r < rounds; r++) {
+        CmpBatchArgs<T> ba;
+        ba.proto = proto;
+        ba.items = items_dev;
+        ba.work = work_dev + round_off[r];
+        ba.nwork = (unsigned)(round_off[r + 1] - round_off[r]);
+        ba.round = r;
+        stage_of(r, ba.hs, ba.first);
+        if (!ba.nwork) continue;
+        const unsigned grid = std::min<unsigned>(ba.nwork, (unsigned)c.num_sms);
+        if (profile) {
+            ProfScope ps(c, "bitonic_batch_round", 0.0, 0.0, st);
+            kern<<<grid, nt, batch_smem<T>(nt), st>>>(ba);
+        } else {
+            kern<<<grid, nt, batch_smem<T>(nt), st>>>(ba);
+        }
+        ORQ_CUDA_CHECK(cudaGetLastError());
+    }
+}
+
+// Autotuner: threads per CTA for a size class, chosen by timing round 0 of
+// the batch on scratch copies of (a prefix of) its keys with every candidate.
+template <typename T>
+int autotune(Ctx& c, const std::vector<CmpBatchItem>& items) {
+    constexpr int W = sizeof(T);
+    const int cands4[] = {256, 384, 512};
+    const int cands8[] = {256, 448};
+    const int* cands = W == 4 ? cands4 : cands8;
+    const int nc = W == 4 ? 3 : 2;
+    // a prefix of items of at most 256 MB of shares
+    std::vector<CmpBatchItem> sub;
+    size_t bytes = 0;
+    for (const auto& it : items) {
+        const size_t b = 2 * it.m * W * 3;
+        if (!sub.empty() && bytes + b > (256u << 20)) break;
+        sub.push_back(it);
+        bytes += b;
+    }
+    Scratch keys(c, bytes + 16), itb(c, sub.size() * sizeof(CmpBatchItem) + 16);
+    size_t off = 0;
+    for (auto& it : sub) {
+        for (int j = 0; j < 3; j++) {
+            void* dst = keys.as<uint8_t>() + off;
+            ORQ_CUDA_CHECK(cudaMemcpyAsync(dst, it.key[j], 2 * it.m * W, cudaMemcpyDeviceToDevice, c.stream));
+            it.key[j] = dst;
+            off += 2 * it.m * W;
+        }
+    }
+    ORQ_CUDA_CHECK(cudaMemcpyAsync(itb.p, sub.data(), sub.size() * sizeof(CmpBatchItem),
+                                   cudaMemcpyHostToDevice, c.stream));
+    const CmpArgs<T> proto = batch_proto<T>(c);
+    cudaEvent_t e0, e1;
+    ORQ_CUDA_CHECK(cudaEventCreate(&e0));
+    ORQ_CUDA_CHECK(cudaEventCreate(&e1));
+    int best = cands[0];
+    float best_ms = 1e30f;
+    for (int k = 0; k < nc; k++) {
+        std::vector<uint2> work;
+        std::vector<size_t> roff;
+        build_work(sub, 1, cands[k], work, roff);
+        Scratch wb(c, work.size() * sizeof(uint2) + 16);
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(wb.p, work.data(), work.size() * sizeof(uint2),
+                                       cudaMemcpyHostToDevice, c.stream));
+        float ms = 0;
+        for (int rep = 0; rep < 2; rep++) {
+            ORQ_CUDA_CHECK(cudaEventRecord(e0, c.stream));
+            launch_rounds<T>(c, c.stream, proto, itb.as<CmpBatchItem>(), wb.as<uint2>(), roff, 1, cands[k], false);
+            ORQ_CUDA_CHECK(cudaEventRecord(e1, c.stream));
+            ORQ_CUDA_CHECK(cudaEventSynchronize(e1));
+            ORQ_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        }
+        c.kernels_launched += 2;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = cands[k];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+template <typename T>
+void bitonic_batch_t(Ctx& c, int count, const size_t* n, const Sh3* keys, const int* desc, bool use_graph) {
+    constexpr int W = sizeof(T);
+    std::vector<CmpBatchItem> items;
+    unsigned long long advance[1];
+    int rounds;
+    build_items<T>(c, count, n, keys, desc, items, advance, rounds);
+    if (rounds == 0) return;
+    // size class: key width and log2 of round 0's pairs
+    unsigned long long pairs0 = 0;
+    for (const auto& it : items) pairs0 += it.stages ? it.m : 0;
+    int lg = 0;
+    while ((1ull << lg) < pairs0) lg++;
+    const std::string cls = "bitonic:" + std::to_string(W) + ":" + std::to_string(lg);
+    int nt;
+    if (auto f = c.tuned.find(cls); f != c.tuned.end()) {
+        nt = f->second;
+    } else {
+        nt = autotune<T>(c, items);
+        c.tuned[cls] = nt;
+    }
+    const CmpArgs<T> proto = batch_proto<T>(c);
+    const size_t ibytes = items.size() * sizeof(CmpBatchItem);
+    if (use_graph) {
+        std::string shape = cls + ":" + std::to_string(nt) + ":";
+        for (int i = 0; i < count; i++) shape += std::to_string(n[i]) + ",";
+        BatchGraph& g = c.graphs[shape];
+        if (!g.exec) {
+            std::vector<uint2> work;
+            std::vector<size_t> roff;
+            build_work(items, rounds, nt, work, roff);
+            ORQ_CUDA_CHECK(cudaMalloc(&g.work, std::max<size_t>(16, work.size() * sizeof(uint2))));
+            ORQ_CUDA_CHECK(cudaMemcpy(g.work, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+            ORQ_CUDA_CHECK(cudaMalloc(&g.items_dev, ibytes));
+            ORQ_CUDA_CHECK(cudaHostAlloc(&g.items_host, ibytes, cudaHostAllocDefault));
+            ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+            g.items_bytes = ibytes;
+            g.nt = nt;
+            if (!c.capture_stream)
+                ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&c.capture_stream, cudaStreamNonBlocking));
+            // the proto's nonces are overwritten per item, so the graph only
+            // depends on the stream keys and the shape
+            cudaGraph_t graph;
+            ORQ_CUDA_CHECK(cudaStreamBeginCapture(c.capture_stream, cudaStreamCaptureModeThreadLocal));
+            ORQ_CUDA_CHECK(cudaMemcpyAsync(g.items_dev, g.items_host, ibytes, cudaMemcpyHostToDevice,
+                                           c.capture_stream));
+            launch_rounds<T>(c, c.capture_stream, proto, (const CmpBatchItem*)g.items_dev,
+                             (const uint2*)g.work, roff, rounds, nt, false);
+            ORQ_CUDA_CHECK(cudaStreamEndCapture(c.capture_stream, &graph));
+            ORQ_CUDA_CHECK(cudaGraphInstantiate(&g.exec, graph, 0));
+            ORQ_CUDA_CHECK(cudaGraphDestroy(graph));
+            for (int r = 0; r < rounds; r++) g.launches += roff[r + 1] > roff[r];
+        }
+        ORQ_CUDA_CHECK(cudaEventSynchronize(g.done));  // the previous replay has read the table
+        std::memcpy(g.items_host, items.data(), ibytes);
+        {
+            ProfScope ps(c, "bitonic_batch_graph", 0.0, 0.0);
+            ORQ_CUDA_CHECK(cudaGraphLaunch(g.exec, c.stream));
+        }
+        ORQ_CUDA_CHECK(cudaEventRecord(g.done, c.stream));
+        c.kernels_launched += g.launches;
+    } else {
+        std::vector<uint2> work;
+        std::vector<size_t> roff;
+        build_work(items, rounds, nt, work, roff);
+        Scratch wb(c, work.size() * sizeof(uint2) + 16), itb(c, ibytes + 16);
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(wb.p, work.data(), work.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                                       c.stream));
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(itb.p, items.data(), ibytes, cudaMemcpyHostToDevice, c.stream));
+        launch_rounds<T>(c, c.stream, proto, itb.as<CmpBatchItem>(), wb.as<uint2>(), roff, rounds, nt,
+                         c.profiling);
+        for (int r = 0; r < rounds; r++) c.kernels_launched += roff[r + 1] > roff[r];
+        // the host vectors are read by the copies above before they return
+        // (pageable memory), and the scratch goes back to the pool in stream order
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    }
+    for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += advance[0];
+}
+
 }  // namespace
 
 void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt) {
@@ -344,4 +646,13 @@ void op_bitonic_sort(Ctx& c, int w, size_t n, Sh3 key, bool desc) {
     else throw std::invalid_argument("bitonic sort supports int32 and int64 keys");
 }
 
+}  // namespace orqcu
+
+namespace orqcu {
+void op_bitonic_sort_batch(Ctx& c, int w, int count, const size_t* n, const Sh3* keys, const int* desc,
+                           bool use_graph) {
+    if (w == 4) bitonic_batch_t<uint32_t>(c, count, n, keys, desc, use_graph);
+    else if (w == 8) bitonic_batch_t<unsigned long long>(c, count, n, keys, desc, use_graph);
+    else throw std::invalid_argument("bitonic sort supports int32 and int64 keys");
+}
 }  // namespace orqcu

@@ -182,6 +182,21 @@ Pool::~Pool() {
     for (auto& kv : live_) cudaFree(kv.first);
 }
 
+void Ctx::release_graphs() {
+    for (auto& kv : graphs) {
+        BatchGraph& g = kv.second;
+        if (g.done) cudaEventSynchronize(g.done);
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.work) cudaFree(g.work);
+        if (g.items_dev) cudaFree(g.items_dev);
+        if (g.items_host) cudaFreeHost(g.items_host);
+        if (g.done) cudaEventDestroy(g.done);
+    }
+    graphs.clear();
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    capture_stream = nullptr;
+}
+
 void Ctx::check_device_error() {
     if (!d_err) return;
     int h = 0;

@@ -76,6 +76,20 @@ struct ProfAgg {
     double ms = 0, bytes = 0, aes_blocks = 0;
 };
 
+// A captured batch of launches, cached per batch shape: the work lists and
+// the item table live on the device; the item table is refreshed from the
+// pinned host copy by the graph's first node on every replay.
+struct BatchGraph {
+    cudaGraphExec_t exec = nullptr;
+    void* work = nullptr;        // device work lists (all rounds)
+    void* items_dev = nullptr;   // device item table
+    void* items_host = nullptr;  // pinned item table (source of the graph's copy)
+    size_t items_bytes = 0;
+    cudaEvent_t done = nullptr;  // last replay finished reading items_host
+    int nt = 0;
+    unsigned long long launches = 0;
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -92,6 +106,10 @@ struct Ctx {
     // (they skip the access); checked at the synchronous points.
     int* d_err = nullptr;
     void check_device_error();
+    std::map<std::string, BatchGraph> graphs;  // batched launches by shape
+    std::map<std::string, int> tuned;          // autotuned threads per CTA by size class
+    cudaStream_t capture_stream = nullptr;     // private stream for graph capture
+    void release_graphs();
     bool profiling = false;
     std::vector<ProfEvent> prof_pending;
     std::map<std::string, ProfAgg> prof_agg;
@@ -194,5 +212,9 @@ void op_compose(Ctx& c, size_t n, Sh3 sigma, Sh3 rho);  // rho <- compose(sigma,
 void op_table_sort(Ctx& c, int w, size_t n, int ncols, const Sh3* cols, const int* desc,
                    const int* single_bit, int na, const Sh3* data_a, int nb, const Sh3* data_b);
 void op_distinct(Ctx& c, int w, size_t n, int nkeys, const CSh3* keys, Sh3 res);
+
+// ---- batched bitonic sort (cmp.cu) ----
+void op_bitonic_sort_batch(Ctx& c, int w, int count, const size_t* n, const Sh3* keys, const int* desc,
+                           bool use_graph);
 
 }  // namespace orqcu

@@ -415,3 +415,34 @@ def test_join_groupby_config3_distributions_vs_sqlite(orq, na):
     d = dict(zip(names, [c.view(np.int64) for c in cols]))
     got = sorted(zip(d["[G]"].tolist(), d["VQ"].tolist(), d["CNT"].tolist()))
     assert got == _sqlite_join_groupby(*data)
+
+
+@pytest.mark.parametrize("w", [4, 8])
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_bitonic_batch_equals_sequential_calls(orq, w, use_graph):
+    """the batched path gives the shares of plain calls in list order, for
+    ragged sizes and mixed orders, on two batches in a row (the second replays
+    a captured graph with new nonces)"""
+    dt = {4: np.uint32, 8: np.uint64}[w]
+    sizes = [1 << k for k in (3, 10, 1, 6, 12, 0, 9, 7)]
+    orders = [orq.ASC, orq.DESC, orq.ASC, orq.ASC, orq.DESC, orq.ASC, orq.DESC, orq.ASC]
+    data = [splitmix(100 + i, n).astype(dt) for i, n in enumerate(sizes)]
+    rb, rs = orq.Runtime(seed=71), orq.Runtime(seed=71)
+    for rep in range(2):
+        vb = [rb.secret_share_b(d, 0) for d in data]
+        vs = [rs.secret_share_b(d, 0) for d in data]
+        orq.bitonic_sort_batch(vb, orders, use_graph=use_graph)
+        for v, o in zip(vs, orders):
+            orq.bitonic_sort(v, o)
+        for a, b in zip(vb, vs):
+            assert same(a.shares.cpu().numpy(), b.shares.cpu().numpy()), rep
+        for d, v, o in zip(data, vb, orders):
+            sd = d.view({4: np.int32, 8: np.int64}[w])
+            want = np.sort(sd)[::-1] if o == orq.DESC else np.sort(sd)
+            assert same(v.open().cpu().numpy().view(sd.dtype), want)
+
+
+def splitmix(seed, n):
+    from oracle.oracle import splitmix64_fast
+
+    return splitmix64_fast(seed, n)
