@@ -394,6 +394,178 @@ class JoinWorkload:
                               f"x {threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
 
 
+def run_batch(args, rank, world, local_rank):
+    """Config 4: 512 independent sorts (256 bitonic with sizes padded to 2^k,
+    256 radix), lengths log-uniform over 2^10..2^20, int32 keys uniform over
+    32 bits. Batched path: one bitonic_sort_batch (persistent work-list kernel
+    per network round, autotuned CTA size, CUDA graph) then the radix sorts;
+    plain path: 512 per-call operators in the same order (bitonic items, then
+    radix items), which yields the same shares. Timed with CUDA events on the
+    runtime's stream; both paths' opened outputs are checked."""
+    import numpy as np
+    import torch
+
+    import orq_b200 as orq
+
+    torch.cuda.set_device(local_rank)
+    rng = np.random.Generator(np.random.PCG64(args.seed_batch + rank))
+    count = args.batch_items
+    kinds = ["bitonic"] * (count // 2) + ["radix"] * (count - count // 2)
+    rng.shuffle(kinds)
+    sizes = [int(round(2 ** rng.uniform(10, 20))) for _ in range(count)]
+    keys = [splitmix(1000 + 7 * i + rank, n).astype(np.uint32).view(np.int32) for i, n in enumerate(sizes)]
+    padded = []
+    for kind, k in zip(kinds, keys):
+        if kind == "bitonic":
+            m = 1 << max(0, (len(k) - 1).bit_length())
+            k = np.concatenate([k, np.full(m - len(k), np.iinfo(np.int32).max, dtype=np.int32)])
+        padded.append(k)
+    rows = sum(sizes)
+    rt = orq.Runtime(seed=7 + rank, device=local_rank)
+    vecs = [rt.secret_share_b(k, 0) for k in padded]
+    orig = [v.shares.clone() for v in vecs]
+    bit_idx = [i for i, kd in enumerate(kinds) if kd == "bitonic"]
+    rad_idx = [i for i, kd in enumerate(kinds) if kd == "radix"]
+
+    def restore():
+        for v, o in zip(vecs, orig):
+            v.shares.copy_(o)
+
+    def batched():
+        orq.bitonic_sort_batch([vecs[i] for i in bit_idx], orq.ASC, use_graph=True)
+        for i in rad_idx:
+            orq.radix_sort(vecs[i], orq.ASC, 32)
+
+    def plain():
+        for i in bit_idx:
+            orq.bitonic_sort(vecs[i], orq.ASC)
+        for i in rad_idx:
+            orq.radix_sort(vecs[i], orq.ASC, 32)
+
+    def check():
+        ok = True
+        for i, (k, n) in enumerate(zip(keys, sizes)):
+            o = vecs[i].open().cpu().numpy().view(np.int32)[:n]
+            ok = ok and np.array_equal(o, np.sort(k))
+        return bool(ok)
+
+    def timed(fn, steps):
+        ms = 0.0
+        for _ in range(steps):
+            restore()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms / steps
+
+    for _ in range(args.warmup):
+        restore()
+        batched()
+    torch.cuda.synchronize()
+    ok = check()
+    k0 = rt.kernels_launched()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms_b = timed(batched, args.steps)
+    clk = clocks.stop()
+    launches = (rt.kernels_launched() - k0) // max(1, args.steps)
+    restore()
+    plain()
+    torch.cuda.synchronize()
+    ok = ok and check()
+    ms_p = timed(plain, max(1, min(args.steps, 2)))
+    rt.close()
+    return {"rows": rows, "ms_batched": ms_b, "ms_plain": ms_p, "ok": ok, "clocks": clk,
+            "launches_per_step": launches, "items": count,
+            "padded_rows": int(sum(len(p) for p in padded))}
+
+
+def run_serve(args, rank, world, local_rank):
+    """Config 5: Poisson arrivals of mixed requests (60% sort, 30% group-by
+    over 2^10 groups, 10% PK-FK join with a 4x foreign-key side), sizes
+    log-uniform over 2^12..2^22 rows, int64 keys. Capacity is measured first
+    on the plain per-request path (one slot, all requests queued at once);
+    the trace then arrives at 80% of that capacity and is served (a) by the
+    continuous-batching server and (b) by the plain path. Every result is
+    checked against its plaintext answer."""
+    import torch
+
+    from orq_b200.serve import Server, make_trace
+
+    torch.cuda.set_device(local_rank)
+    # warm-up: a small trace through both paths (tables, pools, kernels)
+    for _ in range(max(1, args.warmup)):
+        for slots in (1, args.slots):
+            srv = Server(slots=slots, device=local_rank)
+            srv.run(make_trace(6, 0.0, seed=99, min_log=10, max_log=12))
+            srv.close()
+    # capacity of the plain path
+    calib = make_trace(args.serve_requests, 0.0, seed=5 + rank, max_log=args.serve_max_log)
+    srv = Server(slots=1, device=local_rank)
+    cap_stats = srv.run(calib)
+    srv.close()
+    capacity = cap_stats["requests"] / cap_stats["makespan_s"]
+    rate = 0.8 * capacity
+    out = {"capacity_req_per_s": capacity, "rate_req_per_s": rate}
+    for name, slots in (("serving", args.slots), ("plain", 1)):
+        trace = make_trace(args.serve_requests, rate, seed=5 + rank, max_log=args.serve_max_log)
+        srv = Server(slots=slots, device=local_rank)
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        st = srv.run(trace, check=True)
+        st["clocks"] = clocks.stop()
+        srv.close()
+        st["ok"] = all(r.ok for r in trace)
+        out[name] = st
+    return out
+
+
+class BatchReference:
+    """CPU reference arm of the ragged batch: ORQ's own bitonic and radix sorts
+    of a bounded sample of items, one call per item."""
+
+    name = "batch"
+
+    def __init__(self, args, seed):
+        self.config = {"workload": "ragged batch of independent 3PC sorts (half bitonic, half radix), "
+                                   "lengths log-uniform 2^10..2^20, 32-bit keys", "seed": seed}
+
+    def cpu_reference(self, sample, threads):
+        n = max(1024, min(sample, 1 << 14))
+        sb = run_ref_seconds("bitonic_time", n, 1, 32, threads)
+        sr = run_ref_seconds("radix_time", n, 7, 32, threads)
+        return 2 * n / (sb + sr), sb + sr, (f"one bitonic sort of {n} int32 keys and one radix sort of {n} "
+                                            f"32-bit keys (bounded sample of the 512-item batch), ORQ's own "
+                                            f"operators, 3 party processes x {threads} worker threads")
+
+
+class ServeReference:
+    """CPU reference arm of the serving mix: ORQ's own sort, group-by and join
+    on bounded request sizes, one request at a time."""
+
+    name = "serve"
+
+    def __init__(self, args, seed):
+        self.config = {"workload": "mixed requests (60% sort, 30% group-by, 10% join) served one at a time",
+                       "seed": seed}
+
+    def cpu_reference(self, sample, threads):
+        n = max(1024, min(sample, 1 << 12))
+        ss = run_ref_seconds("radix_time", n, 7, 64, threads)
+        sj = run_ref_seconds("join_time", n // 4, 7, 64, threads)
+        rows = 0.6 * n + 0.1 * (5 * (n // 4))
+        sec = 0.6 * ss + 0.1 * sj
+        return rows / sec, sec, (f"a {n}-row 64-bit radix sort and a {n // 4} x {n} join (bounded "
+                                 f"samples) weighted 0.6 / 0.1 by the request mix (group-by runs the same "
+                                 f"table sort as a sort), ORQ's own operators, 3 party processes x "
+                                 f"{threads} worker threads")
+
+
 WORKLOADS = {"radix": RadixWorkload, "bitonic": BitonicWorkload, "join": JoinWorkload}
 
 
@@ -553,13 +725,18 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="orq", choices=["orq", "reference"])
-    ap.add_argument("--workload", default="radix", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="radix", choices=sorted(WORKLOADS) + ["batch", "serve"])
     ap.add_argument("--n", type=int, default=DEFAULT_N)
     ap.add_argument("--na", type=int, default=1 << 22, help="join: rows of A (B has 4x)")
     ap.add_argument("--bits", type=int, default=40)
     ap.add_argument("--cpu-sample", type=int, default=1 << 17)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-items", type=int, default=512)
+    ap.add_argument("--seed-batch", type=int, default=4)
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--serve-max-log", type=int, default=22)
     args = ap.parse_args()
     if args.workload == "join" and args.cpu_sample == 1 << 17:
         args.cpu_sample = 1 << 11
@@ -571,7 +748,8 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        wl = WORKLOADS[args.workload](args, 7)
+        refs = dict(WORKLOADS, batch=BatchReference, serve=ServeReference)
+        wl = refs[args.workload](args, 7)
         config = dict(wl.config, parallelism=f"replicas x{args.gpus}")
         threads = max(1, nproc // 3)
         for _ in range(args.warmup):
@@ -587,6 +765,46 @@ def main():
             "cpu_baseline": {"value": v, "unit": "rows/s", "cores": 3 * threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    if args.workload in ("batch", "serve") and args.impl == "orq":
+        fn = run_batch if args.workload == "batch" else run_serve
+        res = fn(args, rank, world, local_rank)
+        if rank != 0:
+            return
+        if args.workload == "batch":
+            value = world * res["rows"] / (res["ms_batched"] / 1e3)
+            line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+                    "warmup": args.warmup, "ms_per_step": res["ms_batched"], "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                    "config": {"workload": f"ragged batch: {res['items']} independent 3PC sorts (half bitonic "
+                                           "padded to 2^k, half radix), lengths log-uniform 2^10..2^20, int32 "
+                                           "keys uniform; batched bitonic work-list kernels + CUDA graph",
+                               "rows_per_gpu": res["rows"], "padded_rows": res["padded_rows"],
+                               "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
+                    "correct": res["ok"], "gpu_launches": res["launches_per_step"] * args.steps,
+                    "clocks": res["clocks"],
+                    "plain": {"value": world * res["rows"] / (res["ms_plain"] / 1e3), "unit": "rows/s",
+                              "ms_per_step": res["ms_plain"]},
+                    "batched_over_plain": res["ms_plain"] / res["ms_batched"]}
+        else:
+            sv, pl = res["serving"], res["plain"]
+            line = {"metric": METRIC, "value": world * sv["rows_per_s"], "unit": "rows/s", "n_gpus": world,
+                    "steps": 1, "warmup": args.warmup, "ms_per_step": 1e3 * sv["makespan_s"],
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                    "data": "synthetic",
+                    "config": {"workload": f"serving loop: {args.serve_requests} Poisson arrivals at 80% of the "
+                                           "plain path's capacity, 60% sort / 30% group-by (2^10 groups) / 10% "
+                                           f"PK-FK join (4x fk side), rows log-uniform 2^12..2^{args.serve_max_log}, "
+                                           f"int64 keys; continuous batching over {args.slots} slots",
+                               "parallelism": f"replicas x{world}", "slots": args.slots},
+                    "correct": sv["ok"] and pl["ok"], "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
+                    "clocks": sv["clocks"], "capacity_req_per_s": res["capacity_req_per_s"],
+                    "rate_req_per_s": res["rate_req_per_s"],
+                    "plain": {"value": pl["rows_per_s"], "unit": "rows/s", "p50_ms": pl["p50_ms"],
+                              "p99_ms": pl["p99_ms"], "makespan_s": pl["makespan_s"]},
+                    "timing": "host wall clock from each request's arrival to its opened result on the host"}
+        print(json.dumps(line))
         return
 
     wl, ms, launches, prof, clk, e2e, ok = run_orq(args, rank, world, local_rank)

@@ -230,6 +230,18 @@ int orqcu_distinct(orqcu_runtime* rt, int width, size_t n, int nkeys, const void
 int orqcu_bitonic_sort_batch(orqcu_runtime* rt, int width, int count, const size_t* n,
                              void* const* keys, const int* descending, int use_graph);
 
+/* Re-key the runtime as orqcu_runtime_create(seed) would (fresh keys, nonces
+ * at zero, reserved permutations dropped) while keeping its stream, its
+ * cached device memory, tuned launch shapes and captured graphs. A serving
+ * slot runs each request on its own seed this way, so a request's shares do
+ * not depend on what ran before it. No reference counterpart (one
+ * orq_init per process there). */
+int orqcu_runtime_reseed(orqcu_runtime* rt, uint64_t seed);
+/* Return the runtime's cached (unused) device memory to the device, ordered
+ * on the runtime's stream (no device-wide synchronisation); writes the bytes
+ * that were cached to *cached_before when non-NULL. */
+int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before);
+
 #ifdef __cplusplus
 }
 #endif

@@ -126,6 +126,16 @@ class Runtime:
     def synchronize(self):
         _check(self.lib.orqcu_synchronize(self.h))
 
+    def reseed(self, seed: int):
+        """Fresh keys and nonces for `seed`, keeping stream and cached memory."""
+        _check(self.lib.orqcu_runtime_reseed(self.h, ctypes.c_uint64(seed)))
+
+    def trim(self) -> int:
+        """Return cached device memory (stream-ordered); bytes that were cached."""
+        v = ctypes.c_size_t()
+        _check(self.lib.orqcu_runtime_trim(self.h, ctypes.byref(v)))
+        return v.value
+
     # -- sharing ----------------------------------------------------------
     def _alloc(self, n: int, width: int):
         torch = _torch()

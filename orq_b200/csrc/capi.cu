@@ -479,4 +479,23 @@ int orqcu_bitonic_sort_batch(orqcu_runtime* rt, int width, int count, const size
     });
 }
 
+int orqcu_runtime_reseed(orqcu_runtime* rt, uint64_t seed) {
+    return guard([&] {
+        need_rt(rt);
+        for (auto& sp : rt->ctx.perm_queue) rt->ctx.free_perm(sp);
+        rt->ctx.perm_queue.clear();
+        rt->ctx.perm_queue_n = 0;
+        orqcu::init_ctx_keys(rt->ctx, seed);
+        for (int s = 0; s < orqcu::NSTREAMS; s++) rt->ctx.nonce[s] = 0;
+    });
+}
+
+int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before) {
+    return guard([&] {
+        need_rt(rt);
+        if (cached_before) *cached_before = rt->ctx.pool.cached_bytes();
+        rt->ctx.pool.trim(rt->ctx.stream);
+    });
+}
+
 }  // extern "C"

@@ -130,7 +130,10 @@ void upload_aes_tables(int device) {
 // ---------------------------------------------------------------------------
 // Pool: size-bucketed reuse of device allocations (buckets are powers of two
 // above 1 MiB, 256-byte multiples below), so the per-round temporaries of a
-// sort do not go back to cudaMalloc.
+// sort do not go back to the allocator. New blocks come from the stream-ordered
+// allocator on the runtime's stream and trim() returns cached blocks the same
+// way, so neither ever synchronises the device (runtimes on different streams
+// allocate and release independently).
 static size_t bucket(size_t bytes) {
     if (bytes < 256) return 256;
     if (bytes <= (1u << 20)) return (bytes + 255) & ~size_t(255);
@@ -139,7 +142,7 @@ static size_t bucket(size_t bytes) {
     return b;
 }
 
-void* Pool::get(size_t bytes) {
+void* Pool::get(size_t bytes, cudaStream_t stream) {
     const size_t b = bucket(bytes);
     {
         std::lock_guard<std::mutex> lk(mu_);
@@ -152,11 +155,12 @@ void* Pool::get(size_t bytes) {
         }
     }
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, b);
+    cudaError_t e = cudaMallocAsync(&p, b, stream);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        trim();
-        ORQ_CUDA_CHECK(cudaMalloc(&p, b));
+        trim(stream);
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(stream));
+        ORQ_CUDA_CHECK(cudaMallocAsync(&p, b, stream));
     }
     std::lock_guard<std::mutex> lk(mu_);
     live_[p] = b;
@@ -171,10 +175,17 @@ void Pool::put(void* p) {
     live_.erase(it);
 }
 
-void Pool::trim() {
+void Pool::trim(cudaStream_t stream) {
     std::lock_guard<std::mutex> lk(mu_);
-    for (auto& kv : free_) cudaFree(kv.second);
+    for (auto& kv : free_) cudaFreeAsync(kv.second, stream);
     free_.clear();
+}
+
+size_t Pool::cached_bytes() {
+    std::lock_guard<std::mutex> lk(mu_);
+    size_t b = 0;
+    for (auto& kv : free_) b += kv.first;
+    return b;
 }
 
 Pool::~Pool() {

@@ -43,9 +43,10 @@ struct DevBuf {
 
 class Pool {
    public:
-    void* get(size_t bytes);
+    void* get(size_t bytes, cudaStream_t stream);
     void put(void* p);
-    void trim();
+    void trim(cudaStream_t stream);
+    size_t cached_bytes();
     ~Pool();
 
    private:
@@ -121,7 +122,7 @@ struct Ctx {
         a.nonce = nonce[s] + extra_nonces;
         return a;
     }
-    void* alloc(size_t bytes) { return pool.get(bytes); }
+    void* alloc(size_t bytes) { return pool.get(bytes, stream); }
     void release(void* p) {
         if (p) pool.put(p);
     }

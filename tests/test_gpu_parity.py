@@ -446,3 +446,33 @@ def splitmix(seed, n):
     from oracle.oracle import splitmix64_fast
 
     return splitmix64_fast(seed, n)
+
+
+def test_serving_results_same_alone_and_in_the_mix(orq):
+    """continuous batching: every request's shares-derived opened result (and
+    its exact output) are the same when it runs alone on a fresh runtime and
+    when it runs concurrently with others on the server's slots"""
+    import torch
+
+    from orq_b200.serve import Server, check_result, make_trace, run_request
+
+    trace = make_trace(12, rate=0.0, seed=3, min_log=8, max_log=11)
+    srv = Server(slots=3)
+    try:
+        stats = srv.run(trace, check=True)
+    finally:
+        srv.close()
+    assert stats["requests"] == 12
+    assert all(r.ok for r in trace)
+    assert len({r.slot for r in trace}) > 1
+    for r in trace:
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            rt = orq.Runtime(seed=r.seed)
+            rt.reseed(r.seed)
+            alone = run_request(rt, r)
+            rt.close()
+        assert alone.keys() == r.result.keys()
+        for k in alone:
+            assert same(alone[k], r.result[k]), (r.kind, r.n, k)
+        assert check_result(r, alone)
