@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 
 #include "launch.cuh"
 
@@ -162,6 +163,7 @@ __global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
 
 struct FyScanArgs {
     uint32_t n, count, tiles;
+    uint32_t g0;                   // group of block 0 (one launch per group)
     unsigned long long win_tile0;  // absolute index of the window's first tile
     FyLayout lay;
     const uint32_t* ev;
@@ -177,20 +179,23 @@ struct FyScanArgs {
 // ---------------------------------------------------------------------------
 // The scanner. One 1024-thread CTA per group replays the acceptance of its
 // chain exactly. A step takes the next cs entries (<= 32768) of the current
-// level, staged through shared memory with coalesced loads; thread t then owns
-// entries [32t, 32t+32). Level 1: entry q is certainly accepted if
+// level; warp w owns entries [1024w, 1024w + 1024) and at iteration u its lane
+// l holds entry q = 1024w + 32u + l, so loads, ranks and the stores of
+// accepted values are all lane-parallel (ballots and popcounts, no per-thread
+// serial loops) and coalesced. Level 1: entry q is certainly accepted if
 // v + q <= T (at most q acceptances precede it), certainly rejected if v > T,
 // otherwise uncertain. Level 2 (warp 0, 32 uncertain entries at a time):
 // with c = certain accepts before an uncertain entry and a = uncertain accepts
 // before it, it is accepted iff a <= T - c - v ("slack"); lane j of a chunk is
 // certain if slack >= a_chunk + j, rejected if slack < a_chunk, and only the
-// rest is decided lane by lane. One packed block scan per step gives ranks.
+// rest is decided lane by lane. A step with more uncertain entries than the
+// list holds is halved until they fit (a step of at most kUncCap entries
+// always does).
 constexpr uint32_t kMaxStepEntries = 32768;
 constexpr int kPerThread = kMaxStepEntries / kScanThreads;  // 32
+constexpr int kScanWarps = kScanThreads / 32;
 constexpr uint32_t kUncCap = 2048;
-constexpr size_t kScanSmem = (kMaxStepEntries + kMaxStepEntries / 32) * 4;  // padded staging
-
-__device__ __forceinline__ uint32_t pad_idx(uint32_t q) { return q + (q >> 5); }
+constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4;
 
 // entries per step at level L: uncertain entries of a step are about
 // cs^2 / (2 n/4^L); keep that near 512
@@ -212,15 +217,17 @@ __device__ __forceinline__ uint32_t tile_in(const uint32_t* P, uint32_t lo, uint
 }
 
 __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
-    extern __shared__ uint32_t sv[];  // staged entry values, padded
+    extern __shared__ __align__(16) uint32_t sv[];  // step entries, sv[q]
     __shared__ uint32_t red[33];
     __shared__ uint32_t P[kMaxWindowTiles + 1];  // prefix of level-L counts over the window
     __shared__ uint32_t unc_v[kUncCap], unc_cp[kUncCap], unc_pre[kUncCap + 1];
-    __shared__ uint32_t s_last_q, s_uacc;
-    const uint32_t g = blockIdx.x;
+    __shared__ uint32_t wtot[kScanWarps], wpre[kScanWarps];
+    __shared__ uint32_t s_last_q, s_uacc, s_tot;
+    const uint32_t g = a.g0 + blockIdx.x;
     const uint32_t n = a.n;
     const uint32_t tiles = a.tiles;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
     // scan state, identical in every thread
     uint32_t i = a.state[g].i, m = a.state[g].m, done = a.state[g].done;
     unsigned long long start = a.state[g].start_tile;
@@ -263,18 +270,19 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             }
             continue;
         }
-        const uint32_t cs = min(step_entries(n, L), eend - e0);
+        uint32_t cs = min(step_entries(n, L), eend - e0);
         const unsigned long long t_l0 = clock64();
-        // ---- stage entry values (coalesced: consecutive threads, consecutive
-        // entries); each lane walks its tile cursor forward, no searches
+        const uint32_t qw = (uint32_t)warp * 1024u + lane;  // this thread's entry at u = 0
+        // ---- stage this thread's entries (coalesced per iteration; each lane
+        // walks its tile cursor forward) into shared memory at sv[q]
         {
             const size_t off = a.lay.off[L];
             uint32_t t = tau;
             uint32_t vals[kPerThread];
 #pragma unroll
             for (int u = 0; u < kPerThread; u++) {
-                const uint32_t q = u * kScanThreads + threadIdx.x;
-                vals[u] = 0;
+                const uint32_t q = qw + 32u * u;
+                vals[u] = 0xffffffffu;
                 if (q < cs) {
                     const uint32_t e = e0 + q;
                     while (P[t + 1] <= e) t++;
@@ -282,134 +290,138 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                 }
             }
 #pragma unroll
-            for (int u = 0; u < kPerThread; u++) {
-                const uint32_t q = u * kScanThreads + threadIdx.x;
-                if (q < cs) sv[pad_idx(q)] = vals[u];
-            }
+            for (int u = 0; u < kPerThread; u++) sv[qw + 32u * u] = vals[u];
         }
-        __syncthreads();
-        // ---- level 1
-        uint32_t certain = 0, unc = 0;
-        {
-            const uint32_t q0 = threadIdx.x * kPerThread;
+        __syncwarp();
+        // ---- level 1 counts per warp, block prefix over warps; halve the step
+        // while the uncertain entries do not fit the list
+        uint32_t tot_c, tot_u;
+        for (;;) {
+            uint32_t wc = 0, wu = 0;
 #pragma unroll
             for (int u = 0; u < kPerThread; u++) {
-                const uint32_t q = q0 + u;
-                if (q < cs) {
-                    const uint32_t v = sv[pad_idx(q)];
-                    if ((unsigned long long)v + q <= T) certain |= 1u << u;
-                    else if (v <= T) unc |= 1u << u;
-                }
+                const uint32_t q = qw + 32u * u;
+                const uint32_t v = sv[q];
+                const bool cert = q < cs && (unsigned long long)v + q <= T;
+                const bool unc = q < cs && !cert && v <= T;
+                wc += __popc(__ballot_sync(0xffffffffu, cert));
+                wu += __popc(__ballot_sync(0xffffffffu, unc));
             }
+            if (lane == 0) wtot[warp] = wc | (wu << 16);
+            __syncthreads();
+            if (warp == 0) {
+                const uint32_t x = wtot[lane];
+                uint32_t inc = x;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += y;
+                }
+                wpre[lane] = inc - x;
+                if (lane == 31) s_tot = inc;
+            }
+            __syncthreads();
+            tot_c = s_tot & 0xffffu;
+            tot_u = s_tot >> 16;
+            if (tot_u <= kUncCap) break;
+            cs >>= 1;  // uniform: every thread read the same total
+            __syncthreads();
         }
-        uint32_t tot;
-        const uint32_t pre = block_excl_sum(__popc(certain) | (__popc(unc) << 16), red, tot);
-        const uint32_t cpre = pre & 0xffffu, upre = pre >> 16;
-        const uint32_t tot_c = tot & 0xffffu, tot_u = tot >> 16;
+        const uint32_t cbase = wpre[warp] & 0xffffu, ubase = wpre[warp] >> 16;
         st_steps++;
         st_ent += cs;
         st_cyc_load += clock64() - t_l0;
-        uint32_t accept = certain, tot_a = tot_c, rank_base = cpre;
+        // ---- list the uncertain entries in order, with the certain accepts
+        // before each
         if (tot_u) {
-            const unsigned long long t_u0 = clock64();
+            uint32_t rc = cbase, ru = ubase;
+#pragma unroll
+            for (int u = 0; u < kPerThread; u++) {
+                const uint32_t q = qw + 32u * u;
+                const uint32_t v = sv[q];
+                const bool cert = q < cs && (unsigned long long)v + q <= T;
+                const bool unc = q < cs && !cert && v <= T;
+                const uint32_t bc = __ballot_sync(0xffffffffu, cert);
+                const uint32_t bu = __ballot_sync(0xffffffffu, unc);
+                if (unc) {
+                    const uint32_t k = ru + __popc(bu & lt);
+                    unc_v[k] = v;
+                    unc_cp[k] = rc + __popc(bc & lt);
+                }
+                rc += __popc(bc);
+                ru += __popc(bu);
+            }
+        }
+        __syncthreads();
+        const unsigned long long t_u0 = clock64();
+        if (warp == 0) {
+            // level 2 over the listed uncertain entries
+            uint32_t acc_so_far = 0;
+            for (uint32_t base = 0; base < tot_u; base += 32) {
+                const uint32_t k = base + lane;
+                const bool valid = k < tot_u;
+                long long slack = -1;
+                if (valid) slack = (long long)T - unc_cp[k] - unc_v[k];
+                const bool cert = valid && slack >= (long long)acc_so_far + lane;
+                const bool und = valid && !cert && slack >= (long long)acc_so_far;
+                uint32_t okmask = __ballot_sync(0xffffffffu, cert);
+                const uint32_t undmask = __ballot_sync(0xffffffffu, und);
+                if (undmask) {
+                    // decide the chunk lane by lane
+                    okmask = 0;
+                    uint32_t cur = acc_so_far;
+                    for (int j = 0; j < 32; j++) {
+                        const long long sj = __shfl_sync(0xffffffffu, slack, j);
+                        if (base + j < tot_u && sj >= (long long)cur) {
+                            okmask |= 1u << j;
+                            cur++;
+                        }
+                    }
+                }
+                if (valid) {
+                    unc_pre[k] = acc_so_far + __popc(okmask & lt);
+                    unc_cp[k] = (okmask >> lane) & 1u;  // reuse as the decision
+                }
+                acc_so_far += __popc(okmask);
+            }
+            if (lane == 0) {
+                unc_pre[tot_u] = acc_so_far;
+                s_uacc = acc_so_far;
+            }
+        }
+        __syncthreads();
+        if (tot_u) {
             st_unc_steps++;
             st_unc += tot_u;
-            const bool listed = tot_u <= kUncCap;
-            if (listed) {
-                uint32_t k = upre, cc = cpre;
-                const uint32_t q0 = threadIdx.x * kPerThread;
-                for (int u = 0; u < kPerThread; u++) {
-                    if ((unc >> u) & 1u) {
-                        unc_v[k] = sv[pad_idx(q0 + u)];
-                        unc_cp[k] = cc;
-                        k++;
-                    }
-                    if ((certain >> u) & 1u) cc++;
-                }
-            }
-            __syncthreads();
-            if (threadIdx.x < 32) {
-                // level 2 over the listed uncertain entries, or (too many) over
-                // every entry of the step in order with no certain ones
-                const uint32_t cnt = listed ? tot_u : cs;
-                uint32_t acc_so_far = 0;
-                for (uint32_t base = 0; base < cnt; base += 32) {
-                    const uint32_t k = base + lane;
-                    const bool valid = k < cnt;
-                    long long slack = -1;
-                    if (valid) {
-                        const uint32_t v = listed ? unc_v[k] : sv[pad_idx(k)];
-                        const uint32_t cp = listed ? unc_cp[k] : 0u;
-                        slack = (long long)T - cp - v;
-                    }
-                    const bool cert = valid && slack >= (long long)acc_so_far + lane;
-                    const bool und = valid && !cert && slack >= (long long)acc_so_far;
-                    uint32_t okmask = __ballot_sync(0xffffffffu, cert);
-                    const uint32_t undmask = __ballot_sync(0xffffffffu, und);
-                    if (undmask) {
-                        // decide the chunk lane by lane
-                        okmask = 0;
-                        uint32_t cur = acc_so_far;
-                        for (int j = 0; j < 32; j++) {
-                            const long long sj = __shfl_sync(0xffffffffu, slack, j);
-                            if (base + j < cnt && sj >= (long long)cur) {
-                                okmask |= 1u << j;
-                                cur++;
-                            }
-                        }
-                    }
-                    if (valid) {
-                        const uint32_t before = acc_so_far + __popc(okmask & ((1u << lane) - 1u));
-                        if (listed) {
-                            unc_pre[k] = before;
-                            unc_cp[k] = (okmask >> lane) & 1u;  // reuse as the decision
-                        } else {
-                            sv[pad_idx(k)] = ((okmask >> lane) & 1u) ? sv[pad_idx(k)] : 0xffffffffu;
-                        }
-                    }
-                    acc_so_far += __popc(okmask);
-                }
-                if (lane == 0) {
-                    if (listed) unc_pre[tot_u] = acc_so_far;
-                    s_uacc = acc_so_far;
-                }
-            }
-            __syncthreads();
-            if (listed) {
-                uint32_t k = upre;
-                rank_base = cpre + unc_pre[upre];
-                for (int u = 0; u < kPerThread; u++)
-                    if ((unc >> u) & 1u) {
-                        if (unc_cp[k]) accept |= 1u << u;
-                        k++;
-                    }
-                tot_a = tot_c + s_uacc;
-            } else {
-                // every accepted entry kept its value, rejected ones became ~0
-                accept = 0;
-                const uint32_t q0 = threadIdx.x * kPerThread;
-                for (int u = 0; u < kPerThread; u++)
-                    if (q0 + u < cs && sv[pad_idx(q0 + u)] != 0xffffffffu) accept |= 1u << u;
-                uint32_t t2;
-                rank_base = block_excl_sum(__popc(accept), red, t2);
-                tot_a = t2;
-                st_seq++;
-            }
             st_cyc_unc += clock64() - t_u0;
         }
+        // ---- accept, rank, store (consecutive accepted lanes store to
+        // consecutive ranks)
+        const uint32_t tot_a = tot_c + s_uacc;
         const uint32_t need = n - i;
         uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
         {
-            uint32_t r = rank_base;
-            const uint32_t q0 = threadIdx.x * kPerThread;
-            for (int u = 0; u < kPerThread; u++)
-                if ((accept >> u) & 1u) {
+            uint32_t rc = cbase, ru = ubase;
+#pragma unroll
+            for (int u = 0; u < kPerThread; u++) {
+                const uint32_t q = qw + 32u * u;
+                const uint32_t v = sv[q];
+                const bool cert = q < cs && (unsigned long long)v + q <= T;
+                const bool unc = q < cs && !cert && v <= T;
+                const uint32_t bc = __ballot_sync(0xffffffffu, cert);
+                const uint32_t bu = __ballot_sync(0xffffffffu, unc);
+                const uint32_t k = ru + __popc(bu & lt);  // uncertain entries before q
+                const bool accepted = cert || (unc && unc_cp[k]);
+                if (accepted) {
+                    const uint32_t r = rc + __popc(bc & lt) + unc_pre[k];
                     if (r < need) {
-                        acc[i + r] = sv[pad_idx(q0 + u)];
-                        if (r == need - 1) s_last_q = q0 + u;
+                        acc[i + r] = v;
+                        if (r == need - 1) s_last_q = q;
                     }
-                    r++;
                 }
+                rc += __popc(bc);
+                ru += __popc(bu);
+            }
         }
         if (tot_a >= need) {
             __syncthreads();
@@ -437,7 +449,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                 ix = enew - P[tau];
             }
         }
-        __syncthreads();  // sv and the lists are reused by the next step
+        __syncthreads();  // the lists and counters are reused by the next step
     }
     if (threadIdx.x == 0) {
         a.state[g].i = i;
@@ -647,8 +659,20 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     }
     const size_t ents_b = (size_t)3 * tiles * lay.slot * 4;
     const size_t cnt_b = (size_t)3 * tiles * kMaxLevels * 4;
-    Scratch ev0(c, ents_b), ev1(c, ents_b), ep0(c, ents_b), ep1(c, ents_b), cnt0(c, cnt_b),
-        cnt1(c, cnt_b);
+    // Ring of window buffers: the draws of a window do not depend on the scan
+    // (windows are consecutive buffers of the group streams), so the generator
+    // runs up to kRing-1 windows ahead. It stays ahead through the dense start
+    // of a permutation (scan-bound) and the scanner catches up through the
+    // sparse tail (generation-bound). The three groups are scanned on three
+    // streams: their dense phases fall in different windows, and a shared
+    // launch per window would cost the slowest group every time.
+    constexpr int kRing = 6;
+    std::vector<std::unique_ptr<Scratch>> ring_ev, ring_ep, ring_cnt;
+    for (int k = 0; k < kRing; k++) {
+        ring_ev.emplace_back(new Scratch(c, ents_b));
+        ring_ep.emplace_back(new Scratch(c, ents_b));
+        ring_cnt.emplace_back(new Scratch(c, cnt_b));
+    }
     Scratch state(c, 3 * sizeof(FyState));
     Scratch acc(c, (size_t)3 * count * n * 4);
     Scratch refills(c, (size_t)3 * count * 4);
@@ -660,28 +684,39 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
 
     // generator and scanner run on private non-blocking streams so they overlap
     // whatever the caller's stream is (the legacy default stream included)
-    cudaStream_t gs, ss;
-    ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
-    ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking));
-    cudaEvent_t ev_start, gen_done[2], scan_done[2];
+    // the scanner's stream has the highest priority: when generator CTAs
+    // (which fill an SM's registers and shared memory) retire, a pending scan
+    // is dispatched before the next generator window
+    int prio_lo = 0, prio_hi = 0;
+    ORQ_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    cudaStream_t gs, ss[3];
+    ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&gs, cudaStreamNonBlocking, prio_lo));
+    for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&ss[g], cudaStreamNonBlocking, prio_hi));
+    cudaEvent_t ev_start, gen_done[kRing], scan_done[3][kRing], st_ev[3][kRing];
     ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < kRing; k++) {
         ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&gen_done[k], cudaEventDisableTiming));
-        ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&scan_done[k], cudaEventDisableTiming));
+        for (int g = 0; g < 3; g++) {
+            ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&scan_done[g][k], cudaEventDisableTiming));
+            ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&st_ev[g][k], cudaEventDisableTiming));
+        }
     }
     ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
     ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
-    ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss, ev_start, 0));
+    for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], ev_start, 0));
 
-    FyState* hstate = nullptr;
-    ORQ_CUDA_CHECK(cudaMallocHost(&hstate, 3 * sizeof(FyState)));
     prep_aes_kernel(k_fy_gen);
     ORQ_CUDA_CHECK(cudaFuncSetAttribute(k_fy_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem));
 
     const unsigned gen_grid = (unsigned)std::max(1, c.num_sms - 3);
-    uint32_t* evp[2] = {ev0.as<uint32_t>(), ev1.as<uint32_t>()};
-    uint32_t* epp[2] = {ep0.as<uint32_t>(), ep1.as<uint32_t>()};
-    uint32_t* cntp[2] = {cnt0.as<uint32_t>(), cnt1.as<uint32_t>()};
+    uint32_t* evp[kRing];
+    uint32_t* epp[kRing];
+    uint32_t* cntp[kRing];
+    for (int k = 0; k < kRing; k++) {
+        evp[k] = ring_ev[k]->as<uint32_t>();
+        epp[k] = ring_ep[k]->as<uint32_t>();
+        cntp[k] = ring_cnt[k]->as<uint32_t>();
+    }
 
     const unsigned long long limit_windows =
         (unsigned long long)(count * (per_perm * 4.0 + 64.0) / W + 16);
@@ -696,9 +731,10 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     };
     std::vector<std::array<int, 4>> tl_idx;
     auto launch_gen = [&](unsigned long long w) {
-        const int b = (int)(w & 1);
-        // buffer b was last read by the scanner of window w-2
-        if (w >= 2) ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, scan_done[b], 0));
+        const int b = (int)(w % kRing);
+        // buffer b was last read by the three scans of window w-kRing
+        if (w >= (unsigned long long)kRing)
+            for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, scan_done[g][b], 0));
         FyGenArgs ga;
         for (int g = 0; g < 3; g++) ga.st[g] = c.stream_arg(G01 + g, 4ull * W * w);
         ga.n = (uint32_t)n;
@@ -721,18 +757,21 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         ORQ_CUDA_CHECK(cudaEventRecord(gen_done[b], gs));
         c.kernels_launched++;
     };
-    launch_gen(0);
-    unsigned long long w = 0;
-    bool all_done = false;
-    while (!all_done) {
-        if (w > limit_windows)
-            throw std::runtime_error("permutation generation did not converge");
-        const int b = (int)(w & 1);
-        ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss, gen_done[b], 0));
+    // Each group's scans are queued up to kRing-1 windows ahead of the host's
+    // completion check, so a scan stream always holds its next scan (its CTA
+    // takes the SM the previous one frees before any generator CTA can, by
+    // stream priority) and no host round trip idles a scanner. A scan queued
+    // after its group's last permutation completed sees `done` and returns.
+    FyState* hst = nullptr;
+    ORQ_CUDA_CHECK(cudaMallocHost(&hst, (size_t)kRing * 3 * sizeof(FyState)));
+    auto launch_scan = [&](unsigned long long w, int g) {
+        const int b = (int)(w % kRing);
+        ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], gen_done[b], 0));
         FyScanArgs sa;
         sa.n = (uint32_t)n;
         sa.count = (uint32_t)count;
         sa.tiles = tiles;
+        sa.g0 = (uint32_t)g;
         sa.win_tile0 = (unsigned long long)w * tiles;
         sa.lay = lay;
         sa.ev = evp[b];
@@ -743,25 +782,37 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         sa.refills = refills.as<uint32_t>();
         sa.stats = want_stats ? stats.as<unsigned long long>() : nullptr;
         if (tl_idx.size() <= w) tl_idx.resize(w + 1, {-1, -1, -1, -1});
-        tl_idx[w][2] = tl_event(ss);
+        if (g == 0) tl_idx[w][2] = tl_event(ss[0]);
         {
-            ProfScope ps(c, "fy_scan", 0.0, 0.0, ss);
-            k_fy_scan<<<3, kScanThreads, kScanSmem, ss>>>(sa);
+            ProfScope ps(c, "fy_scan", 0.0, 0.0, ss[g]);
+            k_fy_scan<<<1, kScanThreads, kScanSmem, ss[g]>>>(sa);
         }
-        tl_idx[w][3] = tl_event(ss);
+        if (g == 0) tl_idx[w][3] = tl_event(ss[0]);
         ORQ_CUDA_CHECK(cudaGetLastError());
-        ORQ_CUDA_CHECK(cudaEventRecord(scan_done[b], ss));
+        ORQ_CUDA_CHECK(cudaEventRecord(scan_done[g][b], ss[g]));
         c.kernels_launched++;
-        ORQ_CUDA_CHECK(cudaMemcpyAsync(hstate, state.p, 3 * sizeof(FyState),
-                                       cudaMemcpyDeviceToHost, ss));
-        // generate the next window while this one is scanned
-        launch_gen(w + 1);
-        ORQ_CUDA_CHECK(cudaStreamSynchronize(ss));
-        all_done = hstate[0].done && hstate[1].done && hstate[2].done;
-        w++;
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(hst + 3 * b + g, state.as<FyState>() + g, sizeof(FyState),
+                                       cudaMemcpyDeviceToHost, ss[g]));
+        ORQ_CUDA_CHECK(cudaEventRecord(st_ev[g][b], ss[g]));
+    };
+    for (unsigned long long w = 0;; w++) {
+        if (w > limit_windows)
+            throw std::runtime_error("permutation generation did not converge");
+        launch_gen(w);
+        for (int g = 0; g < 3; g++) launch_scan(w, g);
+        if (w + 1 < (unsigned long long)kRing) continue;
+        // completion of the window kRing-1 behind
+        const int pb = (int)((w + 1 - kRing) % kRing);
+        bool all = true;
+        for (int g = 0; g < 3; g++) {
+            ORQ_CUDA_CHECK(cudaEventSynchronize(st_ev[g][pb]));
+            all = all && hst[3 * pb + g].done;
+        }
+        if (all) break;
     }
+    const unsigned long long w = tl_idx.size();
     ORQ_CUDA_CHECK(cudaStreamSynchronize(gs));
-    ORQ_CUDA_CHECK(cudaStreamSynchronize(ss));
+    for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamSynchronize(ss[g]));
 
     // nonce accounting: 4 nonces per getNext buffer
     std::vector<uint32_t> hr(3 * count);
@@ -776,7 +827,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     if (want_stats) {
         std::fprintf(stderr, "[fy] windows %llu of %u buffers, %.3f ms\n", w, W,
                      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
-        for (size_t k = 0; k < tl_idx.size() && k < 6; k++) {
+        for (size_t k = 0; k < tl_idx.size(); k++) {
             float g0 = 0, g1 = 0, s0 = 0, s1 = 0;
             if (tl_idx[k][0] >= 0) cudaEventElapsedTime(&g0, tl[0], tl[tl_idx[k][0]]);
             if (tl_idx[k][1] >= 0) cudaEventElapsedTime(&g1, tl[0], tl[tl_idx[k][1]]);
@@ -837,14 +888,17 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // scratch reuse
     }
     c.check_device_error();
-    cudaFreeHost(hstate);
+    cudaFreeHost(hst);
     cudaEventDestroy(ev_start);
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < kRing; k++) {
         cudaEventDestroy(gen_done[k]);
-        cudaEventDestroy(scan_done[k]);
+        for (int g = 0; g < 3; g++) {
+            cudaEventDestroy(scan_done[g][k]);
+            cudaEventDestroy(st_ev[g][k]);
+        }
     }
     cudaStreamDestroy(gs);
-    cudaStreamDestroy(ss);
+    for (int g = 0; g < 3; g++) cudaStreamDestroy(ss[g]);
 }
 
 // PermutationManager::reserve (permutation_manager.h:102-181): keep a queue of
