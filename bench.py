@@ -734,8 +734,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-items", type=int, default=512)
     ap.add_argument("--seed-batch", type=int, default=4)
-    ap.add_argument("--slots", type=int, default=4)
-    ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--slots", type=int, default=2)
+    ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-max-log", type=int, default=22)
     args = ap.parse_args()
     if args.workload == "join" and args.cpu_sample == 1 << 17:

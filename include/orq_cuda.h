@@ -242,6 +242,12 @@ int orqcu_runtime_reseed(orqcu_runtime* rt, uint64_t seed);
  * that were cached to *cached_before when non-NULL. */
 int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before);
 
+/* Size this runtime's grids for `sms` SMs (0 = all; at least 4) instead of the
+ * whole device, so that runtimes working concurrently on one GPU (serving
+ * slots) keep their kernels resident side by side instead of each filling
+ * every SM in turn. Results do not depend on it. No reference counterpart. */
+int orqcu_runtime_set_sm_limit(orqcu_runtime* rt, int sms);
+
 #ifdef __cplusplus
 }
 #endif

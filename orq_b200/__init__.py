@@ -130,6 +130,10 @@ class Runtime:
         """Fresh keys and nonces for `seed`, keeping stream and cached memory."""
         _check(self.lib.orqcu_runtime_reseed(self.h, ctypes.c_uint64(seed)))
 
+    def set_sm_limit(self, sms: int):
+        """Size this runtime's grids for `sms` SMs (0 = the whole device)."""
+        _check(self.lib.orqcu_runtime_set_sm_limit(self.h, int(sms)))
+
     def trim(self) -> int:
         """Return cached device memory (stream-ordered); bytes that were cached."""
         v = ctypes.c_size_t()

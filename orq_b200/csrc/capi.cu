@@ -1,4 +1,5 @@
 // capi.cu — extern "C" entry points (include/orq_cuda.h).
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -69,6 +70,12 @@ int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out) {
         ORQ_CUDA_CHECK(cudaMemset(rt->ctx.d_err, 0, sizeof(int)));
         orqcu::init_ctx_keys(rt->ctx, seed);
         orqcu::upload_aes_tables(device);
+        // memory a runtime trims stays in the device's stream-ordered pool for
+        // the next allocation (any runtime) instead of going back to the OS
+        cudaMemPool_t mp;
+        ORQ_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&mp, device));
+        uint64_t keep = UINT64_MAX;
+        ORQ_CUDA_CHECK(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep));
         *out = rt;
     });
 }
@@ -81,6 +88,7 @@ int orqcu_runtime_destroy(orqcu_runtime* rt) {
         for (auto& sp : rt->ctx.perm_queue) rt->ctx.free_perm(sp);
         rt->ctx.perm_queue.clear();
         rt->ctx.release_graphs();
+        orqcu::release_fy(rt->ctx);
         if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
         if (rt->ctx.d_err) cudaFree(rt->ctx.d_err);
         delete rt;
@@ -495,6 +503,16 @@ int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before) {
         need_rt(rt);
         if (cached_before) *cached_before = rt->ctx.pool.cached_bytes();
         rt->ctx.pool.trim(rt->ctx.stream);
+    });
+}
+
+int orqcu_runtime_set_sm_limit(orqcu_runtime* rt, int sms) {
+    return guard([&] {
+        need_rt(rt);
+        int total = 0;
+        ORQ_CUDA_CHECK(cudaDeviceGetAttribute(&total, cudaDevAttrMultiProcessorCount, rt->ctx.device));
+        need(sms >= 0, "negative SM limit");
+        rt->ctx.num_sms = (sms == 0 || sms > total) ? total : std::max(sms, 4);
     });
 }
 

@@ -614,6 +614,50 @@ __global__ void k_fin_final(FinArgs a) {
 // Generate `count` sharded permutations of size n from the three 2-party group
 // streams, in ORQ's order: permutation-major, groups {0,1},{0,2},{1,2}
 // (generateBatch, hm_sharded_permutation_generator.h:178-194).
+namespace {
+FyRes& fy_res(Ctx& c) {
+    FyRes& R = c.fy;
+    if (R.ready) return R;
+    // the scanners' streams have the highest priority: when generator CTAs
+    // (which fill an SM's registers and shared memory) retire, pending scans
+    // are dispatched before the next generator window
+    int prio_lo = 0, prio_hi = 0;
+    ORQ_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&R.gs, cudaStreamNonBlocking, prio_lo));
+    for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&R.ss[g], cudaStreamNonBlocking, prio_hi));
+    ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&R.ev_start, cudaEventDisableTiming));
+    for (int k = 0; k < kFyRingMax; k++) {
+        ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&R.gen_done[k], cudaEventDisableTiming));
+        for (int g = 0; g < 3; g++) {
+            ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&R.scan_done[g][k], cudaEventDisableTiming));
+            ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&R.st_ev[g][k], cudaEventDisableTiming));
+        }
+    }
+    ORQ_CUDA_CHECK(cudaMallocHost(&R.hst, (size_t)kFyRingMax * 3 * sizeof(FyState)));
+    R.ready = true;
+    return R;
+}
+}  // namespace
+
+void release_fy(Ctx& c) {
+    FyRes& R = c.fy;
+    if (!R.ready) return;
+    cudaStreamSynchronize(R.gs);
+    for (int g = 0; g < 3; g++) cudaStreamSynchronize(R.ss[g]);
+    cudaEventDestroy(R.ev_start);
+    for (int k = 0; k < kFyRingMax; k++) {
+        cudaEventDestroy(R.gen_done[k]);
+        for (int g = 0; g < 3; g++) {
+            cudaEventDestroy(R.scan_done[g][k]);
+            cudaEventDestroy(R.st_ev[g][k]);
+        }
+    }
+    cudaStreamDestroy(R.gs);
+    for (int g = 0; g < 3; g++) cudaStreamDestroy(R.ss[g]);
+    cudaFreeHost(R.hst);
+    R = FyRes{};
+}
+
 void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>& out) {
     out.clear();
     if (count == 0) return;
@@ -687,20 +731,14 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     // the scanner's stream has the highest priority: when generator CTAs
     // (which fill an SM's registers and shared memory) retire, a pending scan
     // is dispatched before the next generator window
-    int prio_lo = 0, prio_hi = 0;
-    ORQ_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    cudaStream_t gs, ss[3];
-    ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&gs, cudaStreamNonBlocking, prio_lo));
-    for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&ss[g], cudaStreamNonBlocking, prio_hi));
-    cudaEvent_t ev_start, gen_done[kRing], scan_done[3][kRing], st_ev[3][kRing];
-    ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
-    for (int k = 0; k < kRing; k++) {
-        ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&gen_done[k], cudaEventDisableTiming));
-        for (int g = 0; g < 3; g++) {
-            ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&scan_done[g][k], cudaEventDisableTiming));
-            ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&st_ev[g][k], cudaEventDisableTiming));
-        }
-    }
+    FyRes& R = fy_res(c);
+    cudaStream_t gs = R.gs;
+    cudaStream_t* ss = R.ss;
+    cudaEvent_t ev_start = R.ev_start;
+    auto& gen_done = R.gen_done;
+    auto& scan_done = R.scan_done;
+    auto& st_ev = R.st_ev;
+    static_assert(kRing <= kFyRingMax, "ring deeper than the cached events");
     ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
     ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
     for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], ev_start, 0));
@@ -762,8 +800,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     // takes the SM the previous one frees before any generator CTA can, by
     // stream priority) and no host round trip idles a scanner. A scan queued
     // after its group's last permutation completed sees `done` and returns.
-    FyState* hst = nullptr;
-    ORQ_CUDA_CHECK(cudaMallocHost(&hst, (size_t)kRing * 3 * sizeof(FyState)));
+    FyState* hst = static_cast<FyState*>(R.hst);
     auto launch_scan = [&](unsigned long long w, int g) {
         const int b = (int)(w % kRing);
         ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], gen_done[b], 0));
@@ -795,20 +832,29 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
                                        cudaMemcpyDeviceToHost, ss[g]));
         ORQ_CUDA_CHECK(cudaEventRecord(st_ev[g][b], ss[g]));
     };
-    for (unsigned long long w = 0;; w++) {
+    // The host checks completion up to kRing-1 windows behind the launches
+    // while more windows are expected (no idle scanner, no host round trip on
+    // the critical path), then window by window, so a chain that ends early
+    // does not leave a ring's worth of windows queued.
+    const unsigned long long expect = (unsigned long long)std::ceil(per_perm * (double)count / W);
+    unsigned long long checked = 0;
+    bool finished = false;
+    for (unsigned long long w = 0; !finished; w++) {
         if (w > limit_windows)
             throw std::runtime_error("permutation generation did not converge");
         launch_gen(w);
         for (int g = 0; g < 3; g++) launch_scan(w, g);
-        if (w + 1 < (unsigned long long)kRing) continue;
-        // completion of the window kRing-1 behind
-        const int pb = (int)((w + 1 - kRing) % kRing);
-        bool all = true;
-        for (int g = 0; g < 3; g++) {
-            ORQ_CUDA_CHECK(cudaEventSynchronize(st_ev[g][pb]));
-            all = all && hst[3 * pb + g].done;
+        const unsigned long long lag = (w + 1 < expect) ? (unsigned long long)(kRing - 1) : 0ull;
+        while (!finished && checked + lag <= w) {
+            const int pb = (int)(checked % kRing);
+            bool all = true;
+            for (int g = 0; g < 3; g++) {
+                ORQ_CUDA_CHECK(cudaEventSynchronize(st_ev[g][pb]));
+                all = all && hst[3 * pb + g].done;
+            }
+            finished = all;
+            checked++;
         }
-        if (all) break;
     }
     const unsigned long long w = tl_idx.size();
     ORQ_CUDA_CHECK(cudaStreamSynchronize(gs));
@@ -888,17 +934,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // scratch reuse
     }
     c.check_device_error();
-    cudaFreeHost(hst);
-    cudaEventDestroy(ev_start);
-    for (int k = 0; k < kRing; k++) {
-        cudaEventDestroy(gen_done[k]);
-        for (int g = 0; g < 3; g++) {
-            cudaEventDestroy(scan_done[g][k]);
-            cudaEventDestroy(st_ev[g][k]);
-        }
-    }
-    cudaStreamDestroy(gs);
-    for (int g = 0; g < 3; g++) cudaStreamDestroy(ss[g]);
+
 }
 
 // PermutationManager::reserve (permutation_manager.h:102-181): keep a queue of

@@ -91,6 +91,21 @@ struct BatchGraph {
     unsigned long long launches = 0;
 };
 
+// Streams, events and pinned state of the permutation generator, created on
+// first use and kept for the runtime's life (creating them per call cost
+// device-wide synchronisation when the pinned buffer was freed).
+constexpr int kFyRingMax = 8;
+struct FyRes {
+    bool ready = false;
+    cudaStream_t gs = nullptr;
+    cudaStream_t ss[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_start = nullptr;
+    cudaEvent_t gen_done[kFyRingMax] = {};
+    cudaEvent_t scan_done[3][kFyRingMax] = {};
+    cudaEvent_t st_ev[3][kFyRingMax] = {};
+    void* hst = nullptr;  // pinned scanner states, [ring slot][group]
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -107,6 +122,7 @@ struct Ctx {
     // (they skip the access); checked at the synchronous points.
     int* d_err = nullptr;
     void check_device_error();
+    FyRes fy;
     std::map<std::string, BatchGraph> graphs;  // batched launches by shape
     std::map<std::string, int> tuned;          // autotuned threads per CTA by size class
     cudaStream_t capture_stream = nullptr;     // private stream for graph capture
@@ -174,6 +190,7 @@ void op_zero_share(Ctx& c, bool arith, int w, size_t n, Sh3 r);
 void op_reshare(Ctx& c, bool arith, int w, size_t n, int group, Sh3 s);
 
 // ---- permutations (perm.cu) ----
+void release_fy(Ctx& c);
 void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>& out);
 void reserve_perms(Ctx& c, size_t n, size_t count);
 ShardedPerm next_perm(Ctx& c, size_t n);

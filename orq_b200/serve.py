@@ -135,25 +135,31 @@ def check_result(req, out):
 
 
 class _Slot:
-    def __init__(self, idx, device):
+    def __init__(self, idx, device, sm_limit=0):
         torch = _torch()
         self.idx = idx
         self.stream = torch.cuda.Stream(device=device)
         with torch.cuda.stream(self.stream):
             self.rt = Runtime(seed=1, device=device)
+        if sm_limit:
+            self.rt.set_sm_limit(sm_limit)
         self.busy = False
 
 
 class Server:
     """Continuous-batching server over `slots` concurrent runtimes."""
 
-    def __init__(self, slots=4, device=0, budget_fraction=0.8, budget_bytes=None):
+    def __init__(self, slots=4, device=0, budget_fraction=0.8, budget_bytes=None, share_sms=True):
         torch = _torch()
         torch.cuda.set_device(device)
         free, _ = torch.cuda.mem_get_info(device)
         self.budget = int(budget_bytes if budget_bytes is not None else free * budget_fraction)
         self.device = device
-        self.slots = [_Slot(i, device) for i in range(slots)]
+        # with several slots, each slot's grids are sized for its share of the
+        # SMs so concurrent requests' kernels stay resident side by side
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+        limit = sms // slots if (share_sms and slots > 1) else 0
+        self.slots = [_Slot(i, device, limit) for i in range(slots)]
 
     def close(self):
         for s in self.slots:
@@ -248,11 +254,14 @@ def make_trace(count, rate, seed=1, min_log=12, max_log=22, mix=(0.6, 0.3, 0.1))
     """Poisson arrivals at `rate` requests/s of mixed requests (sort, groupby,
     join with probabilities `mix`), sizes log-uniform over 2^min_log..2^max_log
     rows (a join's n is its primary-key side; its foreign-key side is 4n)."""
+    # requests and arrivals come from separate generators: the same seed gives
+    # the same requests at any rate (capacity is measured on them at rate 0)
     rng = np.random.Generator(np.random.PCG64(seed))
+    arr = np.random.Generator(np.random.PCG64(seed + 7919))
     t = 0.0
     out = []
     for k in range(count):
-        t += rng.exponential(1.0 / rate) if rate > 0 else 0.0
+        t += arr.exponential(1.0 / rate) if rate > 0 else 0.0
         kind = KINDS[int(rng.choice(3, p=list(mix)))]
         n = int(round(2 ** rng.uniform(min_log, max_log)))
         out.append(Request(k, kind, n, seed * 1000003 + k, t))
