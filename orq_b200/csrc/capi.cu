@@ -70,12 +70,6 @@ int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out) {
         ORQ_CUDA_CHECK(cudaMemset(rt->ctx.d_err, 0, sizeof(int)));
         orqcu::init_ctx_keys(rt->ctx, seed);
         orqcu::upload_aes_tables(device);
-        // memory a runtime trims stays in the device's stream-ordered pool for
-        // the next allocation (any runtime) instead of going back to the OS
-        cudaMemPool_t mp;
-        ORQ_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&mp, device));
-        uint64_t keep = UINT64_MAX;
-        ORQ_CUDA_CHECK(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep));
         *out = rt;
     });
 }

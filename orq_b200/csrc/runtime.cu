@@ -128,18 +128,21 @@ void upload_aes_tables(int device) {
 }
 
 // ---------------------------------------------------------------------------
-// Pool: size-bucketed reuse of device allocations (buckets are powers of two
-// above 1 MiB, 256-byte multiples below), so the per-round temporaries of a
-// sort do not go back to the allocator. New blocks come from the stream-ordered
+// Pool: size-bucketed reuse of device allocations (above 1 MiB a bucket is a
+// multiple of an eighth of the size's power of two, so at most 12.5 % is
+// wasted on the multi-gigabyte buffers of large sorts; 256-byte multiples
+// below), so the per-round temporaries of a sort do not go back to the
+// allocator. New blocks come from the stream-ordered
 // allocator on the runtime's stream and trim() returns cached blocks the same
 // way, so neither ever synchronises the device (runtimes on different streams
 // allocate and release independently).
 static size_t bucket(size_t bytes) {
     if (bytes < 256) return 256;
     if (bytes <= (1u << 20)) return (bytes + 255) & ~size_t(255);
-    size_t b = size_t(1) << 20;
-    while (b < bytes) b <<= 1;
-    return b;
+    size_t p = size_t(1) << 20;
+    while (p * 2 <= bytes) p <<= 1;  // p <= bytes < 2p
+    const size_t step = p / 8;
+    return (bytes + step - 1) / step * step;
 }
 
 void* Pool::get(size_t bytes, cudaStream_t stream) {

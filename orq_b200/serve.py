@@ -9,9 +9,10 @@ requests have not reserved, so requests that arrive while others run start
 as soon as a slot and memory free up, and their kernels overlap on the
 device. A slot re-keys its runtime with the request's own seed before
 running it (orqcu_runtime_reseed): a request's shares and opened result are
-the same whether it runs alone or in a mix. After each request the slot
-returns its cached memory to the device (stream-ordered, no device-wide
-synchronisation), so reservations track real use.
+the same whether it runs alone or in a mix. A slot keeps its device memory
+pool warm between requests (re-allocating and re-mapping gigabytes per
+request costs more than the request); with several slots each slot's grids
+are sized for its share of the SMs.
 
 Latency is measured from a request's arrival to the host having its opened
 result; the server reports throughput (rows/s over the whole trace) and the
@@ -189,7 +190,6 @@ class Server:
                     with torch.cuda.stream(slot.stream):
                         slot.rt.reseed(req.seed)
                         req.result = run_request(slot.rt, req)
-                        slot.rt.trim()
                         slot.stream.synchronize()
                     req.t_done = time.perf_counter() - t0
                     if check:
