@@ -164,6 +164,13 @@ int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key
  * launch: log2(8*width)+1 AND rounds on every pair and the packed sign fix-up. */
 int orqcu_compare_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
                     const void* const y[3], void* const eq[3], void* const gt[3]);
+/* BSharedVector::operator== (b_shared_vector.h:493-504): bit_same (log2(8W)
+ * AND rounds, b_shared_vector.h:164-178) then mask(1); eq is a B-shared bit. */
+int orqcu_equal_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                  const void* const y[3], void* const eq[3]);
+/* not_b_1 (replicated_3pc.h:207), BSharedVector::operator!: every share
+ * becomes !(s & 1), the logical NOT of a B-shared bit. Local. */
+int orqcu_not_b_1(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
 /* bitonic_sort (sorting.h:266-353) of one B-shared key column in place, in the
  * signed order; n a power of two, width 4 or 8. One launch per network stage
  * (compare + two multiplexes, operators/common.h:20-28). */

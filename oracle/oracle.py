@@ -215,6 +215,19 @@ class Oracle:
                               self._ptrs(res))
         return res
 
+    def equal(self, x, y):
+        w = x[0].dtype.itemsize
+        eq = self.new(len(x[0]), w)
+        self.lib.oro_equal(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(x[0])), self._ptrs(x),
+                           self._ptrs(y), self._ptrs(eq))
+        return eq
+
+    def not_b1(self, x):
+        w = x[0].dtype.itemsize
+        y = self.new(len(x[0]), w)
+        self.lib.oro_not_b1(w, ctypes.c_size_t(len(x[0])), self._ptrs(x), self._ptrs(y))
+        return y
+
     def bitonic_sort(self, key, desc=False):
         w = key[0].dtype.itemsize
         self.lib.oro_bitonic_sort(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(key[0])), self._ptrs(key),

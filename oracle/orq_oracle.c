@@ -1269,3 +1269,14 @@ void oro_distinct(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, voi
     }
     free3(E);
 }
+
+/* BSharedVector::operator== (b_shared_vector.h:493-504): bit_same, mask(1). */
+void oro_equal(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* eq[3]) {
+    eq3(c, w, n, x, y, eq);
+}
+
+/* not_b_1 (replicated_3pc.h:207): every share becomes !(s & 1). */
+void oro_not_b1(int w, size_t n, void* const x[3], void* y[3]) {
+    for (int j = 0; j < 3; j++)
+        for (size_t i = 0; i < n; i++) st(y[j], i, w, (ld(x[j], i, w) & 1) ^ 1);
+}

@@ -130,6 +130,10 @@ void oro_table_sort(oro_ctx* c, int w, size_t n, int ncols, void* const* cols, c
  * keys (adjacent rows only). */
 void oro_distinct(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, void* res[3]);
 
+/* operator== (b_shared_vector.h:493-504) and not_b_1 (replicated_3pc.h:207). */
+void oro_equal(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* eq[3]);
+void oro_not_b1(int w, size_t n, void* const x[3], void* y[3]);
+
 #ifdef __cplusplus
 }
 #endif

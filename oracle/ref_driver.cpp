@@ -294,6 +294,33 @@ int main(int argc, char** argv) {
                 d.plain("open_key", o);
             }
         }
+    } else if (op == "relops32" || op == "relops64") {
+        // operator== != >= <= of B-shared x vs y, in that order; a quarter of
+        // the pairs are equal
+        uint64_t st = seed;
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            auto x = gen<T>(n, st, ~0ull);
+            auto y = gen<T>(n, st, ~0ull);
+            for (size_t i = 0; i < n; i += 4) y[i] = x[i];
+            BSharedVector<T> xb = secret_share_b(x, 0);
+            BSharedVector<T> yb = secret_share_b(y, 1);
+            auto e = xb == yb;
+            auto ne = xb != yb;
+            auto ge = xb >= yb;
+            auto le = xb <= yb;
+            d.shares("eq", *e);
+            d.shares("ne", *ne);
+            d.shares("ge", *ge);
+            d.shares("le", *le);
+            auto oe = e->open(), one = ne->open(), oge = ge->open(), ole = le->open();
+            d.plain("open_eq", oe);
+            d.plain("open_ne", one);
+            d.plain("open_ge", oge);
+            d.plain("open_le", ole);
+        };
+        if (op == "relops32") run(int32_t{});
+        else run(int64_t{});
     } else if (op == "compare32" || op == "compare64") {
         // BSharedVector::_compare of x vs y; a quarter of the pairs are equal
         uint64_t st = seed;

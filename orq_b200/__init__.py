@@ -313,6 +313,36 @@ class BSharedVector(SharedVector):
         """operator< (b_shared_vector.h:556-558): other > self."""
         return other._compare(self)[1]
 
+    def __eq__(self, other: "BSharedVector") -> "BSharedVector":
+        """operator== (b_shared_vector.h:493-504): bit_same, then mask(1)."""
+        if other.size() != self.size() or other.width != self.width:
+            raise ValueError("size/width mismatch")
+        eq = self.rt._alloc(self.size(), self.width)
+        _check(self.rt.lib.orqcu_equal_b(self.rt.h, self.width, ctypes.c_size_t(self.size()),
+                                         _p3(self.shares), _p3(other.shares), _p3(eq)))
+        return BSharedVector(self.rt, eq)
+
+    def lnot(self) -> "BSharedVector":
+        """operator! (not_b_1, replicated_3pc.h:207): logical NOT of a bit."""
+        y = self.rt._alloc(self.size(), self.width)
+        _check(self.rt.lib.orqcu_not_b_1(self.rt.h, self.width, ctypes.c_size_t(self.size()),
+                                         _p3(self.shares), _p3(y)))
+        return BSharedVector(self.rt, y)
+
+    def __ne__(self, other: "BSharedVector") -> "BSharedVector":
+        """operator!= (b_shared_vector.h:514-516): !(self == other)."""
+        return (self == other).lnot()
+
+    def __ge__(self, other: "BSharedVector") -> "BSharedVector":
+        """operator>= (b_shared_vector.h:566-568): !(self < other)."""
+        return (self < other).lnot()
+
+    def __le__(self, other: "BSharedVector") -> "BSharedVector":
+        """operator<= (b_shared_vector.h:578-580): !(self > other)."""
+        return (self > other).lnot()
+
+    __hash__ = object.__hash__
+
 
 class ASharedVector(SharedVector):
     """Arithmetic shares mod 2^(8w) (core/containers/a_shared_vector.h)."""

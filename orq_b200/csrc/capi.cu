@@ -510,4 +510,26 @@ int orqcu_runtime_set_sm_limit(orqcu_runtime* rt, int sms) {
     });
 }
 
+int orqcu_equal_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
+                  const void* const y[3], void* const eq[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "equality supports 4 and 8-byte keys");
+        need_sh(x, n, "null x");
+        need_sh(y, n, "null y");
+        need_sh((const void* const*)eq, n, "null eq");
+        orqcu::op_equal(rt->ctx, width, n, c3(x), c3(y), m3(eq));
+    });
+}
+
+int orqcu_not_b_1(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "not_b_1 supports 4 and 8-byte shares");
+        need_sh(x, n, "null x");
+        need_sh((const void* const*)y, n, "null y");
+        orqcu::op_not1(rt->ctx, width, n, c3(x), m3(y));
+    });
+}
+
 }  // extern "C"

@@ -74,7 +74,7 @@ __device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&
     constexpr int W = sizeof(T);
     constexpr int B = 8 * W;               // pairs per packed word
     constexpr int L = (W == 4) ? 5 : 6;    // bit_same rounds
-    constexpr int NFULL = MODE == 0 ? L + 3 : L + 1;
+    constexpr int NFULL = MODE == 0 ? L + 3 : (MODE == 1 ? L + 1 : L);
     constexpr int WORDS = 32 * W / 4;      // keystream words per call and stream per warp
     constexpr int NB = 32 * W / 16;        // AES blocks per call and stream per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -115,7 +115,7 @@ __device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&
             o[2] = ks.z;
             o[3] = ks.w;
         }
-        if (lane < 3) {
+        if (MODE != 2 && lane < 3) {
             // the packed AND: word c = pair / B covers pairs [cB, cB+B)
             const unsigned long long c = p0w / B;
             const unsigned long long nl = lane == 0 ? nonce[0] : (lane == 1 ? nonce[1] : nonce[2]);
@@ -154,6 +154,14 @@ __device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&
             and3(Sm, Tm, K, Z);
 #pragma unroll
             for (int j = 0; j < 3; j++) Sm[j] = Z[j];
+        }
+        if constexpr (MODE == 2) {
+            // operator== : bit_same then mask(1)
+            if (valid)
+#pragma unroll
+                for (int j = 0; j < 3; j++) a.eq[j][p] = Sm[j] & 1;
+            __syncthreads();  // keystream buffers are rewritten by the next tile
+            return;
         }
         // ---- gt = parity(((eq >> 1) ^ eq) & this)
         T G[3];
@@ -335,7 +343,7 @@ template <typename T, int MODE>
 void launch_cmp(Ctx& c, const CmpArgs<T>& a, const char* name) {
     constexpr int W = sizeof(T);
     constexpr int L = (W == 4) ? 5 : 6;
-    constexpr int NFULL = MODE == 0 ? L + 3 : L + 1;
+    constexpr int NFULL = MODE == 0 ? L + 3 : (MODE == 1 ? L + 1 : L);
     constexpr int kCmpThreads = cmp_threads<W>();
     // spread small stages over every SM: threads per CTA a multiple of 64
     // (whole packed words for both widths) up to the maximum
@@ -349,8 +357,8 @@ void launch_cmp(Ctx& c, const CmpArgs<T>& a, const char* name) {
     const unsigned long long units = ceil_div(a.m, nt);
     const unsigned grid = (unsigned)std::min<unsigned long long>(units ? units : 1, (unsigned long long)c.num_sms);
     const double calls = NFULL;
-    ProfScope ps(c, name, 12.0 * W * a.m,
-                 calls * 3.0 * ceil_div(a.m * W, 16) + 3.0 * ceil_div(ceil_div(a.m, 8 * W) * W, 16));
+    ProfScope ps(c, name, (MODE == 2 ? 9.0 : 12.0) * W * a.m,
+                 calls * 3.0 * ceil_div(a.m * W, 16) + (MODE == 2 ? 0.0 : 3.0 * ceil_div(ceil_div(a.m, 8 * W) * W, 16)));
     kern<<<grid, nt, smem, c.stream>>>(a);
     ORQ_CUDA_CHECK(cudaGetLastError());
     c.kernels_launched++;
@@ -373,6 +381,32 @@ void compare_t(Ctx& c, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt) {
     a.m = n;
     if (n) launch_cmp<T, 1>(c, a, "compare");
     for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += (unsigned long long)(L + 1) * a.C + a.Cp;
+}
+
+template <typename T>
+void equal_t(Ctx& c, size_t n, CSh3 x, CSh3 y, Sh3 eq) {
+    constexpr int W = sizeof(T);
+    constexpr int L = (W == 4) ? 5 : 6;
+    CmpArgs<T> a{};
+    for (int j = 0; j < 3; j++) {
+        a.x[j] = (const T*)x.p[j];
+        a.y[j] = (const T*)y.p[j];
+        a.eq[j] = (T*)eq.p[j];
+        a.pair[j] = c.stream_arg(PAIR0 + j);
+    }
+    a.C = chunks_of((unsigned long long)n * W);
+    a.m = n;
+    if (n) launch_cmp<T, 2>(c, a, "equal");
+    for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += (unsigned long long)L * a.C;
+}
+
+// not_b_1 (replicated_3pc.h:207): every share becomes !(s & 1)
+template <typename T>
+__global__ void k_not1(CSh3 x, Sh3 y, unsigned long long n) {
+    for (unsigned long long i = gtid(); i < n; i += gstride())
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            reinterpret_cast<T*>(y.p[j])[i] = (reinterpret_cast<const T*>(x.p[j])[i] & 1) ^ 1;
 }
 
 template <typename T>
@@ -636,6 +670,23 @@ void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt) {
     if (w == 4) compare_t<uint32_t>(c, n, x, y, eq, gt);
     else if (w == 8) compare_t<unsigned long long>(c, n, x, y, eq, gt);
     else throw std::invalid_argument("compare supports int32 and int64 keys");
+}
+
+void op_equal(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq) {
+    if (w == 4) equal_t<uint32_t>(c, n, x, y, eq);
+    else if (w == 8) equal_t<unsigned long long>(c, n, x, y, eq);
+    else throw std::invalid_argument("equality supports int32 and int64 keys");
+}
+
+void op_not1(Ctx& c, int w, size_t n, CSh3 x, Sh3 y) {
+    if (!n) return;
+    const unsigned g = plain_grid(c, n);
+    ProfScope ps(c, "not_b_1", 6.0 * w * n);
+    if (w == 4) k_not1<uint32_t><<<g, 256, 0, c.stream>>>(x, y, n);
+    else if (w == 8) k_not1<unsigned long long><<<g, 256, 0, c.stream>>>(x, y, n);
+    else throw std::invalid_argument("not_b_1 supports 4 and 8-byte shares");
+    ORQ_CUDA_CHECK(cudaGetLastError());
+    c.kernels_launched++;
 }
 
 void op_bitonic_sort(Ctx& c, int w, size_t n, Sh3 key, bool desc) {

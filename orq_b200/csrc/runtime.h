@@ -214,6 +214,8 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
 // ---- compare circuit and bitonic sort (cmp.cu) ----
 void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt);
 void op_bitonic_sort(Ctx& c, int w, size_t n, Sh3 key, bool desc);
+void op_equal(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq);
+void op_not1(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
 
 // ---- aggregation network (agg.cu) ----
 enum AggFunc { AGG_SUM = 0, AGG_COUNT = 1, AGG_COPY = 2, AGG_VALID = 3, AGG_BIT_OR = 4, AGG_MIN = 5, AGG_MAX = 6 };

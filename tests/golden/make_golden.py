@@ -60,6 +60,8 @@ CASES = [
     ("distinct_n5000", "distinct", 5000, 6, 5, 64, False),
     ("join_agg_n16", "join_agg", 16, 7, 2, 64, True),
     ("join_agg_n300", "join_agg", 300, 8, 3, 64, False),
+    ("relops32_n500", "relops32", 500, 7, 2, 32, True),
+    ("relops64_n333", "relops64", 333, 8, 3, 64, True),
 ]
 
 

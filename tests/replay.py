@@ -55,6 +55,14 @@ class OracleBackend:
     def compare(self, x, y):
         return self.o.compare(x, y)
 
+    def relops(self, x, y):
+        o = self.o
+        eq = o.equal(x, y)
+        ne = o.not_b1(o.equal(x, y))
+        ge = o.not_b1(o.compare(y, x)[1])
+        le = o.not_b1(o.compare(x, y)[1])
+        return eq, ne, ge, le
+
     def aggregate(self, keys, bs, as_, reverse, sel):
         return self.o.aggregate(keys, bs, as_, reverse, sel)
 
@@ -109,6 +117,9 @@ class GpuBackend:
 
     def compare(self, x, y):
         return x._compare(y)
+
+    def relops(self, x, y):
+        return x == y, x != y, x >= y, x <= y
 
     def aggregate(self, keys, bs, as_, reverse, sel):
         orq, rt = self.orq, self.rt
@@ -193,6 +204,19 @@ def replay_compare(be, n, seed, w):
     out = {"xb": be.np(xb), "yb": be.np(yb), "eq": be.np(eq), "gt": be.np(gt)}
     out["open_eq"] = be.open(eq, False)[None]
     out["open_gt"] = be.open(gt, False)[None]
+    return out, (x, y)
+
+
+def replay_relops(be, n, seed, w):
+    """The "relops32"/"relops64" ops of ref_driver.cpp: == != >= <= in order."""
+    x, y = compare_inputs(n, seed, _U[w])
+    xb = be.share(x, False, 0)
+    yb = be.share(y, False, 1)
+    outs = be.relops(xb, yb)
+    out = {}
+    for nm, v in zip(("eq", "ne", "ge", "le"), outs):
+        out[nm] = be.np(v)
+        out["open_" + nm] = be.open(v, False)[None]
     return out, (x, y)
 
 

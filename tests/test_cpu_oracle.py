@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 from replay import (OracleBackend, replay_agg, replay_bitonic, replay_compare, replay_prims,
+                    replay_relops,
                     replay_radix, replay_tsort, same)
 
 
@@ -203,3 +204,16 @@ def test_table_sort_plaintext_order(oracle_lib):
     order = sorted(range(n), key=lambda i: (int(v0[i]), -int(v1[i]), int(v2[i])))
     assert out["open_c1"][0].tolist() == [int(v1[i]) for i in order]
     assert sorted(out["open_da"][0].tolist()) == sorted(int(x) for x in va)
+
+
+@pytest.mark.parametrize("tag,w", [("relops32_n500", 4), ("relops64_n333", 8)])
+def test_relational_operators_match_reference_shares(oracle_lib, golden, digests, tag, w):
+    """operator== != >= <= (b_shared_vector.h:493-580), share for share"""
+    m = digests[tag]["meta"]
+    out, (x, y) = replay_relops(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    sd = {4: np.int32, 8: np.int64}[w]
+    xs, ys = x.view(sd), y.view(sd)
+    for nm, want in (("eq", xs == ys), ("ne", xs != ys), ("ge", xs >= ys), ("le", xs <= ys)):
+        assert np.array_equal(out["open_" + nm][0], want.astype(x.dtype)), nm

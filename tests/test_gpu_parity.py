@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from replay import (GpuBackend, OracleBackend, radix_inputs, replay_agg, replay_bitonic,
-                    replay_compare, replay_join, replay_prims, replay_radix, replay_tsort,
+                    replay_compare, replay_join, replay_prims, replay_relops, replay_radix, replay_tsort,
                     same)
 
 pytestmark = pytest.mark.gpu
@@ -476,3 +476,16 @@ def test_serving_results_same_alone_and_in_the_mix(orq):
         for k in alone:
             assert same(alone[k], r.result[k]), (r.kind, r.n, k)
         assert check_result(r, alone)
+
+
+@pytest.mark.parametrize("tag,w", [("relops32_n500", 4), ("relops64_n333", 8)])
+def test_relational_operators_match_reference_shares(orq, golden, digests, tag, w):
+    """operator== != >= <= (b_shared_vector.h:493-580), share for share"""
+    m = digests[tag]["meta"]
+    out, (x, y) = replay_relops(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    sd = {4: np.int32, 8: np.int64}[w]
+    xs, ys = x.view(sd), y.view(sd)
+    for nm, want in (("eq", xs == ys), ("ne", xs != ys), ("ge", xs >= ys), ("le", xs <= ys)):
+        assert np.array_equal(out["open_" + nm][0], want.astype(x.dtype)), nm
