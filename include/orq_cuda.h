@@ -176,6 +176,30 @@ int orqcu_not_b_1(orqcu_runtime* rt, int width, size_t n, const void* const x[3]
  * (compare + two multiplexes, operators/common.h:20-28). */
 int orqcu_bitonic_sort(orqcu_runtime* rt, int width, size_t n, void* const key[3],
                        int descending);
+/* bitonic_sort (sorting.h:266-353) over nkeys B-shared key columns (keys[3*k+p],
+ * most significant first, each ascending or descending) with na A-shared and
+ * nb B-shared data columns moved along, in place; n a power of two, width 4
+ * or 8, at most 8 keys and 40 columns. Per network stage one compare_rows
+ * launch and one swap launch (keys and B data with the bits, A data with
+ * b2a_bit of them). One key and no data take the fused orqcu_bitonic_sort path. */
+int orqcu_bitonic_sort_rows(orqcu_runtime* rt, int width, size_t n, int nkeys, void* const* keys,
+                            const int* descending, int na, void* const* data_a, int nb,
+                            void* const* data_b);
+/* compare_rows (sorting.h:80-108): gt[i] = row i of the nkeys key columns x
+ * (x[3*k+p]) is greater than row i of y in their lexicographic order, key k
+ * ascending or descending; gt is a B-shared bit. One fused launch. */
+int orqcu_compare_rows(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* x,
+                       const void* const* y, const int* descending, void* const gt[3]);
+/* swap (sorting.h:146-212): for each of ncols column pairs (x[3*k+p],
+ * y[3*k+p]) exchange rows i where bits[i] is 1, with two multiplexes per
+ * column (operators/common.h:20-49): B-shared columns with B-shared bits
+ * (arith = 0), A-shared columns with A-shared bits (arith = 1). x and y must
+ * not alias. One fused launch. */
+int orqcu_swap(orqcu_runtime* rt, int arith, int width, size_t n, int ncols, void* const* x,
+               void* const* y, const void* const bits[3]);
+/* BSharedVector::extend_lsb (b_shared_vector.h:145-147): every share becomes
+ * all ones where its LSB is set, else zero. Local. */
+int orqcu_extend_lsb(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
 
 /* Aggregation functions (aggregation.h:27-140). */
 enum {

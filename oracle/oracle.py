@@ -113,6 +113,9 @@ class Oracle:
     def add_a(self, x, y):
         return self._bin(self.lib.oro_add_a, x, y, ctx=False)
 
+    def sub_a(self, x, y):
+        return self._bin(self.lib.oro_sub_a, x, y, ctx=False)
+
     def b2a_bit(self, x):
         w = x[0].dtype.itemsize
         y = self.new(len(x[0]), w)
@@ -232,3 +235,37 @@ class Oracle:
         w = key[0].dtype.itemsize
         self.lib.oro_bitonic_sort(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(key[0])), self._ptrs(key),
                                   int(desc))
+
+    @staticmethod
+    def _flat(arrs):
+        return (ctypes.c_void_p * max(1, 3 * len(arrs)))(*[x.ctypes.data for a in arrs for x in a])
+
+    def extend_lsb(self, x):
+        w = x[0].dtype.itemsize
+        y = self.new(len(x[0]), w)
+        self.lib.oro_extend_lsb(w, ctypes.c_size_t(len(x[0])), self._ptrs(x), self._ptrs(y))
+        return y
+
+    def compare_rows(self, xs, ys, desc):
+        """operators::compare_rows over the key columns xs vs ys; returns gt."""
+        w = xs[0][0].dtype.itemsize
+        n = len(xs[0][0])
+        gt = self.new(n, w)
+        self.lib.oro_compare_rows(ctypes.byref(self.ctx), w, ctypes.c_size_t(n), len(xs), self._flat(xs),
+                                  self._flat(ys), (ctypes.c_int * len(xs))(*[int(d) for d in desc]),
+                                  self._ptrs(gt))
+        return gt
+
+    def swap(self, xs, ys, bits, arith):
+        """operators::swap of column pairs (in place) with B- or A-shared bits."""
+        w = bits[0].dtype.itemsize
+        self.lib.oro_swap(ctypes.byref(self.ctx), int(arith), w, ctypes.c_size_t(len(bits[0])), len(xs),
+                          self._flat(xs), self._flat(ys), self._ptrs(bits))
+
+    def bitonic_sort_rows(self, keys, desc, data_a=(), data_b=()):
+        """operators::bitonic_sort over several key columns with data columns."""
+        w = keys[0][0].dtype.itemsize
+        self.lib.oro_bitonic_sort_rows(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(keys[0][0])),
+                                       len(keys), self._flat(keys),
+                                       (ctypes.c_int * len(keys))(*[int(d) for d in desc]),
+                                       len(data_a), self._flat(data_a), len(data_b), self._flat(data_b))

@@ -1280,3 +1280,192 @@ void oro_not_b1(int w, size_t n, void* const x[3], void* y[3]) {
     for (int j = 0; j < 3; j++)
         for (size_t i = 0; i < n; i++) st(y[j], i, w, (ld(x[j], i, w) & 1) ^ 1);
 }
+
+/* ------------------------------------------------------------------------- */
+/* compare_rows, swap and multi-column bitonic sort (operators/sorting.h:80-353,
+ * operators/common.h:20-49). */
+
+/* BSharedVector::extend_lsb (b_shared_vector.h:145-147) */
+void oro_extend_lsb(int w, size_t n, void* const x[3], void* y[3]) { ext3(y, x, n, w); }
+
+/* multiplex(sel, a, b) = a + sel * (b - a) on A-shared columns (common.h:43-49) */
+static void mux_a(oro_ctx* c, int w, size_t m, void* const sel[3], void* const a[3],
+                  void* const b[3], void* res[3]) {
+    void* t[3];
+    alloc3(t, m, w);
+    oro_sub_a(w, m, b, a, t);
+    oro_mul_a(c, w, m, sel, t, t);
+    oro_add_a(w, m, a, t, res);
+    free3(t);
+}
+
+/* compare_rows (sorting.h:80-108) of m row pairs over nkeys key columns given
+ * as widened arrays xa[3k+j], ya[3k+j]: gt of key 0, then per further key
+ * gt ^= new_gt & eq and eq &= new_eq; gt comes out masked to its LSB. */
+static void compare_rows_u(oro_ctx* c, int w, size_t m, int nkeys, u128* const* xa,
+                           u128* const* ya, const int* desc, void* gt[3]) {
+    u128 *e[3], *g[3];
+    void *EQ[3], *NE[3], *NG[3];
+    for (int j = 0; j < 3; j++) {
+        e[j] = (u128*)xalloc(m * 16 + 16);
+        g[j] = (u128*)xalloc(m * 16 + 16);
+    }
+    alloc3(EQ, m, w);
+    alloc3(NE, m, w);
+    alloc3(NG, m, w);
+    for (int k = 0; k < nkeys; k++) {
+        u128* const* t = desc[k] ? ya + 3 * k : xa + 3 * k;
+        u128* const* o = desc[k] ? xa + 3 * k : ya + 3 * k;
+        compare_pairs(c, w, m, t, o, e, g);
+        void** G = k ? NG : gt;
+        void** Q = k ? NE : EQ;
+        for (int j = 0; j < 3; j++)
+            for (size_t p = 0; p < m; p++) {
+                st(G[j], p, w, g[j][p]);
+                st(Q[j], p, w, e[j][p]);
+            }
+        if (k) {
+            oro_and_b(c, w, m, NG, EQ, NG);
+            oro_xor_b(w, m, gt, NG, gt);
+            oro_and_b(c, w, m, EQ, NE, EQ);
+        }
+    }
+    mask3(gt, m, w, 1);
+    for (int j = 0; j < 3; j++) {
+        free(e[j]);
+        free(g[j]);
+    }
+    free3(EQ);
+    free3(NE);
+    free3(NG);
+}
+
+void oro_compare_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* x, void* const* y,
+                      const int* desc, void* gt[3]) {
+    u128** xa = (u128**)xalloc(sizeof(u128*) * 3 * (size_t)nkeys);
+    u128** ya = (u128**)xalloc(sizeof(u128*) * 3 * (size_t)nkeys);
+    for (int k = 0; k < 3 * nkeys; k++) {
+        xa[k] = (u128*)xalloc(n * 16 + 16);
+        ya[k] = (u128*)xalloc(n * 16 + 16);
+        for (size_t p = 0; p < n; p++) {
+            xa[k][p] = ld(x[k], p, w);
+            ya[k][p] = ld(y[k], p, w);
+        }
+    }
+    compare_rows_u(c, w, n, nkeys, xa, ya, desc, gt);
+    for (int k = 0; k < 3 * nkeys; k++) {
+        free(xa[k]);
+        free(ya[k]);
+    }
+    free(xa);
+    free(ya);
+}
+
+/* swap (sorting.h:146-212): per column tmp = multiplex(bits, x, y),
+ * y = multiplex(bits, y, x), x = tmp; boolean or arithmetic multiplex. */
+static void swap_cols(oro_ctx* c, int arith, int w, size_t m, int ncols, void* const* x,
+                      void* const* y, void* const bits[3]) {
+    void* tmp[3];
+    alloc3(tmp, m, w);
+    for (int k = 0; k < ncols; k++) {
+        void* X[3] = {x[3 * k], x[3 * k + 1], x[3 * k + 2]};
+        void* Y[3] = {y[3 * k], y[3 * k + 1], y[3 * k + 2]};
+        if (arith) {
+            mux_a(c, w, m, bits, X, Y, tmp);
+            mux_a(c, w, m, bits, Y, X, Y);
+        } else {
+            mux_b(c, w, m, bits, X, Y, tmp);
+            mux_b(c, w, m, bits, Y, X, Y);
+        }
+        copy3(X, tmp, m, w);
+    }
+    free3(tmp);
+}
+
+void oro_swap(oro_ctx* c, int arith, int w, size_t n, int ncols, void* const* x, void* const* y,
+              void* const bits[3]) {
+    swap_cols(c, arith, w, n, ncols, x, y, bits);
+}
+
+/* bitonic_sort (sorting.h:266-353) over nkeys key columns with na A-shared and
+ * nb B-shared data columns: per stage compare_rows on the pair rows of every
+ * key, swap of the keys, swap of the B data with the same bits, and (when there
+ * is A data) b2a_bit of the bits and an arithmetic swap of the A data. */
+void oro_bitonic_sort_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys,
+                           const int* desc, int na, void* const* data_a, int nb,
+                           void* const* data_b) {
+    if (n < 2) return;
+    int rounds = 0;
+    while (((size_t)1 << rounds) < n) rounds++;
+    const size_t m = n / 2;
+    const int ncol = nkeys + nb + na;
+    void** cols = (void**)xalloc(sizeof(void*) * 3 * (size_t)ncol);
+    for (int k = 0; k < 3 * nkeys; k++) cols[k] = keys[k];
+    for (int k = 0; k < 3 * nb; k++) cols[3 * nkeys + k] = data_b[k];
+    for (int k = 0; k < 3 * na; k++) cols[3 * (nkeys + nb) + k] = data_a[k];
+    void** X = (void**)xalloc(sizeof(void*) * 3 * (size_t)ncol);
+    void** Y = (void**)xalloc(sizeof(void*) * 3 * (size_t)ncol);
+    u128** xa = (u128**)xalloc(sizeof(u128*) * 3 * (size_t)nkeys);
+    u128** ya = (u128**)xalloc(sizeof(u128*) * 3 * (size_t)nkeys);
+    for (int k = 0; k < 3 * ncol; k++) {
+        X[k] = xalloc(m * (size_t)w + 16);
+        Y[k] = xalloc(m * (size_t)w + 16);
+    }
+    for (int k = 0; k < 3 * nkeys; k++) {
+        xa[k] = (u128*)xalloc(m * 16 + 16);
+        ya[k] = (u128*)xalloc(m * 16 + 16);
+    }
+    size_t* xi = (size_t*)xalloc(m * sizeof(size_t));
+    size_t* yi = (size_t*)xalloc(m * sizeof(size_t));
+    void *bits[3], *bits_a[3];
+    alloc3(bits, m, w);
+    alloc3(bits_a, m, w);
+    for (int i = 0; i < rounds; i++) {
+        for (int jj = 0; jj <= i; jj++) {
+            const size_t h = (size_t)1 << (i - jj);
+            for (size_t p = 0; p < m; p++) {
+                size_t cb = p / h, k = p % h;
+                xi[p] = cb * 2 * h + k;
+                yi[p] = jj == 0 ? cb * 2 * h + 2 * h - 1 - k : cb * 2 * h + h + k;
+            }
+            for (int k = 0; k < 3 * ncol; k++)
+                for (size_t p = 0; p < m; p++) {
+                    st(X[k], p, w, ld(cols[k], xi[p], w));
+                    st(Y[k], p, w, ld(cols[k], yi[p], w));
+                }
+            for (int k = 0; k < 3 * nkeys; k++)
+                for (size_t p = 0; p < m; p++) {
+                    xa[k][p] = ld(X[k], p, w);
+                    ya[k][p] = ld(Y[k], p, w);
+                }
+            compare_rows_u(c, w, m, nkeys, xa, ya, desc, bits);
+            swap_cols(c, 0, w, m, nkeys + nb, X, Y, bits);
+            if (na) {
+                oro_b2a_bit(c, w, m, bits, bits_a);
+                swap_cols(c, 1, w, m, na, X + 3 * (nkeys + nb), Y + 3 * (nkeys + nb), bits_a);
+            }
+            for (int k = 0; k < 3 * ncol; k++)
+                for (size_t p = 0; p < m; p++) {
+                    st(cols[k], xi[p], w, ld(X[k], p, w));
+                    st(cols[k], yi[p], w, ld(Y[k], p, w));
+                }
+        }
+    }
+    for (int k = 0; k < 3 * ncol; k++) {
+        free(X[k]);
+        free(Y[k]);
+    }
+    for (int k = 0; k < 3 * nkeys; k++) {
+        free(xa[k]);
+        free(ya[k]);
+    }
+    free3(bits);
+    free3(bits_a);
+    free(xi);
+    free(yi);
+    free(X);
+    free(Y);
+    free(xa);
+    free(ya);
+    free(cols);
+}

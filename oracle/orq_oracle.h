@@ -133,6 +133,14 @@ void oro_distinct(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, voi
 /* operator== (b_shared_vector.h:493-504) and not_b_1 (replicated_3pc.h:207). */
 void oro_equal(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* eq[3]);
 void oro_not_b1(int w, size_t n, void* const x[3], void* y[3]);
+void oro_extend_lsb(int w, size_t n, void* const x[3], void* y[3]);
+void oro_compare_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* x, void* const* y,
+                      const int* desc, void* gt[3]);
+void oro_swap(oro_ctx* c, int arith, int w, size_t n, int ncols, void* const* x, void* const* y,
+              void* const bits[3]);
+void oro_bitonic_sort_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys,
+                           const int* desc, int na, void* const* data_a, int nb,
+                           void* const* data_b);
 
 #ifdef __cplusplus
 }

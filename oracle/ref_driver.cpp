@@ -294,6 +294,90 @@ int main(int argc, char** argv) {
                 d.plain("open_key", o);
             }
         }
+    } else if (op == "rows32" || op == "rows64") {
+        // bitonic_sort over two key columns (k0 in [-4, 3], so rows tie on
+        // it, ASC; k1 over all bits, DESC) with one B and two A data columns
+        uint64_t st = seed;
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            using B = BSharedVector<T>;
+            using A = ASharedVector<T>;
+            using orq::operators::SortOrder;
+            auto k0 = gen<T>(n, st, 7);
+            for (size_t i = 0; i < n; i++) k0[i] = (T)(k0[i] - 4);
+            auto k1 = gen<T>(n, st, ~0ull);
+            auto b0 = gen<T>(n, st, ~0ull);
+            auto a0 = gen<T>(n, st, 0xffffffffull);
+            auto a1 = gen<T>(n, st, 0xffffull);
+            B K0 = secret_share_b(k0, 0), K1 = secret_share_b(k1, 1), B0 = secret_share_b(b0, 2);
+            A A0 = secret_share_a(a0, 0), A1 = secret_share_a(a1, 1);
+            orq::operators::bitonic_sort(std::vector<B*>{&K0, &K1}, std::vector<A*>{&A0, &A1},
+                                         std::vector<B*>{&B0}, {SortOrder::ASC, SortOrder::DESC});
+            d.shares("k0", K0);
+            d.shares("k1", K1);
+            d.shares("b0", B0);
+            d.shares("a0", A0);
+            d.shares("a1", A1);
+            auto o0 = K0.open(), o1 = K1.open(), ob = B0.open(), oa0 = A0.open(), oa1 = A1.open();
+            d.plain("open_k0", o0);
+            d.plain("open_k1", o1);
+            d.plain("open_b0", ob);
+            d.plain("open_a0", oa0);
+            d.plain("open_a1", oa1);
+        };
+        if (op == "rows32") run(int32_t{});
+        else run(int64_t{});
+    } else if (op == "cmprows32" || op == "cmprows64") {
+        // compare_rows of (x0, x1) vs (y0, y1), x0/y0 in [0, 3] (ties), key 0
+        // ASC and key 1 DESC; then extend_lsb, multiplex (B and A), and swap
+        // of the key columns and of two A columns with b2a_bit of the bits
+        uint64_t st = seed;
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            using B = BSharedVector<T>;
+            using A = ASharedVector<T>;
+            using orq::operators::SortOrder;
+            auto x0 = gen<T>(n, st, 3);
+            auto y0 = gen<T>(n, st, 3);
+            auto x1 = gen<T>(n, st, ~0ull);
+            auto y1 = gen<T>(n, st, ~0ull);
+            for (size_t i = 0; i < n; i += 4) y1[i] = x1[i];
+            auto u = gen<T>(n, st, 0xffffffffull);
+            auto v = gen<T>(n, st, 0xffffffffull);
+            B X0 = secret_share_b(x0, 0), X1 = secret_share_b(x1, 0);
+            B Y0 = secret_share_b(y0, 1), Y1 = secret_share_b(y1, 1);
+            A U = secret_share_a(u, 2), V = secret_share_a(v, 2);
+            B gt = orq::operators::compare_rows(std::vector<B*>{&X0, &X1}, std::vector<B*>{&Y0, &Y1},
+                                                {SortOrder::ASC, SortOrder::DESC});
+            d.shares("gt", gt);
+            auto gta = gt.b2a_bit();
+            d.shares("gta", *gta);
+            B ext(n);
+            ext.extend_lsb(gt);
+            d.shares("ext", ext);
+            B mb = orq::operators::multiplex(gt, X1, Y1);
+            d.shares("mux_b", mb);
+            A ma = orq::operators::multiplex(*gta, U, V);
+            d.shares("mux_a", ma);
+            std::vector<B*> px{&X0, &X1}, py{&Y0, &Y1};
+            orq::operators::swap(px, py, gt);
+            std::vector<A*> pu{&U}, pv{&V};
+            orq::operators::swap(pu, pv, *gta);
+            d.shares("x0", X0);
+            d.shares("x1", X1);
+            d.shares("y0", Y0);
+            d.shares("y1", Y1);
+            d.shares("u", U);
+            d.shares("v", V);
+            auto og = gt.open(), ox1 = X1.open(), oy1 = Y1.open(), ou = U.open(), ov = V.open();
+            d.plain("open_gt", og);
+            d.plain("open_x1", ox1);
+            d.plain("open_y1", oy1);
+            d.plain("open_u", ou);
+            d.plain("open_v", ov);
+        };
+        if (op == "cmprows32") run(int32_t{});
+        else run(int64_t{});
     } else if (op == "relops32" || op == "relops64") {
         // operator== != >= <= of B-shared x vs y, in that order; a quarter of
         // the pairs are equal

@@ -287,6 +287,15 @@ class BSharedVector(SharedVector):
                                        _p3(self.shares), _p3(z)))
         return BSharedVector(self.rt, z)
 
+    def extend_lsb(self, inp: "BSharedVector"):
+        """BSharedVector::extend_lsb (b_shared_vector.h:145-147): every element
+        of self becomes all ones where inp's LSB is set (local)."""
+        if inp.size() != self.size() or inp.width != self.width:
+            raise ValueError("size/width mismatch")
+        _check(self.rt.lib.orqcu_extend_lsb(self.rt.h, self.width, ctypes.c_size_t(self.size()),
+                                            _p3(inp.shares), _p3(self.shares)))
+        return self
+
     def b2a_bit(self) -> "ASharedVector":
         """b2a_bit (b_shared_vector.h:279-284, replicated_3pc.h:220-251)."""
         z = self.rt._alloc(self.size(), self.width)
@@ -399,12 +408,75 @@ def oblivious_apply_elementwise_perm(x: SharedVector, perm: ASharedVector):
                                                _p3(perm.shares)))
 
 
-def bitonic_sort(v: BSharedVector, order: int = ASC):
-    """orq::operators::bitonic_sort (sorting.h:266-353) of one key column, in
-    place; the size must be a power of two."""
-    rt = v.rt
-    _check(rt.lib.orqcu_bitonic_sort(rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares),
-                                     int(order == DESC)))
+def bitonic_sort(columns, data_a=(), data_b=(), order=ASC):
+    """orq::operators::bitonic_sort (sorting.h:266-353,394-399), in place; the
+    size must be a power of two. Either one B-shared key column and one order
+    (bitonic_sort(vec, order)), or a list of key columns (most significant
+    first) with A- and B-shared data columns moved along and one order per key
+    column (bitonic_sort(columns, data_a, data_b, order))."""
+    if isinstance(columns, BSharedVector):
+        if data_a or data_b:
+            raise ValueError("data columns need the list form")
+        v = columns
+        if isinstance(order, (list, tuple)):
+            order = order[0]
+        _check(v.rt.lib.orqcu_bitonic_sort(v.rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares),
+                                           int(order == DESC)))
+        return
+    columns = list(columns)
+    rt, n, w = columns[0].rt, columns[0].size(), columns[0].width
+    orders = list(order) if isinstance(order, (list, tuple)) else [order] * len(columns)
+    if len(orders) != len(columns):
+        raise ValueError("one order per key column")
+    for v in list(columns) + list(data_a) + list(data_b):
+        if v.size() != n or v.width != w:
+            raise ValueError("size/width mismatch")
+    _check(rt.lib.orqcu_bitonic_sort_rows(rt.h, w, ctypes.c_size_t(n), len(columns), _flat(columns),
+                                          (ctypes.c_int * len(columns))(*[int(o == DESC) for o in orders]),
+                                          len(data_a), _flat(data_a), len(data_b), _flat(data_b)))
+
+
+def compare_rows(x_vec, y_vec, order) -> BSharedVector:
+    """orq::operators::compare_rows (sorting.h:80-108): row i of x is greater
+    than row i of y in the lexicographic order of the key columns (each ASC or
+    DESC); returns the B-shared result bits."""
+    if not x_vec or len(x_vec) != len(y_vec) or len(order) != len(x_vec):
+        raise ValueError("compare_rows needs matching key lists and one order per key")
+    rt, n, w = x_vec[0].rt, x_vec[0].size(), x_vec[0].width
+    for v in list(x_vec) + list(y_vec):
+        if v.size() != n or v.width != w:
+            raise ValueError("size/width mismatch")
+    gt = rt._alloc(n, w)
+    _check(rt.lib.orqcu_compare_rows(rt.h, w, ctypes.c_size_t(n), len(x_vec), _flat(x_vec), _flat(y_vec),
+                                     (ctypes.c_int * len(x_vec))(*[int(o == DESC) for o in order]),
+                                     _p3(gt)))
+    return BSharedVector(rt, gt)
+
+
+def swap(x_vec, y_vec, bits):
+    """orq::operators::swap (sorting.h:146-212): rows i of the column pairs
+    (x, y) are exchanged in place where bits[i] is 1. B-shared bits swap
+    B-shared columns (multiplex on the LSB), A-shared bits A-shared columns.
+    Single vectors are accepted for one column pair."""
+    if isinstance(x_vec, SharedVector):
+        x_vec, y_vec = [x_vec], [y_vec]
+    arith = isinstance(bits, ASharedVector)
+    rt, n, w = bits.rt, bits.size(), bits.width
+    for v in list(x_vec) + list(y_vec):
+        if v.size() != n or v.width != w or v.arith != arith:
+            raise ValueError("swap columns must match the bits in size, width and sharing")
+    _check(rt.lib.orqcu_swap(rt.h, int(arith), w, ctypes.c_size_t(n), len(x_vec), _flat(x_vec),
+                             _flat(y_vec), _p3(bits.shares)))
+
+
+def multiplex(sel, a, b):
+    """orq::operators::multiplex (operators/common.h:20-49): b where sel is 1,
+    else a. B-shared: a ^ (extend_lsb(sel) & (b ^ a)); A-shared: a + sel*(b - a)."""
+    if isinstance(sel, BSharedVector):
+        ext = BSharedVector(sel.rt, sel.rt._alloc(sel.size(), sel.width))
+        ext.extend_lsb(sel)
+        return a ^ (ext & (b ^ a))
+    return a + sel * (b - a)
 
 
 class aggregators:

@@ -532,4 +532,81 @@ int orqcu_not_b_1(orqcu_runtime* rt, int width, size_t n, const void* const x[3]
     });
 }
 
+int orqcu_extend_lsb(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "extend_lsb supports 4 and 8-byte shares");
+        need_sh(x, n, "null x");
+        need_sh((const void* const*)y, n, "null y");
+        orqcu::op_extend_lsb(rt->ctx, width, n, c3(x), m3(y));
+    });
+}
+
+int orqcu_compare_rows(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* x,
+                       const void* const* y, const int* descending, void* const gt[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "compare_rows supports 4 and 8-byte keys");
+        need(nkeys >= 1 && nkeys <= 8, "compare_rows takes 1 to 8 key columns");
+        need(x && y && descending, "null key arrays");
+        std::vector<orqcu::CSh3> xs(nkeys), ys(nkeys);
+        for (int k = 0; k < nkeys; k++) {
+            need_sh(x + 3 * k, n, "null x key");
+            need_sh(y + 3 * k, n, "null y key");
+            xs[k] = c3(x + 3 * k);
+            ys[k] = c3(y + 3 * k);
+        }
+        need_sh((const void* const*)gt, n, "null gt");
+        orqcu::op_compare_rows(rt->ctx, width, n, nkeys, xs.data(), ys.data(), descending, m3(gt));
+    });
+}
+
+int orqcu_swap(orqcu_runtime* rt, int arith, int width, size_t n, int ncols, void* const* x,
+               void* const* y, const void* const bits[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "swap supports 4 and 8-byte shares");
+        need(ncols >= 0 && ncols <= 40, "swap takes 0 to 40 column pairs");
+        need(ncols == 0 || (x && y), "null column arrays");
+        need_sh(bits, n, "null bits");
+        std::vector<orqcu::Sh3> xs(ncols), ys(ncols);
+        for (int k = 0; k < ncols; k++) {
+            need_sh((const void* const*)x + 3 * k, n, "null x column");
+            need_sh((const void* const*)y + 3 * k, n, "null y column");
+            for (int j = 0; j < 3; j++) need(x[3 * k + j] != y[3 * k + j], "swap columns x and y must differ");
+            xs[k] = m3(x + 3 * k);
+            ys[k] = m3(y + 3 * k);
+        }
+        orqcu::op_swap(rt->ctx, width, n, arith != 0, ncols, xs.data(), ys.data(), c3(bits));
+    });
+}
+
+int orqcu_bitonic_sort_rows(orqcu_runtime* rt, int width, size_t n, int nkeys, void* const* keys,
+                            const int* descending, int na, void* const* data_a, int nb,
+                            void* const* data_b) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "bitonic sort supports 4 and 8-byte keys");
+        need((n & (n - 1)) == 0, "bitonic sort needs a power-of-two size");
+        need(nkeys >= 1 && nkeys <= 8, "bitonic sort takes 1 to 8 key columns");
+        need(na >= 0 && nb >= 0 && nkeys + na + nb <= 40, "bitonic sort takes at most 40 columns");
+        need(keys && descending && (na == 0 || data_a) && (nb == 0 || data_b), "null column arrays");
+        std::vector<orqcu::Sh3> k(nkeys), a(na), b(nb);
+        for (int i = 0; i < nkeys; i++) {
+            need_sh((const void* const*)keys + 3 * i, n, "null key column");
+            k[i] = m3(keys + 3 * i);
+        }
+        for (int i = 0; i < na; i++) {
+            need_sh((const void* const*)data_a + 3 * i, n, "null A data column");
+            a[i] = m3(data_a + 3 * i);
+        }
+        for (int i = 0; i < nb; i++) {
+            need_sh((const void* const*)data_b + 3 * i, n, "null B data column");
+            b[i] = m3(data_b + 3 * i);
+        }
+        orqcu::op_bitonic_sort_rows(rt->ctx, width, n, nkeys, k.data(), descending, na, a.data(), nb,
+                                    b.data());
+    });
+}
+
 }  // extern "C"

@@ -64,6 +64,109 @@ __device__ __forceinline__ void and3(const T x[3], const T y[3], const T k[3], T
     }
 }
 
+// bit_same (b_shared_vector.h:164-178) of one pair for all parties: the
+// prefix-AND of ~(a ^ b) from the MSB down; AND round lev uses keystream call
+// lev (kword(call, stream) is this thread's word of that call).
+template <typename T, typename KW>
+__device__ __forceinline__ void bit_same3(const T (&A)[3], const T (&Bv)[3], const KW& kword, T (&Sm)[3]) {
+    constexpr int L = (sizeof(T) == 4) ? 5 : 6;
+#pragma unroll
+    for (int j = 0; j < 3; j++) Sm[j] = ~(A[j] ^ Bv[j]);
+#pragma unroll
+    for (int lev = 0; lev < L; lev++) {
+        T Tm[3], K[3], Z[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            Tm[j] = ashr(Sm[j], 1 << lev);
+            K[j] = kword(lev, j);
+        }
+        and3(Sm, Tm, K, Z);
+#pragma unroll
+        for (int j = 0; j < 3; j++) Sm[j] = Z[j];
+    }
+}
+
+// The rest of _compare (circuits.h:249-292) once bit_same is in Sm: gt =
+// parity(((eq >> 1) ^ eq) & this) on keystream call L, then the signed fix-up
+// on words of 8W packed pairs with one packed AND whose keystream block is kp
+// (this warp's [stream][word]). A warp holds pairs [p0w, p0w + 32); for 8-byte
+// shares two warps make one packed word, exchanged through `ballots` (every
+// thread of the CTA must call this). Returns the masked gt bit of the pair.
+template <typename T, typename KW>
+__device__ __forceinline__ void gt_bits3(const T (&A)[3], const T (&Bv)[3], const T (&Sm)[3], bool valid,
+                                         unsigned long long p, unsigned long long p0w, int warp,
+                                         const KW& kword, const uint32_t (*kp)[4],
+                                         uint32_t (*ballots)[3][3], T (&gt)[3]) {
+    constexpr int W = sizeof(T);
+    constexpr int B = 8 * W;
+    constexpr int L = (W == 4) ? 5 : 6;
+    T G[3];
+    {
+        T Gi[3], K[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            Gi[j] = ashr(Sm[j], 1) ^ Sm[j];
+            K[j] = kword(L, j);
+        }
+        and3(Gi, A, K, G);
+    }
+    uint32_t b1[3], b2[3], br[3];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        b1[j] = __ballot_sync(0xffffffffu, valid && ((A[j] >> (B - 1)) & 1));
+        b2[j] = __ballot_sync(0xffffffffu, valid && ((Bv[j] >> (B - 1)) & 1));
+        br[j] = __ballot_sync(0xffffffffu, valid && (__popcll((unsigned long long)G[j]) & 1));
+    }
+    T s1[3], s2[3], r[3];
+    if constexpr (W == 4) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            s1[j] = b1[j];
+            s2[j] = b2[j];
+            r[j] = br[j];
+        }
+    } else {
+        // two warps per 64-pair word
+        const int lane = threadIdx.x & 31;
+        __syncthreads();
+        if (lane == 0)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                ballots[warp][0][j] = b1[j];
+                ballots[warp][1][j] = b2[j];
+                ballots[warp][2][j] = br[j];
+            }
+        __syncthreads();
+        const int w0 = warp & ~1;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            s1[j] = (T)ballots[w0][0][j] | ((T)ballots[w0 + 1][0][j] << 32);
+            s2[j] = (T)ballots[w0][1][j] | ((T)ballots[w0 + 1][1][j] << 32);
+            r[j] = (T)ballots[w0][2][j] | ((T)ballots[w0 + 1][2][j] << 32);
+        }
+    }
+    {
+        // r ^= s2 ; s2 ^= s1 ; s2 = ~(~s2 & ~r) ; s1 ^= s2
+        T ns2[3], nr[3], K[3], Z[3];
+        const unsigned long long c = p0w / B;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const T rr = r[j] ^ s2[j];
+            const T ss = s2[j] ^ s1[j];
+            ns2[j] = ~ss;
+            nr[j] = ~rr;
+            if constexpr (W == 4) K[j] = (T)kp[j][c & 3];
+            else K[j] = (T)kp[j][2 * (c & 1)] | ((T)kp[j][2 * (c & 1) + 1] << 32);
+        }
+        and3(ns2, nr, K, Z);
+#pragma unroll
+        for (int j = 0; j < 3; j++) s1[j] ^= ~Z[j];
+    }
+    const int bitpos = (int)(p % B);
+#pragma unroll
+    for (int j = 0; j < 3; j++) gt[j] = (s1[j] >> bitpos) & 1;
+}
+
 // One CTA tile of a bitonic stage (MODE 0) or of a compare (MODE 1): the
 // pairs [base, base + blockDim.x).
 template <typename T, int MODE>
@@ -139,22 +242,8 @@ __device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&
             if constexpr (W == 4) return (T)w[lane];
             else return (T)w[2 * lane] | ((T)w[2 * lane + 1] << 32);
         };
-        // ---- bit_same: prefix-AND from the MSB down
         T Sm[3];
-#pragma unroll
-        for (int j = 0; j < 3; j++) Sm[j] = ~(A[j] ^ Bv[j]);
-#pragma unroll
-        for (int lev = 0; lev < L; lev++) {
-            T Tm[3], K[3], Z[3];
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                Tm[j] = ashr(Sm[j], 1 << lev);
-                K[j] = kword(lev, j);
-            }
-            and3(Sm, Tm, K, Z);
-#pragma unroll
-            for (int j = 0; j < 3; j++) Sm[j] = Z[j];
-        }
+        bit_same3(A, Bv, kword, Sm);
         if constexpr (MODE == 2) {
             // operator== : bit_same then mask(1)
             if (valid)
@@ -163,76 +252,10 @@ __device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&
             __syncthreads();  // keystream buffers are rewritten by the next tile
             return;
         }
-        // ---- gt = parity(((eq >> 1) ^ eq) & this)
-        T G[3];
-        {
-            T Gi[3], K[3];
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                Gi[j] = ashr(Sm[j], 1) ^ Sm[j];
-                K[j] = kword(L, j);
-            }
-            and3(Gi, A, K, G);
-        }
-        // ---- sign fix-up on words of B packed pairs
-        uint32_t b1[3], b2[3], br[3];
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            b1[j] = __ballot_sync(0xffffffffu, valid && ((A[j] >> (B - 1)) & 1));
-            b2[j] = __ballot_sync(0xffffffffu, valid && ((Bv[j] >> (B - 1)) & 1));
-            br[j] = __ballot_sync(0xffffffffu, valid && (__popcll((unsigned long long)G[j]) & 1));
-        }
-        T s1[3], s2[3], r[3];
-        if constexpr (W == 4) {
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                s1[j] = b1[j];
-                s2[j] = b2[j];
-                r[j] = br[j];
-            }
-        } else {
-            // two warps per 64-pair word
-            __syncthreads();
-            if (lane == 0)
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    ballots[warp][0][j] = b1[j];
-                    ballots[warp][1][j] = b2[j];
-                    ballots[warp][2][j] = br[j];
-                }
-            __syncthreads();
-            const int w0 = warp & ~1;
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                s1[j] = (T)ballots[w0][0][j] | ((T)ballots[w0 + 1][0][j] << 32);
-                s2[j] = (T)ballots[w0][1][j] | ((T)ballots[w0 + 1][1][j] << 32);
-                r[j] = (T)ballots[w0][2][j] | ((T)ballots[w0 + 1][2][j] << 32);
-            }
-        }
-        {
-            // r ^= s2 ; s2 ^= s1 ; s2 = ~(~s2 & ~r) ; s1 ^= s2
-            T ns2[3], nr[3], K[3], Z[3];
-            const unsigned long long c = p0w / B;
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const T rr = r[j] ^ s2[j];
-                const T ss = s2[j] ^ s1[j];
-                ns2[j] = ~ss;
-                nr[j] = ~rr;
-                if constexpr (W == 4) K[j] = (T)ksp[warp][j][c & 3];
-                else K[j] = (T)ksp[warp][j][2 * (c & 1)] | ((T)ksp[warp][j][2 * (c & 1) + 1] << 32);
-            }
-            and3(ns2, nr, K, Z);
-#pragma unroll
-            for (int j = 0; j < 3; j++) s1[j] ^= ~Z[j];
-        }
-        const int bitpos = (int)(p % B);
         T gt[3], eq[3];
+        gt_bits3(A, Bv, Sm, valid, p, p0w, warp, kword, ksp[warp], ballots, gt);
 #pragma unroll
-        for (int j = 0; j < 3; j++) {
-            gt[j] = (s1[j] >> bitpos) & 1;
-            eq[j] = Sm[j] & 1;
-        }
+        for (int j = 0; j < 3; j++) eq[j] = Sm[j] & 1;
         if (MODE == 1) {
             if (valid)
 #pragma unroll
@@ -280,6 +303,305 @@ __global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_cmp(CmpArgs<T> 
     for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < a.m;
          base += (unsigned long long)gridDim.x * blockDim.x)
         cmp_tile<T, MODE>(a, a.pair, nonce, base, S, sm + kAesSmemBytes / 4, ksp, ballots);
+}
+
+// ---- compare_rows and swap over several columns -------------------------------
+// compare_rows (operators/sorting.h:80-108) runs _compare on every key column,
+// in order, and folds key k >= 1 in with two ANDs: gt ^= new_gt & eq, then
+// eq &= new_eq. The calls of key k follow each other on the PAIR streams:
+// L + 1 full calls and one packed call for the compare, then (k >= 1) the two
+// fold calls. A key's keystream is staged per warp exactly as in a compare.
+constexpr int kMaxRowKeys = 8;
+constexpr int kMaxRowCols = 40;
+
+template <typename T>
+struct RowsCmpArgs {
+    const T* x[kMaxRowKeys][3];  // bitonic: the key columns (x and y the same)
+    const T* y[kMaxRowKeys][3];
+    int desc[kMaxRowKeys];
+    int nkeys;
+    T* gt[3];            // the masked comparison bit per pair
+    StreamArg pair[3];   // nonces at the first call
+    unsigned long long C, Cp, m;
+    int hs;              // bitonic half-box size 2^hs, or -1: pair p is (x[p], y[p])
+    int first;
+};
+
+// pair p's two rows in a bitonic stage: the box of 2h rows that holds it, row
+// k of the first half against row k (or, at j == 0, row h-1-k) of the second
+__device__ __forceinline__ void bitonic_rows(unsigned long long p, int hs, int first,
+                                             unsigned long long& xi, unsigned long long& yi) {
+    const unsigned long long h = 1ull << hs, cb = p >> hs, k = p & (h - 1);
+    xi = (cb << (hs + 1)) + k;
+    yi = first ? (cb << (hs + 1)) + 2 * h - 1 - k : (cb << (hs + 1)) + h + k;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_rows_cmp(RowsCmpArgs<T> a) {
+    constexpr int W = sizeof(T);
+    constexpr int B = 8 * W;
+    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int NCALL = L + 3;
+    constexpr int WORDS = 32 * W / 4;
+    constexpr int NB = 32 * W / 16;
+    constexpr int kThreads = cmp_threads<W>();
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t ksp[kThreads / 32][3][4];
+    __shared__ uint32_t ballots[kThreads / 32][3][3];
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* myks = sm + kAesSmemBytes / 4 + (size_t)warp * NCALL * 3 * WORDS;
+    auto kword = [&](int call, int q) -> T {
+        const uint32_t* w = myks + (call * 3 + q) * WORDS;
+        if constexpr (W == 4) return (T)w[lane];
+        else return (T)w[2 * lane] | ((T)w[2 * lane + 1] << 32);
+    };
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < a.m;
+         base += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long p0w = base + warp * 32, p = p0w + lane;
+        const bool valid = p < a.m;
+        unsigned long long xi = p, yi = p;
+        if (a.hs >= 0) bitonic_rows(p, a.hs, a.first, xi, yi);
+        T G[3] = {0, 0, 0}, E[3] = {0, 0, 0};
+        unsigned long long koff = 0;  // nonce offset of key k's first call
+        for (int k = 0; k < a.nkeys; k++) {
+            T X[3] = {0, 0, 0}, Y[3] = {0, 0, 0};
+            if (valid)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    X[j] = a.x[k][j][xi];
+                    Y[j] = a.y[k][j][yi];
+                }
+            const int ncall = k ? L + 3 : L + 1;
+            __syncwarp();  // the previous key's keystream has been read
+            for (int idx = lane; idx < ncall * 3 * NB; idx += 32) {
+                const int call = idx / (3 * NB), q = (idx / NB) % 3, b = idx % NB;
+                const unsigned long long off =
+                    koff + (call <= L ? (unsigned long long)call * a.C
+                                      : (unsigned long long)(L + 1) * a.C + a.Cp + (unsigned long long)(call - L - 1) * a.C);
+                const uint4 ks = keystream_block_n(S, a.pair[q].rk, a.pair[q].nonce + off, p0w * W / 16 + b);
+                uint32_t* o = myks + (call * 3 + q) * WORDS + b * 4;
+                o[0] = ks.x;
+                o[1] = ks.y;
+                o[2] = ks.z;
+                o[3] = ks.w;
+            }
+            if (lane < 3) {
+                const uint4 ks = keystream_block_n(S, a.pair[lane].rk,
+                                                   a.pair[lane].nonce + koff + (unsigned long long)(L + 1) * a.C,
+                                                   (p0w / B) * W / 16);
+                ksp[warp][lane][0] = ks.x;
+                ksp[warp][lane][1] = ks.y;
+                ksp[warp][lane][2] = ks.z;
+                ksp[warp][lane][3] = ks.w;
+            }
+            __syncwarp();
+            T A[3], Bv[3], Sm[3], g[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                A[j] = a.desc[k] ? Y[j] : X[j];
+                Bv[j] = a.desc[k] ? X[j] : Y[j];
+            }
+            bit_same3(A, Bv, kword, Sm);
+            gt_bits3(A, Bv, Sm, valid, p, p0w, warp, kword, ksp[warp], ballots, g);
+            if (k == 0) {
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    G[j] = g[j];
+                    E[j] = Sm[j] & 1;
+                }
+            } else {
+                T K[3], Z[3], e[3];
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    K[j] = kword(L + 1, j);
+                    e[j] = Sm[j] & 1;
+                }
+                and3(g, E, K, Z);
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    G[j] ^= Z[j];
+                    K[j] = kword(L + 2, j);
+                }
+                and3(E, e, K, Z);
+#pragma unroll
+                for (int j = 0; j < 3; j++) E[j] = Z[j];
+            }
+            koff += (unsigned long long)ncall * a.C + a.Cp;
+        }
+        if (valid)
+#pragma unroll
+            for (int j = 0; j < 3; j++) a.gt[j][p] = G[j] & 1;
+    }
+}
+
+// swap (operators/sorting.h:146-212) of nbool B-shared then narith A-shared
+// column pairs with the same bits: per column tmp = multiplex(b, x, y),
+// y = multiplex(b, y, x), x = tmp (operators/common.h:20-49), two AND (or
+// multiply_a) calls on the PAIR streams, columns in order. With b2a the
+// arithmetic columns use b2a_bit(bits) (replicated_3pc.h:220-251, three
+// arithmetic calls after the boolean columns), as bitonic_sort does for its
+// A-shared data; otherwise `bits` is already A-shared. One thread owns 16/W
+// consecutive pairs and one AES block per stream and call.
+template <typename T>
+struct RowsSwapArgs {
+    T* x[kMaxRowCols][3];
+    T* y[kMaxRowCols][3];
+    int nbool, narith, b2a;
+    const T* bits[3];
+    StreamArg pair[3];  // nonces at the first swap call
+    unsigned long long C, m;
+    int hs, first;      // bitonic mapping as in RowsCmpArgs (hs < 0: none)
+};
+
+// keystream of one 16-byte unit u of a call that starts `off` nonces past the
+// PAIR streams' nonces: K[e][stream] is element e's word of each stream
+template <typename T, int E>
+__device__ __forceinline__ void unit_keystream(const AesSmem& S, const StreamArg (&pair)[3],
+                                               unsigned long long off, unsigned long long u, T (&K)[E][3]) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const uint4 b = keystream_block_n(S, pair[q].rk, pair[q].nonce + off, u);
+        if constexpr (sizeof(T) == 4) {
+            K[0][q] = b.x;
+            K[1][q] = b.y;
+            K[2][q] = b.z;
+            K[3][q] = b.w;
+        } else {
+            K[0][q] = (T)b.x | ((T)b.y << 32);
+            K[1][q] = (T)b.z | ((T)b.w << 32);
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kAesThreads, 1) k_rows_swap(RowsSwapArgs<T> a) {
+    constexpr int W = sizeof(T);
+    constexpr int E = 16 / W;
+    extern __shared__ __align__(16) uint32_t sm[];
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    const unsigned long long units = ceil_div(a.m, (unsigned long long)E);
+    for (unsigned long long u = gtid(); u < units; u += gstride()) {
+        auto rows = [&](int e, unsigned long long& xi, unsigned long long& yi) {
+            const unsigned long long p = u * E + e;
+            xi = yi = p;
+            if (a.hs >= 0) bitonic_rows(p, a.hs, a.first, xi, yi);
+        };
+        auto ok = [&](int e) { return u * E + e < a.m; };
+        T bt[E][3];
+#pragma unroll
+        for (int e = 0; e < E; e++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) bt[e][j] = ok(e) ? a.bits[j][u * E + e] : (T)0;
+        unsigned long long call = 0;
+        T K[E][3];
+#define ORQ_NEXT_CALL() (unit_keystream(S, a.pair, call++ * a.C, u, K))
+#pragma unroll 1
+        for (int c = 0; c < a.nbool; c++) {
+            T D[E][3];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                unsigned long long xi, yi;
+                rows(e, xi, yi);
+#pragma unroll
+                for (int j = 0; j < 3; j++) D[e][j] = ok(e) ? a.x[c][j][xi] ^ a.y[c][j][yi] : (T)0;
+            }
+            // x' = x ^ (ext(b) & (y ^ x)) on the first call, y' on the second
+#pragma unroll 1  // one AES call in flight keeps the tile in registers
+            for (int side = 0; side < 2; side++) {
+                ORQ_NEXT_CALL();
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    if (!ok(e)) continue;
+                    unsigned long long xi, yi;
+                    rows(e, xi, yi);
+                    T Ex[3], Z[3];
+#pragma unroll
+                    for (int j = 0; j < 3; j++) Ex[j] = (bt[e][j] & 1) ? ~(T)0 : (T)0;  // extend_lsb
+                    and3(Ex, D[e], K[e], Z);
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        T* const v = side ? a.y[c][j] + yi : a.x[c][j] + xi;
+                        *v ^= Z[j];
+                    }
+                }
+            }
+        }
+        if (a.narith == 0) continue;
+        if (a.b2a) {
+            // b2a_bit: d = s0 - s1 from two zero-sharings, then d * d on the third
+            T d[E][3];
+#pragma unroll 1  // one AES call in flight keeps the tile in registers
+            for (int t = 0; t < 3; t++) {
+                ORQ_NEXT_CALL();
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    T z[3];
+#pragma unroll
+                    for (int p = 0; p < 3; p++) z[p] = K[e][(p + 2) % 3] - K[e][p];
+                    if (t == 0) {
+#pragma unroll
+                        for (int p = 0; p < 3; p++) d[e][p] = z[p];
+                        d[e][0] += (bt[e][0] ^ bt[e][1]) & 1;  // P0 folds its two masked shares
+                    } else if (t == 1) {
+#pragma unroll
+                        for (int p = 0; p < 3; p++) d[e][p] -= z[p];
+                        d[e][1] -= bt[e][2] & 1;  // P1 adds its second masked share to s1
+                    } else {
+#pragma unroll
+                        for (int p = 0; p < 3; p++) {
+                            const int q = (p + 1) % 3;
+                            bt[e][p] = z[p] + d[e][p] * d[e][p] + d[e][p] * d[e][q] + d[e][q] * d[e][p];
+                        }
+                    }
+                }
+            }
+        }
+        // bt now holds A-shared bits
+#pragma unroll 1
+        for (int c = a.nbool; c < a.nbool + a.narith; c++) {
+            T D[E][3];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                unsigned long long xi, yi;
+                rows(e, xi, yi);
+#pragma unroll
+                for (int j = 0; j < 3; j++) D[e][j] = ok(e) ? a.y[c][j][yi] - a.x[c][j][xi] : (T)0;
+            }
+            // multiply_a (replicated_3pc.h:44-67) of the bits with y - x, then
+            // with x - y: z_p = r_p + s_p d_p + s_p d_q + s_q d_p
+#pragma unroll 1  // one AES call in flight keeps the tile in registers
+            for (int side = 0; side < 2; side++) {
+                ORQ_NEXT_CALL();
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    if (!ok(e)) continue;
+                    unsigned long long xi, yi;
+                    rows(e, xi, yi);
+#pragma unroll
+                    for (int p = 0; p < 3; p++) {
+                        const int q = (p + 1) % 3;
+                        const T prod = bt[e][p] * D[e][p] + bt[e][p] * D[e][q] + bt[e][q] * D[e][p];
+                        T* const v = side ? a.y[c][p] + yi : a.x[c][p] + xi;
+                        *v += (K[e][(p + 2) % 3] - K[e][p]) + (side ? (T)0 - prod : prod);
+                    }
+                }
+            }
+        }
+    }
+}
+#undef ORQ_NEXT_CALL
+
+// BSharedVector::extend_lsb (b_shared_vector.h:145-147): every share becomes
+// all ones where its LSB is set (local: repeating a bit is XOR-linear)
+template <typename T>
+__global__ void k_extend_lsb(CSh3 x, Sh3 y, unsigned long long n) {
+    for (unsigned long long i = gtid(); i < n; i += gstride())
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            reinterpret_cast<T*>(y.p[j])[i] = (T)0 - (reinterpret_cast<const T*>(x.p[j])[i] & 1);
 }
 
 // ---- batched bitonic sorting -------------------------------------------------
@@ -664,7 +986,188 @@ void bitonic_batch_t(Ctx& c, int count, const size_t* n, const Sh3* keys, const 
     for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += advance[0];
 }
 
+// nonces of one compare_rows over nkeys keys (each call of m pairs)
+template <int W>
+unsigned long long rows_cmp_nonces(int nkeys, unsigned long long C, unsigned long long Cp) {
+    constexpr int L = (W == 4) ? 5 : 6;
+    return (unsigned long long)nkeys * ((L + 1) * C + Cp) + 2ull * (nkeys - 1) * C;
+}
+
+template <typename T>
+void launch_rows_cmp(Ctx& c, const RowsCmpArgs<T>& a) {
+    constexpr int W = sizeof(T);
+    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int kThreads = cmp_threads<W>();
+    const unsigned long long per_sm = ceil_div(a.m, (unsigned long long)c.num_sms);
+    const int nt = (int)std::min<unsigned long long>(kThreads, std::max<unsigned long long>(64, ceil_div(per_sm, 64) * 64));
+    const size_t per_warp = (size_t)(L + 3) * 3 * (32 * W / 4) * 4;
+    const size_t smem = kAesSmemBytes + (size_t)(nt / 32) * per_warp;
+    auto kern = k_rows_cmp<T>;
+    ORQ_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(kAesSmemBytes + (size_t)(kThreads / 32) * per_warp)));
+    const unsigned long long units = ceil_div(a.m, (unsigned long long)nt);
+    const unsigned grid = (unsigned)std::min<unsigned long long>(units ? units : 1, (unsigned long long)c.num_sms);
+    const double full_calls = (double)a.nkeys * (L + 1) + 2.0 * (a.nkeys - 1);
+    ProfScope ps(c, "compare_rows", (6.0 * a.nkeys + 3.0) * W * a.m,
+                 full_calls * 3.0 * ceil_div(a.m * W, 16) + 3.0 * a.nkeys * ceil_div(ceil_div(a.m, 8 * W) * W, 16));
+    kern<<<grid, nt, smem, c.stream>>>(a);
+    ORQ_CUDA_CHECK(cudaGetLastError());
+    c.kernels_launched++;
+}
+
+// launches one swap and returns the nonces it used: two calls per column and
+// three for the b2a of the bits
+template <typename T>
+unsigned long long launch_rows_swap(Ctx& c, const RowsSwapArgs<T>& a) {
+    constexpr int W = sizeof(T);
+    const unsigned long long calls = 2ull * (a.nbool + a.narith) + (a.b2a && a.narith ? 3ull : 0ull);
+    if (a.m && (a.nbool + a.narith))
+        launch_aes(c, "swap", (12.0 * (a.nbool + a.narith) + 3.0) * W * a.m,
+                   3.0 * calls * ceil_div(a.m * W, 16), k_rows_swap<T>, ceil_div(a.m, (unsigned long long)(16 / W)), a);
+    return calls * a.C;
+}
+
+template <typename T>
+void compare_rows_t(Ctx& c, size_t n, int nkeys, const CSh3* x, const CSh3* y, const int* desc, Sh3 gt) {
+    constexpr int W = sizeof(T);
+    RowsCmpArgs<T> a{};
+    for (int k = 0; k < nkeys; k++) {
+        for (int j = 0; j < 3; j++) {
+            a.x[k][j] = (const T*)x[k].p[j];
+            a.y[k][j] = (const T*)y[k].p[j];
+        }
+        a.desc[k] = desc[k] != 0;
+    }
+    for (int j = 0; j < 3; j++) {
+        a.gt[j] = (T*)gt.p[j];
+        a.pair[j] = c.stream_arg(PAIR0 + j);
+    }
+    a.nkeys = nkeys;
+    a.m = n;
+    a.hs = -1;
+    a.C = chunks_of((unsigned long long)n * W);
+    a.Cp = chunks_of(ceil_div(n, 8 * W) * W);
+    if (n) launch_rows_cmp(c, a);
+    for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += rows_cmp_nonces<W>(nkeys, a.C, a.Cp);
+}
+
+template <typename T>
+void swap_t(Ctx& c, size_t n, bool arith, int ncols, const Sh3* x, const Sh3* y, CSh3 bits) {
+    constexpr int W = sizeof(T);
+    RowsSwapArgs<T> a{};
+    for (int k = 0; k < ncols; k++)
+        for (int j = 0; j < 3; j++) {
+            a.x[k][j] = (T*)x[k].p[j];
+            a.y[k][j] = (T*)y[k].p[j];
+        }
+    for (int j = 0; j < 3; j++) {
+        a.bits[j] = (const T*)bits.p[j];
+        a.pair[j] = c.stream_arg(PAIR0 + j);
+    }
+    a.nbool = arith ? 0 : ncols;
+    a.narith = arith ? ncols : 0;
+    a.m = n;
+    a.hs = -1;
+    a.C = chunks_of((unsigned long long)n * W);
+    const unsigned long long used = launch_rows_swap(c, a);
+    for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += used;
+}
+
+// bitonic_sort (operators/sorting.h:266-353) over several key columns with
+// A- and B-shared data columns: per stage one compare_rows launch writes the
+// comparison bits, one swap launch moves keys, B data and (through b2a_bit of
+// the bits) A data.
+template <typename T>
+void bitonic_rows_t(Ctx& c, size_t n, int nkeys, const Sh3* keys, const int* desc, int na,
+                    const Sh3* data_a, int nb, const Sh3* data_b) {
+    constexpr int W = sizeof(T);
+    int rounds = 0;
+    while (((size_t)1 << rounds) < n) rounds++;
+    const size_t m = n / 2;
+    Scratch bits(c, 3 * m * W);
+    RowsCmpArgs<T> ca{};
+    RowsSwapArgs<T> sa{};
+    for (int k = 0; k < nkeys; k++) {
+        for (int j = 0; j < 3; j++) {
+            ca.x[k][j] = ca.y[k][j] = (const T*)keys[k].p[j];
+            sa.x[k][j] = sa.y[k][j] = (T*)keys[k].p[j];
+        }
+        ca.desc[k] = desc[k] != 0;
+    }
+    for (int k = 0; k < nb; k++)
+        for (int j = 0; j < 3; j++) sa.x[nkeys + k][j] = sa.y[nkeys + k][j] = (T*)data_b[k].p[j];
+    for (int k = 0; k < na; k++)
+        for (int j = 0; j < 3; j++) sa.x[nkeys + nb + k][j] = sa.y[nkeys + nb + k][j] = (T*)data_a[k].p[j];
+    for (int j = 0; j < 3; j++) {
+        ca.gt[j] = bits.as<T>() + j * m;
+        sa.bits[j] = bits.as<T>() + j * m;
+    }
+    ca.nkeys = nkeys;
+    ca.m = sa.m = m;
+    ca.C = sa.C = chunks_of((unsigned long long)m * W);
+    ca.Cp = chunks_of(ceil_div(m, 8 * W) * W);
+    sa.nbool = nkeys + nb;
+    sa.narith = na;
+    sa.b2a = 1;
+    for (int i = 0; i < rounds; i++)
+        for (int jj = 0; jj <= i; jj++) {
+            ca.hs = sa.hs = i - jj;
+            ca.first = sa.first = jj == 0;
+            for (int q = 0; q < 3; q++) ca.pair[q] = c.stream_arg(PAIR0 + q);
+            launch_rows_cmp(c, ca);
+            for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += rows_cmp_nonces<W>(nkeys, ca.C, ca.Cp);
+            for (int q = 0; q < 3; q++) sa.pair[q] = c.stream_arg(PAIR0 + q);
+            const unsigned long long used = launch_rows_swap(c, sa);
+            for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += used;
+        }
+}
+
+template <typename T>
+void extend_lsb_t(Ctx& c, size_t n, CSh3 x, Sh3 y) {
+    if (!n) return;
+    ProfScope ps(c, "extend_lsb", 6.0 * sizeof(T) * n);
+    k_extend_lsb<T><<<plain_grid(c, n), 256, 0, c.stream>>>(x, y, n);
+    ORQ_CUDA_CHECK(cudaGetLastError());
+    c.kernels_launched++;
+}
+
 }  // namespace
+
+void op_compare_rows(Ctx& c, int w, size_t n, int nkeys, const CSh3* x, const CSh3* y, const int* desc, Sh3 gt) {
+    if (nkeys < 1 || nkeys > kMaxRowKeys) throw std::invalid_argument("compare_rows takes 1 to 8 key columns");
+    if (w == 4) compare_rows_t<uint32_t>(c, n, nkeys, x, y, desc, gt);
+    else if (w == 8) compare_rows_t<unsigned long long>(c, n, nkeys, x, y, desc, gt);
+    else throw std::invalid_argument("compare_rows supports int32 and int64 keys");
+}
+
+void op_swap(Ctx& c, int w, size_t n, bool arith, int ncols, const Sh3* x, const Sh3* y, CSh3 bits) {
+    if (ncols < 0 || ncols > kMaxRowCols) throw std::invalid_argument("swap takes 0 to 40 column pairs");
+    if (w == 4) swap_t<uint32_t>(c, n, arith, ncols, x, y, bits);
+    else if (w == 8) swap_t<unsigned long long>(c, n, arith, ncols, x, y, bits);
+    else throw std::invalid_argument("swap supports 4 and 8-byte shares");
+}
+
+void op_extend_lsb(Ctx& c, int w, size_t n, CSh3 x, Sh3 y) {
+    if (w == 4) extend_lsb_t<uint32_t>(c, n, x, y);
+    else if (w == 8) extend_lsb_t<unsigned long long>(c, n, x, y);
+    else throw std::invalid_argument("extend_lsb supports 4 and 8-byte shares");
+}
+
+void op_bitonic_sort_rows(Ctx& c, int w, size_t n, int nkeys, const Sh3* keys, const int* desc, int na,
+                          const Sh3* data_a, int nb, const Sh3* data_b) {
+    if (n & (n - 1)) throw std::invalid_argument("bitonic sort needs a power-of-two size");
+    if (nkeys < 1 || nkeys > kMaxRowKeys) throw std::invalid_argument("bitonic sort takes 1 to 8 key columns");
+    if (na < 0 || nb < 0 || nkeys + na + nb > kMaxRowCols)
+        throw std::invalid_argument("bitonic sort takes at most 40 key and data columns");
+    if (w != 4 && w != 8) throw std::invalid_argument("bitonic sort supports int32 and int64 keys");
+    if (n < 2) return;
+    if (nkeys == 1 && na == 0 && nb == 0) {  // one fused launch per stage
+        op_bitonic_sort(c, w, n, keys[0], desc[0] != 0);
+        return;
+    }
+    if (w == 4) bitonic_rows_t<uint32_t>(c, n, nkeys, keys, desc, na, data_a, nb, data_b);
+    else bitonic_rows_t<unsigned long long>(c, n, nkeys, keys, desc, na, data_a, nb, data_b);
+}
 
 void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt) {
     if (w == 4) compare_t<uint32_t>(c, n, x, y, eq, gt);

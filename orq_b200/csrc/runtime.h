@@ -216,6 +216,11 @@ void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt);
 void op_bitonic_sort(Ctx& c, int w, size_t n, Sh3 key, bool desc);
 void op_equal(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq);
 void op_not1(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
+void op_compare_rows(Ctx& c, int w, size_t n, int nkeys, const CSh3* x, const CSh3* y, const int* desc, Sh3 gt);
+void op_swap(Ctx& c, int w, size_t n, bool arith, int ncols, const Sh3* x, const Sh3* y, CSh3 bits);
+void op_extend_lsb(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
+void op_bitonic_sort_rows(Ctx& c, int w, size_t n, int nkeys, const Sh3* keys, const int* desc, int na,
+                          const Sh3* data_a, int nb, const Sh3* data_b);
 
 // ---- aggregation network (agg.cu) ----
 enum AggFunc { AGG_SUM = 0, AGG_COUNT = 1, AGG_COPY = 2, AGG_VALID = 3, AGG_BIT_OR = 4, AGG_MIN = 5, AGG_MAX = 6 };

@@ -10,8 +10,8 @@ distinct shares S0, S1, S2:
   aes_gcm_kat.json  AES-256-GCM keystream known answers from Python
                     `cryptography` (FIPS-197 / SP 800-38D)
 
-Usage: python tests/golden/make_golden.py   (needs the reference tree; run in
-the build container, not at test time)
+Usage: python tests/golden/make_golden.py [--only tag1,tag2]   (needs the
+reference tree; run in the build container, not at test time)
 """
 from __future__ import annotations
 
@@ -62,6 +62,12 @@ CASES = [
     ("join_agg_n300", "join_agg", 300, 8, 3, 64, False),
     ("relops32_n500", "relops32", 500, 7, 2, 32, True),
     ("relops64_n333", "relops64", 333, 8, 3, 64, True),
+    ("rows32_n256", "rows32", 256, 7, 2, 32, True),
+    ("rows64_n128", "rows64", 128, 8, 3, 64, True),
+    ("rows32_n2048", "rows32", 2048, 9, 4, 32, False),
+    ("cmprows32_n500", "cmprows32", 500, 7, 2, 32, True),
+    ("cmprows64_n333", "cmprows64", 333, 8, 3, 64, True),
+    ("cmprows64_n20000", "cmprows64", 20000, 9, 4, 64, False),
 ]
 
 
@@ -90,9 +96,20 @@ def aes_kat():
 
 
 def main():
+    # --only tag1,tag2 regenerates those cases and keeps every other fixture
+    only = None
+    if "--only" in sys.argv:
+        only = set(sys.argv[sys.argv.index("--only") + 1].split(","))
     arrays = {}
     digests = {}
+    if only:
+        with np.load(os.path.join(HERE, "ref_golden.npz")) as z:
+            arrays = {k: z[k] for k in z.files}
+        with open(os.path.join(HERE, "ref_digests.json")) as f:
+            digests = json.load(f)
     for tag, op, n, dseed, sseed, bits, full in CASES:
+        if only and tag not in only:
+            continue
         dumps, _ = run_ref.run(op, n, dseed, shim_seed=sseed, bits=bits)
         meta = {"op": op, "n": n, "data_seed": dseed, "shim_seed": sseed, "bits": bits}
         digests[tag] = {"meta": meta, "arrays": {}}

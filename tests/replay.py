@@ -69,6 +69,28 @@ class OracleBackend:
     def bitonic(self, key, desc):
         self.o.bitonic_sort(key, desc)
 
+    def bitonic_rows(self, keys, desc, data_a, data_b):
+        self.o.bitonic_sort_rows(keys, desc, data_a, data_b)
+
+    def compare_rows(self, xs, ys, desc):
+        return self.o.compare_rows(xs, ys, desc)
+
+    def extend_lsb(self, x):
+        return self.o.extend_lsb(x)
+
+    def mux_b(self, sel, a, b):
+        """multiplex (operators/common.h:20-28) as the reference composes it."""
+        o = self.o
+        return o.xor_b(a, o.and_b(o.extend_lsb(sel), o.xor_b(b, a)))
+
+    def mux_a(self, sel, a, b):
+        """multiplex (operators/common.h:43-49): a + sel * (b - a)."""
+        o = self.o
+        return o.add_a(a, o.mul_a(sel, o.sub_a(b, a)))
+
+    def swap(self, xs, ys, bits, arith):
+        self.o.swap(xs, ys, bits, arith)
+
 
 class GpuBackend:
     def __init__(self, seed, device=0):
@@ -133,6 +155,28 @@ class GpuBackend:
 
     def bitonic(self, key, desc):
         self.orq.bitonic_sort(key, self.orq.DESC if desc else self.orq.ASC)
+
+    def bitonic_rows(self, keys, desc, data_a, data_b):
+        o = self.orq
+        o.bitonic_sort(keys, data_a, data_b, [o.DESC if d else o.ASC for d in desc])
+
+    def compare_rows(self, xs, ys, desc):
+        o = self.orq
+        return o.compare_rows(xs, ys, [o.DESC if d else o.ASC for d in desc])
+
+    def extend_lsb(self, x):
+        y = self.orq.BSharedVector(self.rt, self.rt._alloc(x.size(), x.width))
+        y.extend_lsb(x)
+        return y
+
+    def mux_b(self, sel, a, b):
+        return self.orq.multiplex(sel, a, b)
+
+    def mux_a(self, sel, a, b):
+        return self.orq.multiplex(sel, a, b)
+
+    def swap(self, xs, ys, bits, arith):
+        self.orq.swap(xs, ys, bits)
 
 
 def prim_inputs(n, seed, dt):
@@ -227,6 +271,74 @@ def replay_bitonic(be, n, seed, w, desc=False):
     be.bitonic(kb, desc)
     out = {"key": be.np(kb), "open_key": be.open(kb, False)[None]}
     return out, key
+
+
+def rows_inputs(n, seed, w):
+    """Inputs of the "rows32"/"rows64" ops of ref_driver.cpp."""
+    dt = _U[w]
+    st = splitmix64_fast(seed, 5 * n)
+    k0 = ((st[:n] & np.uint64(7)) - np.uint64(4)).astype(dt)
+    k1 = st[n:2 * n].astype(dt)
+    b0 = st[2 * n:3 * n].astype(dt)
+    a0 = (st[3 * n:4 * n] & np.uint64(0xFFFFFFFF)).astype(dt)
+    a1 = (st[4 * n:5 * n] & np.uint64(0xFFFF)).astype(dt)
+    return k0, k1, b0, a0, a1
+
+
+def replay_rows(be, n, seed, w):
+    """The "rows32"/"rows64" ops: bitonic_sort over (k0 ASC, k1 DESC) with
+    data columns a0, a1 (A-shared) and b0 (B-shared)."""
+    k0, k1, b0, a0, a1 = rows_inputs(n, seed, w)
+    K0, K1, B0 = be.share(k0, False, 0), be.share(k1, False, 1), be.share(b0, False, 2)
+    A0, A1 = be.share(a0, True, 0), be.share(a1, True, 1)
+    be.bitonic_rows([K0, K1], [False, True], [A0, A1], [B0])
+    out = {}
+    for nm, v, ar in (("k0", K0, False), ("k1", K1, False), ("b0", B0, False), ("a0", A0, True),
+                      ("a1", A1, True)):
+        out[nm] = be.np(v)
+        out["open_" + nm] = be.open(v, ar)[None]
+    return out, (k0, k1, b0, a0, a1)
+
+
+def cmprows_inputs(n, seed, w):
+    """Inputs of the "cmprows32"/"cmprows64" ops of ref_driver.cpp."""
+    dt = _U[w]
+    st = splitmix64_fast(seed, 6 * n)
+    x0 = (st[:n] & np.uint64(3)).astype(dt)
+    y0 = (st[n:2 * n] & np.uint64(3)).astype(dt)
+    x1 = st[2 * n:3 * n].astype(dt)
+    y1 = st[3 * n:4 * n].astype(dt)
+    y1[::4] = x1[::4]
+    u = (st[4 * n:5 * n] & np.uint64(0xFFFFFFFF)).astype(dt)
+    v = (st[5 * n:6 * n] & np.uint64(0xFFFFFFFF)).astype(dt)
+    return x0, y0, x1, y1, u, v
+
+
+def replay_cmprows(be, n, seed, w):
+    """The "cmprows32"/"cmprows64" ops: compare_rows((x0, x1), (y0, y1),
+    {ASC, DESC}), b2a_bit of it, extend_lsb, multiplex B and A, then swap of
+    the key columns and of (u, v) with the A-shared bits."""
+    x0, y0, x1, y1, u, v = cmprows_inputs(n, seed, w)
+    X0, X1 = be.share(x0, False, 0), be.share(x1, False, 0)
+    Y0, Y1 = be.share(y0, False, 1), be.share(y1, False, 1)
+    U, V = be.share(u, True, 2), be.share(v, True, 2)
+    gt = be.compare_rows([X0, X1], [Y0, Y1], [False, True])
+    out = {"gt": be.np(gt)}
+    gta = be.b2a_bit(gt)
+    out["gta"] = be.np(gta)
+    out["ext"] = be.np(be.extend_lsb(gt))
+    out["mux_b"] = be.np(be.mux_b(gt, X1, Y1))
+    out["mux_a"] = be.np(be.mux_a(gta, U, V))
+    be.swap([X0, X1], [Y0, Y1], gt, False)
+    be.swap([U], [V], gta, True)
+    for nm, x in (("x0", X0), ("x1", X1), ("y0", Y0), ("y1", Y1), ("u", U), ("v", V)):
+        out[nm] = be.np(x)
+    out["open_gt"] = be.open(gt, False)[None]
+    out["open_x1"] = be.open(X1, False)[None]
+    out["open_y1"] = be.open(Y1, False)[None]
+    out["open_u"] = be.open(U, True)[None]
+    out["open_v"] = be.open(V, True)[None]
+    return out, (x0, y0, x1, y1, u, v)
 
 
 # aggregation function codes (the reference's aggregators, in this order)

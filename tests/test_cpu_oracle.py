@@ -9,9 +9,8 @@ import hashlib
 import numpy as np
 import pytest
 
-from replay import (OracleBackend, replay_agg, replay_bitonic, replay_compare, replay_prims,
-                    replay_relops,
-                    replay_radix, replay_tsort, same)
+from replay import (OracleBackend, replay_agg, replay_bitonic, replay_cmprows, replay_compare,
+                    replay_prims, replay_radix, replay_relops, replay_rows, replay_tsort, same)
 
 
 def sha(a):
@@ -217,3 +216,67 @@ def test_relational_operators_match_reference_shares(oracle_lib, golden, digests
     xs, ys = x.view(sd), y.view(sd)
     for nm, want in (("eq", xs == ys), ("ne", xs != ys), ("ge", xs >= ys), ("le", xs <= ys)):
         assert np.array_equal(out["open_" + nm][0], want.astype(x.dtype)), nm
+
+
+@pytest.mark.parametrize("tag,w", [("rows32_n256", 4), ("rows64_n128", 8)])
+def test_bitonic_rows_match_reference_shares(oracle_lib, golden, digests, tag, w):
+    """bitonic_sort over two keys with A and B data (sorting.h:266-353)"""
+    m = digests[tag]["meta"]
+    out, ins = replay_rows(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    sd = {4: np.int32, 8: np.int64}[w]
+    k0, k1 = ins[0].view(sd), ins[1].view(sd)
+    rows = sorted(zip(k0.tolist(), (-k1.astype(object)).tolist(), ins[2].tolist(), ins[3].tolist(),
+                      ins[4].tolist()))
+    got_k0 = out["open_k0"][0].view(sd).tolist()
+    got_k1 = out["open_k1"][0].view(sd).tolist()
+    assert got_k0 == [r[0] for r in rows]
+    assert got_k1 == [-r[1] for r in rows]
+    got = sorted(zip(got_k0, got_k1, out["open_b0"][0].tolist(), out["open_a0"][0].tolist(),
+                     out["open_a1"][0].tolist()))
+    assert got == sorted(zip(k0.tolist(), k1.tolist(), ins[2].tolist(), ins[3].tolist(), ins[4].tolist()))
+
+
+def test_bitonic_rows_large_matches_reference_digests(oracle_lib, digests):
+    d = digests["rows32_n2048"]
+    m = d["meta"]
+    out, _ = replay_rows(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 4)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+def test_bitonic_rows_one_key_equals_bitonic(oracle_lib, golden):
+    """the multi-column network on one key and no data is the one-column sort"""
+    from oracle.oracle import splitmix64_fast
+
+    o = OracleBackend(2).o
+    key = splitmix64_fast(7, 256).astype(np.uint32)
+    kb = o.secret_share(key, False, 0)
+    o.bitonic_sort_rows([kb], [False])
+    assert same(np.stack(kb), golden["bitonic32_n256/key"])
+
+
+@pytest.mark.parametrize("tag,w", [("cmprows32_n500", 4), ("cmprows64_n333", 8)])
+def test_compare_rows_swap_multiplex_match_reference_shares(oracle_lib, golden, digests, tag, w):
+    """compare_rows, extend_lsb, multiplex (B, A) and swap (B, A), share for share"""
+    m = digests[tag]["meta"]
+    out, (x0, y0, x1, y1, u, v) = replay_cmprows(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    sd = {4: np.int32, 8: np.int64}[w]
+    a0, b0, a1, b1 = x0.view(sd), y0.view(sd), x1.view(sd), y1.view(sd)
+    want = (a0 > b0) | ((a0 == b0) & (b1 > a1))  # key 0 ASC, key 1 DESC
+    assert np.array_equal(out["open_gt"][0], want.astype(x0.dtype))
+    assert np.array_equal(out["open_x1"][0], np.where(want, y1, x1))
+    assert np.array_equal(out["open_y1"][0], np.where(want, x1, y1))
+    assert np.array_equal(out["open_u"][0], np.where(want, v, u))
+    assert np.array_equal(out["open_v"][0], np.where(want, u, v))
+
+
+def test_compare_rows_large_matches_reference_digests(oracle_lib, digests):
+    d = digests["cmprows64_n20000"]
+    m = d["meta"]
+    out, _ = replay_cmprows(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 8)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name

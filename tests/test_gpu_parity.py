@@ -9,8 +9,8 @@ import numpy as np
 import pytest
 
 from replay import (GpuBackend, OracleBackend, radix_inputs, replay_agg, replay_bitonic,
-                    replay_compare, replay_join, replay_prims, replay_relops, replay_radix, replay_tsort,
-                    same)
+                    replay_cmprows, replay_compare, replay_join, replay_prims, replay_relops, replay_radix,
+                    replay_rows, replay_tsort, same)
 
 pytestmark = pytest.mark.gpu
 
@@ -489,3 +489,83 @@ def test_relational_operators_match_reference_shares(orq, golden, digests, tag, 
     xs, ys = x.view(sd), y.view(sd)
     for nm, want in (("eq", xs == ys), ("ne", xs != ys), ("ge", xs >= ys), ("le", xs <= ys)):
         assert np.array_equal(out["open_" + nm][0], want.astype(x.dtype)), nm
+
+
+@pytest.mark.parametrize("tag,w", [("rows32_n256", 4), ("rows64_n128", 8)])
+def test_bitonic_rows_match_reference_shares(orq, golden, digests, tag, w):
+    """bitonic_sort over (k0 ASC, k1 DESC) with A and B data, share for share"""
+    m = digests[tag]["meta"]
+    out, _ = replay_rows(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+def test_bitonic_rows_large_matches_reference_digests(orq, digests):
+    d = digests["rows32_n2048"]
+    m = d["meta"]
+    out, _ = replay_rows(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], 4)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("w", [4, 8])
+@pytest.mark.parametrize("n", [2, 64, 1 << 12])
+def test_bitonic_rows_matches_restatement(orq, w, n):
+    gpu, _ = replay_rows(GpuBackend(31), n, 5, w)
+    cpu, _ = replay_rows(OracleBackend(31), n, 5, w)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), k
+
+
+def test_bitonic_rows_full_size_properties(orq):
+    """2^18 int64 rows: keys in lexicographic (k0 ASC, k1 DESC) order and
+    every row's data carried with it"""
+    n = 1 << 18
+    out, (k0, k1, b0, a0, a1) = replay_rows(GpuBackend(8), n, 9, 8)
+    g0 = out["open_k0"][0].view(np.int64)
+    g1 = out["open_k1"][0].view(np.int64)
+    o = np.lexsort((~k1.view(np.int64), k0.view(np.int64)))  # ~x orders x descending
+    assert np.array_equal(g0, k0.view(np.int64)[o])
+    assert np.array_equal(g1, k1.view(np.int64)[o])
+    for nm, col in (("open_b0", b0), ("open_a0", a0), ("open_a1", a1)):
+        assert np.array_equal(out[nm][0], col[o]), nm
+
+
+@pytest.mark.parametrize("tag,w", [("cmprows32_n500", 4), ("cmprows64_n333", 8)])
+def test_compare_rows_swap_multiplex_match_reference_shares(orq, golden, digests, tag, w):
+    """compare_rows, extend_lsb, multiplex and swap (B and A), share for share"""
+    m = digests[tag]["meta"]
+    out, _ = replay_cmprows(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+def test_compare_rows_large_matches_reference_digests(orq, digests):
+    d = digests["cmprows64_n20000"]
+    m = d["meta"]
+    out, _ = replay_cmprows(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], 8)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("w", [4, 8])
+@pytest.mark.parametrize("n", [1, 33, 100003])
+def test_compare_rows_matches_restatement(orq, w, n):
+    """ragged sizes: partial warps and partial packed words"""
+    gpu, _ = replay_cmprows(GpuBackend(17), n, 3, w)
+    cpu, _ = replay_cmprows(OracleBackend(17), n, 3, w)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), k
+
+
+def test_rows_errors(orq):
+    rt = orq.Runtime(seed=1)
+    a = rt.secret_share_b(np.arange(6, dtype=np.uint32), 0)
+    b = rt.secret_share_b(np.arange(6, dtype=np.uint32), 1)
+    with pytest.raises(orq.OrqError):  # not a power of two
+        orq.bitonic_sort([a, b], [], [], [orq.ASC, orq.ASC])
+    bits = a < b
+    with pytest.raises(orq.OrqError):  # x and y alias
+        orq.swap([a], [a], bits)
+    with pytest.raises(orq.OrqError):  # more than 8 keys
+        orq.compare_rows([a] * 9, [b] * 9, [orq.ASC] * 9)
