@@ -415,9 +415,11 @@ def bitonic_sort(columns, data_a=(), data_b=(), order=ASC):
     first) with A- and B-shared data columns moved along and one order per key
     column (bitonic_sort(columns, data_a, data_b, order))."""
     if isinstance(columns, BSharedVector):
+        v = columns
+        if isinstance(data_a, int):  # bitonic_sort(vec, order)
+            order, data_a = data_a, ()
         if data_a or data_b:
             raise ValueError("data columns need the list form")
-        v = columns
         if isinstance(order, (list, tuple)):
             order = order[0]
         _check(v.rt.lib.orqcu_bitonic_sort(v.rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares),
