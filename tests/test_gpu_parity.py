@@ -528,7 +528,7 @@ def test_bitonic_rows_full_size_properties(orq):
     assert np.array_equal(g0, k0.view(np.int64)[o])
     assert np.array_equal(g1, k1.view(np.int64)[o])
     for nm, col in (("open_b0", b0), ("open_a0", a0), ("open_a1", a1)):
-        assert np.array_equal(out[nm][0], col[o]), nm
+        assert np.array_equal(out[nm][0].view(col.dtype), col[o]), nm
 
 
 @pytest.mark.parametrize("tag,w", [("cmprows32_n500", 4), ("cmprows64_n333", 8)])
