@@ -74,8 +74,8 @@ struct FyGenArgs {
     StreamArg st[3];  // nonce = chain start nonce + 4 * (window start buffer)
     uint32_t n, mask, tiles;
     FyLayout lay;
-    uint32_t* ev;   // [3][tiles][slot] entry values v
-    uint32_t* ep;   // [3][tiles][slot] entry positions within the tile
+    uint32_t* ev;    // [3][tiles][slot] entry values v
+    uint32_t* last;  // [3][tiles] masked value of each tile's last draw
     uint32_t* cnt;  // [3][tiles][kMaxLevels]
     const FyState* state;
     int* err;
@@ -83,7 +83,7 @@ struct FyGenArgs {
 
 constexpr int kHalfBlocks = kBlocksPerThread / 2;  // blocks per thread per half tile
 
-__global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
+__global__ void __launch_bounds__(kGenThreads, 1) k_fy_gen(FyGenArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t red[33];
     __shared__ uint32_t sdone;
@@ -100,7 +100,6 @@ __global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
         if (sdone) continue;
         const size_t slot = (size_t)g * a.tiles + tile;
         uint32_t* ov = a.ev + slot * a.lay.slot;
-        uint32_t* op = a.ep + slot * a.lay.slot;
         for (int half = 0; half < 2; half++) {
             // this thread's 32 consecutive draws of the half tile
             uint32_t v[4 * kHalfBlocks];
@@ -113,7 +112,7 @@ __global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
                 v[4 * b + 2] = ks.z & a.mask;
                 v[4 * b + 3] = ks.w & a.mask;
             }
-            const uint32_t pos0 = blk0 * 4;
+            if (half == 1 && threadIdx.x == kGenThreads - 1) a.last[slot] = v[4 * kHalfBlocks - 1];
             // two levels per block-wide scan (16-bit fields; half-tile totals <= 16384)
             for (uint32_t L = 0; L < a.lay.nl; L += 2) {
                 const uint32_t t0 = level_threshold(a.n, L);
@@ -136,14 +135,9 @@ __global__ void __launch_bounds__(kGenThreads) k_fy_gen(FyGenArgs a) {
                         continue;
                     }
                     uint32_t* olv = ov + a.lay.off[Lh];
-                    uint32_t* olp = op + a.lay.off[Lh];
 #pragma unroll
                     for (int k = 0; k < 4 * kHalfBlocks; k++)
-                        if (v[k] < th) {
-                            olv[o] = v[k];
-                            olp[o] = pos0 + k;
-                            o++;
-                        }
+                        if (v[k] < th) olv[o++] = v[k];
                 }
                 __syncthreads();
                 if (threadIdx.x == 0) {
@@ -167,7 +161,7 @@ struct FyScanArgs {
     unsigned long long win_tile0;  // absolute index of the window's first tile
     FyLayout lay;
     const uint32_t* ev;
-    const uint32_t* ep;
+    const uint32_t* last;  // [3][tiles] masked value of each tile's last draw
     const uint32_t* cnt;
     FyState* state;     // [3]
     uint32_t* acc;      // [3][count][n] accepted offsets v_i (swap with i + v_i)
@@ -206,6 +200,13 @@ __device__ __forceinline__ uint32_t step_entries(uint32_t n, uint32_t L) {
     return s;
 }
 
+// 4-byte global -> shared copy that completes asynchronously (cp.async)
+__device__ __forceinline__ void cp_async4(uint32_t* dst_smem, const uint32_t* src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // tile holding entry e, searching P[lo..hi] (P[lo] <= e < P[hi+1])
 __device__ __forceinline__ uint32_t tile_in(const uint32_t* P, uint32_t lo, uint32_t hi, uint32_t e) {
     while (lo < hi) {
@@ -222,6 +223,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
     __shared__ uint32_t P[kMaxWindowTiles + 1];  // prefix of level-L counts over the window
     __shared__ uint32_t unc_v[kUncCap], unc_cp[kUncCap], unc_pre[kUncCap + 1];
     __shared__ uint32_t wtot[kScanWarps], wpre[kScanWarps];
+    __shared__ uint32_t wmask[kScanWarps][kPerThread][2];  // per warp and iteration: certain, uncertain ballots
     __shared__ uint32_t s_last_q, s_uacc, s_tot;
     const uint32_t g = a.g0 + blockIdx.x;
     const uint32_t n = a.n;
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
     unsigned long long start = a.state[g].start_tile;
     uint32_t tau = 0, ix = 0, L = 0, Lp = 0xffffffffu;
     const uint32_t* EV = a.ev + (size_t)g * tiles * a.lay.slot;
-    const uint32_t* EP = a.ep + (size_t)g * tiles * a.lay.slot;
+    const uint32_t* LAST = a.last + (size_t)g * tiles;
     const uint32_t* C = a.cnt + (size_t)g * tiles * kMaxLevels;
     unsigned long long st_steps = 0, st_unc_steps = 0, st_seq = 0, st_ent = 0, st_unc = 0,
                        st_cyc_load = 0, st_cyc_unc = 0, st_cyc_all = 0;
@@ -274,25 +276,26 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         const unsigned long long t_l0 = clock64();
         const uint32_t qw = (uint32_t)warp * 1024u + lane;  // this thread's entry at u = 0
         // ---- stage this thread's entries (coalesced per iteration; each lane
-        // walks its tile cursor forward) into shared memory at sv[q]
+        // walks its tile cursor forward) into shared memory at sv[q] with
+        // asynchronous copies: no registers hold them, so all of a thread's
+        // loads are in flight at once. Each thread reads back only its own
+        // entries, so its own wait makes them visible.
         {
             const size_t off = a.lay.off[L];
             uint32_t t = tau;
-            uint32_t vals[kPerThread];
 #pragma unroll
             for (int u = 0; u < kPerThread; u++) {
                 const uint32_t q = qw + 32u * u;
-                vals[u] = 0xffffffffu;
                 if (q < cs) {
                     const uint32_t e = e0 + q;
                     while (P[t + 1] <= e) t++;
-                    vals[u] = __ldg(EV + (size_t)t * a.lay.slot + off + (e - P[t]));
+                    cp_async4(sv + q, EV + (size_t)t * a.lay.slot + off + (e - P[t]));
+                } else {
+                    sv[q] = 0xffffffffu;
                 }
             }
-#pragma unroll
-            for (int u = 0; u < kPerThread; u++) sv[qw + 32u * u] = vals[u];
+            cp_async_wait_all();
         }
-        __syncwarp();
         // ---- level 1 counts per warp, block prefix over warps; halve the step
         // while the uncertain entries do not fit the list
         uint32_t tot_c, tot_u;
@@ -304,8 +307,14 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                 const uint32_t v = sv[q];
                 const bool cert = q < cs && (unsigned long long)v + q <= T;
                 const bool unc = q < cs && !cert && v <= T;
-                wc += __popc(__ballot_sync(0xffffffffu, cert));
-                wu += __popc(__ballot_sync(0xffffffffu, unc));
+                const uint32_t bc = __ballot_sync(0xffffffffu, cert);
+                const uint32_t bu = __ballot_sync(0xffffffffu, unc);
+                wc += __popc(bc);
+                wu += __popc(bu);
+                if (lane == 0) {
+                    wmask[warp][u][0] = bc;
+                    wmask[warp][u][1] = bu;
+                }
             }
             if (lane == 0) wtot[warp] = wc | (wu << 16);
             __syncthreads();
@@ -337,15 +346,10 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             uint32_t rc = cbase, ru = ubase;
 #pragma unroll
             for (int u = 0; u < kPerThread; u++) {
-                const uint32_t q = qw + 32u * u;
-                const uint32_t v = sv[q];
-                const bool cert = q < cs && (unsigned long long)v + q <= T;
-                const bool unc = q < cs && !cert && v <= T;
-                const uint32_t bc = __ballot_sync(0xffffffffu, cert);
-                const uint32_t bu = __ballot_sync(0xffffffffu, unc);
-                if (unc) {
+                const uint32_t bc = wmask[warp][u][0], bu = wmask[warp][u][1];
+                if ((bu >> lane) & 1u) {
                     const uint32_t k = ru + __popc(bu & lt);
-                    unc_v[k] = v;
+                    unc_v[k] = sv[qw + 32u * u];
                     unc_cp[k] = rc + __popc(bc & lt);
                 }
                 rc += __popc(bc);
@@ -405,17 +409,15 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
 #pragma unroll
             for (int u = 0; u < kPerThread; u++) {
                 const uint32_t q = qw + 32u * u;
-                const uint32_t v = sv[q];
-                const bool cert = q < cs && (unsigned long long)v + q <= T;
-                const bool unc = q < cs && !cert && v <= T;
-                const uint32_t bc = __ballot_sync(0xffffffffu, cert);
-                const uint32_t bu = __ballot_sync(0xffffffffu, unc);
+                const uint32_t bc = wmask[warp][u][0], bu = wmask[warp][u][1];
+                const bool cert = (bc >> lane) & 1u;
+                const bool unc = (bu >> lane) & 1u;
                 const uint32_t k = ru + __popc(bu & lt);  // uncertain entries before q
                 const bool accepted = cert || (unc && unc_cp[k]);
                 if (accepted) {
                     const uint32_t r = rc + __popc(bc & lt) + unc_pre[k];
                     if (r < need) {
-                        acc[i + r] = v;
+                        acc[i + r] = sv[q];
                         if (r == need - 1) s_last_q = q;
                     }
                 }
@@ -428,9 +430,12 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             // permutation complete: locate its last draw, count the getNext buffers
             const uint32_t e = e0 + s_last_q;
             const uint32_t t = tile_in(P, tau, tiles - 1, e);
-            const uint32_t pos = EP[(size_t)t * a.lay.slot + a.lay.off[L] + (e - P[t])];
+            // only a last draw at the very end of a getNext buffer changes the
+            // count below: that is the tile's last draw, and then it is the
+            // last entry of the tile's list
+            const bool tile_end = e + 1 == P[t + 1] && LAST[t] < level_threshold(n, L);
             const unsigned long long kend =
-                (a.win_tile0 + t - start) * (unsigned long long)kTileDraws + pos;
+                (a.win_tile0 + t - start) * (unsigned long long)kTileDraws + (tile_end ? kTileDraws - 1 : 0);
             const unsigned long long R = 1 + ((kend + 1) >> 20);
             if (threadIdx.x == 0) a.refills[(size_t)g * a.count + m] = (uint32_t)R;
             start = (start / kTilesPerRefill + R) * kTilesPerRefill;
@@ -711,10 +716,10 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     // streams: their dense phases fall in different windows, and a shared
     // launch per window would cost the slowest group every time.
     constexpr int kRing = 6;
-    std::vector<std::unique_ptr<Scratch>> ring_ev, ring_ep, ring_cnt;
+    std::vector<std::unique_ptr<Scratch>> ring_ev, ring_last, ring_cnt;
     for (int k = 0; k < kRing; k++) {
         ring_ev.emplace_back(new Scratch(c, ents_b));
-        ring_ep.emplace_back(new Scratch(c, ents_b));
+        ring_last.emplace_back(new Scratch(c, (size_t)3 * tiles * 4));
         ring_cnt.emplace_back(new Scratch(c, cnt_b));
     }
     Scratch state(c, 3 * sizeof(FyState));
@@ -748,11 +753,11 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
 
     const unsigned gen_grid = (unsigned)std::max(1, c.num_sms - 3);
     uint32_t* evp[kRing];
-    uint32_t* epp[kRing];
+    uint32_t* lastp[kRing];
     uint32_t* cntp[kRing];
     for (int k = 0; k < kRing; k++) {
         evp[k] = ring_ev[k]->as<uint32_t>();
-        epp[k] = ring_ep[k]->as<uint32_t>();
+        lastp[k] = ring_last[k]->as<uint32_t>();
         cntp[k] = ring_cnt[k]->as<uint32_t>();
     }
 
@@ -780,7 +785,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         ga.tiles = tiles;
         ga.lay = lay;
         ga.ev = evp[b];
-        ga.ep = epp[b];
+        ga.last = lastp[b];
         ga.cnt = cntp[b];
         ga.state = state.as<FyState>();
         ga.err = c.d_err;
@@ -812,7 +817,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         sa.win_tile0 = (unsigned long long)w * tiles;
         sa.lay = lay;
         sa.ev = evp[b];
-        sa.ep = epp[b];
+        sa.last = lastp[b];
         sa.cnt = cntp[b];
         sa.state = state.as<FyState>();
         sa.acc = acc.as<uint32_t>();
