@@ -43,7 +43,6 @@ constexpr int kGenThreads = 512;
 constexpr int kBlocksPerThread = kTileBlocks / kGenThreads;     // 16 blocks = 64 draws
 constexpr int kMaxLevels = 16;
 constexpr int kScanThreads = 1024;
-constexpr uint32_t kStep = 8192;  // entries per scan step (8 per thread)
 constexpr uint32_t kMaxWindowTiles = 1024;
 
 // Level L of a tile keeps, in draw order, the draws with v < n >> 2L (level 0:
@@ -478,22 +477,25 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
 
 // ---- finalize: accepted offsets -> permutation -----------------------------
 // Step i swaps positions i and j_i = i + v_i (j_i >= i), so position i is final
-// after step i. Let A(k) be the value at position k when step k starts: A(k) =
-// A(parent(k)) where parent(k) is the last earlier step whose target was k, or
-// k itself when no earlier step touched k (identity start). Then
-//   p[i] = value at j_i just before step i
-//        = A(previous step that targeted j_i)  or  j_i if there is none,
-// and self-swaps (j_i = i) give p[i] = A(i). Parents come from an atomicMax
-// over targets, A from chasing parent links, the "previous step with the same
-// target" from a small bucket per target.
+// after step i. The steps s != k with j_s = k (all s < k) form the bucket of
+// position k, s_1 < ... < s_c in step order. Position k holds k until step s_1
+// and A(s_m) after step s_m, where A(s) is the value at position s just before
+// step s. So step s_m outputs p[s_m] = A(s_{m-1}) (k for m = 1), and A(k) =
+// A(s_c) (k for an empty bucket): A(k) is the root of k in the forest of links
+// k -> max(bucket(k)). A self-swap (j_k = k) outputs p[k] = A(k).
+// Buckets are built by a counting sort: counts per target, an exclusive scan
+// per permutation, then an atomic cursor per target places the steps (the
+// cursor ends at the bucket's end, which is also the next bucket's start).
+constexpr int kFinThreads = 1024;
+constexpr uint32_t kFinChunk = kFinThreads * 8;  // scan chunk
+
 struct FinArgs {
     const uint32_t* acc;  // [P][n]
-    uint32_t n, P;
-    int32_t* par;         // [P][n]  last earlier step targeting k (-1)
-    uint32_t* cnt;        // [P][n]  non-self steps per target
-    uint32_t* off;        // [P][n]  bucket offsets (exclusive, per permutation)
-    uint32_t* fill;       // [P][n]
-    int32_t* bucket;      // [P][n]
+    uint32_t n, P, chunks;
+    uint32_t* cur;        // [P][n] bucket sizes, then starts (scan), then ends (place)
+    uint32_t* part;       // [P][chunks] chunk sums, then their exclusive scan
+    int32_t* bucket;      // [P][n] steps grouped by target
+    int32_t* par;         // [P][n] max(bucket(k)), -1 when empty
     int32_t* A;           // [P][n]
     int32_t* const* perm_out;  // [P] -> n
     int32_t* const* inv_out;   // [P] -> n
@@ -511,50 +513,68 @@ __device__ __forceinline__ uint32_t fin_target(const FinArgs& a, size_t t, uint3
     return (uint32_t)j;
 }
 
-__global__ void k_fin_init(FinArgs a) {
-    const size_t tot = (size_t)a.P * a.n;
-    for (size_t t = gtid(); t < tot; t += gstride()) {
-        a.par[t] = -1;
-        a.cnt[t] = 0;
-        a.fill[t] = 0;
-    }
-}
-__global__ void k_fin_targets(FinArgs a) {
+__global__ void k_fin_count(FinArgs a) {
     const size_t tot = (size_t)a.P * a.n;
     for (size_t t = gtid(); t < tot; t += gstride()) {
         const size_t pm = t / a.n;
         const uint32_t i = (uint32_t)(t % a.n);
         const uint32_t j = fin_target(a, t, i);
-        if (j != i) {
-            atomicMax(&a.par[pm * a.n + j], (int32_t)i);
-            atomicAdd(&a.cnt[pm * a.n + j], 1u);
-        }
+        if (j != i) atomicAdd(&a.cur[pm * a.n + j], 1u);
     }
 }
-// exclusive scan of cnt within each permutation (one CTA per permutation)
-__global__ void __launch_bounds__(1024) k_fin_scan(FinArgs a) {
+
+// sum of chunk (blockIdx.x % chunks) of permutation (blockIdx.x / chunks)
+__global__ void __launch_bounds__(kFinThreads) k_fin_part(FinArgs a) {
     __shared__ uint32_t red[33];
-    const size_t pm = blockIdx.x;
-    const uint32_t* c = a.cnt + pm * a.n;
-    uint32_t* o = a.off + pm * a.n;
+    const size_t pm = blockIdx.x / a.chunks, ch = blockIdx.x % a.chunks;
+    const uint32_t* c = a.cur + pm * a.n;
+    uint32_t s = 0;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        const size_t k = ch * kFinChunk + (size_t)u * kFinThreads + threadIdx.x;
+        s += k < a.n ? c[k] : 0u;
+    }
+    uint32_t tot;
+    block_excl_sum(s, red, tot);
+    if (threadIdx.x == 0) a.part[pm * a.chunks + ch] = tot;
+}
+
+// exclusive scan of one permutation's chunk sums (one CTA per permutation)
+__global__ void __launch_bounds__(kFinThreads) k_fin_top(FinArgs a) {
+    __shared__ uint32_t red[33];
+    uint32_t* p = a.part + (size_t)blockIdx.x * a.chunks;
     uint32_t carry = 0;
-    for (uint32_t b0 = 0; b0 < a.n; b0 += 1024 * 4) {
-        uint32_t v[4], s = 0;
-        for (int u = 0; u < 4; u++) {
-            const uint32_t k = b0 + threadIdx.x * 4 + u;
-            v[u] = k < a.n ? c[k] : 0;
-            s += v[u];
-        }
+    for (uint32_t b0 = 0; b0 < a.chunks; b0 += kFinThreads) {
+        const uint32_t k = b0 + threadIdx.x;
+        const uint32_t v = k < a.chunks ? p[k] : 0u;
         uint32_t tot;
-        uint32_t pre = block_excl_sum(s, red, tot) + carry;
-        for (int u = 0; u < 4; u++) {
-            const uint32_t k = b0 + threadIdx.x * 4 + u;
-            if (k < a.n) o[k] = pre;
-            pre += v[u];
-        }
+        const uint32_t pre = block_excl_sum(v, red, tot);
+        if (k < a.chunks) p[k] = carry + pre;
         carry += tot;
     }
 }
+
+// bucket starts: exclusive scan of the sizes, in place
+__global__ void __launch_bounds__(kFinThreads) k_fin_starts(FinArgs a) {
+    __shared__ uint32_t red[33];
+    const size_t pm = blockIdx.x / a.chunks, ch = blockIdx.x % a.chunks;
+    uint32_t* c = a.cur + pm * a.n;
+    const size_t k0 = ch * kFinChunk + (size_t)threadIdx.x * 8;  // 8 consecutive per thread
+    uint32_t v[8], s = 0;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        v[u] = k0 + u < a.n ? c[k0 + u] : 0u;
+        s += v[u];
+    }
+    uint32_t tot;
+    uint32_t pre = block_excl_sum(s, red, tot) + a.part[pm * a.chunks + ch];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        if (k0 + u < a.n) c[k0 + u] = pre;
+        pre += v[u];
+    }
+}
+
 __global__ void k_fin_place(FinArgs a) {
     const size_t tot = (size_t)a.P * a.n;
     for (size_t t = gtid(); t < tot; t += gstride()) {
@@ -562,13 +582,39 @@ __global__ void k_fin_place(FinArgs a) {
         const uint32_t i = (uint32_t)(t % a.n);
         const uint32_t j = fin_target(a, t, i);
         if (j != i) {
-            const uint32_t s = atomicAdd(&a.fill[pm * a.n + j], 1u);
-            const unsigned long long slot = (unsigned long long)a.off[pm * a.n + j] + s;
+            const uint32_t slot = atomicAdd(&a.cur[pm * a.n + j], 1u);
             if (slot < a.n) a.bucket[pm * a.n + slot] = (int32_t)i;
             else atomicOr(a.err, 2);
         }
     }
 }
+
+// bucket of position k after placement: [end(k-1), end(k)), clamped to n
+__device__ __forceinline__ void fin_bucket(const FinArgs& a, size_t pm, uint32_t k, uint32_t& b, uint32_t& e) {
+    const uint32_t* cur = a.cur + pm * a.n;
+    e = min(cur[k], a.n);
+    b = k ? min(cur[k - 1], e) : 0u;
+}
+
+__global__ void k_fin_par(FinArgs a) {
+    const size_t tot = (size_t)a.P * a.n;
+    for (size_t t = gtid(); t < tot; t += gstride()) {
+        const size_t pm = t / a.n;
+        const uint32_t k = (uint32_t)(t % a.n);
+        uint32_t b, e;
+        fin_bucket(a, pm, k, b, e);
+        const int32_t* bk = a.bucket + pm * a.n;
+        int32_t mx = -1;
+        for (uint32_t m = b; m < e; m++) mx = max(mx, bk[m]);
+        // bucket entries are steps before k; anything else is corruption
+        if (mx >= (int32_t)k) {
+            atomicOr(a.err, 8);
+            mx = -1;
+        }
+        a.par[t] = mx;
+    }
+}
+
 __global__ void k_fin_roots(FinArgs a) {
     const size_t tot = (size_t)a.P * a.n;
     for (size_t t = gtid(); t < tot; t += gstride()) {
@@ -576,40 +622,44 @@ __global__ void k_fin_roots(FinArgs a) {
         const int32_t* par = a.par + pm * a.n;
         int32_t k = (int32_t)(t % a.n);
         int32_t p = par[k];
-        while (p >= 0) {
+        while (p >= 0) {  // strictly decreasing links: ends at a root
             k = p;
             p = par[k];
         }
         a.A[t] = k;
     }
 }
+
+__device__ __forceinline__ void fin_emit(const FinArgs& a, size_t pm, uint32_t s, int32_t val) {
+    if ((uint32_t)val >= a.n) {
+        atomicOr(a.err, 4);
+        val = (int32_t)s;
+    }
+    a.perm_out[pm][s] = val;
+    a.inv_out[pm][val] = (int32_t)s;
+}
+
+// per position k: its own step if it is a self-swap, and every step of its
+// bucket (predecessor found by a scan of the small bucket)
 __global__ void k_fin_final(FinArgs a) {
     const size_t tot = (size_t)a.P * a.n;
     for (size_t t = gtid(); t < tot; t += gstride()) {
         const size_t pm = t / a.n;
-        const uint32_t i = (uint32_t)(t % a.n);
-        const uint32_t j = fin_target(a, t, i);
+        const uint32_t k = (uint32_t)(t % a.n);
         const int32_t* A = a.A + pm * a.n;
-        int32_t val;
-        if (j == i) {
-            val = A[i];
-        } else {
-            const uint32_t o = a.off[pm * a.n + j];
-            const uint32_t c = min(a.cnt[pm * a.n + j], a.n - min(o, a.n));
-            const int32_t* b = a.bucket + pm * a.n + o;
+        if (fin_target(a, t, k) == k) fin_emit(a, pm, k, A[k]);
+        uint32_t b, e;
+        fin_bucket(a, pm, k, b, e);
+        const int32_t* bk = a.bucket + pm * a.n;
+        for (uint32_t m = b; m < e; m++) {
+            const int32_t s = bk[m];
             int32_t pred = -1;
-            for (uint32_t k = 0; k < c; k++) {
-                const int32_t s = b[k];
-                if (s < (int32_t)i && s > pred) pred = s;
+            for (uint32_t q = b; q < e; q++) {
+                const int32_t x = bk[q];
+                if (x < s && x > pred) pred = x;
             }
-            val = pred >= 0 ? A[pred] : (int32_t)j;
+            fin_emit(a, pm, (uint32_t)s, pred >= 0 ? A[pred] : (int32_t)k);
         }
-        if ((uint32_t)val >= a.n) {
-            atomicOr(a.err, 4);
-            val = (int32_t)i;
-        }
-        a.perm_out[pm][i] = val;
-        a.inv_out[pm][val] = (int32_t)i;
     }
 }
 
@@ -902,8 +952,9 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     for (size_t p0 = 0; p0 < 3 * count; p0 += per_batch) {
         const size_t P = std::min(per_batch, 3 * count - p0);
         const size_t el = P * n;
-        Scratch par(c, el * 4), cnt(c, el * 4), off(c, el * 4), fill(c, el * 4), bucket(c, el * 4),
-            A(c, el * 4), ptrs(c, 2 * P * sizeof(void*));
+        const uint32_t chunks = (uint32_t)ceil_div(n, (size_t)kFinChunk);
+        Scratch cur(c, el * 4), part(c, P * chunks * 4), bucket(c, el * 4), par(c, el * 4), A(c, el * 4),
+            ptrs(c, 2 * P * sizeof(void*));
         std::vector<int32_t*> hp(2 * P);
         for (size_t k = 0; k < P; k++) {
             // acc is laid out [group][perm]; permutation index pm = p0 + k
@@ -917,25 +968,29 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         fa.acc = acc.as<uint32_t>() + p0 * n;
         fa.n = (uint32_t)n;
         fa.P = (uint32_t)P;
-        fa.par = par.as<int32_t>();
-        fa.cnt = cnt.as<uint32_t>();
-        fa.off = off.as<uint32_t>();
-        fa.fill = fill.as<uint32_t>();
+        fa.chunks = chunks;
+        fa.cur = cur.as<uint32_t>();
+        fa.part = part.as<uint32_t>();
         fa.bucket = bucket.as<int32_t>();
+        fa.par = par.as<int32_t>();
         fa.A = A.as<int32_t>();
         fa.perm_out = ptrs.as<int32_t*>();
         fa.inv_out = ptrs.as<int32_t*>() + P;
         fa.err = c.d_err;
         const unsigned gg = plain_grid(c, el);
+        const unsigned gc = (unsigned)(P * chunks);
         ProfScope ps(c, "fy_finalize", 0.0);
-        k_fin_init<<<gg, 256, 0, c.stream>>>(fa);
-        k_fin_targets<<<gg, 256, 0, c.stream>>>(fa);
-        k_fin_scan<<<(unsigned)P, 1024, 0, c.stream>>>(fa);
+        ORQ_CUDA_CHECK(cudaMemsetAsync(cur.p, 0, el * 4, c.stream));
+        k_fin_count<<<gg, 256, 0, c.stream>>>(fa);
+        k_fin_part<<<gc, kFinThreads, 0, c.stream>>>(fa);
+        k_fin_top<<<(unsigned)P, kFinThreads, 0, c.stream>>>(fa);
+        k_fin_starts<<<gc, kFinThreads, 0, c.stream>>>(fa);
         k_fin_place<<<gg, 256, 0, c.stream>>>(fa);
+        k_fin_par<<<gg, 256, 0, c.stream>>>(fa);
         k_fin_roots<<<gg, 256, 0, c.stream>>>(fa);
         k_fin_final<<<gg, 256, 0, c.stream>>>(fa);
         ORQ_CUDA_CHECK(cudaGetLastError());
-        c.kernels_launched += 6;
+        c.kernels_launched += 8;
         ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // scratch reuse
     }
     c.check_device_error();
