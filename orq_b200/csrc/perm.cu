@@ -187,6 +187,7 @@ struct FyScanArgs {
 constexpr uint32_t kMaxStepEntries = 32768;
 constexpr int kPerThread = kMaxStepEntries / kScanThreads;  // 32
 constexpr int kScanWarps = kScanThreads / 32;
+constexpr int kQuads = kPerThread / 4;  // lane-quads per thread and step
 constexpr uint32_t kUncCap = 2048;
 constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4;
 
@@ -206,6 +207,28 @@ __device__ __forceinline__ void cp_async4(uint32_t* dst_smem, const uint32_t* sr
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// class of entry q with value v in a step of cs entries at bound T: bit 0
+// certainly accepted (v + q <= T: at most q acceptances precede it), bit 4
+// uncertain (v <= T but not certain); rejected otherwise
+__device__ __forceinline__ uint32_t fy_class(uint32_t q, uint32_t v, uint32_t cs, uint32_t T) {
+    const bool cert = q < cs && (unsigned long long)v + q <= T;
+    const bool unc = q < cs && !cert && v <= T;
+    return (uint32_t)cert | ((uint32_t)unc << 4);
+}
+
+// exclusive warp prefix and warp total of a lane-quad's (certain | uncertain << 16)
+__device__ __forceinline__ void quad_prefix(uint32_t code, int lane, uint32_t& excl, uint32_t& total) {
+    const uint32_t x = __popc(code & 0xfu) | (__popc(code >> 4) << 16);
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    total = __shfl_sync(0xffffffffu, inc, 31);
+    excl = inc - x;
+}
+
 // tile holding entry e, searching P[lo..hi] (P[lo] <= e < P[hi+1])
 __device__ __forceinline__ uint32_t tile_in(const uint32_t* P, uint32_t lo, uint32_t hi, uint32_t e) {
     while (lo < hi) {
@@ -222,7 +245,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
     __shared__ uint32_t P[kMaxWindowTiles + 1];  // prefix of level-L counts over the window
     __shared__ uint32_t unc_v[kUncCap], unc_cp[kUncCap], unc_pre[kUncCap + 1];
     __shared__ uint32_t wtot[kScanWarps], wpre[kScanWarps];
-    __shared__ uint32_t wmask[kScanWarps][kPerThread][2];  // per warp and iteration: certain, uncertain ballots
+    __shared__ uint8_t codes[kScanWarps][kQuads][32];  // entry classes per warp, iteration and lane
     __shared__ uint32_t s_last_q, s_uacc, s_tot;
     const uint32_t g = a.g0 + blockIdx.x;
     const uint32_t n = a.n;
@@ -273,12 +296,12 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         }
         uint32_t cs = min(step_entries(n, L), eend - e0);
         const unsigned long long t_l0 = clock64();
-        const uint32_t qw = (uint32_t)warp * 1024u + lane;  // this thread's entry at u = 0
-        // ---- stage this thread's entries (coalesced per iteration; each lane
-        // walks its tile cursor forward) into shared memory at sv[q] with
+        const uint32_t qw = (uint32_t)warp * 1024u + lane;  // staging: this thread's entry at u = 0
+        // ---- stage the step's entries into shared memory at sv[q] with
         // asynchronous copies: no registers hold them, so all of a thread's
-        // loads are in flight at once. Each thread reads back only its own
-        // entries, so its own wait makes them visible.
+        // loads are in flight at once (coalesced per iteration; each lane walks
+        // its tile cursor forward). Warp w stages and then processes entries
+        // [1024w, 1024w + 1024), so a warp-level sync publishes them.
         {
             const size_t off = a.lay.off[L];
             uint32_t t = tau;
@@ -295,37 +318,40 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             }
             cp_async_wait_all();
         }
+        __syncwarp();
+        // In the passes below lane l of warp w holds, at iteration u, the four
+        // consecutive entries q = 1024w + 128u + 4l + r (r = 0..3); codes[w][u][l]
+        // keeps their classification (bit r: certainly accepted, bit 4 + r:
+        // uncertain): a lane-quad is one 16-byte shared load, and ranks come
+        // from one packed warp scan per 128 entries.
+        const uint32_t q0 = (uint32_t)warp * 1024u + 4u * (uint32_t)lane;
         // ---- level 1 counts per warp, block prefix over warps; halve the step
         // while the uncertain entries do not fit the list
         uint32_t tot_c, tot_u;
         for (;;) {
-            uint32_t wc = 0, wu = 0;
+            uint32_t x = 0;
 #pragma unroll
-            for (int u = 0; u < kPerThread; u++) {
-                const uint32_t q = qw + 32u * u;
-                const uint32_t v = sv[q];
-                const bool cert = q < cs && (unsigned long long)v + q <= T;
-                const bool unc = q < cs && !cert && v <= T;
-                const uint32_t bc = __ballot_sync(0xffffffffu, cert);
-                const uint32_t bu = __ballot_sync(0xffffffffu, unc);
-                wc += __popc(bc);
-                wu += __popc(bu);
-                if (lane == 0) {
-                    wmask[warp][u][0] = bc;
-                    wmask[warp][u][1] = bu;
-                }
+            for (int u = 0; u < kQuads; u++) {
+                const uint32_t q = q0 + 128u * u;
+                const uint4 v4 = *reinterpret_cast<const uint4*>(sv + q);
+                const uint32_t code = fy_class(q, v4.x, cs, T) | (fy_class(q + 1, v4.y, cs, T) << 1) |
+                                      (fy_class(q + 2, v4.z, cs, T) << 2) | (fy_class(q + 3, v4.w, cs, T) << 3);
+                codes[warp][u][lane] = (uint8_t)code;
+                x += __popc(code & 0xfu) | (__popc(code >> 4) << 16);
             }
-            if (lane == 0) wtot[warp] = wc | (wu << 16);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) wtot[warp] = x;
             __syncthreads();
             if (warp == 0) {
-                const uint32_t x = wtot[lane];
-                uint32_t inc = x;
+                const uint32_t y = wtot[lane];
+                uint32_t inc = y;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-                    if (lane >= o) inc += y;
+                    const uint32_t z = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += z;
                 }
-                wpre[lane] = inc - x;
+                wpre[lane] = inc - y;
                 if (lane == 31) s_tot = inc;
             }
             __syncthreads();
@@ -344,15 +370,25 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         if (tot_u) {
             uint32_t rc = cbase, ru = ubase;
 #pragma unroll
-            for (int u = 0; u < kPerThread; u++) {
-                const uint32_t bc = wmask[warp][u][0], bu = wmask[warp][u][1];
-                if ((bu >> lane) & 1u) {
-                    const uint32_t k = ru + __popc(bu & lt);
-                    unc_v[k] = sv[qw + 32u * u];
-                    unc_cp[k] = rc + __popc(bc & lt);
+            for (int u = 0; u < kQuads; u++) {
+                const uint32_t code = codes[warp][u][lane];
+                uint32_t ex, tot;
+                quad_prefix(code, lane, ex, tot);
+                if (code >> 4) {
+                    const uint32_t q = q0 + 128u * u;
+                    uint32_t c = rc + (ex & 0xffffu), k = ru + (ex >> 16);
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        if ((code >> (4 + r)) & 1u) {
+                            unc_v[k] = sv[q + r];
+                            unc_cp[k] = c;
+                            k++;
+                        }
+                        c += (code >> r) & 1u;
+                    }
                 }
-                rc += __popc(bc);
-                ru += __popc(bu);
+                rc += tot & 0xffffu;
+                ru += tot >> 16;
             }
         }
         __syncthreads();
@@ -398,30 +434,39 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             st_unc += tot_u;
             st_cyc_unc += clock64() - t_u0;
         }
-        // ---- accept, rank, store (consecutive accepted lanes store to
-        // consecutive ranks)
+        // ---- accept, rank, store (a lane's accepted entries go to consecutive
+        // ranks, consecutive lanes to consecutive runs)
         const uint32_t tot_a = tot_c + s_uacc;
         const uint32_t need = n - i;
         uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
         {
             uint32_t rc = cbase, ru = ubase;
 #pragma unroll
-            for (int u = 0; u < kPerThread; u++) {
-                const uint32_t q = qw + 32u * u;
-                const uint32_t bc = wmask[warp][u][0], bu = wmask[warp][u][1];
-                const bool cert = (bc >> lane) & 1u;
-                const bool unc = (bu >> lane) & 1u;
-                const uint32_t k = ru + __popc(bu & lt);  // uncertain entries before q
-                const bool accepted = cert || (unc && unc_cp[k]);
-                if (accepted) {
-                    const uint32_t r = rc + __popc(bc & lt) + unc_pre[k];
-                    if (r < need) {
-                        acc[i + r] = sv[q];
-                        if (r == need - 1) s_last_q = q;
+            for (int u = 0; u < kQuads; u++) {
+                const uint32_t code = codes[warp][u][lane];
+                uint32_t ex, tot;
+                quad_prefix(code, lane, ex, tot);
+                if (code) {
+                    const uint32_t q = q0 + 128u * u;
+                    const uint4 v4 = *reinterpret_cast<const uint4*>(sv + q);
+                    const uint32_t vv[4] = {v4.x, v4.y, v4.z, v4.w};
+                    uint32_t c = rc + (ex & 0xffffu), k = ru + (ex >> 16);  // certain / uncertain before q + r
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        const bool cert = (code >> r) & 1u, unc = (code >> (4 + r)) & 1u;
+                        if (cert || (unc && unc_cp[k])) {
+                            const uint32_t rank = c + unc_pre[k];
+                            if (rank < need) {
+                                acc[i + rank] = vv[r];
+                                if (rank == need - 1) s_last_q = q + r;
+                            }
+                        }
+                        c += cert;
+                        k += unc;
                     }
                 }
-                rc += __popc(bc);
-                ru += __popc(bu);
+                rc += tot & 0xffffu;
+                ru += tot >> 16;
             }
         }
         if (tot_a >= need) {
