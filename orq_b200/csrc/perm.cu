@@ -165,7 +165,7 @@ struct FyScanArgs {
     FyState* state;     // [3]
     uint32_t* acc;      // [3][count][n] accepted offsets v_i (swap with i + v_i)
     uint32_t* refills;  // [3][count] getNext buffers used
-    unsigned long long* stats;  // optional [3][8] diagnostic counters (ORQ_FY_STATS)
+    unsigned long long* stats;  // optional [3][kFyStats] diagnostic counters (ORQ_FY_STATS)
 };
 
 
@@ -187,6 +187,7 @@ struct FyScanArgs {
 constexpr uint32_t kMaxStepEntries = 32768;
 constexpr int kPerThread = kMaxStepEntries / kScanThreads;  // 32
 constexpr int kScanWarps = kScanThreads / 32;
+constexpr int kFyStats = 10;  // diagnostic counters per group
 constexpr int kQuads = kPerThread / 4;  // lane-quads per thread and step
 constexpr uint32_t kUncCap = 2048;
 constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4;
@@ -206,6 +207,11 @@ __device__ __forceinline__ void cp_async4(uint32_t* dst_smem, const uint32_t* sr
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// bulk prefetch of [addr, addr + bytes) into L2; addr and bytes multiples of 16
+// (the range may round a list out to 16 bytes: list buffers carry slack)
+__device__ __forceinline__ void prefetch_l2(uintptr_t addr, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(addr), "r"(bytes) : "memory");
+}
 
 // class of entry q with value v in a step of cs entries at bound T: bit 0
 // certainly accepted (v + q <= T: at most q acceptances precede it), bit 4
@@ -259,8 +265,8 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
     const uint32_t* EV = a.ev + (size_t)g * tiles * a.lay.slot;
     const uint32_t* LAST = a.last + (size_t)g * tiles;
     const uint32_t* C = a.cnt + (size_t)g * tiles * kMaxLevels;
-    unsigned long long st_steps = 0, st_unc_steps = 0, st_seq = 0, st_ent = 0, st_unc = 0,
-                       st_cyc_load = 0, st_cyc_unc = 0, st_cyc_all = 0;
+    unsigned long long st_steps = 0, st_unc_steps = 0, st_ent = 0, st_unc = 0,
+                       st_cyc_load = 0, st_cyc_unc = 0, st_cyc_all = 0, st_cyc_list = 0, st_cyc_acc = 0;
     const unsigned long long t_begin = clock64();
     for (int guard = 0; guard < (1 << 24) && !done; guard++) {
         // never look before the current permutation's first tile
@@ -296,6 +302,24 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         }
         uint32_t cs = min(step_entries(n, L), eend - e0);
         const unsigned long long t_l0 = clock64();
+        if (warp == 0) {
+            // warm L2 with the entries of the next two steps (a hint: the
+            // staging of a later step then reads L2 instead of DRAM); lane j
+            // covers the j-th tile of that range
+            const uint32_t pf0 = e0 + cs, pf1 = min(P[tiles], e0 + cs + 2 * step_entries(n, L));
+            if (pf0 < pf1) {
+                const uint32_t t = tile_in(P, tau, tiles - 1, pf0) + lane;
+                if (t < tiles && P[t] < pf1) {
+                    const uint32_t s0 = max(P[t], pf0), s1 = min(P[t + 1], pf1);
+                    if (s0 < s1) {
+                        const uint32_t* src = EV + (size_t)t * a.lay.slot + a.lay.off[L] + (s0 - P[t]);
+                        const uintptr_t lo = (uintptr_t)src & ~(uintptr_t)15;
+                        const uintptr_t hi = ((uintptr_t)(src + (s1 - s0)) + 15) & ~(uintptr_t)15;
+                        prefetch_l2(lo, (uint32_t)(hi - lo));
+                    }
+                }
+            }
+        }
         const uint32_t qw = (uint32_t)warp * 1024u + lane;  // staging: this thread's entry at u = 0
         // ---- stage the step's entries into shared memory at sv[q] with
         // asynchronous copies: no registers hold them, so all of a thread's
@@ -365,6 +389,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         st_steps++;
         st_ent += cs;
         st_cyc_load += clock64() - t_l0;
+        const unsigned long long t_li0 = clock64();
         // ---- list the uncertain entries in order, with the certain accepts
         // before each
         if (tot_u) {
@@ -393,6 +418,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         }
         __syncthreads();
         const unsigned long long t_u0 = clock64();
+        st_cyc_list += t_u0 - t_li0;
         if (warp == 0) {
             // level 2 over the listed uncertain entries
             uint32_t acc_so_far = 0;
@@ -436,6 +462,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         }
         // ---- accept, rank, store (a lane's accepted entries go to consecutive
         // ranks, consecutive lanes to consecutive runs)
+        const unsigned long long t_a0 = clock64();
         const uint32_t tot_a = tot_c + s_uacc;
         const uint32_t need = n - i;
         uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
@@ -499,6 +526,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             }
         }
         __syncthreads();  // the lists and counters are reused by the next step
+        st_cyc_acc += clock64() - t_a0;
     }
     if (threadIdx.x == 0) {
         a.state[g].i = i;
@@ -507,15 +535,16 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         a.state[g].start_tile = start;
         if (a.stats) {
             st_cyc_all = clock64() - t_begin;
-            unsigned long long* st = a.stats + g * 8;
+            unsigned long long* st = a.stats + g * kFyStats;
             st[0] += st_steps;
             st[1] += st_unc_steps;
-            st[2] += st_seq;
             st[3] += st_ent;
             st[4] += st_unc;
             st[5] += st_cyc_load;
             st[6] += st_cyc_unc;
             st[7] += st_cyc_all;
+            st[8] += st_cyc_list;
+            st[9] += st_cyc_acc;
         }
     }
 }
@@ -813,7 +842,7 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     constexpr int kRing = 6;
     std::vector<std::unique_ptr<Scratch>> ring_ev, ring_last, ring_cnt;
     for (int k = 0; k < kRing; k++) {
-        ring_ev.emplace_back(new Scratch(c, ents_b));
+        ring_ev.emplace_back(new Scratch(c, ents_b + 256));  // slack for 16-byte rounded prefetches
         ring_last.emplace_back(new Scratch(c, (size_t)3 * tiles * 4));
         ring_cnt.emplace_back(new Scratch(c, cnt_b));
     }
@@ -823,8 +852,8 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     ORQ_CUDA_CHECK(cudaMemsetAsync(state.p, 0, 3 * sizeof(FyState), c.stream));
     const bool want_stats = std::getenv("ORQ_FY_STATS") != nullptr;
     const auto t_start = std::chrono::steady_clock::now();
-    Scratch stats(c, 3 * 8 * 8);
-    if (want_stats) ORQ_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 3 * 8 * 8, c.stream));
+    Scratch stats(c, 3 * kFyStats * 8);
+    if (want_stats) ORQ_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 3 * kFyStats * 8, c.stream));
 
     // generator and scanner run on private non-blocking streams so they overlap
     // whatever the caller's stream is (the legacy default stream included)
@@ -982,14 +1011,15 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
             std::fprintf(stderr, "[fy] window %zu: gen %.3f-%.3f scan %.3f-%.3f ms\n", k, g0, g1, s0, s1);
         }
         for (auto e : tl) cudaEventDestroy(e);
-        unsigned long long hs[24];
+        unsigned long long hs[3 * kFyStats];
         ORQ_CUDA_CHECK(cudaMemcpy(hs, stats.p, sizeof(hs), cudaMemcpyDeviceToHost));
-        for (int g = 0; g < 3; g++)
+        for (int g = 0; g < 3; g++) {
+            const unsigned long long* h = hs + g * kFyStats;
             std::fprintf(stderr,
-                         "[fy] n=%zu perms=%zu windows=%llu group %d: steps %llu unc_steps %llu seq %llu "
-                         "entries %llu unc %llu cyc_load %llu cyc_unc %llu cyc_all %llu\n",
-                         n, count, w, g, hs[g * 8], hs[g * 8 + 1], hs[g * 8 + 2], hs[g * 8 + 3],
-                         hs[g * 8 + 4], hs[g * 8 + 5], hs[g * 8 + 6], hs[g * 8 + 7]);
+                         "[fy] n=%zu perms=%zu windows=%llu group %d: steps %llu unc_steps %llu entries %llu "
+                         "unc %llu cyc_load %llu cyc_list %llu cyc_unc %llu cyc_acc %llu cyc_all %llu\n",
+                         n, count, w, g, h[0], h[1], h[3], h[4], h[5], h[8], h[6], h[9], h[7]);
+        }
     }
 
     // finalize, a few permutations at a time to bound scratch
