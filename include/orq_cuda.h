@@ -158,14 +158,26 @@ int orqcu_apply_elementwise_perm(orqcu_runtime* rt, int x_arith, int x_width, si
 int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int bits,
                      int descending, void* const perm_out[3]);
 
+/* quicksort (quicksort.h:214-246): sorts the B-shared key (width 4 or 8) in
+ * the signed order, ascending or descending, and writes the A-shared int32
+ * sorting permutation to perm_out. The protocol of quicksort_body
+ * (quicksort.h:61-200): the padded rows are shuffled, then each round compares
+ * every non-pivot row with its segment's pivot (opened) and partitions every
+ * segment as the reference's Lomuto partition does, so the rounds, their
+ * compare sizes and the PRG use equal the reference's. Reserves 2
+ * permutations and 1 pair up front. Synchronous. */
+int orqcu_quicksort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int descending,
+                    void* const perm_out[3]);
 /* BSharedVector::_compare (circuits.h:231-295, bit_same at
  * b_shared_vector.h:164-178): eq = (x == y), gt = (x > y) in the signed order,
- * both as B-shared single bits (LSB of each share). width 4 or 8. One fused
- * launch: log2(8*width)+1 AND rounds on every pair and the packed sign fix-up. */
+ * both as B-shared single bits (LSB of each share). width 4, 8 or 16 (the
+ * padded int64 keys of the sorts). One fused launch: log2(8*width)+1 AND
+ * rounds on every pair and the packed sign fix-up. */
 int orqcu_compare_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
                     const void* const y[3], void* const eq[3], void* const gt[3]);
 /* BSharedVector::operator== (b_shared_vector.h:493-504): bit_same (log2(8W)
- * AND rounds, b_shared_vector.h:164-178) then mask(1); eq is a B-shared bit. */
+ * AND rounds, b_shared_vector.h:164-178) then mask(1); eq is a B-shared bit.
+ * width 4, 8 or 16. */
 int orqcu_equal_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
                   const void* const y[3], void* const eq[3]);
 /* not_b_1 (replicated_3pc.h:207), BSharedVector::operator!: every share

@@ -269,3 +269,16 @@ class Oracle:
                                        len(keys), self._flat(keys),
                                        (ctypes.c_int * len(keys))(*[int(d) for d in desc]),
                                        len(data_a), self._flat(data_a), len(data_b), self._flat(data_b))
+
+    def quicksort(self, key, payloads=(), desc=False):
+        """operators::quicksort of key (3 share arrays) in place; payloads
+        (A-shared, the key's width) are permuted in place. Returns the A-shared
+        permutation."""
+        kw = key[0].dtype.itemsize
+        n = len(key[0])
+        pay = [a for p in payloads for a in p]
+        pay_arr = (ctypes.c_void_p * max(1, len(pay)))(*[a.ctypes.data for a in pay])
+        perm = self.new(n, 4)
+        self.lib.oro_quicksort(ctypes.byref(self.ctx), kw, ctypes.c_size_t(n), self._ptrs(key), int(desc),
+                               len(payloads), pay_arr, self._ptrs(perm))
+        return perm

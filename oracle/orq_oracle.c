@@ -531,8 +531,10 @@ static void apply_elementwise(oro_ctx* c, pqueue* pq, int x_arith, int w, size_t
 /* radix_sort (operators/radixsort.h:116-229) with pad_input/remove_padding
  * (operators/sorting.h:405-495) and ElementwisePermutation::b2a/invert
  * (containers/permutation.h:205-258). */
-static void radix_sort_pq(oro_ctx* c, pqueue* pqp, int kw, size_t n, void* key[3], int bits,
-                          int desc, int npayload, void** payloads, int32_t* perm_out[3]);
+static void sort_pq(oro_ctx* c, pqueue* pqp, int proto, int kw, size_t n, void* key[3], int bits,
+                    int desc, int npayload, int payw, void** payloads, int32_t* perm_out[3]);
+#define radix_sort_pq(c, pqp, kw, n, key, bits, desc, np, pl, po) \
+    sort_pq(c, pqp, 0, kw, n, key, bits, desc, np, 8, pl, po)
 
 void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int desc,
                     int npayload, void** payloads, int32_t* perm_out[3]) {
@@ -542,9 +544,114 @@ void oro_radix_sort(oro_ctx* c, int kw, size_t n, void* key[3], int bits, int de
     free(pq.q);
 }
 
-/* radix_sort with the caller's PermutationManager queue */
-static void radix_sort_pq(oro_ctx* c, pqueue* pqp, int kw, size_t n, void* key[3], int bits,
-                          int desc, int npayload, void** payloads, int32_t* perm_out[3]) {
+/* quicksort (operators/quicksort.h:214-246): the same padding, permutation
+ * extraction and inversion as radix_sort around quicksort_body; payloads are
+ * kw-byte A-shared columns permuted with the result. */
+void oro_quicksort(oro_ctx* c, int kw, size_t n, void* key[3], int desc, int npayload,
+                   void** payloads, int32_t* perm_out[3]) {
+    pqueue pq = {0};
+    sort_pq(c, &pq, 1, kw, n, key, 0, desc, npayload, kw, payloads, perm_out);
+    while (pq.head < pq.tail) sperm_free(&pq.q[pq.head++]);
+    free(pq.q);
+}
+
+static void compare_pairs(oro_ctx* c, int w, size_t m, u128* const xa[3], u128* const ya[3],
+                          u128* eq[3], u128* gt[3]);
+
+/* partition (quicksort.h:28-49): Lomuto partition of rows [start, end] around
+ * the row at start, driven by the opened comparisons (0: row <= pivot) */
+static void qs_partition(int pw, void* P[3], const uint8_t* cmp, long start, long end, long* piv) {
+    long i = start;
+    for (long j = start + 1; j <= end; j++)
+        if (cmp[j] == 0) {
+            i++;
+            for (int k = 0; k < 3; k++) {
+                u128 a = ld(P[k], (size_t)j, pw), b = ld(P[k], (size_t)i, pw);
+                st(P[k], (size_t)j, pw, b);
+                st(P[k], (size_t)i, pw, a);
+            }
+        }
+    for (int k = 0; k < 3; k++) {
+        u128 a = ld(P[k], (size_t)start, pw), b = ld(P[k], (size_t)i, pw);
+        st(P[k], (size_t)start, pw, b);
+        st(P[k], (size_t)i, pw, a);
+    }
+    piv[i] = i;
+    if (i + 1 <= end) piv[i + 1] = i + 1;
+}
+
+/* quicksort_body (quicksort.h:61-200): shuffle, then rounds of comparing every
+ * non-pivot row with the pivot heading its segment (_compare, opened) and
+ * partitioning each segment, until every row is a pivot */
+static void quicksort_body(oro_ctx* c, pqueue* pq, int pw, size_t n, void* P[3]) {
+    sperm sp = pq_next(c, pq, n);
+    apply_sharded(c, 0, pw, n, P, &sp);
+    sperm_free(&sp);
+    if (n == 0) return;
+    long* piv = (long*)xalloc(n * sizeof(long));
+    uint8_t* cmp = (uint8_t*)xalloc(n);
+    for (size_t q = 0; q < n; q++) piv[q] = -1;
+    piv[0] = 0;
+    size_t num_pivots = 1;
+    u128 *R[3], *PV[3], *e[3], *g[3];
+    for (int j = 0; j < 3; j++) {
+        R[j] = (u128*)xalloc(n * 16 + 16);
+        PV[j] = (u128*)xalloc(n * 16 + 16);
+        e[j] = (u128*)xalloc(n * 16 + 16);
+        g[j] = (u128*)xalloc(n * 16 + 16);
+    }
+    for (;;) {
+        const size_t size = n - num_pivots;
+        long head = 0;
+        size_t k = 0;
+        for (size_t q = 0; q < n; q++) {
+            if (piv[q] >= 0) {
+                head = piv[q] > head ? piv[q] : head;
+                continue;
+            }
+            for (int j = 0; j < 3; j++) {
+                R[j][k] = ld(P[j], q, pw);
+                PV[j][k] = ld(P[j], (size_t)head, pw);
+            }
+            k++;
+        }
+        /* reduced._compare(pivot): gt = row > pivot */
+        compare_pairs(c, pw, size, R, PV, e, g);
+        k = 0;
+        for (size_t q = 0; q < n; q++)
+            if (piv[q] < 0) {
+                cmp[q] = (uint8_t)((g[0][k] ^ g[1][k] ^ g[2][k]) & 1);
+                k++;
+            }
+        long index = -1;
+        for (long p = 0; p < (long)n; p++) {
+            if (piv[p] < 0) continue;
+            if (p - index == 1) {
+                index++;
+                continue;
+            }
+            qs_partition(pw, P, cmp, index, p - 1, piv);
+            index = p;
+        }
+        qs_partition(pw, P, cmp, index, (long)n - 1, piv);
+        num_pivots = 0;
+        for (size_t q = 0; q < n; q++) num_pivots += piv[q] >= 0;
+        if (num_pivots >= n) break;
+    }
+    for (int j = 0; j < 3; j++) {
+        free(R[j]);
+        free(PV[j]);
+        free(e[j]);
+        free(g[j]);
+    }
+    free(piv);
+    free(cmp);
+}
+
+/* radix_sort (proto 0) or quicksort (proto 1) with the caller's
+ * PermutationManager queue */
+static void sort_pq(oro_ctx* c, pqueue* pqp, int proto, int kw, size_t n, void* key[3], int bits,
+                    int desc, int npayload, int payw, void** payloads, int32_t* perm_out[3]) {
 #define pq (*pqp)
     const int pw = (kw == 8) ? 16 : 8; /* PadWidth: int64 -> int128, else int64 */
     const int full_width = (kw * 8 == bits);
@@ -566,8 +673,13 @@ static void radix_sort_pq(oro_ctx* c, pqueue* pqp, int kw, size_t n, void* key[3
                 st(P[j], n - 1 - i, pw, a);
             }
 
-    /* radix_sort_body: reserve 1 permutation + (bits + 1) pairs */
-    pq_reserve(c, &pq, n, (size_t)bits + 2);
+    /* radix_sort_body: reserve 1 permutation + (bits + 1) pairs; quicksort:
+     * 2 permutations (shuffle, remove_padding) + 1 pair (invert) */
+    pq_reserve(c, &pq, n, proto ? 3 : (size_t)bits + 2);
+    if (proto) {
+        quicksort_body(c, &pq, pw, n, P);
+        bits = 0; /* no radix passes */
+    }
     int32_t* vp[3];
     int32_t* f1[3];
     int32_t* s[3];
@@ -671,7 +783,7 @@ static void radix_sort_pq(oro_ctx* c, pqueue* pqp, int kw, size_t n, void* key[3
             free(inv[j]);
         }
     }
-    for (int k = 0; k < npayload; k++) apply_elementwise(c, &pq, 1, 8, n, &payloads[3 * k], pm);
+    for (int k = 0; k < npayload; k++) apply_elementwise(c, &pq, 1, payw, n, &payloads[3 * k], pm);
     if (perm_out)
         for (int j = 0; j < 3; j++) memcpy(perm_out[j], pm[j], n * 4);
 

@@ -294,6 +294,38 @@ int main(int argc, char** argv) {
                 d.plain("open_key", o);
             }
         }
+    } else if (op == "qsort" || op == "qsort_desc" || op == "qsort32") {
+        // quicksort(key, order) then the permutation applied to two A-shared
+        // payloads of the key's type (int64 keys uniform in [0, 2^bits);
+        // int32 keys over all 32 bits; payloads u32)
+        uint64_t st = seed;
+        const auto order =
+            op == "qsort_desc" ? orq::operators::SortOrder::DESC : orq::operators::SortOrder::ASC;
+        auto run = [&](auto tag, uint64_t km) {
+            using T = decltype(tag);
+            auto key = gen<T>(n, st, km);
+            auto p1 = gen<T>(n, st, 0xffffffffull);
+            auto p2 = gen<T>(n, st, 0xffffffffull);
+            BSharedVector<T> kb = secret_share_b(key, 0);
+            ASharedVector<T> a1 = secret_share_a(p1, 0);
+            ASharedVector<T> a2 = secret_share_a(p2, 0);
+            t0 = std::chrono::steady_clock::now();
+            auto perm = orq::operators::quicksort(kb, order);
+            orq::operators::oblivious_apply_elementwise_perm(a1, perm);
+            orq::operators::oblivious_apply_elementwise_perm(a2, perm);
+            secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            d.shares("key", kb);
+            d.shares("pay1", a1);
+            d.shares("pay2", a2);
+            auto pa = perm.getASharedPerm();
+            d.shares("perm", pa);
+            auto ko = kb.open(), o1 = a1.open(), o2 = a2.open();
+            d.plain("open_key", ko);
+            d.plain("open_pay1", o1);
+            d.plain("open_pay2", o2);
+        };
+        if (op == "qsort32") run(int32_t{}, ~0ull);
+        else run(int64_t{}, bits >= 64 ? ~0ull : ((1ull << bits) - 1));
     } else if (op == "rows32" || op == "rows64") {
         // bitonic_sort over two key columns (k0 in [-4, 3], so rows tie on
         // it, ASC; k1 over all bits, DESC) with one B and two A data columns

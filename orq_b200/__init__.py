@@ -570,6 +570,16 @@ def bitonic_sort_batch(vectors, order=ASC, use_graph: bool = True):
                                            int(bool(use_graph))))
 
 
+def quicksort(v: BSharedVector, order: int = ASC) -> ElementwisePermutation:
+    """orq::operators::quicksort (quicksort.h:214-246): sorts v in place and
+    returns the A-shared sorting permutation."""
+    rt = v.rt
+    perm = rt._alloc(v.size(), 4)
+    _check(rt.lib.orqcu_quicksort(rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares),
+                                  int(order == DESC), _p3(perm)))
+    return ElementwisePermutation(rt, perm)
+
+
 def radix_sort(v: BSharedVector, order: int = ASC, bits: int | None = None) -> ElementwisePermutation:
     """orq::operators::radix_sort (radixsort.h:205-229): sorts v in place and
     returns the A-shared sorting permutation."""

@@ -361,11 +361,23 @@ int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key
     });
 }
 
+int orqcu_quicksort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int descending,
+                    void* const perm_out[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(key_width == 4 || key_width == 8, "quicksort keys must be int32 or int64");
+        need_sh((const void* const*)key, n, "null key");
+        need_sh((const void* const*)perm_out, n, "null perm_out");
+        orqcu::op_quicksort(rt->ctx, key_width, n, m3(key), descending != 0, m3(perm_out));
+        rt->ctx.check_device_error();
+    });
+}
+
 int orqcu_compare_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
                     const void* const y[3], void* const eq[3], void* const gt[3]) {
     return guard([&] {
         need_rt(rt);
-        need(width == 4 || width == 8, "compare supports 4 and 8-byte keys");
+        need(width == 4 || width == 8 || width == 16, "compare supports 4, 8 and 16-byte keys");
         need_sh(x, n, "null x");
         need_sh(y, n, "null y");
         need_sh((const void* const*)eq, n, "null eq");
@@ -514,7 +526,7 @@ int orqcu_equal_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3]
                   const void* const y[3], void* const eq[3]) {
     return guard([&] {
         need_rt(rt);
-        need(width == 4 || width == 8, "equality supports 4 and 8-byte keys");
+        need(width == 4 || width == 8 || width == 16, "equality supports 4, 8 and 16-byte keys");
         need_sh(x, n, "null x");
         need_sh(y, n, "null y");
         need_sh((const void* const*)eq, n, "null eq");

@@ -28,8 +28,14 @@ namespace {
 // memory, so one CTA runs per SM; the per-warp keystream buffers take the rest
 // (3 KiB per warp for int32 stages, 6.75 KiB for int64; 512 threads keep the
 // int32 tile within 128 registers a thread).
+// 16-byte shares (padded int64 keys) only run compares (MODE 1) and equality:
+// 256 threads keep 8 keystream calls of 128 words per warp within shared memory.
 template <int W>
-constexpr int cmp_threads() { return W == 4 ? 512 : 448; }
+constexpr int cmp_threads() { return W == 4 ? 512 : (W == 8 ? 448 : 256); }
+
+// bit_same rounds: log2 of the share's bit width
+template <int W>
+constexpr int cmp_levels() { return W == 4 ? 5 : (W == 8 ? 6 : 7); }
 
 template <typename T>
 struct CmpArgs {
@@ -48,8 +54,15 @@ struct CmpArgs {
 
 template <typename T>
 __device__ __forceinline__ T ashr(T v, int s) {
-    using S = typename std::make_signed<T>::type;
-    return (T)((S)v >> s);
+    if constexpr (sizeof(T) == 16) return (T)((__int128)v >> s);
+    else return (T)((typename std::make_signed<T>::type)v >> s);
+}
+
+// parity of the bits of v
+template <typename T>
+__device__ __forceinline__ int parity(T v) {
+    if constexpr (sizeof(T) == 16) return (__popcll((unsigned long long)v) ^ __popcll((unsigned long long)(v >> 64))) & 1;
+    else return __popcll((unsigned long long)v) & 1;
 }
 
 // binary and_b of one element for all three parties: z_p = r_p ^ x_p&y_p ^
@@ -69,7 +82,7 @@ __device__ __forceinline__ void and3(const T x[3], const T y[3], const T k[3], T
 // lev (kword(call, stream) is this thread's word of that call).
 template <typename T, typename KW>
 __device__ __forceinline__ void bit_same3(const T (&A)[3], const T (&Bv)[3], const KW& kword, T (&Sm)[3]) {
-    constexpr int L = (sizeof(T) == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<sizeof(T)>();
 #pragma unroll
     for (int j = 0; j < 3; j++) Sm[j] = ~(A[j] ^ Bv[j]);
 #pragma unroll
@@ -99,7 +112,7 @@ __device__ __forceinline__ void gt_bits3(const T (&A)[3], const T (&Bv)[3], cons
                                          uint32_t (*ballots)[3][3], T (&gt)[3]) {
     constexpr int W = sizeof(T);
     constexpr int B = 8 * W;
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     T G[3];
     {
         T Gi[3], K[3];
@@ -115,7 +128,7 @@ __device__ __forceinline__ void gt_bits3(const T (&A)[3], const T (&Bv)[3], cons
     for (int j = 0; j < 3; j++) {
         b1[j] = __ballot_sync(0xffffffffu, valid && ((A[j] >> (B - 1)) & 1));
         b2[j] = __ballot_sync(0xffffffffu, valid && ((Bv[j] >> (B - 1)) & 1));
-        br[j] = __ballot_sync(0xffffffffu, valid && (__popcll((unsigned long long)G[j]) & 1));
+        br[j] = __ballot_sync(0xffffffffu, valid && parity(G[j]));
     }
     T s1[3], s2[3], r[3];
     if constexpr (W == 4) {
@@ -126,7 +139,8 @@ __device__ __forceinline__ void gt_bits3(const T (&A)[3], const T (&Bv)[3], cons
             r[j] = br[j];
         }
     } else {
-        // two warps per 64-pair word
+        // W / 4 warps per packed word of 8W pairs
+        constexpr int WPW = W / 4;
         const int lane = threadIdx.x & 31;
         __syncthreads();
         if (lane == 0)
@@ -137,12 +151,16 @@ __device__ __forceinline__ void gt_bits3(const T (&A)[3], const T (&Bv)[3], cons
                 ballots[warp][2][j] = br[j];
             }
         __syncthreads();
-        const int w0 = warp & ~1;
+        const int w0 = warp & ~(WPW - 1);
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            s1[j] = (T)ballots[w0][0][j] | ((T)ballots[w0 + 1][0][j] << 32);
-            s2[j] = (T)ballots[w0][1][j] | ((T)ballots[w0 + 1][1][j] << 32);
-            r[j] = (T)ballots[w0][2][j] | ((T)ballots[w0 + 1][2][j] << 32);
+            s1[j] = s2[j] = r[j] = 0;
+#pragma unroll
+            for (int k = 0; k < WPW; k++) {
+                s1[j] |= (T)ballots[w0 + k][0][j] << (32 * k);
+                s2[j] |= (T)ballots[w0 + k][1][j] << (32 * k);
+                r[j] |= (T)ballots[w0 + k][2][j] << (32 * k);
+            }
         }
     }
     {
@@ -156,7 +174,8 @@ __device__ __forceinline__ void gt_bits3(const T (&A)[3], const T (&Bv)[3], cons
             ns2[j] = ~ss;
             nr[j] = ~rr;
             if constexpr (W == 4) K[j] = (T)kp[j][c & 3];
-            else K[j] = (T)kp[j][2 * (c & 1)] | ((T)kp[j][2 * (c & 1) + 1] << 32);
+            else if constexpr (W == 8) K[j] = (T)kp[j][2 * (c & 1)] | ((T)kp[j][2 * (c & 1) + 1] << 32);
+            else K[j] = (T)kp[j][0] | ((T)kp[j][1] << 32) | ((T)kp[j][2] << 64) | ((T)kp[j][3] << 96);
         }
         and3(ns2, nr, K, Z);
 #pragma unroll
@@ -176,7 +195,7 @@ __device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&
                                          uint32_t (*ksp)[3][4], uint32_t (*ballots)[3][3]) {
     constexpr int W = sizeof(T);
     constexpr int B = 8 * W;               // pairs per packed word
-    constexpr int L = (W == 4) ? 5 : 6;    // bit_same rounds
+    constexpr int L = cmp_levels<W>();     // bit_same rounds
     constexpr int NFULL = MODE == 0 ? L + 3 : (MODE == 1 ? L + 1 : L);
     constexpr int WORDS = 32 * W / 4;      // keystream words per call and stream per warp
     constexpr int NB = 32 * W / 16;        // AES blocks per call and stream per warp
@@ -240,7 +259,10 @@ __device__ __forceinline__ void cmp_tile(const CmpArgs<T>& a, const StreamArg (&
         auto kword = [&](int call, int q) -> T {
             const uint32_t* w = myks + (call * 3 + q) * WORDS;
             if constexpr (W == 4) return (T)w[lane];
-            else return (T)w[2 * lane] | ((T)w[2 * lane + 1] << 32);
+            else if constexpr (W == 8) return (T)w[2 * lane] | ((T)w[2 * lane + 1] << 32);
+            else
+                return (T)w[4 * lane] | ((T)w[4 * lane + 1] << 32) | ((T)w[4 * lane + 2] << 64) |
+                       ((T)w[4 * lane + 3] << 96);
         };
         T Sm[3];
         bit_same3(A, Bv, kword, Sm);
@@ -340,7 +362,7 @@ template <typename T>
 __global__ void __launch_bounds__(cmp_threads<sizeof(T)>(), 1) k_rows_cmp(RowsCmpArgs<T> a) {
     constexpr int W = sizeof(T);
     constexpr int B = 8 * W;
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     constexpr int NCALL = L + 3;
     constexpr int WORDS = 32 * W / 4;
     constexpr int NB = 32 * W / 16;
@@ -635,7 +657,7 @@ constexpr int batch_max_threads() { return W == 4 ? 512 : 448; }
 template <typename T>
 __global__ void __launch_bounds__(batch_max_threads<sizeof(T)>(), 1) k_cmp_batch(CmpBatchArgs<T> ba) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     constexpr int kCmpThreads = batch_max_threads<W>();
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t ksp[kCmpThreads / 32][3][4];
@@ -664,13 +686,14 @@ __global__ void __launch_bounds__(batch_max_threads<sizeof(T)>(), 1) k_cmp_batch
 template <typename T, int MODE>
 void launch_cmp(Ctx& c, const CmpArgs<T>& a, const char* name) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     constexpr int NFULL = MODE == 0 ? L + 3 : (MODE == 1 ? L + 1 : L);
     constexpr int kCmpThreads = cmp_threads<W>();
     // spread small stages over every SM: threads per CTA a multiple of 64
     // (whole packed words for both widths) up to the maximum
     const unsigned long long per_sm = ceil_div(a.m, (unsigned long long)c.num_sms);
-    const int nt = (int)std::min<unsigned long long>(kCmpThreads, std::max<unsigned long long>(64, ceil_div(per_sm, 64) * 64));
+    constexpr unsigned long long G = W == 16 ? 128 : 64;  // threads of whole packed words
+    const int nt = (int)std::min<unsigned long long>(kCmpThreads, std::max<unsigned long long>(G, ceil_div(per_sm, G) * G));
     const size_t ks_bytes = (size_t)(nt / 32) * NFULL * 3 * (32 * W / 4) * 4;
     const size_t smem = kAesSmemBytes + ks_bytes;
     const size_t smem_max = kAesSmemBytes + (size_t)(kCmpThreads / 32) * NFULL * 3 * (32 * W / 4) * 4;
@@ -689,7 +712,7 @@ void launch_cmp(Ctx& c, const CmpArgs<T>& a, const char* name) {
 template <typename T>
 void compare_t(Ctx& c, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     CmpArgs<T> a{};
     for (int j = 0; j < 3; j++) {
         a.x[j] = (const T*)x.p[j];
@@ -708,7 +731,7 @@ void compare_t(Ctx& c, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt) {
 template <typename T>
 void equal_t(Ctx& c, size_t n, CSh3 x, CSh3 y, Sh3 eq) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     CmpArgs<T> a{};
     for (int j = 0; j < 3; j++) {
         a.x[j] = (const T*)x.p[j];
@@ -734,7 +757,7 @@ __global__ void k_not1(CSh3 x, Sh3 y, unsigned long long n) {
 template <typename T>
 void bitonic_t(Ctx& c, size_t n, Sh3 key, bool desc) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     int rounds = 0;
     while (((size_t)1 << rounds) < n) rounds++;
     const size_t m = n / 2;
@@ -767,7 +790,7 @@ template <typename T>
 void build_items(Ctx& c, int count, const size_t* n, const Sh3* keys, const int* desc,
                  std::vector<CmpBatchItem>& items, unsigned long long advance[1], int& rounds) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     items.resize(count);
     unsigned long long off = 0;
     rounds = 0;
@@ -807,7 +830,7 @@ void build_work(const std::vector<CmpBatchItem>& items, int rounds, int nt, std:
 template <typename T>
 size_t batch_smem(int nt) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     return kAesSmemBytes + (size_t)(nt / 32) * (L + 3) * 3 * (32 * W / 4) * 4;
 }
 
@@ -989,14 +1012,14 @@ void bitonic_batch_t(Ctx& c, int count, const size_t* n, const Sh3* keys, const 
 // nonces of one compare_rows over nkeys keys (each call of m pairs)
 template <int W>
 unsigned long long rows_cmp_nonces(int nkeys, unsigned long long C, unsigned long long Cp) {
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     return (unsigned long long)nkeys * ((L + 1) * C + Cp) + 2ull * (nkeys - 1) * C;
 }
 
 template <typename T>
 void launch_rows_cmp(Ctx& c, const RowsCmpArgs<T>& a) {
     constexpr int W = sizeof(T);
-    constexpr int L = (W == 4) ? 5 : 6;
+    constexpr int L = cmp_levels<W>();
     constexpr int kThreads = cmp_threads<W>();
     const unsigned long long per_sm = ceil_div(a.m, (unsigned long long)c.num_sms);
     const int nt = (int)std::min<unsigned long long>(kThreads, std::max<unsigned long long>(64, ceil_div(per_sm, 64) * 64));
@@ -1172,13 +1195,15 @@ void op_bitonic_sort_rows(Ctx& c, int w, size_t n, int nkeys, const Sh3* keys, c
 void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt) {
     if (w == 4) compare_t<uint32_t>(c, n, x, y, eq, gt);
     else if (w == 8) compare_t<unsigned long long>(c, n, x, y, eq, gt);
-    else throw std::invalid_argument("compare supports int32 and int64 keys");
+    else if (w == 16) compare_t<unsigned __int128>(c, n, x, y, eq, gt);
+    else throw std::invalid_argument("compare supports 4, 8 and 16-byte keys");
 }
 
 void op_equal(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq) {
     if (w == 4) equal_t<uint32_t>(c, n, x, y, eq);
     else if (w == 8) equal_t<unsigned long long>(c, n, x, y, eq);
-    else throw std::invalid_argument("equality supports int32 and int64 keys");
+    else if (w == 16) equal_t<unsigned __int128>(c, n, x, y, eq);
+    else throw std::invalid_argument("equality supports 4, 8 and 16-byte keys");
 }
 
 void op_not1(Ctx& c, int w, size_t n, CSh3 x, Sh3 y) {

@@ -10,6 +10,7 @@
 //   3. k_radix_perm  t = s0 + f1 * (s1 - s0)  (multiply_a + add_a)      (1 pass)
 //   4. op_apply_elementwise(padded, t)        (3 passes, one per group)
 #include <algorithm>
+#include <functional>
 #include <numeric>
 #include <vector>
 
@@ -271,15 +272,17 @@ __global__ void k_minus_one(Sh3 m, unsigned long long n) {
 
 }  // namespace
 
-void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out) {
-    if (kw != 4 && kw != 8) throw std::invalid_argument("radix sort keys must be int32 or int64");
-    if (bits < 1 || bits > kw * 8) throw std::invalid_argument("bits out of range");
-    if (n >= (1ull << 31)) throw std::invalid_argument("radix sort supports n < 2^31");
+// The frame both sort protocols share (radix_sort, radixsort.h:205-229, and
+// quicksort, quicksort.h:214-246): pad_input, the protocol's body on the
+// padded rows, remove_padding (permutation b2a, negate for descending order)
+// and invert. `reserve` is the number of permutations the body and the frame
+// take from the PermutationManager queue, reserved up front.
+void sort_padded(Ctx& c, int kw, size_t n, Sh3 key, bool desc, Sh3 perm_out, size_t reserve,
+                 const std::function<void(Sh3 P, int PW)>& body) {
+    if (kw != 4 && kw != 8) throw std::invalid_argument("sort keys must be int32 or int64");
+    if (n >= (1ull << 31)) throw std::invalid_argument("sorts support n < 2^31");
     const int PW = kw == 8 ? 16 : 8;
-    const bool full_width = (kw * 8 == bits);
-
-    // radix_sort_body: 1 permutation for remove_padding + (bits + 1) pairs
-    reserve_perms(c, n, (size_t)bits + 2);
+    reserve_perms(c, n, reserve);
 
     Scratch Pbuf(c, 3 * std::max<size_t>(n, 1) * PW);
     Sh3 P;
@@ -292,73 +295,8 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
         ORQ_CUDA_CHECK(cudaGetLastError());
         c.kernels_launched++;
     }
-
+    body(P, PW);
     const size_t n1 = std::max<size_t>(n, 1);
-    Scratch f1b(c, 3 * n1 * 4), scb(c, 3 * 2 * n1 * 4), tb(c, 3 * n1 * 4);
-    const uint32_t tiles = (uint32_t)ceil_div(2 * n1, kScanTile);
-    Scratch tsb(c, 3 * (size_t)tiles * 4);
-    uint32_t* f1[3];
-    uint32_t* sc[3];
-    uint32_t* t[3];
-    for (int j = 0; j < 3; j++) {
-        f1[j] = f1b.as<uint32_t>() + j * n1;
-        sc[j] = scb.as<uint32_t>() + j * 2 * n1;
-        t[j] = tb.as<uint32_t>() + j * n1;
-    }
-    const unsigned long long ch4 = chunks_of((unsigned long long)n * 4);
-
-    for (int b = 0; b < bits; b++) {
-        if (n) {
-            RadixB2AArgs ba;
-            for (int j = 0; j < 3; j++) {
-                ba.P[j] = P.p[j];
-                ba.f1[j] = f1[j];
-                ba.pair[j] = c.stream_arg(PAIR0 + j);
-            }
-            ba.chunks = ch4;
-            ba.n = n;
-            ba.shift = 32 + b;
-            ba.invert = (full_width && b == bits - 1) ? 1u : 0u;
-            const double by = 24.0 * n, bl = 9.0 * ceil_div(n, 4);
-            if (PW == 16) launch_aes(c, "radix_bit_b2a", by, bl, k_radix_b2a<16>, ceil_div(n, 4), ba);
-            else launch_aes(c, "radix_bit_b2a", by, bl, k_radix_b2a<8>, ceil_div(n, 4), ba);
-        }
-        for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += 3 * ch4;
-
-        if (n) {
-            ScanArgs sa;
-            for (int j = 0; j < 3; j++) {
-                sa.f1[j] = f1[j];
-                sa.sc[j] = sc[j];
-            }
-            sa.tsum = tsb.as<uint32_t>();
-            sa.n = n;
-            sa.tiles = tiles;
-            const dim3 grid(std::min<uint32_t>(tiles, (uint32_t)c.num_sms * 8), 3);
-            {
-                ProfScope ps(c, "radix_scan", 72.0 * n);
-                k_scan_up<<<grid, 256, 0, c.stream>>>(sa);
-                k_scan_mid<<<3, 1024, 0, c.stream>>>(sa);
-                k_scan_down<<<grid, 256, 0, c.stream>>>(sa);
-            }
-            ORQ_CUDA_CHECK(cudaGetLastError());
-            c.kernels_launched += 3;
-
-            PermMulArgs pa;
-            for (int j = 0; j < 3; j++) {
-                pa.f1[j] = f1[j];
-                pa.sc[j] = sc[j];
-                pa.t[j] = t[j];
-                pa.pair[j] = c.stream_arg(PAIR0 + j);
-            }
-            pa.n = n;
-            launch_aes(c, "radix_perm_mul", 48.0 * n, 3.0 * ceil_div(n, 4), k_radix_perm, ceil_div(n, 4), pa);
-        }
-        for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += ch4;
-
-        CSh3 tp{{t[0], t[1], t[2]}};
-        op_apply_elementwise(c, false, PW, n, P, tp);
-    }
 
     // remove_padding: permutation = low 32 bits (B-shared), key = padded >> 32
     Scratch pm(c, 3 * n1 * 4);
@@ -420,6 +358,81 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
             if (n)
                 ORQ_CUDA_CHECK(cudaMemcpyAsync(perm_out.p[j], I.p[j], n * 4, cudaMemcpyDeviceToDevice, c.stream));
     }
+}
+
+void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out) {
+    if (kw != 4 && kw != 8) throw std::invalid_argument("radix sort keys must be int32 or int64");
+    if (bits < 1 || bits > kw * 8) throw std::invalid_argument("bits out of range");
+    const bool full_width = (kw * 8 == bits);
+    // radix_sort_body: 1 permutation for remove_padding + (bits + 1) pairs
+    sort_padded(c, kw, n, key, desc, perm_out, (size_t)bits + 2, [&](Sh3 P, int PW) {
+        const size_t n1 = std::max<size_t>(n, 1);
+        Scratch f1b(c, 3 * n1 * 4), scb(c, 3 * 2 * n1 * 4), tb(c, 3 * n1 * 4);
+        const uint32_t tiles = (uint32_t)ceil_div(2 * n1, kScanTile);
+        Scratch tsb(c, 3 * (size_t)tiles * 4);
+        uint32_t* f1[3];
+        uint32_t* sc[3];
+        uint32_t* t[3];
+        for (int j = 0; j < 3; j++) {
+            f1[j] = f1b.as<uint32_t>() + j * n1;
+            sc[j] = scb.as<uint32_t>() + j * 2 * n1;
+            t[j] = tb.as<uint32_t>() + j * n1;
+        }
+        const unsigned long long ch4 = chunks_of((unsigned long long)n * 4);
+
+        for (int b = 0; b < bits; b++) {
+            if (n) {
+                RadixB2AArgs ba;
+                for (int j = 0; j < 3; j++) {
+                    ba.P[j] = P.p[j];
+                    ba.f1[j] = f1[j];
+                    ba.pair[j] = c.stream_arg(PAIR0 + j);
+                }
+                ba.chunks = ch4;
+                ba.n = n;
+                ba.shift = 32 + b;
+                ba.invert = (full_width && b == bits - 1) ? 1u : 0u;
+                const double by = 24.0 * n, bl = 9.0 * ceil_div(n, 4);
+                if (PW == 16) launch_aes(c, "radix_bit_b2a", by, bl, k_radix_b2a<16>, ceil_div(n, 4), ba);
+                else launch_aes(c, "radix_bit_b2a", by, bl, k_radix_b2a<8>, ceil_div(n, 4), ba);
+            }
+            for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += 3 * ch4;
+
+            if (n) {
+                ScanArgs sa;
+                for (int j = 0; j < 3; j++) {
+                    sa.f1[j] = f1[j];
+                    sa.sc[j] = sc[j];
+                }
+                sa.tsum = tsb.as<uint32_t>();
+                sa.n = n;
+                sa.tiles = tiles;
+                const dim3 grid(std::min<uint32_t>(tiles, (uint32_t)c.num_sms * 8), 3);
+                {
+                    ProfScope ps(c, "radix_scan", 72.0 * n);
+                    k_scan_up<<<grid, 256, 0, c.stream>>>(sa);
+                    k_scan_mid<<<3, 1024, 0, c.stream>>>(sa);
+                    k_scan_down<<<grid, 256, 0, c.stream>>>(sa);
+                }
+                ORQ_CUDA_CHECK(cudaGetLastError());
+                c.kernels_launched += 3;
+
+                PermMulArgs pa;
+                for (int j = 0; j < 3; j++) {
+                    pa.f1[j] = f1[j];
+                    pa.sc[j] = sc[j];
+                    pa.t[j] = t[j];
+                    pa.pair[j] = c.stream_arg(PAIR0 + j);
+                }
+                pa.n = n;
+                launch_aes(c, "radix_perm_mul", 48.0 * n, 3.0 * ceil_div(n, 4), k_radix_perm, ceil_div(n, 4), pa);
+            }
+            for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += ch4;
+
+            CSh3 tp{{t[0], t[1], t[2]}};
+            op_apply_elementwise(c, false, PW, n, P, tp);
+        }
+    });
 }
 
 }  // namespace orqcu

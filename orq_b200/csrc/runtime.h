@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <deque>
 #include <map>
 #include <string>
@@ -216,6 +217,11 @@ void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt);
 void op_bitonic_sort(Ctx& c, int w, size_t n, Sh3 key, bool desc);
 void op_equal(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq);
 void op_not1(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
+// pad_input -> body(padded rows, padded width) -> remove_padding -> invert;
+// reserves `reserve` permutations first (radix sort and quicksort share it)
+void sort_padded(Ctx& c, int kw, size_t n, Sh3 key, bool desc, Sh3 perm_out, size_t reserve,
+                 const std::function<void(Sh3 P, int PW)>& body);
+void op_quicksort(Ctx& c, int kw, size_t n, Sh3 key, bool desc, Sh3 perm_out);
 void op_compare_rows(Ctx& c, int w, size_t n, int nkeys, const CSh3* x, const CSh3* y, const int* desc, Sh3 gt);
 void op_swap(Ctx& c, int w, size_t n, bool arith, int ncols, const Sh3* x, const Sh3* y, CSh3 bits);
 void op_extend_lsb(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);

@@ -68,6 +68,12 @@ CASES = [
     ("cmprows32_n500", "cmprows32", 500, 7, 2, 32, True),
     ("cmprows64_n333", "cmprows64", 333, 8, 3, 64, True),
     ("cmprows64_n20000", "cmprows64", 20000, 9, 4, 64, False),
+    ("qsort_n1000_b40", "qsort", 1000, 7, 3, 40, True),
+    ("qsort_desc_n333_b64", "qsort_desc", 333, 8, 4, 64, True),
+    ("qsort32_n500", "qsort32", 500, 9, 5, 32, True),
+    ("qsort_n2_b40", "qsort", 2, 5, 2, 40, True),
+    ("qsort_n20000_b40", "qsort", 20000, 10, 6, 40, False),
+    ("qsort32_n30000", "qsort32", 30000, 11, 7, 32, False),
 ]
 
 

@@ -69,6 +69,9 @@ class OracleBackend:
     def bitonic(self, key, desc):
         self.o.bitonic_sort(key, desc)
 
+    def qsort(self, key, payloads, desc=False):
+        return self.o.quicksort(key, payloads, desc)
+
     def bitonic_rows(self, keys, desc, data_a, data_b):
         self.o.bitonic_sort_rows(keys, desc, data_a, data_b)
 
@@ -156,6 +159,12 @@ class GpuBackend:
     def bitonic(self, key, desc):
         self.orq.bitonic_sort(key, self.orq.DESC if desc else self.orq.ASC)
 
+    def qsort(self, key, payloads, desc=False):
+        perm = self.orq.quicksort(key, self.orq.DESC if desc else self.orq.ASC)
+        for p in payloads:
+            self.orq.oblivious_apply_elementwise_perm(p, perm)
+        return perm
+
     def bitonic_rows(self, keys, desc, data_a, data_b):
         o = self.orq
         o.bitonic_sort(keys, data_a, data_b, [o.DESC if d else o.ASC for d in desc])
@@ -225,6 +234,30 @@ def replay_radix(be, n, seed, bits, desc=False):
     a1 = be.share(p1, True, 0)
     a2 = be.share(p2, True, 0)
     perm = be.radix(kb, bits, [a1, a2], desc)
+    out = {"key": be.np(kb), "pay1": be.np(a1), "pay2": be.np(a2), "perm": be.np(perm)}
+    out["open_key"] = be.open(kb, False)[None]
+    out["open_pay1"] = be.open(a1, True)[None]
+    out["open_pay2"] = be.open(a2, True)[None]
+    return out, (key, p1, p2)
+
+
+def qsort_inputs(n, seed, bits, w):
+    """Inputs of the "qsort"/"qsort_desc" (int64) and "qsort32" ops."""
+    st = splitmix64_fast(seed, 3 * n)
+    if w == 4:
+        m32 = np.uint64(0xFFFFFFFF)
+        return st[:n].astype(np.uint32), (st[n:2 * n] & m32).astype(np.uint32), (st[2 * n:] & m32).astype(np.uint32)
+    return radix_inputs(n, seed, bits)
+
+
+def replay_qsort(be, n, seed, bits, w=8, desc=False):
+    """The quicksort ops of ref_driver.cpp: quicksort(key, order) then the
+    permutation applied to two A-shared payloads of the key's width."""
+    key, p1, p2 = qsort_inputs(n, seed, bits, w)
+    kb = be.share(key, False, 0)
+    a1 = be.share(p1, True, 0)
+    a2 = be.share(p2, True, 0)
+    perm = be.qsort(kb, [a1, a2], desc)
     out = {"key": be.np(kb), "pay1": be.np(a1), "pay2": be.np(a2), "perm": be.np(perm)}
     out["open_key"] = be.open(kb, False)[None]
     out["open_pay1"] = be.open(a1, True)[None]

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from replay import (OracleBackend, replay_agg, replay_bitonic, replay_cmprows, replay_compare,
-                    replay_prims, replay_radix, replay_relops, replay_rows, replay_tsort, same)
+                    replay_prims, replay_qsort, replay_radix, replay_relops, replay_rows, replay_tsort, same)
 
 
 def sha(a):
@@ -278,5 +278,30 @@ def test_compare_rows_large_matches_reference_digests(oracle_lib, digests):
     d = digests["cmprows64_n20000"]
     m = d["meta"]
     out, _ = replay_cmprows(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 8)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag,w,desc", [("qsort_n1000_b40", 8, False), ("qsort_desc_n333_b64", 8, True),
+                                        ("qsort32_n500", 4, False), ("qsort_n2_b40", 8, False)])
+def test_quicksort_matches_reference_shares(oracle_lib, golden, digests, tag, w, desc):
+    """quicksort (quicksort.h:61-246): shuffle, opened pivot comparisons,
+    Lomuto partitions, remove_padding and invert, share for share"""
+    m = digests[tag]["meta"]
+    out, (key, p1, p2) = replay_qsort(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], w, desc)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    sd = {4: np.int32, 8: np.int64}[w]
+    k = key.view(sd)
+    o = np.argsort(-k if desc else k, kind="stable")
+    assert np.array_equal(out["open_key"][0].view(sd), k[o])
+    assert np.array_equal(out["open_pay1"][0].view(p1.dtype), p1[o])
+
+
+@pytest.mark.parametrize("tag,w", [("qsort_n20000_b40", 8), ("qsort32_n30000", 4)])
+def test_quicksort_large_matches_reference_digests(oracle_lib, digests, tag, w):
+    d = digests[tag]
+    m = d["meta"]
+    out, _ = replay_qsort(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], w)
     for name, arr in out.items():
         assert [sha(a) for a in arr] == d["arrays"][name], name

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from replay import (GpuBackend, OracleBackend, radix_inputs, replay_agg, replay_bitonic,
-                    replay_cmprows, replay_compare, replay_join, replay_prims, replay_relops, replay_radix,
+                    replay_cmprows, replay_compare, replay_join, replay_prims, replay_qsort, replay_relops, replay_radix,
                     replay_rows, replay_tsort, same)
 
 pytestmark = pytest.mark.gpu
@@ -569,3 +569,43 @@ def test_rows_errors(orq):
         orq.swap([a], [a], bits)
     with pytest.raises(orq.OrqError):  # more than 8 keys
         orq.compare_rows([a] * 9, [b] * 9, [orq.ASC] * 9)
+
+
+@pytest.mark.parametrize("tag,w,desc", [("qsort_n1000_b40", 8, False), ("qsort_desc_n333_b64", 8, True),
+                                        ("qsort32_n500", 4, False), ("qsort_n2_b40", 8, False)])
+def test_quicksort_matches_reference_shares(orq, golden, digests, tag, w, desc):
+    """quicksort: shuffle, rounds of opened pivot compares (16-byte padded keys
+    for int64) and Lomuto partitions, remove_padding, invert; share for share"""
+    m = digests[tag]["meta"]
+    out, _ = replay_qsort(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], w, desc)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+@pytest.mark.parametrize("tag,w", [("qsort_n20000_b40", 8), ("qsort32_n30000", 4)])
+def test_quicksort_large_matches_reference_digests(orq, digests, tag, w):
+    d = digests[tag]
+    m = d["meta"]
+    out, _ = replay_qsort(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], w)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("w,desc,n", [(8, False, 1), (8, True, 3), (4, True, 4097), (8, False, 70000)])
+def test_quicksort_matches_restatement(orq, w, desc, n):
+    gpu, _ = replay_qsort(GpuBackend(23), n, 4, 40, w, desc)
+    cpu, _ = replay_qsort(OracleBackend(23), n, 4, 40, w, desc)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), k
+
+
+def test_quicksort_full_size_properties(orq):
+    """2^20 int64 keys over all 64 bits with many duplicates: opened keys sorted
+    (signed order), payloads carried, permutation a bijection"""
+    n = 1 << 20
+    out, (key, p1, p2) = replay_qsort(GpuBackend(5), n, 12, 64, 8)
+    k = key.view(np.int64)
+    o = np.argsort(k, kind="stable")
+    assert np.array_equal(out["open_key"][0].view(np.int64), k[o])
+    assert np.array_equal(out["open_pay1"][0].view(np.uint64), p1[o])
+    assert np.array_equal(out["open_pay2"][0].view(np.uint64), p2[o])
