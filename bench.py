@@ -156,9 +156,12 @@ class RadixWorkload:
         self.kb.shares.copy_(self.orig[0])
         self.a1.shares.copy_(self.orig[1])
         self.a2.shares.copy_(self.orig[2])
-        perm = orq.radix_sort(self.kb, orq.ASC, self.bits)
+        perm = self.sort(self.kb)
         orq.oblivious_apply_elementwise_perm(self.a1, perm)
         orq.oblivious_apply_elementwise_perm(self.a2, perm)
+
+    def sort(self, kb):
+        return self.orq.radix_sort(kb, self.orq.ASC, self.bits)
 
     def check(self):
         np = self.np
@@ -181,7 +184,7 @@ class RadixWorkload:
         k = rt.secret_share_b(self.dbuf[0], 0)
         x1 = rt.secret_share_a(self.dbuf[1], 0)
         x2 = rt.secret_share_a(self.dbuf[2], 0)
-        perm = orq.radix_sort(k, orq.ASC, self.bits)
+        perm = self.sort(k)
         orq.oblivious_apply_elementwise_perm(x1, perm)
         orq.oblivious_apply_elementwise_perm(x2, perm)
         for v, o in zip((k, x1, x2), self.outs):
@@ -194,6 +197,27 @@ class RadixWorkload:
         sec = run_ref_seconds("radix_time", sample, 7, self.bits, threads)
         return sample / sec, sec, (f"n={sample} rows of the same distributions (bounded sample of the 2^22 "
                               f"workload), ORQ's own radix_sort + 2 payload applies, 3 party processes x "
+                              f"{threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
+
+
+class QuicksortWorkload(RadixWorkload):
+    """The headline's rows (2^22 int64 keys uniform in [0, 2^40) + two payload
+    applies) sorted by quicksort, the reference's default sort protocol."""
+
+    name = "qsort"
+
+    def __init__(self, args, seed):
+        super().__init__(args, seed)
+        self.config["workload"] = WORKLOAD.replace("shuffle-based radix sort", "quicksort (shuffle + opened "
+                                                   "pivot compares)")
+
+    def sort(self, kb):
+        return self.orq.quicksort(kb, self.orq.ASC)
+
+    def cpu_reference(self, sample, threads):
+        sec = run_ref_seconds("qsort_time", sample, 7, self.bits, threads)
+        return sample / sec, sec, (f"n={sample} rows of the same distributions (bounded sample of the 2^22 "
+                              f"workload), ORQ's own quicksort + 2 payload applies, 3 party processes x "
                               f"{threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
 
 
@@ -566,7 +590,8 @@ class ServeReference:
                                  f"{threads} worker threads")
 
 
-WORKLOADS = {"radix": RadixWorkload, "bitonic": BitonicWorkload, "join": JoinWorkload}
+WORKLOADS = {"radix": RadixWorkload, "qsort": QuicksortWorkload, "bitonic": BitonicWorkload,
+             "join": JoinWorkload}
 
 
 def run_orq(args, rank, world, local_rank):

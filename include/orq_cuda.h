@@ -247,15 +247,18 @@ int orqcu_aggregate(orqcu_runtime* rt, int width, size_t n, int nkeys, const voi
  * rho's). sigma is consumed (left shuffled). Synchronous. */
 int orqcu_compose_permutations(orqcu_runtime* rt, size_t n, void* const sigma[3],
                                void* const rho[3]);
-/* table_sort (sorting.h:509-612) with SortingProtocol::RADIXSORT over n rows
- * of width-byte columns (4 or 8): ncols B-shared key columns (cols[3*k+p]),
- * each ascending or descending and sorted on 1 bit (single_bit, e.g. valid
- * and table-id columns) or on its full width; na A-shared and nb B-shared
- * data columns are permuted along. Reserves its permutations up front like
- * the reference. Synchronous. */
+/* SortingProtocol (sorting.h:15-21), in the reference's order. */
+enum { ORQCU_SORT_BITONIC = 0, ORQCU_SORT_QUICK = 1, ORQCU_SORT_RADIX = 2 };
+/* table_sort (sorting.h:509-612) over n rows of width-byte columns (4 or 8):
+ * ncols B-shared key columns (cols[3*k+p]), each ascending or descending and
+ * sorted on 1 bit (single_bit, e.g. valid and table-id columns, by a 1-bit
+ * radix sort) or on its full width by the protocol (ORQCU_SORT_QUICK or
+ * ORQCU_SORT_RADIX; others are "Unknown table sort protocol"); na A-shared and
+ * nb B-shared data columns are permuted along. Reserves its permutations up
+ * front like the reference. Synchronous. */
 int orqcu_table_sort(orqcu_runtime* rt, int width, size_t n, int ncols, void* const* cols,
                      const int* descending, const int* single_bit, int na, void* const* data_a,
-                     int nb, void* const* data_b);
+                     int nb, void* const* data_b, int protocol);
 /* distinct (distinct.h:20-53): res[0] = 1 and res[i] = 1 where row i differs
  * from row i-1 in any of the nkeys B-shared key columns (keys[3*k+p]); one
  * fused launch. */

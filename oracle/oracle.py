@@ -199,15 +199,16 @@ class Oracle:
                                           self._ptrs(sigma), self._ptrs(rho))
         return rho
 
-    def table_sort(self, cols, desc, single_bit, data_a=(), data_b=()):
-        """operators::table_sort (radix protocol); every column sorted in place."""
+    def table_sort(self, cols, desc, single_bit, data_a=(), data_b=(), quick=False):
+        """operators::table_sort (radix or quicksort protocol); every column
+        sorted in place."""
         w = cols[0][0].dtype.itemsize
         flat = lambda arrs: (ctypes.c_void_p * max(1, 3 * len(arrs)))(
             *[x.ctypes.data for a in arrs for x in a])
         self.lib.oro_table_sort(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(cols[0][0])), len(cols),
                                 flat(cols), (ctypes.c_int * len(cols))(*[int(d) for d in desc]),
                                 (ctypes.c_int * len(cols))(*[int(b) for b in single_bit]),
-                                len(data_a), flat(data_a), len(data_b), flat(data_b))
+                                len(data_a), flat(data_a), len(data_b), flat(data_b), int(quick))
 
     def distinct(self, keys):
         w = keys[0][0].dtype.itemsize

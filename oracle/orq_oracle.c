@@ -1296,14 +1296,22 @@ void oro_compose_permutations(oro_ctx* c, size_t n, int32_t* sigma[3], int32_t* 
  * earlier column after applying the running permutation to it, composing the
  * permutations; finally apply the total permutation to the key columns, the
  * arithmetic data columns and the boolean data columns, in that order. */
+/* sort_sub (sorting.h:565-576): single-bit columns by a 1-bit radix sort,
+ * the rest by quicksort (quick) or a full-width radix sort */
+static void table_sort_sub(oro_ctx* c, pqueue* pq, int quick, int w, size_t n, void* col[3], int single,
+                           int desc, int32_t* perm[3]) {
+    if (single || !quick) radix_sort_pq(c, pq, w, n, col, single ? 1 : 8 * w, desc, 0, NULL, perm);
+    else sort_pq(c, pq, 1, w, n, col, 0, desc, 0, w, NULL, perm);
+}
+
 void oro_table_sort(oro_ctx* c, int w, size_t n, int ncols, void* const* cols, const int* desc,
                     const int* single_bit, int na, void* const* data_a, int nb,
-                    void* const* data_b) {
+                    void* const* data_b, int quick) {
     int ns = 0;
     for (int k = 0; k < ncols; k++) ns += single_bit[k] != 0;
     const int nk = ncols - ns, nc = na + nb, L = 8 * w;
-    const size_t perms = (size_t)(nk + ns - 1) + (size_t)(nk + ns);
-    const size_t pairs = (size_t)(4 * ns + 3 * nk + nc - 1) + (size_t)nk * L;
+    const size_t perms = (size_t)(nk + ns - 1) + (size_t)(nk + ns) + (quick ? (size_t)nk : 0);
+    const size_t pairs = (size_t)(4 * ns + 3 * nk + nc - 1) + (quick ? 0 : (size_t)nk * L);
     pqueue pq = {0};
     pq_reserve(c, &pq, n, perms + pairs);
     void* orig[3];
@@ -1318,14 +1326,14 @@ void oro_table_sort(oro_ctx* c, int w, size_t n, int ncols, void* const* cols, c
     {
         void* col[3] = {cols[3 * C], cols[3 * C + 1], cols[3 * C + 2]};
         copy3(orig, col, n, w);
-        radix_sort_pq(c, &pq, w, n, col, single_bit[C] ? 1 : L, desc[C], 0, NULL, sp);
+        table_sort_sub(c, &pq, quick, w, n, col, single_bit[C], desc[C], sp);
         copy3(col, orig, n, w);
     }
     for (C--; C >= 0; C--) {
         void* col[3] = {cols[3 * C], cols[3 * C + 1], cols[3 * C + 2]};
         copy3(orig, col, n, w);
         apply_elementwise(c, &pq, 0, w, n, col, sp);
-        radix_sort_pq(c, &pq, w, n, col, single_bit[C] ? 1 : L, desc[C], 0, NULL, np_);
+        table_sort_sub(c, &pq, quick, w, n, col, single_bit[C], desc[C], np_);
         copy3(col, orig, n, w);
         compose_pq(c, &pq, n, sp, np_);
         for (int j = 0; j < 3; j++) {

@@ -125,7 +125,7 @@ void oro_compose_permutations(oro_ctx* c, size_t n, int32_t* sigma[3], int32_t* 
  * na arithmetic and nb boolean data columns permuted along. */
 void oro_table_sort(oro_ctx* c, int w, size_t n, int ncols, void* const* cols, const int* desc,
                     const int* single_bit, int na, void* const* data_a, int nb,
-                    void* const* data_b);
+                    void* const* data_b, int quick);
 /* distinct (distinct.h:20-53): res marks the first row of every run of equal
  * keys (adjacent rows only). */
 void oro_distinct(oro_ctx* c, int w, size_t n, int nkeys, void* const* keys, void* res[3]);

@@ -193,10 +193,11 @@ int main(int argc, char** argv) {
         }
         auto T = J.open_with_schema();
         for (size_t k = 0; k < T.second.size(); k++) d.plain("open_" + T.second[k], T.first[k]);
-    } else if (op == "tsort" || op == "distinct") {
-        // tsort: operators::table_sort with the radix protocol on three key
-        // columns [bit ASC, small-int DESC, bit ASC] plus one A and one B data
-        // column. distinct: operators::distinct over two sorted key columns.
+    } else if (op == "tsort" || op == "tsort_qs" || op == "distinct") {
+        // tsort (tsort_qs): operators::table_sort with the radix (quicksort)
+        // protocol on three key columns [bit ASC, small-int DESC, bit ASC] plus
+        // one A and one B data column. distinct: operators::distinct over two
+        // sorted key columns.
         using B = BSharedVector<int64_t>;
         using A = ASharedVector<int64_t>;
         uint64_t st = seed;
@@ -208,14 +209,16 @@ int main(int argc, char** argv) {
         B b0 = secret_share_b(v0, 0), b1 = secret_share_b(v1, 0), b2 = secret_share_b(v2, 0);
         A a0 = secret_share_a(va, 0);
         B b3 = secret_share_b(vb, 0);
-        if (op == "tsort") {
+        if (op != "distinct") {
             std::vector<B*> cols = {&b0, &b1, &b2};
             std::vector<A*> da = {&a0};
             std::vector<B*> db = {&b3};
             orq::operators::table_sort(cols, da, db,
                                        {orq::operators::SortOrder::ASC, orq::operators::SortOrder::DESC,
                                         orq::operators::SortOrder::ASC},
-                                       {true, false, true}, orq::SortingProtocol::RADIXSORT);
+                                       {true, false, true},
+                                       op == "tsort" ? orq::SortingProtocol::RADIXSORT
+                                                     : orq::SortingProtocol::QUICKSORT);
             d.shares("c0", b0);
             d.shares("c1", b1);
             d.shares("c2", b2);
@@ -294,7 +297,7 @@ int main(int argc, char** argv) {
                 d.plain("open_key", o);
             }
         }
-    } else if (op == "qsort" || op == "qsort_desc" || op == "qsort32") {
+    } else if (op == "qsort" || op == "qsort_desc" || op == "qsort32" || op == "qsort_time") {
         // quicksort(key, order) then the permutation applied to two A-shared
         // payloads of the key's type (int64 keys uniform in [0, 2^bits);
         // int32 keys over all 32 bits; payloads u32)
@@ -314,6 +317,7 @@ int main(int argc, char** argv) {
             orq::operators::oblivious_apply_elementwise_perm(a1, perm);
             orq::operators::oblivious_apply_elementwise_perm(a2, perm);
             secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (op == "qsort_time") return;
             d.shares("key", kb);
             d.shares("pay1", a1);
             d.shares("pay2", a2);

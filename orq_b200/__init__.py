@@ -534,18 +534,26 @@ def compose_permutations(sigma: ASharedVector, rho: ASharedVector) -> ASharedVec
     return rho
 
 
-def table_sort(columns, data_a=(), data_b=(), order=None, single_bit=None):
-    """orq::operators::table_sort (sorting.h:509-612) with the radix sort
-    protocol: columns are B-shared key columns (most significant first), each
-    sorted ASC/DESC per `order`, on one bit where `single_bit` says so; data
-    columns are permuted along. Everything is updated in place."""
+class SortingProtocol:
+    """orq::SortingProtocol (sorting.h:15-21). The mirror's DEFAULT is RADIXSORT,
+    the protocol of a reference built with DEFAULT_SORT_PROTO=RADIXSORT."""
+    BITONICSORT, QUICKSORT, RADIXSORT = 0, 1, 2
+    DEFAULT = 2
+
+
+def table_sort(columns, data_a=(), data_b=(), order=None, single_bit=None,
+               protocol: int = SortingProtocol.DEFAULT):
+    """orq::operators::table_sort (sorting.h:509-612) with the quicksort or
+    radix sort protocol: columns are B-shared key columns (most significant
+    first), each sorted ASC/DESC per `order`, on one bit where `single_bit`
+    says so; data columns are permuted along. Everything is updated in place."""
     rt, n, w = columns[0].rt, columns[0].size(), columns[0].width
     order = order or [ASC] * len(columns)
     single_bit = single_bit or [False] * len(columns)
     _check(rt.lib.orqcu_table_sort(rt.h, w, ctypes.c_size_t(n), len(columns), _flat(columns),
                                    (ctypes.c_int * len(columns))(*[int(o == DESC) for o in order]),
                                    (ctypes.c_int * len(columns))(*[int(bool(b)) for b in single_bit]),
-                                   len(data_a), _flat(data_a), len(data_b), _flat(data_b)))
+                                   len(data_a), _flat(data_a), len(data_b), _flat(data_b), int(protocol)))
 
 
 def distinct(keys) -> BSharedVector:

@@ -436,9 +436,10 @@ int orqcu_compose_permutations(orqcu_runtime* rt, size_t n, void* const sigma[3]
 
 int orqcu_table_sort(orqcu_runtime* rt, int width, size_t n, int ncols, void* const* cols,
                      const int* descending, const int* single_bit, int na, void* const* data_a,
-                     int nb, void* const* data_b) {
+                     int nb, void* const* data_b, int protocol) {
     return guard([&] {
         need_rt(rt);
+        need(protocol == ORQCU_SORT_QUICK || protocol == ORQCU_SORT_RADIX, "Unknown table sort protocol");
         need(ncols >= 1 && cols && descending && single_bit, "table sort needs key columns");
         need(na >= 0 && nb >= 0 && (na == 0 || data_a) && (nb == 0 || data_b), "bad data columns");
         need(n < (1ull << 31), "table sort supports n < 2^31");
@@ -456,7 +457,7 @@ int orqcu_table_sort(orqcu_runtime* rt, int width, size_t n, int ncols, void* co
             b[i] = m3(data_b + 3 * i);
         }
         orqcu::op_table_sort(rt->ctx, width, n, ncols, k.data(), descending, single_bit, na, a.data(),
-                             nb, b.data());
+                             nb, b.data(), protocol == ORQCU_SORT_QUICK);
         rt->ctx.check_device_error();
     });
 }

@@ -241,7 +241,7 @@ void op_aggregate(Ctx& c, int w, size_t n, int nkeys, const void* const* keys, i
 // ---- table sort, permutation composition, distinct (tsort.cu) ----
 void op_compose(Ctx& c, size_t n, Sh3 sigma, Sh3 rho);  // rho <- compose(sigma, rho)
 void op_table_sort(Ctx& c, int w, size_t n, int ncols, const Sh3* cols, const int* desc,
-                   const int* single_bit, int na, const Sh3* data_a, int nb, const Sh3* data_b);
+                   const int* single_bit, int na, const Sh3* data_a, int nb, const Sh3* data_b, bool quick);
 void op_distinct(Ctx& c, int w, size_t n, int nkeys, const CSh3* keys, Sh3 res);
 
 // ---- batched bitonic sort (cmp.cu) ----

@@ -1,7 +1,7 @@
 // tsort.cu — multi-column table sort, permutation composition and distinct.
 //
-// table_sort (include/core/operators/sorting.h:509-612) with the radix
-// protocol sorts the last key column first and every earlier column after
+// table_sort (include/core/operators/sorting.h:509-612) with the radix or
+// quicksort protocol sorts the last key column first and every earlier column after
 // applying the running permutation, composing the permutations
 // (compose_permutations, operators/shuffle.h:717-743); all of it is host
 // orchestration of the radix sort and apply kernels. distinct
@@ -169,17 +169,24 @@ void op_compose(Ctx& c, size_t n, Sh3 sigma, Sh3 rho) {
 }
 
 void op_table_sort(Ctx& c, int w, size_t n, int ncols, const Sh3* cols, const int* desc,
-                   const int* single_bit, int na, const Sh3* data_a, int nb, const Sh3* data_b) {
+                   const int* single_bit, int na, const Sh3* data_a, int nb, const Sh3* data_b, bool quick) {
     if (w != 4 && w != 8) throw std::invalid_argument("table sort supports 4 and 8-byte columns");
     if (ncols < 1) throw std::invalid_argument("table sort needs a key column");
     int ns = 0;
     for (int k = 0; k < ncols; k++) ns += single_bit[k] != 0;
     const int nk = ncols - ns, nc = na + nb, L = 8 * w;
     // PermutationManager::reserve(size, perms, pairs): for 3PC pairs are
-    // single permutations too
-    const size_t perms = (size_t)(nk + ns - 1) + (size_t)(nk + ns);
-    const size_t pairs = (size_t)(4 * ns + 3 * nk + nc - 1) + (size_t)nk * L;
+    // single permutations too. Quicksort needs an extra permutation per
+    // multi-bit key (its shuffle), radix sort an extra pair per bit.
+    const size_t perms = (size_t)(nk + ns - 1) + (size_t)(nk + ns) + (quick ? (size_t)nk : 0);
+    const size_t pairs = (size_t)(4 * ns + 3 * nk + nc - 1) + (quick ? 0 : (size_t)nk * L);
     reserve_perms(c, n, perms + pairs);
+    // sort_sub (sorting.h:565-576): single-bit columns by a 1-bit radix sort
+    auto sort_sub = [&](int k, Sh3 perm) {
+        if (single_bit[k]) op_radix_sort(c, w, n, cols[k], 1, desc[k] != 0, perm);
+        else if (quick) op_quicksort(c, w, n, cols[k], desc[k] != 0, perm);
+        else op_radix_sort(c, w, n, cols[k], L, desc[k] != 0, perm);
+    };
     const size_t n1 = std::max<size_t>(n, 1);
     Scratch origb(c, 3 * n1 * w), spb(c, 3 * n1 * 4), npb(c, 3 * n1 * 4);
     Sh3 orig, sp, np;
@@ -190,12 +197,12 @@ void op_table_sort(Ctx& c, int w, size_t n, int ncols, const Sh3* cols, const in
     }
     int C = ncols - 1;
     copy_sh(c, orig, cc(cols[C]), n * w);
-    op_radix_sort(c, w, n, cols[C], single_bit[C] ? 1 : L, desc[C] != 0, sp);
+    sort_sub(C, sp);
     copy_sh(c, cols[C], cc(orig), n * w);
     for (C--; C >= 0; C--) {
         copy_sh(c, orig, cc(cols[C]), n * w);
         op_apply_elementwise(c, false, w, n, cols[C], cc(sp));
-        op_radix_sort(c, w, n, cols[C], single_bit[C] ? 1 : L, desc[C] != 0, np);
+        sort_sub(C, np);
         copy_sh(c, cols[C], cc(orig), n * w);
         op_compose(c, n, sp, np);
         std::swap(sp, np);

@@ -16,8 +16,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import (ASC, DESC, ASharedVector, BSharedVector, Direction, aggregate, aggregators,
-               distinct as _distinct, table_sort, _torch)
+from . import (ASC, DESC, ASharedVector, BSharedVector, Direction, SortingProtocol, aggregate, aggregators,
+               bitonic_sort, distinct as _distinct, table_sort, _torch)
 
 JOIN_ID = "[##TID]"
 VALID = "[##V]"
@@ -157,18 +157,36 @@ class EncodedTable:
         t.schema[JOIN_ID].shares[:, self.rows:n] = one.shares[:, :1]
         return t
 
-    # ---- sort (encoded_table.h:900-998), radix protocol ------------------
-    def sort(self, columns, order=ASC):
+    # ---- sort (encoded_table.h:900-998) ------------------------------------
+    def sort(self, columns, order=ASC, protocol=SortingProtocol.DEFAULT):
+        """Sorts the table on `columns` (names, or (name, order) pairs) with
+        the quicksort or radix protocol (table_sort), or with the bitonic
+        network on the table padded to a power of two (padding rows are cut
+        again when the sort is on the valid column)."""
         spec = [(c, order) for c in columns] if not (columns and isinstance(columns[0], tuple)) else columns
+        original = self.rows
+        if protocol == SortingProtocol.BITONICSORT:
+            self.pad_power_of_two()
         keys = [c for c, _ in spec]
         orders = [o for _, o in spec]
         single_bit = [c in (VALID, JOIN_ID) for c in keys]
+        can_unpad = VALID in keys
+        unpad_from_top = dict(spec).get(VALID, ASC) == ASC
         data_a, data_b = [], []
         for k in self.getColumnNames():
             if k in keys:
                 continue
             (data_b if is_bshared(k) else data_a).append(self.schema[k])
-        table_sort([self.schema[k] for k in keys], data_a, data_b, orders, single_bit)
+        key_cols = [self.schema[k] for k in keys]
+        if protocol == SortingProtocol.BITONICSORT:
+            bitonic_sort(key_cols, data_a, data_b, orders)
+            if can_unpad:
+                if unpad_from_top:
+                    self.tail(original)
+                else:
+                    self.resize(original)
+        else:
+            table_sort(key_cols, data_a, data_b, orders, single_bit, protocol)
         return self
 
     # ---- distinct (encoded_table.h:1198-1212) -----------------------------

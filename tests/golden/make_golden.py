@@ -74,6 +74,8 @@ CASES = [
     ("qsort_n2_b40", "qsort", 2, 5, 2, 40, True),
     ("qsort_n20000_b40", "qsort", 20000, 10, 6, 40, False),
     ("qsort32_n30000", "qsort32", 30000, 11, 7, 32, False),
+    ("tsort_qs_n64", "tsort_qs", 64, 5, 4, 64, True),
+    ("tsort_qs_n3000", "tsort_qs", 3000, 6, 5, 64, False),
 ]
 
 

@@ -46,8 +46,8 @@ class OracleBackend:
         perm = self.o.radix_sort(key, bits, payloads, desc=desc)
         return perm
 
-    def table_sort(self, cols, desc, single_bit, data_a, data_b):
-        self.o.table_sort(cols, desc, single_bit, data_a, data_b)
+    def table_sort(self, cols, desc, single_bit, data_a, data_b, quick=False):
+        self.o.table_sort(cols, desc, single_bit, data_a, data_b, quick)
 
     def distinct(self, keys):
         return self.o.distinct(keys)
@@ -133,9 +133,10 @@ class GpuBackend:
             self.orq.oblivious_apply_elementwise_perm(p, perm)
         return perm
 
-    def table_sort(self, cols, desc, single_bit, data_a, data_b):
+    def table_sort(self, cols, desc, single_bit, data_a, data_b, quick=False):
         o = self.orq
-        o.table_sort(cols, data_a, data_b, [o.DESC if d else o.ASC for d in desc], single_bit)
+        o.table_sort(cols, data_a, data_b, [o.DESC if d else o.ASC for d in desc], single_bit,
+                     o.SortingProtocol.QUICKSORT if quick else o.SortingProtocol.RADIXSORT)
 
     def distinct(self, keys):
         return self.orq.distinct(keys)
@@ -428,15 +429,16 @@ def tsort_inputs(n, seed):
 
 
 def replay_tsort(be, op, n, seed):
-    """The "tsort" op (table_sort on [bit ASC, 3-bit DESC, bit ASC] with one A
-    and one B data column) or the "distinct" op (distinct on the first two
+    """The "tsort" ("tsort_qs") op (table_sort with the radix (quicksort)
+    protocol on [bit ASC, 3-bit DESC, bit ASC] with one A and one B data
+    column) or the "distinct" op (distinct on the first two
     key columns) of ref_driver.cpp."""
     v0, v1, v2, va, vb = tsort_inputs(n, seed)
     b0, b1, b2 = (be.share(v, False, 0) for v in (v0, v1, v2))
     a0 = be.share(va, True, 0)
     b3 = be.share(vb, False, 0)
-    if op == "tsort":
-        be.table_sort([b0, b1, b2], [False, True, False], [True, False, True], [a0], [b3])
+    if op in ("tsort", "tsort_qs"):
+        be.table_sort([b0, b1, b2], [False, True, False], [True, False, True], [a0], [b3], op == "tsort_qs")
         out = {"c0": be.np(b0), "c1": be.np(b1), "c2": be.np(b2), "da": be.np(a0), "db": be.np(b3)}
         for k, v in (("c0", b0), ("c1", b1), ("c2", b2)):
             out["open_" + k] = be.open(v, False)[None]

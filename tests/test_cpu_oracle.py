@@ -179,7 +179,8 @@ def test_radix_desc_large_matches_reference_digests(oracle_lib, digests):
         assert [sha(a) for a in arr] == d["arrays"][name], name
 
 
-@pytest.mark.parametrize("tag,op", [("tsort_n64", "tsort"), ("distinct_n64", "distinct")])
+@pytest.mark.parametrize("tag,op", [("tsort_n64", "tsort"), ("tsort_qs_n64", "tsort_qs"),
+                                    ("distinct_n64", "distinct")])
 def test_table_sort_and_distinct_match_reference_shares(oracle_lib, golden, digests, tag, op):
     m = digests[tag]["meta"]
     out, _ = replay_tsort(OracleBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
@@ -187,7 +188,8 @@ def test_table_sort_and_distinct_match_reference_shares(oracle_lib, golden, dige
         assert same(arr, golden[f"{tag}/{name}"]), name
 
 
-@pytest.mark.parametrize("tag,op", [("tsort_n200", "tsort"), ("distinct_n5000", "distinct")])
+@pytest.mark.parametrize("tag,op", [("tsort_n200", "tsort"), ("tsort_qs_n3000", "tsort_qs"),
+                                    ("distinct_n5000", "distinct")])
 def test_table_sort_and_distinct_large_match_reference_digests(oracle_lib, digests, tag, op):
     d = digests[tag]
     m = d["meta"]

@@ -336,7 +336,8 @@ def test_radix_desc_large_matches_reference_digests(orq, digests):
         assert [sha(a) for a in arr] == d["arrays"][name], name
 
 
-@pytest.mark.parametrize("tag,op", [("tsort_n64", "tsort"), ("distinct_n64", "distinct")])
+@pytest.mark.parametrize("tag,op", [("tsort_n64", "tsort"), ("tsort_qs_n64", "tsort_qs"),
+                                    ("distinct_n64", "distinct")])
 def test_table_sort_and_distinct_match_reference_shares(orq, golden, digests, tag, op):
     m = digests[tag]["meta"]
     out, _ = replay_tsort(GpuBackend(m["shim_seed"]), op, m["n"], m["data_seed"])
@@ -344,7 +345,8 @@ def test_table_sort_and_distinct_match_reference_shares(orq, golden, digests, ta
         assert same(arr, golden[f"{tag}/{name}"]), name
 
 
-@pytest.mark.parametrize("tag,op", [("tsort_n200", "tsort"), ("distinct_n5000", "distinct")])
+@pytest.mark.parametrize("tag,op", [("tsort_n200", "tsort"), ("tsort_qs_n3000", "tsort_qs"),
+                                    ("distinct_n5000", "distinct")])
 def test_table_sort_and_distinct_large_match_reference_digests(orq, digests, tag, op):
     d = digests[tag]
     m = d["meta"]
@@ -353,7 +355,8 @@ def test_table_sort_and_distinct_large_match_reference_digests(orq, digests, tag
         assert [sha(a) for a in arr] == d["arrays"][name], name
 
 
-@pytest.mark.parametrize("op,n", [("tsort", 1), ("tsort", 2), ("tsort", 1000), ("distinct", 1),
+@pytest.mark.parametrize("op,n", [("tsort", 1), ("tsort", 2), ("tsort", 1000), ("tsort_qs", 1), ("tsort_qs", 5),
+                                  ("tsort_qs", 1000), ("distinct", 1),
                                   ("distinct", 2), ("distinct", 33), ("distinct", 300001)])
 def test_table_sort_and_distinct_match_restatement(orq, op, n):
     gpu, _ = replay_tsort(GpuBackend(61), op, n, 3)
@@ -609,3 +612,35 @@ def test_quicksort_full_size_properties(orq):
     assert np.array_equal(out["open_key"][0].view(np.int64), k[o])
     assert np.array_equal(out["open_pay1"][0].view(np.uint64), p1[o])
     assert np.array_equal(out["open_pay2"][0].view(np.uint64), p2[o])
+
+
+@pytest.mark.parametrize("protocol", [0, 1, 2])
+def test_encoded_table_sort_protocols(orq, protocol):
+    """EncodedTable::sort (encoded_table.h:900-998) with the bitonic, quicksort
+    and radix protocols: rows ordered by ([K1] ASC, [K2] DESC), every row's
+    data carried; the bitonic protocol pads to a power of two and, sorting on
+    the valid column first, cuts the padding again"""
+    from orq_b200.table import VALID, EncodedTable
+
+    n = 300
+    rng = np.random.default_rng(3)
+    k1 = rng.integers(-3, 4, n)
+    k2 = rng.integers(-2**40, 2**40, n)
+    v = rng.integers(0, 10**6, n)
+    b = rng.integers(0, 2**62, n)
+    rt = orq.Runtime(seed=4)
+    T = EncodedTable.secret_share(rt, [k1, k2, v, b], ["[K1]", "[K2]", "V", "[B]"])
+    T.sort([("[K1]", orq.ASC), ("[K2]", orq.DESC)], protocol=protocol)
+    cols, names = T.open_with_schema()
+    got = dict(zip(names, (c.view(np.int64) for c in cols)))
+    o = np.lexsort((-k2, k1))
+    for nm, want in (("[K1]", k1), ("[K2]", k2), ("V", v), ("[B]", b)):
+        assert np.array_equal(got[nm], want[o]), nm
+    if protocol == orq.SortingProtocol.BITONICSORT:
+        assert T.size() == 512  # padded, not cut: the sort was not on the valid column
+        T.sort([(VALID, orq.DESC), ("[K1]", orq.ASC)], protocol=protocol)
+        assert T.size() == n
+        cols, names = T.open_with_schema()
+        got = dict(zip(names, (c.view(np.int64) for c in cols)))
+        assert np.array_equal(np.sort(got["[K1]"], kind="stable"), got["[K1]"])
+        assert sorted(got["V"].tolist()) == sorted(v.tolist())
