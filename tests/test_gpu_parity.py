@@ -638,6 +638,8 @@ def test_encoded_table_sort_protocols(orq, protocol):
         assert np.array_equal(got[nm], want[o]), nm
     if protocol == orq.SortingProtocol.BITONICSORT:
         assert T.size() == 512  # padded, not cut: the sort was not on the valid column
+        # a fresh table sorted on the valid column: padded to 512, cut back to n
+        T = EncodedTable.secret_share(rt, [k1, k2, v, b], ["[K1]", "[K2]", "V", "[B]"])
         T.sort([(VALID, orq.DESC), ("[K1]", orq.ASC)], protocol=protocol)
         assert T.size() == n
         cols, names = T.open_with_schema()
