@@ -525,12 +525,12 @@ def run_serve(args, rank, world, local_rank):
     # warm-up: a small trace through both paths (tables, pools, kernels)
     for _ in range(max(1, args.warmup)):
         for slots in (1, args.slots):
-            srv = Server(slots=slots, device=local_rank)
+            srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol)
             srv.run(make_trace(6, 0.0, seed=99, min_log=10, max_log=12))
             srv.close()
     # capacity of the plain path
     calib = make_trace(args.serve_requests, 0.0, seed=5 + rank, max_log=args.serve_max_log)
-    srv = Server(slots=1, device=local_rank)
+    srv = Server(slots=1, device=local_rank, protocol=args.sort_protocol)
     cap_stats = srv.run(calib)
     srv.close()
     capacity = cap_stats["requests"] / cap_stats["makespan_s"]
@@ -538,7 +538,7 @@ def run_serve(args, rank, world, local_rank):
     out = {"capacity_req_per_s": capacity, "rate_req_per_s": rate}
     for name, slots in (("serving", args.slots), ("plain", 1)):
         trace = make_trace(args.serve_requests, rate, seed=5 + rank, max_log=args.serve_max_log)
-        srv = Server(slots=slots, device=local_rank)
+        srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol)
         clocks = ClockSampler(local_rank)
         clocks.start()
         st = srv.run(trace, check=True)
@@ -575,19 +575,22 @@ class ServeReference:
     name = "serve"
 
     def __init__(self, args, seed):
+        self.protocol = args.sort_protocol
         self.config = {"workload": "mixed requests (60% sort, 30% group-by, 10% join) served one at a time",
-                       "seed": seed}
+                       "sort_protocol": self.protocol, "seed": seed}
 
     def cpu_reference(self, sample, threads):
         n = max(1024, min(sample, 1 << 12))
-        ss = run_ref_seconds("radix_time", n, 7, 64, threads)
-        sj = run_ref_seconds("join_time", n // 4, 7, 64, threads)
+        quick = self.protocol == "quick"
+        ss = run_ref_seconds("qsort_time" if quick else "radix_time", n, 7, 64, threads)
+        sj = run_ref_seconds("join_time", n // 4, 7, 64, threads, quick_tables=quick)
         rows = 0.6 * n + 0.1 * (5 * (n // 4))
         sec = 0.6 * ss + 0.1 * sj
-        return rows / sec, sec, (f"a {n}-row 64-bit radix sort and a {n // 4} x {n} join (bounded "
-                                 f"samples) weighted 0.6 / 0.1 by the request mix (group-by runs the same "
-                                 f"table sort as a sort), ORQ's own operators, 3 party processes x "
-                                 f"{threads} worker threads")
+        kind = "quicksort" if quick else "radix sort"
+        return rows / sec, sec, (f"a {n}-row 64-bit {kind} and a {n // 4} x {n} join with {kind} table "
+                                 f"sorts (bounded samples) weighted 0.6 / 0.1 by the request mix (group-by "
+                                 f"runs the same table sort as a sort), ORQ's own operators, 3 party "
+                                 f"processes x {threads} worker threads")
 
 
 WORKLOADS = {"radix": RadixWorkload, "qsort": QuicksortWorkload, "bitonic": BitonicWorkload,
@@ -718,13 +721,15 @@ def roofline(prof, steps, n):
     return out
 
 
-def run_ref_seconds(op, n, seed, bits, threads, timeout=1800):
+def run_ref_seconds(op, n, seed, bits, threads, timeout=1800, quick_tables=False):
     """ORQ's own CPU code for one op (oracle/_ref/ref_driver, three party
-    processes); returns the seconds it reports for the timed region."""
+    processes; with quick_tables the build whose EncodedTable sorts default to
+    quicksort); returns the seconds it reports for the timed region."""
     from oracle import run_ref
 
     t0 = time.time()
-    _, out = run_ref.run(op, n, seed, shim_seed=7, bits=bits, threads=threads, timeout=timeout)
+    _, out = run_ref.run(op, n, seed, shim_seed=7, bits=bits, threads=threads, timeout=timeout,
+                         driver=run_ref.DRIVER_QS if quick_tables else None)
     wall = time.time() - t0
     sec = None
     for line in out.splitlines():
@@ -762,6 +767,9 @@ def main():
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-max-log", type=int, default=22)
+    ap.add_argument("--sort-protocol", default="quick", choices=["quick", "radix"],
+                    help="serve: sort protocol of sort requests and table sorts (the reference's default "
+                         "is quicksort)")
     args = ap.parse_args()
     if args.workload == "join" and args.cpu_sample == 1 << 17:
         args.cpu_sample = 1 << 11
@@ -822,7 +830,8 @@ def main():
                                            "plain path's capacity, 60% sort / 30% group-by (2^10 groups) / 10% "
                                            f"PK-FK join (4x fk side), rows log-uniform 2^12..2^{args.serve_max_log}, "
                                            f"int64 keys; continuous batching over {args.slots} slots",
-                               "parallelism": f"replicas x{world}", "slots": args.slots},
+                               "parallelism": f"replicas x{world}", "slots": args.slots,
+                               "sort_protocol": args.sort_protocol},
                     "correct": sv["ok"] and pl["ok"], "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
                     "clocks": sv["clocks"], "capacity_req_per_s": res["capacity_req_per_s"],
                     "rate_req_per_s": res["rate_req_per_s"],

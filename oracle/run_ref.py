@@ -68,11 +68,16 @@ def parse_dump(path: str) -> dict:
     return out
 
 
+DRIVER_QS = os.path.join(HERE, "_ref", "ref_driver_qs")  # EncodedTable sorts by quicksort
+
+
 def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
-        threads: int = 1, batch: int = -1, timeout: float = 600.0, outdir: str | None = None):
+        threads: int = 1, batch: int = -1, timeout: float = 600.0, outdir: str | None = None,
+        driver: str | None = None):
     """Run one op on 3 parties. Returns (list of per-party dicts, stdout of P0)."""
-    if not os.path.exists(DRIVER):
-        raise FileNotFoundError(DRIVER + " (run `make -C oracle ref`)")
+    driver = driver or DRIVER
+    if not os.path.exists(driver):
+        raise FileNotFoundError(driver + " (run `make -C oracle ref`)")
     tmp = outdir or tempfile.mkdtemp(prefix="orqref_")
     base = _free_base_port()
     procs = []
@@ -85,7 +90,7 @@ def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
             "STARTMPC_BASE_PORT": str(base),
             "ORQ_SHIM_SEED": str(shim_seed),
         })
-        cmd = [DRIVER, str(threads), "1", str(batch), op, str(n), str(data_seed), tmp, str(bits)]
+        cmd = [driver, str(threads), "1", str(batch), op, str(n), str(data_seed), tmp, str(bits)]
         procs.append(subprocess.Popen(cmd, env=env, stdout=subprocess.PIPE,
                                       stderr=subprocess.PIPE, start_new_session=True))
     deadline = time.time() + timeout

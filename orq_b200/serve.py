@@ -14,6 +14,9 @@ pool warm between requests (re-allocating and re-mapping gigabytes per
 request costs more than the request); with several slots each slot's grids
 are sized for its share of the SMs.
 
+Sort requests and the table sorts of group-by and join requests use the
+server's sort protocol: quicksort (the reference's default) or radix sort.
+
 Latency is measured from a request's arrival to the host having its opened
 result; the server reports throughput (rows/s over the whole trace) and the
 latency percentiles. `plain` mode runs the same trace through one slot
@@ -28,7 +31,7 @@ import time
 
 import numpy as np
 
-from . import ASC, Runtime, _torch, aggregators, radix_sort
+from . import ASC, Runtime, SortingProtocol, _torch, aggregators, quicksort, radix_sort
 from .table import EncodedTable
 
 KINDS = ("sort", "groupby", "join")
@@ -79,25 +82,30 @@ class Request:
         return None if self.t_done is None else self.t_done - self.arrival
 
 
-def run_request(rt, req):
+def run_request(rt, req, protocol="quick"):
     """Runs one request on a runtime (on the caller's current CUDA stream) and
-    returns its opened result as host arrays."""
+    returns its opened result as host arrays. `protocol` ("quick" or "radix")
+    sorts sort requests and every table sort of group-by and join requests."""
     torch = _torch()
+    tp = SortingProtocol.QUICKSORT if protocol == "quick" else SortingProtocol.RADIXSORT
     if req.kind == "sort":
         kb = rt.secret_share_b(req.inputs[0], 0)
-        radix_sort(kb, ASC, 64)
+        if protocol == "quick":
+            quicksort(kb, ASC)
+        else:
+            radix_sort(kb, ASC, 64)
         out = {"key": kb.open().cpu().numpy()}
     elif req.kind == "groupby":
         g, v = req.inputs
-        T = EncodedTable.secret_share(rt, [g, v], ["[G]", "V"])
+        T = EncodedTable.secret_share(rt, [g, v], ["[G]", "V"], protocol=tp)
         T.addColumns(["CNT"])
         T.aggregate(["[G]"], [("V", "V", aggregators.sum), ("CNT", "CNT", aggregators.count)])
         cols, names = T.open_with_schema()
         out = dict(zip(names, cols))
     else:
         pk, v, fk, q = req.inputs
-        A = EncodedTable.secret_share(rt, [pk, v], ["[K]", "V"])
-        B = EncodedTable.secret_share(rt, [fk, q], ["[K]", "Q"])
+        A = EncodedTable.secret_share(rt, [pk, v], ["[K]", "V"], protocol=tp)
+        B = EncodedTable.secret_share(rt, [fk, q], ["[K]", "Q"], protocol=tp)
         J = A.inner_join(B, ["[K]"], [("V", "V", aggregators.copy)])
         cols, names = J.open_with_schema()
         out = dict(zip(names, cols))
@@ -150,8 +158,10 @@ class _Slot:
 class Server:
     """Continuous-batching server over `slots` concurrent runtimes."""
 
-    def __init__(self, slots=4, device=0, budget_fraction=0.8, budget_bytes=None, share_sms=True):
+    def __init__(self, slots=4, device=0, budget_fraction=0.8, budget_bytes=None, share_sms=True,
+                 protocol="quick"):
         torch = _torch()
+        self.protocol = protocol
         torch.cuda.set_device(device)
         free, _ = torch.cuda.mem_get_info(device)
         self.budget = int(budget_bytes if budget_bytes is not None else free * budget_fraction)
@@ -189,7 +199,7 @@ class Server:
                 try:
                     with torch.cuda.stream(slot.stream):
                         slot.rt.reseed(req.seed)
-                        req.result = run_request(slot.rt, req)
+                        req.result = run_request(slot.rt, req, self.protocol)
                         slot.stream.synchronize()
                     req.t_done = time.perf_counter() - t0
                     if check:

@@ -37,9 +37,13 @@ class EncodedTable:
 
     WIDTH = 8
 
-    def __init__(self, rt, columns: dict | None = None, rows: int = 0, name: str = ""):
+    def __init__(self, rt, columns: dict | None = None, rows: int = 0, name: str = "",
+                 protocol: int = SortingProtocol.DEFAULT):
         self.rt = rt
         self.tableName = name
+        # SortingProtocol of this table's sorts (the reference fixes it with
+        # DEFAULT_SORT_PROTO); tables derived from it inherit it
+        self.protocol = protocol
         self.schema: dict = {}
         self.rows = rows
         for k, v in (columns or {}).items():
@@ -48,7 +52,8 @@ class EncodedTable:
 
     # ---- construction ----------------------------------------------------
     @classmethod
-    def secret_share(cls, rt, columns, names, party: int = 0, name: str = ""):
+    def secret_share(cls, rt, columns, names, party: int = 0, name: str = "",
+                     protocol: int = SortingProtocol.DEFAULT):
         """secret_share(columns, schema) (encoded_table.h:1687-1707) + the
         EncodedTable(contents) constructor (encoded_table.h:252-265)."""
         assert len(columns) == len(names)
@@ -57,7 +62,7 @@ class EncodedTable:
             d = np.ascontiguousarray(np.asarray(data).astype(np.int64))
             cols[nm] = (rt.secret_share_b if is_bshared(nm) else rt.secret_share_a)(d, party)
         rows = len(columns[0]) if columns else 0
-        return cls(rt, cols, rows, name)
+        return cls(rt, cols, rows, name, protocol)
 
     def _zeros(self, name, n):
         t = self.rt._alloc(n, self.WIDTH)
@@ -144,7 +149,7 @@ class EncodedTable:
         new_schema = [JOIN_ID] + [c for c in self.getColumnNames() if c != JOIN_ID]
         new_schema += [c for c in other.getColumnNames() if c not in self.schema]
         n = self.rows + other.rows
-        t = EncodedTable(self.rt, {}, n, self.tableName + "+" + other.tableName)
+        t = EncodedTable(self.rt, {}, n, self.tableName + "+" + other.tableName, self.protocol)
         for c in new_schema:
             if c not in t.schema:
                 t.add_column(c)
@@ -158,12 +163,13 @@ class EncodedTable:
         return t
 
     # ---- sort (encoded_table.h:900-998) ------------------------------------
-    def sort(self, columns, order=ASC, protocol=SortingProtocol.DEFAULT):
+    def sort(self, columns, order=ASC, protocol=None):
         """Sorts the table on `columns` (names, or (name, order) pairs) with
         the quicksort or radix protocol (table_sort), or with the bitonic
         network on the table padded to a power of two (padding rows are cut
         again when the sort is on the valid column)."""
         spec = [(c, order) for c in columns] if not (columns and isinstance(columns[0], tuple)) else columns
+        protocol = self.protocol if protocol is None else protocol
         original = self.rows
         if protocol == SortingProtocol.BITONICSORT:
             self.pad_power_of_two()
