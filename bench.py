@@ -525,7 +525,8 @@ def run_serve(args, rank, world, local_rank):
     # warm-up: a small trace through both paths (tables, pools, kernels)
     for _ in range(max(1, args.warmup)):
         for slots in (1, args.slots):
-            srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol)
+            srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol,
+                         share_sms=bool(args.share_sms))
             srv.run(make_trace(6, 0.0, seed=99, min_log=10, max_log=12))
             srv.close()
     # capacity of the plain path
@@ -538,7 +539,8 @@ def run_serve(args, rank, world, local_rank):
     out = {"capacity_req_per_s": capacity, "rate_req_per_s": rate}
     for name, slots in (("serving", args.slots), ("plain", 1)):
         trace = make_trace(args.serve_requests, rate, seed=5 + rank, max_log=args.serve_max_log)
-        srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol)
+        srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol,
+                     share_sms=bool(args.share_sms))
         clocks = ClockSampler(local_rank)
         clocks.start()
         st = srv.run(trace, check=True)
@@ -767,6 +769,8 @@ def main():
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-max-log", type=int, default=22)
+    ap.add_argument("--share-sms", type=int, default=1,
+                    help="serve: partition the SMs between slots (1) or let every slot use all of them (0)")
     ap.add_argument("--sort-protocol", default="quick", choices=["quick", "radix"],
                     help="serve: sort protocol of sort requests and table sorts (the reference's default "
                          "is quicksort)")
@@ -831,7 +835,7 @@ def main():
                                            f"PK-FK join (4x fk side), rows log-uniform 2^12..2^{args.serve_max_log}, "
                                            f"int64 keys; continuous batching over {args.slots} slots",
                                "parallelism": f"replicas x{world}", "slots": args.slots,
-                               "sort_protocol": args.sort_protocol},
+                               "sort_protocol": args.sort_protocol, "share_sms": bool(args.share_sms)},
                     "correct": sv["ok"] and pl["ok"], "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
                     "clocks": sv["clocks"], "capacity_req_per_s": res["capacity_req_per_s"],
                     "rate_req_per_s": res["rate_req_per_s"],
