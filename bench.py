@@ -769,7 +769,7 @@ def main():
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-max-log", type=int, default=22)
-    ap.add_argument("--share-sms", type=int, default=1,
+    ap.add_argument("--share-sms", type=int, default=0,
                     help="serve: partition the SMs between slots (1) or let every slot use all of them (0)")
     ap.add_argument("--sort-protocol", default="quick", choices=["quick", "radix"],
                     help="serve: sort protocol of sort requests and table sorts (the reference's default "

@@ -11,8 +11,8 @@ device. A slot re-keys its runtime with the request's own seed before
 running it (orqcu_runtime_reseed): a request's shares and opened result are
 the same whether it runs alone or in a mix. A slot keeps its device memory
 pool warm between requests (re-allocating and re-mapping gigabytes per
-request costs more than the request); with several slots each slot's grids
-are sized for its share of the SMs.
+request costs more than the request); optionally each slot's grids are sized
+for its share of the SMs.
 
 Sort requests and the table sorts of group-by and join requests use the
 server's sort protocol: quicksort (the reference's default) or radix sort.
@@ -158,7 +158,7 @@ class _Slot:
 class Server:
     """Continuous-batching server over `slots` concurrent runtimes."""
 
-    def __init__(self, slots=4, device=0, budget_fraction=0.8, budget_bytes=None, share_sms=True,
+    def __init__(self, slots=4, device=0, budget_fraction=0.8, budget_bytes=None, share_sms=False,
                  protocol="quick"):
         torch = _torch()
         self.protocol = protocol
@@ -166,8 +166,11 @@ class Server:
         free, _ = torch.cuda.mem_get_info(device)
         self.budget = int(budget_bytes if budget_bytes is not None else free * budget_fraction)
         self.device = device
-        # with several slots, each slot's grids are sized for its share of the
-        # SMs so concurrent requests' kernels stay resident side by side
+        # share_sms: with several slots, each slot's grids are sized for its
+        # share of the SMs so concurrent requests' kernels stay resident side by
+        # side. That pays for long requests (radix sorts); with quicksort the
+        # requests are short and a slot running at a fraction of the GPU
+        # costs more latency than the overlap saves, so it is off by default.
         sms = torch.cuda.get_device_properties(device).multi_processor_count
         limit = sms // slots if (share_sms and slots > 1) else 0
         self.slots = [_Slot(i, device, limit) for i in range(slots)]
