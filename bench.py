@@ -333,10 +333,12 @@ class JoinWorkload:
         self.seed = seed
         self.units = self.na + self.nb
         self.flush_l2 = False
+        self.quick = args.sort_protocol == "quick"
         self.config = {"workload": f"3PC PK-FK join + group-by: A {self.na} rows (pk perm, Zipf(1.1, 10^4) "
                                    f"group, value U[0,10^6)), B {self.nb} rows (fk U over pk, qty U[1,50]); "
                                    "inner_join copy g, value; vq = value*qty; aggregate by g: sum(vq), count",
-                       "rows_per_gpu": self.units, "l2": "inputs larger than L2", "seed": seed}
+                       "rows_per_gpu": self.units, "l2": "inputs larger than L2", "seed": seed,
+                       "sort_protocol": args.sort_protocol}
 
     def setup(self, rt, orq):
         import numpy as np
@@ -344,14 +346,15 @@ class JoinWorkload:
         from orq_b200.table import EncodedTable
 
         self.orq, self.rt, self.np, self.ET = orq, rt, np, EncodedTable
+        self.proto = orq.SortingProtocol.QUICKSORT if self.quick else orq.SortingProtocol.RADIXSORT
         self.data = gen_join(self.seed, self.na, self.nb)
         pk, g, v, fk, q = self.data
-        self.A0 = EncodedTable.secret_share(rt, [pk, g, v], ["[K]", "[G]", "V"])
-        self.B0 = EncodedTable.secret_share(rt, [fk, q], ["[K]", "Q"])
+        self.A0 = EncodedTable.secret_share(rt, [pk, g, v], ["[K]", "[G]", "V"], protocol=self.proto)
+        self.B0 = EncodedTable.secret_share(rt, [fk, q], ["[K]", "Q"], protocol=self.proto)
 
     def _copy(self, t):
         cols = {k: type(t[k])(self.rt, t[k].shares.clone()) for k in t.getColumnNames()}
-        return self.ET(self.rt, cols, t.rows)
+        return self.ET(self.rt, cols, t.rows, protocol=self.proto)
 
     def _pipeline(self, A, B):
         ag = self.orq.aggregators
@@ -391,8 +394,9 @@ class JoinWorkload:
             d.copy_(h, non_blocking=True)
         rt, ET = self.rt, self.ET
         A = ET(rt, {"[K]": rt.secret_share_b(self.dbuf[0], 0), "[G]": rt.secret_share_b(self.dbuf[1], 0),
-                    "V": rt.secret_share_a(self.dbuf[2], 0)}, self.na)
-        B = ET(rt, {"[K]": rt.secret_share_b(self.dbuf[3], 0), "Q": rt.secret_share_a(self.dbuf[4], 0)}, self.nb)
+                    "V": rt.secret_share_a(self.dbuf[2], 0)}, self.na, protocol=self.proto)
+        B = ET(rt, {"[K]": rt.secret_share_b(self.dbuf[3], 0), "Q": rt.secret_share_a(self.dbuf[4], 0)}, self.nb,
+               protocol=self.proto)
         J = self._pipeline(A, B)
         # open every column (the result table) and copy it to pinned host memory
         names = J.getColumnNames()
@@ -412,9 +416,10 @@ class JoinWorkload:
 
     def cpu_reference(self, sample, threads):
         na = max(64, sample)
-        sec = run_ref_seconds("join_time", na, self.seed, 64, threads)
+        sec = run_ref_seconds("join_time", na, self.seed, 64, threads, quick_tables=self.quick)
+        kind = "quicksort" if self.quick else "radix sort"
         return 5 * na / sec, sec, (f"A={na}, B={4 * na} rows of the same distributions (bounded sample), ORQ's "
-                              f"own inner_join + product + aggregate (radix sort protocol), 3 party processes "
+                              f"own inner_join + product + aggregate ({kind} protocol), 3 party processes "
                               f"x {threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
 
 
@@ -772,8 +777,8 @@ def main():
     ap.add_argument("--share-sms", type=int, default=0,
                     help="serve: partition the SMs between slots (1) or let every slot use all of them (0)")
     ap.add_argument("--sort-protocol", default="quick", choices=["quick", "radix"],
-                    help="serve: sort protocol of sort requests and table sorts (the reference's default "
-                         "is quicksort)")
+                    help="serve and join: sort protocol of sort requests and table sorts (the reference's "
+                         "default is quicksort)")
     args = ap.parse_args()
     if args.workload == "join" and args.cpu_sample == 1 << 17:
         args.cpu_sample = 1 << 11
