@@ -311,25 +311,30 @@ void quicksort_rounds(Ctx& c, size_t n, Sh3 P) {
     for (size_t round = 0; num_pivots < n; round++) {
         if (round > 4 * n + 64) throw std::runtime_error("quicksort did not converge");
         const uint32_t size = (uint32_t)(n - num_pivots);
-        ProfScope ps(c, "quicksort_round", 0.0);
-        k_qs_part<0><<<chunks, kQsThreads, 0, c.stream>>>(a);
-        k_qs_top<<<1, kQsThreads, 0, c.stream>>>(a);
-        k_qs_heads<<<chunks, kQsThreads, 0, c.stream>>>(a);
         Sh3 R = split(rbuf, size), PV = split(pvbuf, size), E = split(ebuf, size), G = split(gbuf, size);
-        k_qs_gather<PW><<<plain_grid(c, size), 256, 0, c.stream>>>(a, cc(cur), R, PV, size);
-        ORQ_CUDA_CHECK(cudaGetLastError());
-        c.kernels_launched += 4;
+        {
+            ProfScope ps(c, "quicksort_round", 0.0);
+            k_qs_part<0><<<chunks, kQsThreads, 0, c.stream>>>(a);
+            k_qs_top<<<1, kQsThreads, 0, c.stream>>>(a);
+            k_qs_heads<<<chunks, kQsThreads, 0, c.stream>>>(a);
+            k_qs_gather<PW><<<plain_grid(c, size), 256, 0, c.stream>>>(a, cc(cur), R, PV, size);
+            ORQ_CUDA_CHECK(cudaGetLastError());
+            c.kernels_launched += 4;
+        }
         // reduced._compare(pivot): gt = row > pivot, opened
         op_compare(c, PW, size, cc(R), cc(PV), E, G);
         op_open(c, false, PW, size, cc(G), obuf.p);
-        k_qs_bits<PW><<<plain_grid(c, size), 256, 0, c.stream>>>(a, obuf.as<uint8_t>(), size);
-        k_qs_part<1><<<chunks, kQsThreads, 0, c.stream>>>(a);
-        k_qs_top<<<1, kQsThreads, 0, c.stream>>>(a);
-        k_qs_zeros<<<chunks, kQsThreads, 0, c.stream>>>(a);
-        k_qs_seg<<<gg, 256, 0, c.stream>>>(a);
-        k_qs_move<PW><<<gg, 256, 0, c.stream>>>(a, cc(cur), nxt);
-        ORQ_CUDA_CHECK(cudaGetLastError());
-        c.kernels_launched += 6;
+        {
+            ProfScope ps(c, "quicksort_round", 0.0);
+            k_qs_bits<PW><<<plain_grid(c, size), 256, 0, c.stream>>>(a, obuf.as<uint8_t>(), size);
+            k_qs_part<1><<<chunks, kQsThreads, 0, c.stream>>>(a);
+            k_qs_top<<<1, kQsThreads, 0, c.stream>>>(a);
+            k_qs_zeros<<<chunks, kQsThreads, 0, c.stream>>>(a);
+            k_qs_seg<<<gg, 256, 0, c.stream>>>(a);
+            k_qs_move<PW><<<gg, 256, 0, c.stream>>>(a, cc(cur), nxt);
+            ORQ_CUDA_CHECK(cudaGetLastError());
+            c.kernels_launched += 6;
+        }
         std::swap(cur, nxt);
         ORQ_CUDA_CHECK(cudaMemcpyAsync(&num_pivots, a.npiv, 4, cudaMemcpyDeviceToHost, c.stream));
         ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));
