@@ -84,9 +84,10 @@ constexpr int kHalfBlocks = kBlocksPerThread / 2;  // blocks per thread per half
 
 __global__ void __launch_bounds__(kGenThreads, 1) k_fy_gen(FyGenArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
-    __shared__ uint32_t red[33];
     __shared__ uint32_t sdone;
     __shared__ uint32_t sbase[kMaxLevels];
+    __shared__ uint32_t wsum[kGenThreads / 32][kMaxLevels / 2];  // per-warp packed level counts
+    __shared__ uint32_t htot[kMaxLevels / 2];                    // half-tile totals
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const uint32_t total = 3 * a.tiles;
@@ -112,39 +113,70 @@ __global__ void __launch_bounds__(kGenThreads, 1) k_fy_gen(FyGenArgs a) {
                 v[4 * b + 3] = ks.w & a.mask;
             }
             if (half == 1 && threadIdx.x == kGenThreads - 1) a.last[slot] = v[4 * kHalfBlocks - 1];
-            // two levels per block-wide scan (16-bit fields; half-tile totals <= 16384)
-            for (uint32_t L = 0; L < a.lay.nl; L += 2) {
-                const uint32_t t0 = level_threshold(a.n, L);
-                const uint32_t t1 = L + 1 < a.lay.nl ? level_threshold(a.n, L + 1) : 0u;
-                uint32_t c0 = 0, c1 = 0;
+            // every level at once (nested lists: level L keeps v < n >> 2L):
+            // per-thread counts two levels per word (16-bit fields; half-tile
+            // totals <= 16384), one block-wide scan for all of them
+            constexpr int kPk = kMaxLevels / 2;
+            uint32_t pc[kPk], ex[kPk];
 #pragma unroll
-                for (int k = 0; k < 4 * kHalfBlocks; k++) {
-                    c0 += v[k] < t0;
-                    c1 += v[k] < t1;
+            for (int j = 0; j < kPk; j++) pc[j] = 0;
+#pragma unroll
+            for (int L = 0; L < kMaxLevels; L++) {
+                if (L < (int)a.lay.nl) {
+                    const uint32_t th = level_threshold(a.n, L);
+                    uint32_t c = 0;
+#pragma unroll
+                    for (int k = 0; k < 4 * kHalfBlocks; k++) c += v[k] < th;
+                    pc[L >> 1] |= c << (16 * (L & 1));
                 }
-                uint32_t tot;
-                const uint32_t pre = block_excl_sum(c0 | (c1 << 16), red, tot);
-                for (int h = 0; h < 2 && L + h < a.lay.nl; h++) {
-                    const uint32_t Lh = L + h, th = h ? t1 : t0;
-                    const uint32_t base = sbase[Lh];
-                    uint32_t o = base + (h ? (pre >> 16) : (pre & 0xffffu));
-                    const uint32_t tt = h ? (tot >> 16) : (tot & 0xffffu);
-                    if (base + tt > a.lay.cap[Lh]) {
-                        if (threadIdx.x == 0) atomicOr(a.err, 16);
-                        continue;
-                    }
-                    uint32_t* olv = ov + a.lay.off[Lh];
+            }
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+            for (int j = 0; j < kPk; j++) {
+                uint32_t inc = pc[j];
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += y;
+                }
+                ex[j] = inc - pc[j];
+                if (lane == 31) wsum[warp][j] = inc;
+            }
+            __syncthreads();
+            if (threadIdx.x < kPk) {  // exclusive offsets of the warps, and the totals
+                uint32_t run = 0;
+                for (int w = 0; w < kGenThreads / 32; w++) {
+                    const uint32_t t = wsum[w][threadIdx.x];
+                    wsum[w][threadIdx.x] = run;
+                    run += t;
+                }
+                htot[threadIdx.x] = run;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int L = 0; L < kMaxLevels; L++) {
+                if (L >= (int)a.lay.nl) break;
+                const int sh = 16 * (L & 1);
+                const uint32_t mine = (pc[L >> 1] >> sh) & 0xffffu;
+                const uint32_t pre = ((ex[L >> 1] + wsum[warp][L >> 1]) >> sh) & 0xffffu;
+                const uint32_t tt = (htot[L >> 1] >> sh) & 0xffffu;
+                const uint32_t base = sbase[L];
+                if (base + tt > a.lay.cap[L]) {
+                    if (threadIdx.x == 0) atomicOr(a.err, 16);
+                    continue;
+                }
+                if (mine) {
+                    const uint32_t th = level_threshold(a.n, L);
+                    uint32_t* olv = ov + a.lay.off[L] + base + pre;
+                    uint32_t o = 0;
 #pragma unroll
                     for (int k = 0; k < 4 * kHalfBlocks; k++)
                         if (v[k] < th) olv[o++] = v[k];
                 }
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    sbase[L] += tot & 0xffffu;
-                    if (L + 1 < a.lay.nl) sbase[L + 1] += tot >> 16;
-                }
-                __syncthreads();
             }
+            __syncthreads();  // every thread has read sbase
+            if (threadIdx.x < a.lay.nl) sbase[threadIdx.x] += (htot[threadIdx.x >> 1] >> (16 * (threadIdx.x & 1))) & 0xffffu;
+            __syncthreads();
         }
         // an overflowing level was flagged above; its count is clamped so the
         // scanner never reads past the level's list
@@ -190,7 +222,8 @@ constexpr int kScanWarps = kScanThreads / 32;
 constexpr int kFyStats = 10;  // diagnostic counters per group
 constexpr int kQuads = kPerThread / 4;  // lane-quads per thread and step
 constexpr uint32_t kUncCap = 2048;
-constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4;
+// dynamic shared memory: the step's entries, then a 128-entry staging run per warp
+constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4 + (size_t)kScanWarps * 128 * 4;
 
 // entries per step at level L: uncertain entries of a step are about
 // cs^2 / (2 n/4^L); keep that near 512
@@ -460,19 +493,24 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             st_unc += tot_u;
             st_cyc_unc += clock64() - t_u0;
         }
-        // ---- accept, rank, store (a lane's accepted entries go to consecutive
-        // ranks, consecutive lanes to consecutive runs)
+        // ---- accept, rank, store. The accepted entries of one warp iteration
+        // (128 consecutive entries) hold consecutive ranks [lo, hi): they are
+        // placed in a per-warp staging run in shared memory and stored as
+        // whole 128-byte lines.
         const unsigned long long t_a0 = clock64();
         const uint32_t tot_a = tot_c + s_uacc;
         const uint32_t need = n - i;
         uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
         {
             uint32_t rc = cbase, ru = ubase;
-#pragma unroll
+            uint32_t* stg = sv + kMaxStepEntries + warp * 128;  // this warp's staging run
+#pragma unroll 1
             for (int u = 0; u < kQuads; u++) {
                 const uint32_t code = codes[warp][u][lane];
                 uint32_t ex, tot;
                 quad_prefix(code, lane, ex, tot);
+                const uint32_t lo = rc + unc_pre[ru];
+                const uint32_t hi = rc + (tot & 0xffffu) + unc_pre[ru + (tot >> 16)];
                 if (code) {
                     const uint32_t q = q0 + 128u * u;
                     const uint4 v4 = *reinterpret_cast<const uint4*>(sv + q);
@@ -483,15 +521,16 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                         const bool cert = (code >> r) & 1u, unc = (code >> (4 + r)) & 1u;
                         if (cert || (unc && unc_cp[k])) {
                             const uint32_t rank = c + unc_pre[k];
-                            if (rank < need) {
-                                acc[i + rank] = vv[r];
-                                if (rank == need - 1) s_last_q = q + r;
-                            }
+                            stg[rank - lo] = vv[r];
+                            if (rank == need - 1) s_last_q = q + r;
                         }
                         c += cert;
                         k += unc;
                     }
                 }
+                __syncwarp();
+                for (uint32_t j = lane; lo + j < hi && lo + j < need; j += 32) acc[i + lo + j] = stg[j];
+                __syncwarp();  // the run is rewritten by the next iteration
                 rc += tot & 0xffffu;
                 ru += tot >> 16;
             }
@@ -819,8 +858,11 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
 
     FyLayout lay{};
     {
-        uint32_t nl = 0;
-        while (nl < (uint32_t)kMaxLevels && level_threshold((uint32_t)n, nl) >= 1) nl++;
+        // levels down to a threshold of 256: sparser ones would hold almost
+        // nothing, and the scan of a permutation's last steps reads at most a
+        // few thousand entries of the last level instead
+        uint32_t nl = 1;
+        while (nl < (uint32_t)kMaxLevels && level_threshold((uint32_t)n, nl) >= 256) nl++;
         lay.nl = nl;
         uint32_t o = 0;
         for (uint32_t L = 0; L < nl; L++) {
