@@ -222,8 +222,7 @@ constexpr int kScanWarps = kScanThreads / 32;
 constexpr int kFyStats = 10;  // diagnostic counters per group
 constexpr int kQuads = kPerThread / 4;  // lane-quads per thread and step
 constexpr uint32_t kUncCap = 2048;
-// dynamic shared memory: the step's entries, then a 128-entry staging run per warp
-constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4 + (size_t)kScanWarps * 128 * 4;
+constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4;
 
 // entries per step at level L: uncertain entries of a step are about
 // cs^2 / (2 n/4^L); keep that near 512
@@ -493,24 +492,19 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             st_unc += tot_u;
             st_cyc_unc += clock64() - t_u0;
         }
-        // ---- accept, rank, store. The accepted entries of one warp iteration
-        // (128 consecutive entries) hold consecutive ranks [lo, hi): they are
-        // placed in a per-warp staging run in shared memory and stored as
-        // whole 128-byte lines.
+        // ---- accept, rank, store (a lane's accepted entries go to consecutive
+        // ranks, consecutive lanes to consecutive runs)
         const unsigned long long t_a0 = clock64();
         const uint32_t tot_a = tot_c + s_uacc;
         const uint32_t need = n - i;
         uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
         {
             uint32_t rc = cbase, ru = ubase;
-            uint32_t* stg = sv + kMaxStepEntries + warp * 128;  // this warp's staging run
-#pragma unroll 1
+#pragma unroll
             for (int u = 0; u < kQuads; u++) {
                 const uint32_t code = codes[warp][u][lane];
                 uint32_t ex, tot;
                 quad_prefix(code, lane, ex, tot);
-                const uint32_t lo = rc + unc_pre[ru];
-                const uint32_t hi = rc + (tot & 0xffffu) + unc_pre[ru + (tot >> 16)];
                 if (code) {
                     const uint32_t q = q0 + 128u * u;
                     const uint4 v4 = *reinterpret_cast<const uint4*>(sv + q);
@@ -521,16 +515,15 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                         const bool cert = (code >> r) & 1u, unc = (code >> (4 + r)) & 1u;
                         if (cert || (unc && unc_cp[k])) {
                             const uint32_t rank = c + unc_pre[k];
-                            stg[rank - lo] = vv[r];
-                            if (rank == need - 1) s_last_q = q + r;
+                            if (rank < need) {
+                                acc[i + rank] = vv[r];
+                                if (rank == need - 1) s_last_q = q + r;
+                            }
                         }
                         c += cert;
                         k += unc;
                     }
                 }
-                __syncwarp();
-                for (uint32_t j = lane; lo + j < hi && lo + j < need; j += 32) acc[i + lo + j] = stg[j];
-                __syncwarp();  // the run is rewritten by the next iteration
                 rc += tot & 0xffffu;
                 ru += tot >> 16;
             }
