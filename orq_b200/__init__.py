@@ -186,6 +186,15 @@ class Runtime:
         """Wrap existing (3, n) device shares."""
         return (ASharedVector if arith else BSharedVector)(self, shares)
 
+    def input_secret_shares(self, paths, n: int, width: int, arith: bool = False):
+        """BSharedVector / ASharedVector(size, file) (e_vector.h:300-348) for
+        all three parties: paths[p] is party p's share file (orq_b200.io)."""
+        from . import io
+
+        S = io.read_party_shares(paths, n, width)
+        return self.from_shares(self._to_dev(S.view({1: np.int8, 2: np.int16, 4: np.int32,
+                                                        8: np.int64}[width]), width), arith)
+
     # -- randomness -------------------------------------------------------
     def keystream(self, stream: int, nonce0: int, nbytes: int):
         torch = _torch()
@@ -259,6 +268,13 @@ class SharedVector:
 
     def clone(self):
         return type(self)(self.rt, self.shares.clone())
+
+    def outputSecretShares(self, paths):
+        """EVector::output (e_vector.h:249-266) for all three parties: party p
+        writes its replicated shares (S[p], S[p+1]) to paths[p]."""
+        from . import io
+
+        io.write_party_shares(self.shares.cpu().numpy(), paths)
 
 
 class BSharedVector(SharedVector):

@@ -33,13 +33,13 @@ def is_bshared(name: str) -> bool:
 
 
 class EncodedTable:
-    """orq::relational::EncodedTable<int64_t> (8-byte shares)."""
-
-    WIDTH = 8
+    """orq::relational::EncodedTable<int64_t> (8-byte shares; `width` 4 gives
+    EncodedTable<int32_t>)."""
 
     def __init__(self, rt, columns: dict | None = None, rows: int = 0, name: str = "",
-                 protocol: int = SortingProtocol.DEFAULT):
+                 protocol: int = SortingProtocol.DEFAULT, width: int = 8):
         self.rt = rt
+        self.WIDTH = width
         self.tableName = name
         # SortingProtocol of this table's sorts (the reference fixes it with
         # DEFAULT_SORT_PROTO); tables derived from it inherit it
@@ -53,16 +53,78 @@ class EncodedTable:
     # ---- construction ----------------------------------------------------
     @classmethod
     def secret_share(cls, rt, columns, names, party: int = 0, name: str = "",
-                     protocol: int = SortingProtocol.DEFAULT):
+                     protocol: int = SortingProtocol.DEFAULT, width: int = 8):
         """secret_share(columns, schema) (encoded_table.h:1687-1707) + the
         EncodedTable(contents) constructor (encoded_table.h:252-265)."""
         assert len(columns) == len(names)
         cols = {}
         for data, nm in zip(columns, names):
-            d = np.ascontiguousarray(np.asarray(data).astype(np.int64))
+            d = np.ascontiguousarray(np.asarray(data).astype(np.int32 if width == 4 else np.int64))
             cols[nm] = (rt.secret_share_b if is_bshared(nm) else rt.secret_share_a)(d, party)
         rows = len(columns[0]) if columns else 0
-        return cls(rt, cols, rows, name, protocol)
+        return cls(rt, cols, rows, name, protocol, width)
+
+    @classmethod
+    def with_schema(cls, rt, names, rows: int, name: str = "", protocol: int = SortingProtocol.DEFAULT,
+                    width: int = 8):
+        """EncodedTable(name, schema, size): zero columns and every row valid."""
+        t = cls(rt, {}, rows, name, protocol, width)
+        for nm in names:
+            t.add_column(nm)
+        return t
+
+    # ---- share files (orq_b200.io; encoded_table.h:382-590) -----------------
+    def inputCSVTableData(self, path, party: int = 0):
+        """inputCSVTableData (encoded_table.h:396-483): the input party reads a
+        plaintext CSV (header of column names), the valid column becomes 1 for
+        the rows read unless the file has it, and every column, in schema
+        order, is secret-shared by that party."""
+        from . import io
+
+        names = self.getColumnNames()
+        data, nread = io.read_csv_table(path, names, self.rows)
+        if VALID not in data:
+            v = np.zeros(self.rows, dtype=np.int64)
+            v[:nread] = 1
+            data[VALID] = v
+        for k in names:
+            d = data.get(k, np.zeros(self.rows, dtype=np.int64)).astype(self._sdtype())
+            self.schema[k] = (self.rt.secret_share_b if is_bshared(k) else self.rt.secret_share_a)(d, party)
+
+    def inputCSVTableSecretShares(self, paths):
+        """inputCSVTableSecretShares (encoded_table.h:495-562) for the three
+        parties' files; when the files have no valid column, the rows read are
+        made valid by party 0 secret-sharing ones."""
+        from . import io
+
+        cols, nread = io.read_table_shares(paths, self.rows, self.WIDTH)
+        for k, S in cols.items():
+            assert k in self.schema, f"column '{k}' not found"
+            self.schema[k] = type(self.schema[k])(self.rt, self.rt._to_dev(S.view(self._sdtype()), self.WIDTH))
+        if VALID in self.schema and VALID not in cols:
+            ones = self.rt.secret_share_b(np.ones(nread, dtype=self._sdtype()), 0)
+            self.schema[VALID].shares[:, :nread] = ones.shares
+
+    def outputCSVTableSecretShares(self, paths):
+        """outputCSVTableSecretShares (encoded_table.h:564-606): every column
+        in schema order, header NAME_r, one file per party."""
+        from . import io
+
+        io.write_table_shares({k: self.schema[k].shares.cpu().numpy() for k in self.getColumnNames()},
+                              self.rows, paths)
+
+    def inputSecretShares(self, column, paths):
+        """inputSecretShares (encoded_table.h:382-388): a column from vector
+        share files."""
+        v = self.rt.input_secret_shares(paths, self.rows, self.WIDTH, not is_bshared(column))
+        self.schema[column] = v
+
+    def outputSecretShares(self, column, paths):
+        """outputSecretShares (encoded_table.h:608-620)."""
+        self.schema[column].outputSecretShares(paths)
+
+    def _sdtype(self):
+        return np.int32 if self.WIDTH == 4 else np.int64
 
     def _zeros(self, name, n):
         t = self.rt._alloc(n, self.WIDTH)
@@ -149,7 +211,7 @@ class EncodedTable:
         new_schema = [JOIN_ID] + [c for c in self.getColumnNames() if c != JOIN_ID]
         new_schema += [c for c in other.getColumnNames() if c not in self.schema]
         n = self.rows + other.rows
-        t = EncodedTable(self.rt, {}, n, self.tableName + "+" + other.tableName, self.protocol)
+        t = EncodedTable(self.rt, {}, n, self.tableName + "+" + other.tableName, self.protocol, self.WIDTH)
         for c in new_schema:
             if c not in t.schema:
                 t.add_column(c)
@@ -158,7 +220,7 @@ class EncodedTable:
         for c in other.getColumnNames():
             t.schema[c].shares[:, self.rows:n] = other.schema[c].shares
         # table id 1 for the other table's rows: one secret-shared 1, repeated
-        one = self.rt.secret_share_b(np.ones(1, dtype=np.int64), 0)
+        one = self.rt.secret_share_b(np.ones(1, dtype=self._sdtype()), 0)
         t.schema[JOIN_ID].shares[:, self.rows:n] = one.shares[:, :1]
         return t
 

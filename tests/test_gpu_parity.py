@@ -646,3 +646,45 @@ def test_encoded_table_sort_protocols(orq, protocol):
         got = dict(zip(names, (c.view(np.int64) for c in cols)))
         assert np.array_equal(np.sort(got["[K1]"], kind="stable"), got["[K1]"])
         assert sorted(got["V"].tolist()) == sorted(v.tolist())
+
+
+def test_share_files_through_the_runtime(orq, tmp_path):
+    """ORQ's employees share files (tests/test_io.cpp:30-110) loaded into
+    device vectors and tables: opened values, a bitonic sort of the ages, a
+    table read from plaintext by party 0, and written shares read back"""
+    import os
+
+    from orq_b200.table import EncodedTable
+
+    d = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "io")
+    P = lambda stem: [os.path.join(d, f"{stem}_3pc_{p}.csv") for p in range(3)]
+    rows = [list(map(int, ln.split(","))) for ln in open(os.path.join(d, "employees.csv")).read().split()[1:]]
+    emp, reg, age = (np.array(c, dtype=np.int32) for c in zip(*rows))
+    ages32 = np.zeros(32, dtype=np.int32)
+    ages32[:len(age)] = age
+    rt = orq.Runtime(seed=3)
+    v = rt.input_secret_shares(P("employees_age_secrets"), 32, 4)
+    assert np.array_equal(v.open().cpu().numpy(), ages32)
+    orq.bitonic_sort(v, orq.ASC)
+    assert np.array_equal(v.open().cpu().numpy(), np.sort(ages32))
+    out = [str(tmp_path / f"sorted_{p}.csv") for p in range(3)]
+    v.outputSecretShares(out)
+    w = rt.input_secret_shares(out, 32, 4)
+    assert np.array_equal(w.open().cpu().numpy(), np.sort(ages32))
+    names = ["[EMPLOYEE_ID]", "[REGION]", "[AGE]"]
+    for how in ("shares", "plaintext"):
+        T = EncodedTable.with_schema(rt, names, 32, width=4)
+        if how == "shares":
+            T.inputCSVTableSecretShares(P("employees_secrets"))
+        else:
+            T.inputCSVTableData(os.path.join(d, "employees.csv"), 0)
+        cols, nm = T.open_with_schema()
+        got = dict(zip(nm, (c.view(np.int32) for c in cols)))
+        assert np.array_equal(got["[AGE]"], age) and np.array_equal(got["[EMPLOYEE_ID]"], emp)
+        assert np.array_equal(got["[REGION]"], reg)
+    tout = [str(tmp_path / f"t_{p}.csv") for p in range(3)]
+    T.outputCSVTableSecretShares(tout)
+    U = EncodedTable.with_schema(rt, names, 32, width=4)
+    U.inputCSVTableSecretShares(tout)
+    for k in T.getColumnNames():
+        assert np.array_equal(U[k].shares.cpu().numpy(), T[k].shares.cpu().numpy()), k
