@@ -209,6 +209,15 @@ int orqcu_compare_rows(orqcu_runtime* rt, int width, size_t n, int nkeys, const 
  * not alias. One fused launch. */
 int orqcu_swap(orqcu_runtime* rt, int arith, int width, size_t n, int ncols, void* const* x,
                void* const* y, const void* const bits[3]);
+/* operators::shuffle(data_a, data_b, size) (shuffle.h:769-786), as
+ * EncodedTable::shuffle uses it: one random elementwise permutation (the
+ * public identity at the columns' width, B-shared, under a sharded
+ * permutation) applied with oblivious_apply_elementwise_perm to every
+ * A-shared column (data_a[3*k+p]) and then every B-shared column. Synchronous. */
+int orqcu_table_shuffle(orqcu_runtime* rt, int width, size_t n, int na, void* const* data_a, int nb,
+                        void* const* data_b);
+/* BSharedVector::mask(m) (b_shared_vector.h:462-464): every share &= m (local). */
+int orqcu_mask_b(orqcu_runtime* rt, int width, size_t n, void* const shares[3], uint64_t mask);
 /* BSharedVector::extend_lsb (b_shared_vector.h:145-147): every share becomes
  * all ones where its LSB is set, else zero. Local. */
 int orqcu_extend_lsb(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);

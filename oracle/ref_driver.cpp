@@ -193,6 +193,30 @@ int main(int argc, char** argv) {
         }
         auto T = J.open_with_schema();
         for (size_t k = 0; k < T.second.size(); k++) d.plain("open_" + T.second[k], T.first[k]);
+    } else if (op == "tshuffle") {
+        // EncodedTable<int64_t> {[A], [B] (< 256), V (u32), [F] (bits)}:
+        // filter on [F] (those rows invalid), then finalize(): shuffle() and
+        // mask() of every column; each column dumped, and the open
+        uint64_t st = seed;
+        auto a = gen<int64_t>(n, st, ~0ull);
+        auto b = gen<int64_t>(n, st, 0xff);
+        auto v = gen<int64_t>(n, st, 0xffffffffull);
+        auto f = gen<int64_t>(n, st, 1);
+        std::vector<orq::Vector<int64_t>> cols = {a, b, v, f};
+        EncodedTable<int64_t> T = secret_share(cols, {"[A]", "[B]", "V", "[F]"});
+        T.filter(T["[F]"]);
+        T.finalize();
+        for (auto& name : T.getColumnNames()) {
+            if (EncodedTable<int64_t>::isBShared(name)) {
+                auto c = T.asBSharedVector(name);
+                d.shares(name, c);
+            } else {
+                auto c = T.asASharedVector(name);
+                d.shares(name, c);
+            }
+        }
+        auto O = T.open_with_schema(false);
+        for (size_t k = 0; k < O.second.size(); k++) d.plain("open_" + O.second[k], O.first[k]);
     } else if (op == "tsort" || op == "tsort_qs" || op == "distinct") {
         // tsort (tsort_qs): operators::table_sort with the radix (quicksort)
         // protocol on three key columns [bit ASC, small-int DESC, bit ASC] plus

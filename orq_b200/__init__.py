@@ -312,6 +312,12 @@ class BSharedVector(SharedVector):
                                             _p3(inp.shares), _p3(self.shares)))
         return self
 
+    def mask(self, m: int):
+        """BSharedVector::mask (b_shared_vector.h:462-464): shares &= m, in place."""
+        _check(self.rt.lib.orqcu_mask_b(self.rt.h, self.width, ctypes.c_size_t(self.size()), _p3(self.shares),
+                                        ctypes.c_uint64(m & ((1 << (8 * self.width)) - 1))))
+        return self
+
     def b2a_bit(self) -> "ASharedVector":
         """b2a_bit (b_shared_vector.h:279-284, replicated_3pc.h:220-251)."""
         z = self.rt._alloc(self.size(), self.width)
@@ -452,6 +458,15 @@ def bitonic_sort(columns, data_a=(), data_b=(), order=ASC):
     _check(rt.lib.orqcu_bitonic_sort_rows(rt.h, w, ctypes.c_size_t(n), len(columns), _flat(columns),
                                           (ctypes.c_int * len(columns))(*[int(o == DESC) for o in orders]),
                                           len(data_a), _flat(data_a), len(data_b), _flat(data_b)))
+
+
+def shuffle_columns(data_a, data_b):
+    """orq::operators::shuffle(data_a, data_b, size) (shuffle.h:769-786): the
+    rows of every column permuted by one random secret permutation, in place."""
+    first = (list(data_a) + list(data_b))[0]
+    rt, n, w = first.rt, first.size(), first.width
+    _check(rt.lib.orqcu_table_shuffle(rt.h, w, ctypes.c_size_t(n), len(data_a), _flat(data_a), len(data_b),
+                                      _flat(data_b)))
 
 
 def compare_rows(x_vec, y_vec, order) -> BSharedVector:

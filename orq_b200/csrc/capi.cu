@@ -545,6 +545,36 @@ int orqcu_not_b_1(orqcu_runtime* rt, int width, size_t n, const void* const x[3]
     });
 }
 
+int orqcu_table_shuffle(orqcu_runtime* rt, int width, size_t n, int na, void* const* data_a, int nb,
+                        void* const* data_b) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "table shuffle supports 4 and 8-byte columns");
+        need(na >= 0 && nb >= 0 && (na == 0 || data_a) && (nb == 0 || data_b), "bad data columns");
+        need(n < (1ull << 31), "table shuffle supports n < 2^31");
+        std::vector<orqcu::Sh3> a(na), b(nb);
+        for (int i = 0; i < na; i++) {
+            need_sh((const void* const*)data_a + 3 * i, n, "null data column");
+            a[i] = m3(data_a + 3 * i);
+        }
+        for (int i = 0; i < nb; i++) {
+            need_sh((const void* const*)data_b + 3 * i, n, "null data column");
+            b[i] = m3(data_b + 3 * i);
+        }
+        orqcu::op_table_shuffle(rt->ctx, width, n, na, a.data(), nb, b.data());
+        rt->ctx.check_device_error();
+    });
+}
+
+int orqcu_mask_b(orqcu_runtime* rt, int width, size_t n, void* const shares[3], uint64_t mask) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "mask supports 4 and 8-byte shares");
+        need_sh((const void* const*)shares, n, "null shares");
+        orqcu::op_mask_b(rt->ctx, width, n, m3(shares), mask);
+    });
+}
+
 int orqcu_extend_lsb(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]) {
     return guard([&] {
         need_rt(rt);

@@ -222,6 +222,8 @@ void op_not1(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
 void sort_padded(Ctx& c, int kw, size_t n, Sh3 key, bool desc, Sh3 perm_out, size_t reserve,
                  const std::function<void(Sh3 P, int PW)>& body);
 void op_quicksort(Ctx& c, int kw, size_t n, Sh3 key, bool desc, Sh3 perm_out);
+void op_table_shuffle(Ctx& c, int w, size_t n, int na, const Sh3* data_a, int nb, const Sh3* data_b);
+void op_mask_b(Ctx& c, int w, size_t n, Sh3 s, unsigned long long m);
 void op_compare_rows(Ctx& c, int w, size_t n, int nkeys, const CSh3* x, const CSh3* y, const int* desc, Sh3 gt);
 void op_swap(Ctx& c, int w, size_t n, bool arith, int ncols, const Sh3* x, const Sh3* y, CSh3 bits);
 void op_extend_lsb(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);

@@ -140,6 +140,40 @@ __global__ void __launch_bounds__(kAesThreads) k_distinct(DistinctArgs a) {
     }
 }
 
+// ElementwisePermutation(size, BShared) (permutation.h:62-69): the identity,
+// public-shared (S0 = i, S1 = S2 = 0) at width W
+template <typename T>
+__global__ void k_identity(Sh3 p, unsigned long long n) {
+    for (unsigned long long i = gtid(); i < n; i += gstride()) {
+        reinterpret_cast<T*>(p.p[0])[i] = (T)i;
+        reinterpret_cast<T*>(p.p[1])[i] = 0;
+        reinterpret_cast<T*>(p.p[2])[i] = 0;
+    }
+}
+
+// an opened permutation of width W narrowed to int32; a value outside [0, n)
+// sets error bit 128 and becomes i (the scatter then keeps every index valid)
+template <typename T>
+__global__ void k_narrow(const void* src, int32_t* dst, unsigned long long n, int* err) {
+    for (unsigned long long i = gtid(); i < n; i += gstride()) {
+        const unsigned long long v = (unsigned long long)reinterpret_cast<const T*>(src)[i];
+        if (v >= n) {
+            atomicOr(err, 128);
+            dst[i] = (int32_t)i;
+        } else {
+            dst[i] = (int32_t)v;
+        }
+    }
+}
+
+// BSharedVector::mask(m) (b_shared_vector.h:462-464): every share &= m
+template <typename T>
+__global__ void k_mask(Sh3 s, unsigned long long n, T m) {
+    for (unsigned long long i = gtid(); i < n; i += gstride())
+#pragma unroll
+        for (int j = 0; j < 3; j++) reinterpret_cast<T*>(s.p[j])[i] &= m;
+}
+
 void copy_sh(Ctx& c, Sh3 dst, CSh3 src, size_t bytes) {
     if (!bytes) return;
     for (int p = 0; p < 3; p++)
@@ -149,6 +183,66 @@ void copy_sh(Ctx& c, Sh3 dst, CSh3 src, size_t bytes) {
 CSh3 cc(Sh3 s) { return CSh3{{s.p[0], s.p[1], s.p[2]}}; }
 
 }  // namespace
+
+// oblivious_apply_elementwise_perm (shuffle.h:687-706) with a B-shared
+// permutation of width pw (the table shuffle's): x and a copy of the
+// permutation are shuffled by the same sharded permutation (x's reshare
+// before the permutation's on every group stream), the permutation is opened
+// and x scattered by it. Composed from the sharded apply, open and scatter.
+static void apply_elementwise_bperm(Ctx& c, bool x_arith, int xw, size_t n, Sh3 x, CSh3 perm, int pw) {
+    ShardedPerm sp = next_perm(c, n);
+    const size_t n1 = std::max<size_t>(n, 1);
+    Scratch cpb(c, 3 * n1 * pw), opened(c, n1 * pw), sig(c, n1 * 4), tmp(c, 3 * n1 * xw);
+    Sh3 P, Xt;
+    for (int j = 0; j < 3; j++) {
+        P.p[j] = cpb.as<uint8_t>() + j * n1 * pw;
+        Xt.p[j] = tmp.as<uint8_t>() + j * n1 * xw;
+    }
+    copy_sh(c, P, perm, n * pw);
+    op_apply_sharded(c, x_arith, xw, n, x, sp, false);
+    op_apply_sharded(c, false, pw, n, P, sp, false);
+    c.free_perm(sp);
+    if (!n) return;
+    op_open(c, false, pw, n, cc(P), opened.p);
+    if (pw == 4) k_narrow<uint32_t><<<plain_grid(c, n), 256, 0, c.stream>>>(opened.p, sig.as<int32_t>(), n, c.d_err);
+    else k_narrow<unsigned long long><<<plain_grid(c, n), 256, 0, c.stream>>>(opened.p, sig.as<int32_t>(), n, c.d_err);
+    ORQ_CUDA_CHECK(cudaGetLastError());
+    c.kernels_launched++;
+    op_scatter(c, xw, n, cc(x), Xt, sig.as<int32_t>());
+    copy_sh(c, x, cc(Xt), n * xw);
+}
+
+void op_table_shuffle(Ctx& c, int w, size_t n, int na, const Sh3* data_a, int nb, const Sh3* data_b) {
+    if (w != 4 && w != 8) throw std::invalid_argument("table shuffle supports 4 and 8-byte columns");
+    // operators::shuffle(data_a, data_b, size) (shuffle.h:769-786): a random
+    // elementwise permutation (the identity under a sharded permutation),
+    // applied to every arithmetic column, then every boolean one
+    ShardedPerm sp = next_perm(c, n);
+    const size_t n1 = std::max<size_t>(n, 1);
+    Scratch pb(c, 3 * n1 * w);
+    Sh3 P;
+    for (int j = 0; j < 3; j++) P.p[j] = pb.as<uint8_t>() + j * n1 * w;
+    if (n) {
+        if (w == 4) k_identity<uint32_t><<<plain_grid(c, n), 256, 0, c.stream>>>(P, n);
+        else k_identity<unsigned long long><<<plain_grid(c, n), 256, 0, c.stream>>>(P, n);
+        ORQ_CUDA_CHECK(cudaGetLastError());
+        c.kernels_launched++;
+    }
+    op_apply_sharded(c, false, w, n, P, sp, false);
+    c.free_perm(sp);
+    for (int k = 0; k < na; k++) apply_elementwise_bperm(c, true, w, n, data_a[k], cc(P), w);
+    for (int k = 0; k < nb; k++) apply_elementwise_bperm(c, false, w, n, data_b[k], cc(P), w);
+}
+
+void op_mask_b(Ctx& c, int w, size_t n, Sh3 s, unsigned long long m) {
+    if (!n) return;
+    const unsigned g = plain_grid(c, n);
+    if (w == 4) k_mask<uint32_t><<<g, 256, 0, c.stream>>>(s, n, (uint32_t)m);
+    else if (w == 8) k_mask<unsigned long long><<<g, 256, 0, c.stream>>>(s, n, m);
+    else throw std::invalid_argument("mask supports 4 and 8-byte shares");
+    ORQ_CUDA_CHECK(cudaGetLastError());
+    c.kernels_launched++;
+}
 
 void op_compose(Ctx& c, size_t n, Sh3 sigma, Sh3 rho) {
     ShardedPerm sp = next_perm(c, n);

@@ -17,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import (ASC, DESC, ASharedVector, BSharedVector, Direction, SortingProtocol, aggregate, aggregators,
-               bitonic_sort, distinct as _distinct, table_sort, _torch)
+               bitonic_sort, distinct as _distinct, multiplex, shuffle_columns, table_sort, _torch)
 
 JOIN_ID = "[##TID]"
 VALID = "[##V]"
@@ -256,6 +256,42 @@ class EncodedTable:
         else:
             table_sort(key_cols, data_a, data_b, orders, single_bit, protocol)
         return self
+
+    # ---- shuffle, mask, finalize (encoded_table.h:170-222,645-652,1003-1018) -
+    def shuffle(self):
+        """EncodedTable::shuffle: every column (arithmetic ones first, then
+        boolean, each in schema order) permuted by one secret permutation."""
+        data_a, data_b = [], []
+        for k in self.getColumnNames():
+            (data_b if is_bshared(k) else data_a).append(self.schema[k])
+        shuffle_columns(data_a, data_b)
+        return self
+
+    def mask(self, mask_column=VALID, keys=None):
+        """EncodedTable::mask: rows whose mask bit is 0 get MASK_VALUE (the
+        share type's maximum) in every other column, via multiplex on the
+        bit (and on its b2a_bit for arithmetic columns); MASK_VALUE is
+        secret-shared once by party 0, arithmetic sharing first."""
+        sel_b = self.schema[mask_column]
+        n = sel_b.size()
+        sel_a = sel_b.b2a_bit()
+        mv = np.array([(1 << (8 * self.WIDTH - 1)) - 1], dtype=self._sdtype())
+        one_a = self.rt.secret_share_a(mv, 0)
+        one_b = self.rt.secret_share_b(mv, 0)
+        full_a = ASharedVector(self.rt, one_a.shares.expand(3, n).contiguous())
+        full_b = BSharedVector(self.rt, one_b.shares.expand(3, n).contiguous())
+        for k in (keys if keys is not None else self.getColumnNames()):
+            if k == mask_column:
+                continue
+            c = self.schema[k]
+            self.schema[k] = multiplex(sel_b, full_b, c) if is_bshared(k) else multiplex(sel_a, full_a, c)
+        return self
+
+    def finalize(self, do_shuffle=True):
+        """EncodedTable::finalize: shuffle (optionally), then mask."""
+        if do_shuffle:
+            self.shuffle()
+        return self.mask()
 
     # ---- distinct (encoded_table.h:1198-1212) -----------------------------
     def distinct_into(self, keys, res):

@@ -76,6 +76,8 @@ CASES = [
     ("qsort32_n30000", "qsort32", 30000, 11, 7, 32, False),
     ("tsort_qs_n64", "tsort_qs", 64, 5, 4, 64, True),
     ("tsort_qs_n3000", "tsort_qs", 3000, 6, 5, 64, False),
+    ("tshuffle_n64", "tshuffle", 64, 7, 2, 64, True),
+    ("tshuffle_n1000", "tshuffle", 1000, 8, 3, 64, False),
 ]
 
 

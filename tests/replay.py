@@ -500,3 +500,28 @@ def same(a, b):
     a = np.ascontiguousarray(a)
     b = np.ascontiguousarray(b)
     return a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+def tshuffle_inputs(n, seed):
+    """Inputs of the "tshuffle" op of ref_driver.cpp."""
+    st = splitmix64_fast(seed, 4 * n)
+    return (st[:n], st[n:2 * n] & np.uint64(0xFF), st[2 * n:3 * n] & np.uint64(0xFFFFFFFF),
+            st[3 * n:] & np.uint64(1))
+
+
+def replay_tshuffle(rt_seed, n, seed):
+    """The "tshuffle" op on the device runtime: an EncodedTable {[A], [B], V,
+    [F]} filtered on [F], then finalize() (shuffle and mask)."""
+    import orq_b200 as orq
+    from orq_b200.table import EncodedTable
+
+    rt = orq.Runtime(seed=rt_seed)
+    cols = tshuffle_inputs(n, seed)
+    T = EncodedTable.secret_share(rt, [c.view(np.int64) for c in cols], ["[A]", "[B]", "V", "[F]"])
+    T.filter(T["[F]"])
+    T.finalize()
+    out = {k: T[k].shares.cpu().numpy().view(np.uint64) for k in T.getColumnNames()}
+    data, names = T.open_with_schema(remove_invalid=False)
+    for k, d in zip(names, data):
+        out["open_" + k] = d.view(np.uint64)[None]
+    return out, cols

@@ -688,3 +688,35 @@ def test_share_files_through_the_runtime(orq, tmp_path):
     U.inputCSVTableSecretShares(tout)
     for k in T.getColumnNames():
         assert np.array_equal(U[k].shares.cpu().numpy(), T[k].shares.cpu().numpy()), k
+
+
+def test_table_finalize_matches_reference_shares(orq, golden, digests):
+    """EncodedTable filter + finalize (shuffle: an elementwise permutation
+    applied to every column; mask: invalid rows set to MASK_VALUE), share for
+    share with the reference; the opened table is the input permuted, with
+    every invalid row masked"""
+    from replay import replay_tshuffle
+
+    for tag, full in (("tshuffle_n64", True), ("tshuffle_n1000", False)):
+        m = digests[tag]["meta"]
+        out, (a, b, v, f) = replay_tshuffle(m["shim_seed"], m["n"], m["data_seed"])
+        for name, arr in out.items():
+            if full:
+                assert same(arr, golden[f"{tag}/{name}"]), (tag, name)
+            else:
+                assert [sha(x) for x in arr] == digests[tag]["arrays"][name], (tag, name)
+    n = 1000
+    valid = out["open_[##V]"][0].astype(bool)
+    mv = np.uint64(2**63 - 1)
+    assert np.all(out["open_[A]"][0][~valid] == mv) and np.all(out["open_V"][0][~valid] == mv)
+    rows_in = sorted(zip(a[f == 1].tolist(), b[f == 1].tolist(), v[f == 1].tolist()))
+    rows_out = sorted(zip(out["open_[A]"][0][valid].tolist(), out["open_[B]"][0][valid].tolist(),
+                          out["open_V"][0][valid].tolist()))
+    assert rows_in == rows_out and valid.sum() == int(f.sum()) and len(valid) == n
+
+
+def test_mask_b(orq):
+    rt = orq.Runtime(seed=2)
+    x = rt.secret_share_b(np.arange(100, dtype=np.int64) * 12345, 0)
+    x.mask(0xFF0F)
+    assert np.array_equal(x.open().cpu().numpy(), (np.arange(100, dtype=np.int64) * 12345) & 0xFF0F)
