@@ -115,6 +115,12 @@ int orqcu_sub_a(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
                 const void* const y[3], void* const z[3]);
 /* not_b (replicated_3pc.h:199). */
 int orqcu_not_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
+/* ASharedVector::a2b (a_shared_vector.h:138-144): arithmetic -> boolean
+ * sharing of the full width (4 or 8): redistribute_shares_b
+ * (replicated_3pc.h:259-262; party 0 secret-shares S0 + S1, party 2 shares S2)
+ * then the boolean ripple-carry adder (circuits.h:35-76, 8W-1 AND rounds on
+ * bit-packed words), one fused launch for the adder. y must not alias x. */
+int orqcu_a2b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
 /* b2a_bit (replicated_3pc.h:220-251): LSB of a boolean sharing -> arithmetic. */
 int orqcu_b2a_bit(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
 /* Pairwise zero-sharing (zero_sharing_generator.h:101-148). */

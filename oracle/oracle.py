@@ -283,3 +283,10 @@ class Oracle:
         self.lib.oro_quicksort(ctypes.byref(self.ctx), kw, ctypes.c_size_t(n), self._ptrs(key), int(desc),
                                len(payloads), pay_arr, self._ptrs(perm))
         return perm
+
+    def a2b(self, x):
+        """ASharedVector::a2b: the boolean sharing of an arithmetic one."""
+        w = x[0].dtype.itemsize
+        y = self.new(len(x[0]), w)
+        self.lib.oro_a2b(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(x[0])), self._ptrs(x), self._ptrs(y))
+        return y

@@ -1589,3 +1589,59 @@ void oro_bitonic_sort_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* 
     free(ya);
     free(cols);
 }
+
+/* ------------------------------------------------------------------------- */
+/* ASharedVector::a2b (a_shared_vector.h:138-144): redistribute_shares_b
+ * (replicated_3pc.h:259-262: party 0 secret-shares x(0) + x(1) = S0 + S1,
+ * then party 2 shares its x(0) = S2) and ripple_carry_adder
+ * (operators/circuits.h:35-76) on bit-packed words of 8w elements. */
+void oro_a2b(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]) {
+    const int B = 8 * w;
+    const size_t cw = n / B + (n % B > 0);
+    void *v, *F[3], *G[3], *AX[3], *Ai[3], *Cr[3];
+    v = xalloc(n * (size_t)w + 16);
+    for (size_t i = 0; i < n; i++) st(v, i, w, ld(x[0], i, w) + ld(x[1], i, w));
+    alloc3(F, n, w);
+    alloc3(G, n, w);
+    oro_secret_share(c, 0, w, n, v, 0, F);
+    oro_secret_share(c, 0, w, n, x[2], 2, G);
+    alloc3(AX, cw, w);
+    alloc3(Ai, cw, w);
+    alloc3(Cr, cw, w);
+    for (int j = 0; j < 3; j++) {
+        memset(Cr[j], 0, cw * (size_t)w + 16);
+        for (size_t i = 0; i < n; i++) st(y[j], i, w, 0);
+    }
+    for (int b = 0; b < B; b++) {
+        for (int j = 0; j < 3; j++)
+            for (size_t word = 0; word < cw; word++) {
+                u128 ax = 0, ai = 0;
+                for (int k = 0; k < B && word * B + k < n; k++) {
+                    const size_t e = word * B + k;
+                    const u128 fa = ld(F[j], e, w), ga = ld(G[j], e, w);
+                    ax |= (((fa ^ ga) >> b) & 1) << k;
+                    ai |= ((fa >> b) & 1) << k;
+                }
+                st(AX[j], word, w, ax);
+                st(Ai[j], word, w, ai);
+                const u128 s = ax ^ ld(Cr[j], word, w);
+                for (int k = 0; k < B && word * B + k < n; k++) {
+                    const size_t e = word * B + k;
+                    st(y[j], e, w, ld(y[j], e, w) | (((s >> k) & 1) << b));
+                }
+            }
+        if (b == B - 1) break;
+        /* c = ((c ^ a_i) & axb_i) ^ a_i */
+        for (int j = 0; j < 3; j++)
+            for (size_t word = 0; word < cw; word++) st(Cr[j], word, w, ld(Cr[j], word, w) ^ ld(Ai[j], word, w));
+        oro_and_b(c, w, cw, Cr, AX, Cr);
+        for (int j = 0; j < 3; j++)
+            for (size_t word = 0; word < cw; word++) st(Cr[j], word, w, ld(Cr[j], word, w) ^ ld(Ai[j], word, w));
+    }
+    free(v);
+    free3(F);
+    free3(G);
+    free3(AX);
+    free3(Ai);
+    free3(Cr);
+}

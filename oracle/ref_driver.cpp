@@ -193,6 +193,21 @@ int main(int argc, char** argv) {
         }
         auto T = J.open_with_schema();
         for (size_t k = 0; k < T.second.size(); k++) d.plain("open_" + T.second[k], T.first[k]);
+    } else if (op == "a2b32" || op == "a2b64") {
+        // ASharedVector::a2b of values over all bits, shared by party 1
+        uint64_t st = seed;
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            auto x = gen<T>(n, st, ~0ull);
+            ASharedVector<T> xa = secret_share_a(x, 1);
+            auto xb = xa.a2b();
+            d.shares("xa", xa);
+            d.shares("xb", *xb);
+            auto o = xb->open();
+            d.plain("open_xb", o);
+        };
+        if (op == "a2b32") run(int32_t{});
+        else run(int64_t{});
     } else if (op == "tshuffle") {
         // EncodedTable<int64_t> {[A], [B] (< 256), V (u32), [F] (bits)}:
         // filter on [F] (those rows invalid), then finalize(): shuffle() and

@@ -379,6 +379,14 @@ class ASharedVector(SharedVector):
     """Arithmetic shares mod 2^(8w) (core/containers/a_shared_vector.h)."""
     arith = True
 
+    def a2b(self) -> "BSharedVector":
+        """ASharedVector::a2b (a_shared_vector.h:138-144): full-width
+        arithmetic -> boolean conversion (redistribution + ripple-carry adder)."""
+        z = self.rt._alloc(self.size(), self.width)
+        _check(self.rt.lib.orqcu_a2b(self.rt.h, self.width, ctypes.c_size_t(self.size()), _p3(self.shares),
+                                     _p3(z)))
+        return BSharedVector(self.rt, z)
+
     def __mul__(self, o):
         return self._bin(o, self.rt.lib.orqcu_multiply_a, ASharedVector)
 

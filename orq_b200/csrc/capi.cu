@@ -545,6 +545,17 @@ int orqcu_not_b_1(orqcu_runtime* rt, int width, size_t n, const void* const x[3]
     });
 }
 
+int orqcu_a2b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "a2b supports 4 and 8-byte shares");
+        need_sh(x, n, "null x");
+        need_sh((const void* const*)y, n, "null y");
+        for (int j = 0; j < 3; j++) need(n == 0 || x[j] != y[j], "a2b output must not alias its input");
+        orqcu::op_a2b(rt->ctx, width, n, c3(x), m3(y));
+    });
+}
+
 int orqcu_table_shuffle(orqcu_runtime* rt, int width, size_t n, int na, void* const* data_a, int nb,
                         void* const* data_b) {
     return guard([&] {

@@ -1,0 +1,163 @@
+// conv.cu — ASharedVector::a2b (a_shared_vector.h:138-144): the arithmetic
+// sharing is redistributed as two boolean sharings (redistribute_shares_b,
+// replicated_3pc.h:259-262: party 0 shares S0 + S1, party 2 shares S2) whose
+// sum, computed by the boolean ripple-carry adder (operators/circuits.h:35-76),
+// is the boolean sharing of the value.
+//
+// The adder works on bit-packed words: bit i of 8W consecutive elements forms
+// one word (pack_from), and each of the 8W-1 carry rounds is one AND over the
+// ceil(n / 8W) words, c_i = ((c_{i-1} ^ a_i) & (a ^ b)_i) ^ a_i. Here a warp
+// owns one word: lane l holds element l (and element 32 + l for 8-byte
+// shares), a ballot packs a bit of 32 elements, the three lanes 0..2 compute
+// the round's keystream block of the three PAIR streams, and the sum bits are
+// unpacked back into the lanes' elements, all rounds in registers.
+#include <type_traits>
+
+#include "launch.cuh"
+
+namespace orqcu {
+
+namespace {
+
+struct RcaArgs {
+    const void* a[3];
+    const void* b[3];
+    void* sum[3];
+    StreamArg pair[3];     // nonces at the first carry round
+    unsigned long long n;  // elements
+    unsigned long long cw; // packed words (ceil(n / 8W))
+    unsigned long long C;  // nonces per carry round (an AND over cw words)
+};
+
+template <int W>
+__global__ void __launch_bounds__(kAesThreads, 1) k_rca(RcaArgs a) {
+    using T = typename std::conditional<W == 4, uint32_t, unsigned long long>::type;
+    constexpr int B = 8 * W;        // elements per packed word
+    constexpr int H = B / 32;       // elements per lane
+    extern __shared__ __align__(16) uint32_t sm[];
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    const int lane = threadIdx.x & 31;
+    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+    for (unsigned long long c = (unsigned long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+         c < a.cw; c += warps) {
+        T x[H][3], ab[H][3], sum[H][3];
+        bool ok[H];
+#pragma unroll
+        for (int h = 0; h < H; h++) {
+            const unsigned long long e = c * B + 32ull * h + lane;
+            ok[h] = e < a.n;
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                x[h][p] = ok[h] ? reinterpret_cast<const T*>(a.a[p])[e] : (T)0;
+                ab[h][p] = x[h][p] ^ (ok[h] ? reinterpret_cast<const T*>(a.b[p])[e] : (T)0);
+                sum[h][p] = 0;
+            }
+        }
+        T carry[3] = {0, 0, 0};
+#pragma unroll 1
+        for (int i = 0; i < B; i++) {
+            T axb[3], ai[3];
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                axb[p] = ai[p] = 0;
+#pragma unroll
+                for (int h = 0; h < H; h++) {
+                    axb[p] |= (T)__ballot_sync(0xffffffffu, (ab[h][p] >> i) & 1) << (32 * h);
+                    ai[p] |= (T)__ballot_sync(0xffffffffu, (x[h][p] >> i) & 1) << (32 * h);
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                const T s = axb[p] ^ carry[p];
+#pragma unroll
+                for (int h = 0; h < H; h++) sum[h][p] |= ((s >> (32 * h + lane)) & 1) << i;
+            }
+            if (i == B - 1) break;  // no carry out of the top bit
+            // the round's keystream: word c (W bytes at c*W) of each PAIR call
+            uint32_t kw[2] = {0, 0};
+            if (lane < 3) {
+                const uint4 blk = keystream_block_n(S, a.pair[lane].rk, a.pair[lane].nonce + (unsigned long long)i * a.C,
+                                                    c * W / 16);
+                const uint32_t wds[4] = {blk.x, blk.y, blk.z, blk.w};
+                const int o = (int)((c * W / 4) & 3);
+                kw[0] = wds[o];
+                kw[1] = W == 8 ? wds[o + 1] : 0u;
+            }
+            T K[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const uint32_t lo = __shfl_sync(0xffffffffu, kw[0], q);
+                const uint32_t hi = __shfl_sync(0xffffffffu, kw[1], q);
+                K[q] = W == 8 ? (T)(((unsigned long long)hi << 32) | lo) : (T)lo;
+            }
+            // c_i = ((c ^ a_i) & axb_i) ^ a_i, the AND with r_p = K[p-1] ^ K[p]
+            T u[3], z[3];
+#pragma unroll
+            for (int p = 0; p < 3; p++) u[p] = carry[p] ^ ai[p];
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                const int q = (p + 1) % 3, pm = (p + 2) % 3;
+                z[p] = (K[pm] ^ K[p]) ^ (u[p] & axb[p]) ^ (u[p] & axb[q]) ^ (u[q] & axb[p]);
+            }
+#pragma unroll
+            for (int p = 0; p < 3; p++) carry[p] = z[p] ^ ai[p];
+        }
+#pragma unroll
+        for (int h = 0; h < H; h++)
+            if (ok[h]) {
+                const unsigned long long e = c * B + 32ull * h + lane;
+#pragma unroll
+                for (int p = 0; p < 3; p++) reinterpret_cast<T*>(a.sum[p])[e] = sum[h][p];
+            }
+    }
+}
+
+// S0 + S1 (party 0's local value x(0) + x(1)) mod 2^(8W)
+template <typename T>
+__global__ void k_add01(CSh3 x, T* out, unsigned long long n) {
+    for (unsigned long long i = gtid(); i < n; i += gstride())
+        out[i] = reinterpret_cast<const T*>(x.p[0])[i] + reinterpret_cast<const T*>(x.p[1])[i];
+}
+
+}  // namespace
+
+void op_a2b(Ctx& c, int w, size_t n, CSh3 x, Sh3 y) {
+    if (w != 4 && w != 8) throw std::invalid_argument("a2b supports 4 and 8-byte shares");
+    const size_t n1 = std::max<size_t>(n, 1);
+    Scratch v(c, n1 * w), fb(c, 3 * n1 * w), sb(c, 3 * n1 * w);
+    Sh3 F, G;
+    for (int j = 0; j < 3; j++) {
+        F.p[j] = fb.as<uint8_t>() + j * n1 * w;
+        G.p[j] = sb.as<uint8_t>() + j * n1 * w;
+    }
+    if (n) {
+        if (w == 4) k_add01<uint32_t><<<plain_grid(c, n), 256, 0, c.stream>>>(x, v.as<uint32_t>(), n);
+        else k_add01<unsigned long long><<<plain_grid(c, n), 256, 0, c.stream>>>(x, v.as<unsigned long long>(), n);
+        ORQ_CUDA_CHECK(cudaGetLastError());
+        c.kernels_launched++;
+    }
+    // redistribute_shares_b: party 0 shares x(0) + x(1), then party 2 its x(0)
+    op_secret_share(c, false, w, n, v.p, 0, F);
+    op_secret_share(c, false, w, n, x.p[2], 2, G);
+    const unsigned long long B = 8ull * w, cw = (n + B - 1) / B;
+    RcaArgs a;
+    for (int j = 0; j < 3; j++) {
+        a.a[j] = F.p[j];
+        a.b[j] = G.p[j];
+        a.sum[j] = y.p[j];
+        a.pair[j] = c.stream_arg(PAIR0 + j);
+    }
+    a.n = n;
+    a.cw = cw;
+    a.C = chunks_of(cw * (unsigned long long)w);
+    if (n) {
+        const unsigned long long warps = cw;
+        const double blocks = 3.0 * (double)(B - 1) * (double)cw;
+        if (w == 4) launch_aes(c, "a2b", 9.0 * w * n, blocks, k_rca<4>, warps * 32, a);
+        else launch_aes(c, "a2b", 9.0 * w * n, blocks, k_rca<8>, warps * 32, a);
+    }
+    for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += (B - 1) * a.C;
+}
+
+}  // namespace orqcu

@@ -78,6 +78,9 @@ CASES = [
     ("tsort_qs_n3000", "tsort_qs", 3000, 6, 5, 64, False),
     ("tshuffle_n64", "tshuffle", 64, 7, 2, 64, True),
     ("tshuffle_n1000", "tshuffle", 1000, 8, 3, 64, False),
+    ("a2b32_n500", "a2b32", 500, 7, 2, 32, True),
+    ("a2b64_n333", "a2b64", 333, 8, 3, 64, True),
+    ("a2b64_n20000", "a2b64", 20000, 9, 4, 64, False),
 ]
 
 

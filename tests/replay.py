@@ -72,6 +72,9 @@ class OracleBackend:
     def qsort(self, key, payloads, desc=False):
         return self.o.quicksort(key, payloads, desc)
 
+    def a2b(self, x):
+        return self.o.a2b(x)
+
     def bitonic_rows(self, keys, desc, data_a, data_b):
         self.o.bitonic_sort_rows(keys, desc, data_a, data_b)
 
@@ -159,6 +162,9 @@ class GpuBackend:
 
     def bitonic(self, key, desc):
         self.orq.bitonic_sort(key, self.orq.DESC if desc else self.orq.ASC)
+
+    def a2b(self, x):
+        return x.a2b()
 
     def qsort(self, key, payloads, desc=False):
         perm = self.orq.quicksort(key, self.orq.DESC if desc else self.orq.ASC)
@@ -525,3 +531,11 @@ def replay_tshuffle(rt_seed, n, seed):
     for k, d in zip(names, data):
         out["open_" + k] = d.view(np.uint64)[None]
     return out, cols
+
+
+def replay_a2b(be, n, seed, w):
+    """The "a2b32"/"a2b64" ops of ref_driver.cpp."""
+    x = splitmix64_fast(seed, n).astype(_U[w])
+    xa = be.share(x, True, 1)
+    xb = be.a2b(xa)
+    return {"xa": be.np(xa), "xb": be.np(xb), "open_xb": be.open(xb, False)[None]}, x

@@ -307,3 +307,25 @@ def test_quicksort_large_matches_reference_digests(oracle_lib, digests, tag, w):
     out, _ = replay_qsort(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], w)
     for name, arr in out.items():
         assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag,w", [("a2b32_n500", 4), ("a2b64_n333", 8)])
+def test_a2b_matches_reference_shares(oracle_lib, golden, digests, tag, w):
+    """ASharedVector::a2b: redistribute_shares_b + ripple-carry adder, share for share"""
+    from replay import replay_a2b
+
+    m = digests[tag]["meta"]
+    out, x = replay_a2b(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    assert np.array_equal(out["open_xb"][0].view(x.dtype), x)
+
+
+def test_a2b_large_matches_reference_digests(oracle_lib, digests):
+    from replay import replay_a2b
+
+    d = digests["a2b64_n20000"]
+    m = d["meta"]
+    out, _ = replay_a2b(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 8)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name

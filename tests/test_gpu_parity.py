@@ -720,3 +720,38 @@ def test_mask_b(orq):
     x = rt.secret_share_b(np.arange(100, dtype=np.int64) * 12345, 0)
     x.mask(0xFF0F)
     assert np.array_equal(x.open().cpu().numpy(), (np.arange(100, dtype=np.int64) * 12345) & 0xFF0F)
+
+
+@pytest.mark.parametrize("tag,w", [("a2b32_n500", 4), ("a2b64_n333", 8)])
+def test_a2b_matches_reference_shares(orq, golden, digests, tag, w):
+    """ASharedVector::a2b: redistribute_shares_b + ripple-carry adder, share for share"""
+    from replay import replay_a2b
+
+    m = digests[tag]["meta"]
+    out, x = replay_a2b(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    assert np.array_equal(out["open_xb"][0].view(x.dtype), x)
+
+
+def test_a2b_large_matches_reference_digests(orq, digests):
+    from replay import replay_a2b
+
+    d = digests["a2b64_n20000"]
+    m = d["meta"]
+    out, _ = replay_a2b(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], 8)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("w", [4, 8])
+@pytest.mark.parametrize("n", [1, 33, 100001])
+def test_a2b_matches_restatement(orq, w, n):
+    """partial packed words and several CTAs' worth of words"""
+    from replay import replay_a2b
+
+    gpu, x = replay_a2b(GpuBackend(13), n, 5, w)
+    cpu, _ = replay_a2b(OracleBackend(13), n, 5, w)
+    for k in gpu:
+        assert same(gpu[k], cpu[k]), k
+    assert np.array_equal(gpu["open_xb"][0].view(x.dtype), x)
