@@ -604,6 +604,33 @@ WORKLOADS = {"radix": RadixWorkload, "qsort": QuicksortWorkload, "bitonic": Bito
              "join": JoinWorkload}
 
 
+def max_over_ranks(x):
+    """The maximum of a float over the ranks of the default process group (x
+    itself when there is none): every multi-GPU time is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    dev = f"cuda:{torch.cuda.current_device()}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def init_replicas(world):
+    """One process group for the replicas (NCCL, short timeout) when world > 1."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    if not dist.is_initialized():
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
 def run_orq(args, rank, world, local_rank):
     import ctypes
 
@@ -613,13 +640,7 @@ def run_orq(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = f"cuda:{local_rank}"
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = init_replicas(world)
 
     def barrier():
         if dist is not None:
@@ -661,10 +682,7 @@ def run_orq(args, rank, world, local_rank):
     orq._check(_lib.orqcu_profile_report(rt.h, buf, ctypes.c_size_t(len(buf))))
     orq._check(_lib.orqcu_profile_enable(rt.h, 0))
     prof = parse_profile(buf.value.decode())
-    if dist is not None:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms)
 
     # ---- e2e through the public API with host buffers ----------------------
     e2e = None
@@ -682,13 +700,11 @@ def run_orq(args, rank, world, local_rank):
         e1.record()
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ems], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(ems)
         ok = ok and wl.e2e_check()
         e2e = {"value": world * wl.units * ke / (ems / 1e3), "unit": "rows/s",
                "h2d_bytes_per_step": wl.h2d, "d2h_bytes_per_step": wl.d2h, "ms_per_step": ems / ke}
+    ok = max_over_ranks(0.0 if ok else 1.0) == 0.0  # every replica's output checked
     if dist is not None:
         dist.destroy_process_group()
     return wl, ms, launches, prof, clk, e2e, ok
@@ -811,7 +827,22 @@ def main():
 
     if args.workload in ("batch", "serve") and args.impl == "orq":
         fn = run_batch if args.workload == "batch" else run_serve
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        dist = init_replicas(world)
         res = fn(args, rank, world, local_rank)
+        # whole-job figures from the slowest replica
+        if args.workload == "batch":
+            for k in ("ms_batched", "ms_plain"):
+                res[k] = max_over_ranks(res[k])
+        else:
+            for part in ("serving", "plain"):
+                for k in ("makespan_s", "p50_ms", "p99_ms"):
+                    res[part][k] = max_over_ranks(res[part][k])
+                res[part]["rows_per_s"] = res[part]["rows"] / res[part]["makespan_s"]
+        if dist is not None:
+            dist.destroy_process_group()
         if rank != 0:
             return
         if args.workload == "batch":
