@@ -1197,6 +1197,14 @@ __global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
         int32_t id[E];
 #pragma unroll
         for (int e = 0; e < E; e++) id[e] = (k0 + e < a.n) ? __ldg(a.idx + k0 + e) : 0;
+        // ---- vector 1 gathers first: their latency overlaps vector 2's keystream
+        uint4 v1[3][B1];
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                if (k0 + e < a.n)
+                    gather_elem<W1>(a.src1[j], id[e], reinterpret_cast<uint8_t*>(&v1[j][0]) + e * W1);
         // ---- vector 2 (the permutation vector in elementwise application)
         uint32_t sig[E];
         if constexpr (W2 != 0) {
@@ -1237,14 +1245,6 @@ __global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
                 for (int e = 0; e < E; e++) sig[e] = reinterpret_cast<const uint32_t*>(o)[e];
             }
         }
-        // ---- vector 1
-        uint4 v1[3][B1];
-#pragma unroll
-        for (int j = 0; j < 3; j++)
-#pragma unroll
-            for (int e = 0; e < E; e++)
-                if (k0 + e < a.n)
-                    gather_elem<W1>(a.src1[j], id[e], reinterpret_cast<uint8_t*>(&v1[j][0]) + e * W1);
 #pragma unroll
         for (int bb = 0; bb < B1; bb++) {
             const unsigned long long blk = t * B1 + bb;
