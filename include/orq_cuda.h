@@ -115,6 +115,15 @@ int orqcu_sub_a(orqcu_runtime* rt, int width, size_t n, const void* const x[3],
                 const void* const y[3], void* const z[3]);
 /* not_b (replicated_3pc.h:199). */
 int orqcu_not_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]);
+/* BSharedVector::operator+ / operator- (b_shared_vector.h:588-622): addition
+ * and subtraction mod 2^(8*width) of boolean sharings by the ripple-carry
+ * adder (circuits.h:35-76; subtraction adds ~y with a carry-in), 8W-1 AND
+ * rounds on bit-packed words in one launch. width 4 or 8; z must not alias
+ * x or y. */
+int orqcu_add_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], const void* const y[3],
+                void* const z[3]);
+int orqcu_sub_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], const void* const y[3],
+                void* const z[3]);
 /* ASharedVector::a2b (a_shared_vector.h:138-144): arithmetic -> boolean
  * sharing of the full width (4 or 8): redistribute_shares_b
  * (replicated_3pc.h:259-262; party 0 secret-shares S0 + S1, party 2 shares S2)

@@ -290,3 +290,11 @@ class Oracle:
         y = self.new(len(x[0]), w)
         self.lib.oro_a2b(ctypes.byref(self.ctx), w, ctypes.c_size_t(len(x[0])), self._ptrs(x), self._ptrs(y))
         return y
+
+    def add_b(self, x, y):
+        """BSharedVector::operator+ (ripple-carry adder)."""
+        return self._bin(self.lib.oro_add_b, x, y)
+
+    def sub_b(self, x, y):
+        """BSharedVector::operator- (x + ~y + 1 by the adder)."""
+        return self._bin(self.lib.oro_sub_b, x, y)

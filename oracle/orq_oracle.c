@@ -1591,25 +1591,18 @@ void oro_bitonic_sort_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* 
 }
 
 /* ------------------------------------------------------------------------- */
-/* ASharedVector::a2b (a_shared_vector.h:138-144): redistribute_shares_b
- * (replicated_3pc.h:259-262: party 0 secret-shares x(0) + x(1) = S0 + S1,
- * then party 2 shares its x(0) = S2) and ripple_carry_adder
- * (operators/circuits.h:35-76) on bit-packed words of 8w elements. */
-void oro_a2b(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]) {
+/* ripple_carry_adder (operators/circuits.h:35-76) of boolean sharings F and G
+ * on bit-packed words of 8w elements; carry_in starts the carry at all ones
+ * (inplace_invert, for subtraction) */
+static void rca(oro_ctx* c, int w, size_t n, void* const F[3], void* const G[3], void* y[3], int carry_in) {
     const int B = 8 * w;
     const size_t cw = n / B + (n % B > 0);
-    void *v, *F[3], *G[3], *AX[3], *Ai[3], *Cr[3];
-    v = xalloc(n * (size_t)w + 16);
-    for (size_t i = 0; i < n; i++) st(v, i, w, ld(x[0], i, w) + ld(x[1], i, w));
-    alloc3(F, n, w);
-    alloc3(G, n, w);
-    oro_secret_share(c, 0, w, n, v, 0, F);
-    oro_secret_share(c, 0, w, n, x[2], 2, G);
+    void *AX[3], *Ai[3], *Cr[3];
     alloc3(AX, cw, w);
     alloc3(Ai, cw, w);
     alloc3(Cr, cw, w);
     for (int j = 0; j < 3; j++) {
-        memset(Cr[j], 0, cw * (size_t)w + 16);
+        for (size_t word = 0; word < cw; word++) st(Cr[j], word, w, carry_in ? wmask(w) : 0);
         for (size_t i = 0; i < n; i++) st(y[j], i, w, 0);
     }
     for (int b = 0; b < B; b++) {
@@ -1638,10 +1631,38 @@ void oro_a2b(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]) {
         for (int j = 0; j < 3; j++)
             for (size_t word = 0; word < cw; word++) st(Cr[j], word, w, ld(Cr[j], word, w) ^ ld(Ai[j], word, w));
     }
-    free(v);
-    free3(F);
-    free3(G);
     free3(AX);
     free3(Ai);
     free3(Cr);
+}
+
+/* BSharedVector::operator+ / operator- (b_shared_vector.h:588-622): the adder,
+ * subtraction as x + ~y with carry-in */
+void oro_add_b(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]) {
+    rca(c, w, n, x, y, z, 0);
+}
+void oro_sub_b(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]) {
+    void* ny[3];
+    alloc3(ny, n, w);
+    for (int j = 0; j < 3; j++)
+        for (size_t i = 0; i < n; i++) st(ny[j], i, w, ~ld(y[j], i, w));
+    rca(c, w, n, x, ny, z, 1);
+    free3(ny);
+}
+
+/* ASharedVector::a2b (a_shared_vector.h:138-144): redistribute_shares_b
+ * (replicated_3pc.h:259-262: party 0 secret-shares x(0) + x(1) = S0 + S1,
+ * then party 2 shares its x(0) = S2) and the adder. */
+void oro_a2b(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]) {
+    void *v, *F[3], *G[3];
+    v = xalloc(n * (size_t)w + 16);
+    for (size_t i = 0; i < n; i++) st(v, i, w, ld(x[0], i, w) + ld(x[1], i, w));
+    alloc3(F, n, w);
+    alloc3(G, n, w);
+    oro_secret_share(c, 0, w, n, v, 0, F);
+    oro_secret_share(c, 0, w, n, x[2], 2, G);
+    rca(c, w, n, F, G, y, 0);
+    free(v);
+    free3(F);
+    free3(G);
 }

@@ -135,6 +135,8 @@ void oro_equal(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], 
 void oro_not_b1(int w, size_t n, void* const x[3], void* y[3]);
 void oro_extend_lsb(int w, size_t n, void* const x[3], void* y[3]);
 void oro_a2b(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]);
+void oro_add_b(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]);
+void oro_sub_b(oro_ctx* c, int w, size_t n, void* const x[3], void* const y[3], void* z[3]);
 void oro_quicksort(oro_ctx* c, int kw, size_t n, void* key[3], int desc, int npayload,
                    void** payloads, int32_t* perm_out[3]);
 void oro_compare_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* x, void* const* y,

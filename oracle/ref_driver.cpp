@@ -193,6 +193,25 @@ int main(int argc, char** argv) {
         }
         auto T = J.open_with_schema();
         for (size_t k = 0; k < T.second.size(); k++) d.plain("open_" + T.second[k], T.first[k]);
+    } else if (op == "badd32" || op == "badd64") {
+        // BSharedVector operator+ and operator- (the ripple-carry adder)
+        uint64_t st = seed;
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            auto x = gen<T>(n, st, ~0ull);
+            auto y = gen<T>(n, st, ~0ull);
+            BSharedVector<T> xb = secret_share_b(x, 0);
+            BSharedVector<T> yb = secret_share_b(y, 1);
+            auto s = xb + yb;
+            auto df = xb - yb;
+            d.shares("sum", *s);
+            d.shares("diff", *df);
+            auto os = s->open(), od = df->open();
+            d.plain("open_sum", os);
+            d.plain("open_diff", od);
+        };
+        if (op == "badd32") run(int32_t{});
+        else run(int64_t{});
     } else if (op == "a2b32" || op == "a2b64") {
         // ASharedVector::a2b of values over all bits, shared by party 1
         uint64_t st = seed;

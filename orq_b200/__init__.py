@@ -293,6 +293,14 @@ class BSharedVector(SharedVector):
     def __ixor__(self, o):
         return self._ibin(o, self.rt.lib.orqcu_xor_b)
 
+    def __add__(self, o):
+        """operator+ (b_shared_vector.h:588-590): the ripple-carry adder."""
+        return self._bin(o, self.rt.lib.orqcu_add_b, BSharedVector)
+
+    def __sub__(self, o):
+        """operator- (b_shared_vector.h:620-622): self + ~o + 1 by the adder."""
+        return self._bin(o, self.rt.lib.orqcu_sub_b, BSharedVector)
+
     def __or__(self, o):
         """operator| (b_shared_vector.h:438-441): ~(~a & ~b)."""
         return ~((~self) & (~o))

@@ -545,6 +545,32 @@ int orqcu_not_b_1(orqcu_runtime* rt, int width, size_t n, const void* const x[3]
     });
 }
 
+int orqcu_add_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], const void* const y[3],
+                void* const z[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "the boolean adder supports 4 and 8-byte shares");
+        need_sh(x, n, "null x");
+        need_sh(y, n, "null y");
+        need_sh((const void* const*)z, n, "null z");
+        for (int j = 0; j < 3; j++) need(n == 0 || (z[j] != x[j] && z[j] != y[j]), "z must not alias x or y");
+        orqcu::op_rca(rt->ctx, width, n, c3(x), c3(y), m3(z), false);
+    });
+}
+
+int orqcu_sub_b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], const void* const y[3],
+                void* const z[3]) {
+    return guard([&] {
+        need_rt(rt);
+        need(width == 4 || width == 8, "the boolean adder supports 4 and 8-byte shares");
+        need_sh(x, n, "null x");
+        need_sh(y, n, "null y");
+        need_sh((const void* const*)z, n, "null z");
+        for (int j = 0; j < 3; j++) need(n == 0 || (z[j] != x[j] && z[j] != y[j]), "z must not alias x or y");
+        orqcu::op_sub_b(rt->ctx, width, n, c3(x), c3(y), m3(z));
+    });
+}
+
 int orqcu_a2b(orqcu_runtime* rt, int width, size_t n, const void* const x[3], void* const y[3]) {
     return guard([&] {
         need_rt(rt);

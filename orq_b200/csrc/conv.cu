@@ -27,6 +27,7 @@ struct RcaArgs {
     unsigned long long n;  // elements
     unsigned long long cw; // packed words (ceil(n / 8W))
     unsigned long long C;  // nonces per carry round (an AND over cw words)
+    int carry_in;          // subtraction: the carry starts as all ones (inplace_invert)
 };
 
 template <int W>
@@ -54,7 +55,8 @@ __global__ void __launch_bounds__(kAesThreads, 1) k_rca(RcaArgs a) {
                 sum[h][p] = 0;
             }
         }
-        T carry[3] = {0, 0, 0};
+        const T c0 = a.carry_in ? ~(T)0 : (T)0;
+        T carry[3] = {c0, c0, c0};
 #pragma unroll 1
         for (int i = 0; i < B; i++) {
             T axb[3], ai[3];
@@ -122,6 +124,39 @@ __global__ void k_add01(CSh3 x, T* out, unsigned long long n) {
 
 }  // namespace
 
+// ripple_carry_adder (operators/circuits.h:35-76) of two boolean sharings
+void op_rca(Ctx& c, int w, size_t n, CSh3 A, CSh3 Bv, Sh3 sum, bool carry_in) {
+    if (w != 4 && w != 8) throw std::invalid_argument("the boolean adder supports 4 and 8-byte shares");
+    const unsigned long long B = 8ull * w, cw = (n + B - 1) / B;
+    RcaArgs a;
+    for (int j = 0; j < 3; j++) {
+        a.a[j] = A.p[j];
+        a.b[j] = Bv.p[j];
+        a.sum[j] = sum.p[j];
+        a.pair[j] = c.stream_arg(PAIR0 + j);
+    }
+    a.n = n;
+    a.cw = cw;
+    a.C = chunks_of(cw * (unsigned long long)w);
+    a.carry_in = carry_in;
+    if (n) {
+        const double blocks = 3.0 * (double)(B - 1) * (double)cw;
+        if (w == 4) launch_aes(c, "boolean_adder", 9.0 * w * n, blocks, k_rca<4>, cw * 32, a);
+        else launch_aes(c, "boolean_adder", 9.0 * w * n, blocks, k_rca<8>, cw * 32, a);
+    }
+    for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += (B - 1) * a.C;
+}
+
+// BSharedVector::operator- (b_shared_vector.h:620-622): a + ~b + 1
+void op_sub_b(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 z) {
+    const size_t n1 = std::max<size_t>(n, 1);
+    Scratch nb(c, 3 * n1 * w);
+    Sh3 NY;
+    for (int j = 0; j < 3; j++) NY.p[j] = nb.as<uint8_t>() + j * n1 * w;
+    op_not(c, w, n, y, NY);
+    op_rca(c, w, n, x, CSh3{{NY.p[0], NY.p[1], NY.p[2]}}, z, true);
+}
+
 void op_a2b(Ctx& c, int w, size_t n, CSh3 x, Sh3 y) {
     if (w != 4 && w != 8) throw std::invalid_argument("a2b supports 4 and 8-byte shares");
     const size_t n1 = std::max<size_t>(n, 1);
@@ -140,24 +175,7 @@ void op_a2b(Ctx& c, int w, size_t n, CSh3 x, Sh3 y) {
     // redistribute_shares_b: party 0 shares x(0) + x(1), then party 2 its x(0)
     op_secret_share(c, false, w, n, v.p, 0, F);
     op_secret_share(c, false, w, n, x.p[2], 2, G);
-    const unsigned long long B = 8ull * w, cw = (n + B - 1) / B;
-    RcaArgs a;
-    for (int j = 0; j < 3; j++) {
-        a.a[j] = F.p[j];
-        a.b[j] = G.p[j];
-        a.sum[j] = y.p[j];
-        a.pair[j] = c.stream_arg(PAIR0 + j);
-    }
-    a.n = n;
-    a.cw = cw;
-    a.C = chunks_of(cw * (unsigned long long)w);
-    if (n) {
-        const unsigned long long warps = cw;
-        const double blocks = 3.0 * (double)(B - 1) * (double)cw;
-        if (w == 4) launch_aes(c, "a2b", 9.0 * w * n, blocks, k_rca<4>, warps * 32, a);
-        else launch_aes(c, "a2b", 9.0 * w * n, blocks, k_rca<8>, warps * 32, a);
-    }
-    for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += (B - 1) * a.C;
+    op_rca(c, w, n, CSh3{{F.p[0], F.p[1], F.p[2]}}, CSh3{{G.p[0], G.p[1], G.p[2]}}, y, false);
 }
 
 }  // namespace orqcu

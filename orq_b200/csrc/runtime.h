@@ -188,6 +188,8 @@ void op_local(Ctx& c, int op, int w, size_t n, CSh3 x, CSh3 y, Sh3 z);  // 0 xor
 void op_not(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
 void op_b2a_bit(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
 void op_a2b(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
+void op_rca(Ctx& c, int w, size_t n, CSh3 a, CSh3 b, Sh3 sum, bool carry_in);
+void op_sub_b(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 z);
 void op_zero_share(Ctx& c, bool arith, int w, size_t n, Sh3 r);
 void op_reshare(Ctx& c, bool arith, int w, size_t n, int group, Sh3 s);
 

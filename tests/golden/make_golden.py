@@ -81,6 +81,8 @@ CASES = [
     ("a2b32_n500", "a2b32", 500, 7, 2, 32, True),
     ("a2b64_n333", "a2b64", 333, 8, 3, 64, True),
     ("a2b64_n20000", "a2b64", 20000, 9, 4, 64, False),
+    ("badd32_n500", "badd32", 500, 7, 2, 32, True),
+    ("badd64_n333", "badd64", 333, 8, 3, 64, True),
 ]
 
 

@@ -75,6 +75,12 @@ class OracleBackend:
     def a2b(self, x):
         return self.o.a2b(x)
 
+    def add_b(self, x, y):
+        return self.o.add_b(x, y)
+
+    def sub_b(self, x, y):
+        return self.o.sub_b(x, y)
+
     def bitonic_rows(self, keys, desc, data_a, data_b):
         self.o.bitonic_sort_rows(keys, desc, data_a, data_b)
 
@@ -165,6 +171,12 @@ class GpuBackend:
 
     def a2b(self, x):
         return x.a2b()
+
+    def add_b(self, x, y):
+        return x + y
+
+    def sub_b(self, x, y):
+        return x - y
 
     def qsort(self, key, payloads, desc=False):
         perm = self.orq.quicksort(key, self.orq.DESC if desc else self.orq.ASC)
@@ -539,3 +551,13 @@ def replay_a2b(be, n, seed, w):
     xa = be.share(x, True, 1)
     xb = be.a2b(xa)
     return {"xa": be.np(xa), "xb": be.np(xb), "open_xb": be.open(xb, False)[None]}, x
+
+
+def replay_badd(be, n, seed, w):
+    """The "badd32"/"badd64" ops: BSharedVector + and -."""
+    x, y = prim_inputs(n, seed, _U[w])
+    xb, yb = be.share(x, False, 0), be.share(y, False, 1)
+    s, d = be.add_b(xb, yb), be.sub_b(xb, yb)
+    out = {"sum": be.np(s), "diff": be.np(d), "open_sum": be.open(s, False)[None],
+           "open_diff": be.open(d, False)[None]}
+    return out, (x, y)

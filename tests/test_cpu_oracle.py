@@ -329,3 +329,16 @@ def test_a2b_large_matches_reference_digests(oracle_lib, digests):
     out, _ = replay_a2b(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], 8)
     for name, arr in out.items():
         assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+@pytest.mark.parametrize("tag,w", [("badd32_n500", 4), ("badd64_n333", 8)])
+def test_boolean_add_sub_match_reference_shares(oracle_lib, golden, digests, tag, w):
+    """BSharedVector + and - (the ripple-carry adder), share for share"""
+    from replay import replay_badd
+
+    m = digests[tag]["meta"]
+    out, (x, y) = replay_badd(OracleBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    assert np.array_equal(out["open_sum"][0].view(x.dtype), x + y)
+    assert np.array_equal(out["open_diff"][0].view(x.dtype), x - y)

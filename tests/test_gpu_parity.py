@@ -755,3 +755,16 @@ def test_a2b_matches_restatement(orq, w, n):
     for k in gpu:
         assert same(gpu[k], cpu[k]), k
     assert np.array_equal(gpu["open_xb"][0].view(x.dtype), x)
+
+
+@pytest.mark.parametrize("tag,w", [("badd32_n500", 4), ("badd64_n333", 8)])
+def test_boolean_add_sub_match_reference_shares(orq, golden, digests, tag, w):
+    """BSharedVector + and - (the ripple-carry adder), share for share"""
+    from replay import replay_badd
+
+    m = digests[tag]["meta"]
+    out, (x, y) = replay_badd(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], w)
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+    assert np.array_equal(out["open_sum"][0].view(x.dtype), x + y)
+    assert np.array_equal(out["open_diff"][0].view(x.dtype), x - y)
