@@ -1181,9 +1181,83 @@ __device__ __forceinline__ void store_elem(void* dst, int32_t k, const uint8_t* 
     }
 }
 
-// E elements per thread; E*W1 and E*W2 are multiples of 16 bytes.
+// the three shares of elements id[0..E) of src into E*W/16 16-byte words
+// (element e at byte e*W); elements at or past n are left unchanged
+template <int W, int E, int B>
+__device__ __forceinline__ void gather3(const void* const* src, const int32_t (&id)[E], unsigned long long k0,
+                                        unsigned long long n, uint4 (&v)[3][B]) {
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            if (k0 + e >= n) continue;
+            if constexpr (W == 16) {
+                v[j][e] = __ldg(reinterpret_cast<const uint4*>(src[j]) + id[e]);
+            } else if constexpr (W == 8) {
+                const uint2 x = __ldg(reinterpret_cast<const uint2*>(src[j]) + id[e]);
+                if (e & 1) {
+                    v[j][e >> 1].z = x.x;
+                    v[j][e >> 1].w = x.y;
+                } else {
+                    v[j][e >> 1].x = x.x;
+                    v[j][e >> 1].y = x.y;
+                }
+            } else {
+                const uint32_t x = __ldg(reinterpret_cast<const uint32_t*>(src[j]) + id[e]);
+                switch (e & 3) {
+                    case 0: v[j][e >> 2].x = x; break;
+                    case 1: v[j][e >> 2].y = x; break;
+                    case 2: v[j][e >> 2].z = x; break;
+                    default: v[j][e >> 2].w = x; break;
+                }
+            }
+        }
+}
+
+template <int E>
+__device__ __forceinline__ void load_idx(const int32_t* idx, unsigned long long k0, unsigned long long n,
+                                         int32_t (&id)[E]) {
+#pragma unroll
+    for (int e = 0; e < E; e++) id[e] = (k0 + e < n) ? __ldg(idx + k0 + e) : 0;
+}
+
+// Zero-sharing of one 16-byte block of a vector: the keystreams of block blk in
+// the group stream (r0) and at nonce offset ch (r1), r2 = -(r0 + r1) or
+// r0 ^ r1, added to the three shares held at v[.][0]; then v[.][0..B) rotate
+// left by one so the next block sits at index 0 (after B calls the order is
+// restored). Called from loops kept rolled: two AES bodies per vector instead
+// of two per block keep the kernel's loop inside the instruction cache (fully
+// unrolled, ten AES-256 bodies stalled every warp on instruction fetch).
+template <int W, bool A, int B>
+__device__ __forceinline__ void reshare_block(const AesSmem& S, StreamArg gs, unsigned long long ch,
+                                              unsigned long long blk, uint4 (&v)[3][B]) {
+    const uint4 r0 = keystream_block(S, gs, blk);
+    gs.nonce += ch;
+    const uint4 r1 = keystream_block(S, gs, blk);
+    uint4 r2;
+    if constexpr (A) r2 = Ring<W>::sub(Ring<W>::sub(make_uint4(0, 0, 0, 0), r0), r1);
+    else r2 = r0 ^ r1;
+    v[0][0] = Share<W, A>::plus(v[0][0], r0);
+    v[1][0] = Share<W, A>::plus(v[1][0], r1);
+    v[2][0] = Share<W, A>::plus(v[2][0], r2);
+    if constexpr (B > 1) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const uint4 x = v[j][0];
+#pragma unroll
+            for (int b = 0; b + 1 < B; b++) v[j][b] = v[j][b + 1];
+            v[j][B - 1] = x;
+        }
+    }
+}
+
+// E elements per thread and unit; E*W1 and E*W2 are multiples of 16 bytes.
+// Software-pipelined: a unit's gathers are issued in the previous iteration,
+// right after that iteration has consumed the same registers, so each random
+// gather has a whole iteration of keystream work to arrive in; the next unit's
+// indices are loaded at the top of an iteration.
 template <int W1, bool A1, int W2, bool A2, int MODE>
-__global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
+__global__ void __launch_bounds__(kAesThreads, 1) k_apply(ApplyArgs a) {
     constexpr int WMIN = (W2 && W2 < W1) ? W2 : W1;
     constexpr int E = 16 / WMIN;
     constexpr int B1 = E * W1 / 16;
@@ -1192,49 +1266,32 @@ __global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const unsigned long long units = ceil_div(a.n, E);
-    for (unsigned long long t = gtid(); t < units; t += gstride()) {
-        const unsigned long long k0 = t * E;
+    unsigned long long t = gtid();
+    if (t >= units) return;  // no barrier follows the table staging
+    const unsigned long long stride = gstride();
+    uint4 v1[3][B1], v2[3][B2];
+    {
         int32_t id[E];
-#pragma unroll
-        for (int e = 0; e < E; e++) id[e] = (k0 + e < a.n) ? __ldg(a.idx + k0 + e) : 0;
-        // ---- vector 1 gathers first: their latency overlaps vector 2's keystream
-        uint4 v1[3][B1];
-#pragma unroll
-        for (int j = 0; j < 3; j++)
-#pragma unroll
-            for (int e = 0; e < E; e++)
-                if (k0 + e < a.n)
-                    gather_elem<W1>(a.src1[j], id[e], reinterpret_cast<uint8_t*>(&v1[j][0]) + e * W1);
+        load_idx<E>(a.idx, t * E, a.n, id);
+        gather3<W1, E, B1>(a.src1, id, t * E, a.n, v1);
+        if constexpr (W2 != 0) gather3<W2, E, B2>(a.src2, id, t * E, a.n, v2);
+    }
+    for (;;) {
+        const unsigned long long k0 = t * E;
+        const unsigned long long tn = t + stride;
+        const bool more = tn < units;
+        int32_t idn[E];
+        load_idx<E>(a.idx, more ? tn * E : a.n, a.n, idn);
         // ---- vector 2 (the permutation vector in elementwise application)
         uint32_t sig[E];
         if constexpr (W2 != 0) {
-            uint4 v2[3][B2];
-#pragma unroll
-            for (int j = 0; j < 3; j++)
-#pragma unroll
-                for (int e = 0; e < E; e++)
-                    if (k0 + e < a.n)
-                        gather_elem<W2>(a.src2[j], id[e], reinterpret_cast<uint8_t*>(&v2[j][0]) + e * W2);
-#pragma unroll
-            for (int bb = 0; bb < B2; bb++) {
-                const unsigned long long blk = t * B2 + bb;
-                StreamArg gs = a.g2;
-                const uint4 r0 = keystream_block(S, gs, blk);
-                gs.nonce += a.ch2;
-                const uint4 r1 = keystream_block(S, gs, blk);
-                uint4 r2;
-                if constexpr (A2) r2 = Ring<W2>::sub(Ring<W2>::sub(make_uint4(0, 0, 0, 0), r0), r1);
-                else r2 = r0 ^ r1;
-                v2[0][bb] = Share<W2, A2>::plus(v2[0][bb], r0);
-                v2[1][bb] = Share<W2, A2>::plus(v2[1][bb], r1);
-                v2[2][bb] = Share<W2, A2>::plus(v2[2][bb], r2);
-            }
+#pragma unroll 1
+            for (int bb = 0; bb < B2; bb++) reshare_block<W2, A2, B2>(S, a.g2, a.ch2, t * B2 + bb, v2);
             if constexpr (MODE == 0) {
 #pragma unroll
                 for (int j = 0; j < 3; j++)
 #pragma unroll
-                    for (int bb = 0; bb < B2; bb++)
-                        st16(a.dst2[j], t * B2 + bb, a.n * W2, v2[j][bb]);
+                    for (int bb = 0; bb < B2; bb++) st16(a.dst2[j], t * B2 + bb, a.n * W2, v2[j][bb]);
             } else if constexpr (MODE == 2) {
                 // open (W2 == 4): sigma = sum or xor of the three shares
                 uint4 o[B2];
@@ -1244,21 +1301,11 @@ __global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
 #pragma unroll
                 for (int e = 0; e < E; e++) sig[e] = reinterpret_cast<const uint32_t*>(o)[e];
             }
+            if (more) gather3<W2, E, B2>(a.src2, idn, tn * E, a.n, v2);
         }
-#pragma unroll
-        for (int bb = 0; bb < B1; bb++) {
-            const unsigned long long blk = t * B1 + bb;
-            StreamArg gs = a.g1;
-            const uint4 r0 = keystream_block(S, gs, blk);
-            gs.nonce += a.ch1;
-            const uint4 r1 = keystream_block(S, gs, blk);
-            uint4 r2;
-            if constexpr (A1) r2 = Ring<W1>::sub(Ring<W1>::sub(make_uint4(0, 0, 0, 0), r0), r1);
-            else r2 = r0 ^ r1;
-            v1[0][bb] = Share<W1, A1>::plus(v1[0][bb], r0);
-            v1[1][bb] = Share<W1, A1>::plus(v1[1][bb], r1);
-            v1[2][bb] = Share<W1, A1>::plus(v1[2][bb], r2);
-        }
+        // ---- vector 1
+#pragma unroll 1
+        for (int bb = 0; bb < B1; bb++) reshare_block<W1, A1, B1>(S, a.g1, a.ch1, t * B1 + bb, v1);
         if constexpr (MODE == 0) {
 #pragma unroll
             for (int j = 0; j < 3; j++)
@@ -1287,6 +1334,9 @@ __global__ void __launch_bounds__(kAesThreads) k_apply(ApplyArgs a) {
             for (int e = 0; e < E; e++)
                 if (k0 + e < a.n) a.sigma[k0 + e] = reinterpret_cast<const int32_t*>(o)[e];
         }
+        if (!more) break;
+        gather3<W1, E, B1>(a.src1, idn, tn * E, a.n, v1);
+        t = tn;
     }
 }
 
