@@ -47,9 +47,10 @@ AES_LDS_PER_BLOCK = 228
 DEFAULT_N = 1 << 22
 # DRAM traffic of the dominant k_apply instance (padded 16-byte key + int32
 # permutation, one group), dram__bytes_read.sum + dram__bytes_write.sum from
-# one ncu capture at 2^21 rows (profiles/radix_sort_2p22.md): 729 MB, scaled
-# per row to the benchmarked size.
-APPLY_TRAFFIC_BYTES_PER_ROW = 729.0e6 / (1 << 21)
+# one ncu capture at 2^21 rows (profiles/radix_sort_2p22.md): 690.5 MB
+# (dram__bytes.sum.per_second x gpu__time_duration), scaled per row to the
+# benchmarked size.
+APPLY_TRAFFIC_BYTES_PER_ROW = 690.5e6 / (1 << 21)
 
 
 def load_peaks():
