@@ -46,8 +46,11 @@ __global__ void __launch_bounds__(kAesThreads) k_radix_b2a(RadixB2AArgs a) {
     const uint32_t wsel = a.shift >> 5, bsel = a.shift & 31;
     const unsigned long long nbytes = a.n * 4;
     for (unsigned long long b = gtid(); b < units; b += gstride()) {
-        uint4 z[3][3];
-#pragma unroll
+        // z[call][party]; the call loop stays rolled (three AES bodies, not
+        // nine, keep the loop inside the instruction cache): each call shifts
+        // the rows up and appends its own, so z[c] ends up holding call c
+        uint4 z[3][3] = {};
+#pragma unroll 1
         for (int c = 0; c < 3; c++) {
             uint4 k[3];
 #pragma unroll
@@ -56,9 +59,14 @@ __global__ void __launch_bounds__(kAesThreads) k_radix_b2a(RadixB2AArgs a) {
                 st.nonce += (unsigned long long)c * a.chunks;
                 k[q] = keystream_block(S, st, b);
             }
-            z[c][0] = R::sub(k[2], k[0]);
-            z[c][1] = R::sub(k[0], k[1]);
-            z[c][2] = R::sub(k[1], k[2]);
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                z[0][p] = z[1][p];
+                z[1][p] = z[2][p];
+            }
+            z[2][0] = R::sub(k[2], k[0]);
+            z[2][1] = R::sub(k[0], k[1]);
+            z[2][2] = R::sub(k[1], k[2]);
         }
         uint32_t x[3][4];
 #pragma unroll
