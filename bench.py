@@ -46,11 +46,26 @@ WORKLOAD = ("3PC oblivious shuffle-based radix sort, 2^22 rows, uint64 key unifo
 AES_LDS_PER_BLOCK = 228
 DEFAULT_N = 1 << 22
 # DRAM traffic of the dominant k_apply instance (padded 16-byte key + int32
-# permutation, one group), dram__bytes_read.sum + dram__bytes_write.sum from
-# one ncu capture at 2^21 rows (profiles/radix_sort_2p22.md): 690.5 MB
-# (dram__bytes.sum.per_second x gpu__time_duration), scaled per row to the
-# benchmarked size.
+# permutation, one group): dram__bytes_read.sum + dram__bytes_write.sum of one
+# ncu capture of that kernel at 2^21 rows, scaled per row to the benchmarked
+# size. A constant taken from that capture, not measured by this run (a bench
+# run is never under ncu).
 APPLY_TRAFFIC_BYTES_PER_ROW = 690.5e6 / (1 << 21)
+
+
+def cpu_model():
+    """The host CPU's model name and logical core count (reported beside every
+    CPU figure)."""
+    name = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    name = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": name, "logical_cores": os.cpu_count() or 1}
 
 
 def load_peaks():
@@ -659,31 +674,41 @@ def run_orq(args, rank, world, local_rank):
 
     clocks = ClockSampler(local_rank)
     _lib = rt.lib
-    orq._check(_lib.orqcu_profile_enable(rt.h, 1))
+
+    def timed(steps):
+        evs = []
+        for _ in range(steps):
+            if flush is not None:
+                flush.fill_(1.0)  # write 256 MB: evicts L2 between timed steps
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            wl.step()
+            e1.record()
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs)
+
+    # the timed region runs without per-launch events
     k0 = rt.kernels_launched()
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    evs = []
-    for _ in range(args.steps):
-        if flush is not None:
-            flush.fill_(1.0)  # write 256 MB: evicts L2 between timed steps
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        wl.step()
-        e1.record()
-        evs.append((e0, e1))
-    torch.cuda.synchronize()
+    ms = timed(args.steps)
     clk = clocks.stop()
     barrier()
-    ms = sum(a.elapsed_time(b) for a, b in evs)
     launches = rt.kernels_launched() - k0
+    ms = max_over_ranks(ms)
+    # a separate profiled pass (CUDA events around every launch, on the stream
+    # each kernel runs on) gives the per-kernel times of the roofline
+    prof_steps = max(1, min(args.steps, 3))
+    orq._check(_lib.orqcu_profile_enable(rt.h, 1))
+    prof_ms = timed(prof_steps)
     buf = ctypes.create_string_buffer(1 << 16)
     orq._check(_lib.orqcu_profile_report(rt.h, buf, ctypes.c_size_t(len(buf))))
     orq._check(_lib.orqcu_profile_enable(rt.h, 0))
     prof = parse_profile(buf.value.decode())
-    ms = max_over_ranks(ms)
+    prof["_pass"] = {"steps": prof_steps, "ms_per_step": prof_ms / prof_steps}
 
     # ---- e2e through the public API with host buffers ----------------------
     e2e = None
@@ -713,6 +738,9 @@ def run_orq(args, rank, world, local_rank):
 
 def roofline(prof, steps, n):
     hbm, sm_mhz, src = load_peaks()
+    pas = prof.pop("_pass", None)
+    if pas:
+        steps = pas["steps"]
     # dominant kernel by device time among the ones accounted in bytes
     mem = {k: v for k, v in prof.items() if v["bytes"] > 0}
     top = max(mem.items(), key=lambda kv: kv[1]["ms"]) if mem else None
@@ -725,7 +753,8 @@ def roofline(prof, steps, n):
                            "unit": "GB/s", "frac": round(ach / hbm, 4),
                            "traffic": (round(APPLY_TRAFFIC_BYTES_PER_ROW * n)
                                        if name == "apply_group" and n else None),
-                           "traffic_note": "bytes per launch of the key-apply instance, ncu at 2^21 rows scaled by rows",
+                           "traffic_note": ("fixed constant, not measured by this run: bytes per launch of the "
+                                            "key-apply instance from one ncu capture at 2^21 rows, scaled by rows"),
                            "peak_source": src, "launches_per_step": v["launches"] / steps,
                            "avg_launch_ms": round(per_launch_ms, 4)}
     aes = {k: v for k, v in prof.items() if v["aes_blocks"] > 0}
@@ -742,6 +771,10 @@ def roofline(prof, steps, n):
     total = sum(v["ms"] for v in prof.values())
     out["kernel_time_share"] = {k: round(v["ms"] / total, 4) for k, v in
                                 sorted(prof.items(), key=lambda kv: -kv[1]["ms"])} if total else {}
+    if pas:
+        out["profile_pass"] = {"steps": pas["steps"], "ms_per_step": round(pas["ms_per_step"], 3),
+                               "note": ("per-kernel times come from this separate pass with CUDA events "
+                                        "around every launch; value is timed without them")}
     return out
 
 
@@ -783,7 +816,8 @@ def main():
     ap.add_argument("--n", type=int, default=DEFAULT_N)
     ap.add_argument("--na", type=int, default=1 << 22, help="join: rows of A (B has 4x)")
     ap.add_argument("--bits", type=int, default=40)
-    ap.add_argument("--cpu-sample", type=int, default=1 << 17)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 20,
+                    help="rows of the bounded CPU sample (radix/qsort; join uses 2^11 rows of A)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-items", type=int, default=512)
@@ -797,7 +831,7 @@ def main():
                     help="serve and join: sort protocol of sort requests and table sorts (the reference's "
                          "default is quicksort)")
     args = ap.parse_args()
-    if args.workload == "join" and args.cpu_sample == 1 << 17:
+    if args.workload == "join" and args.cpu_sample == 1 << 20:
         args.cpu_sample = 1 << 11
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -810,9 +844,18 @@ def main():
         refs = dict(WORKLOADS, batch=BatchReference, serve=ServeReference)
         wl = refs[args.workload](args, 7)
         config = dict(wl.config, parallelism=f"replicas x{args.gpus}")
-        threads = max(1, nproc // 3)
+        # the reference's best configuration on this host: one worker per party
+        # (shares identical to the GPU's) or every core (nproc/3 per party),
+        # whichever is faster on a 1/16 sample; the reference splits each call
+        # over its workers, which does not always pay
+        calib_sample = max(args.cpu_sample // 16, min(args.cpu_sample, 1 << 10))
+        cands = sorted({1, max(1, nproc // 3)})
+        calib = {t: wl.cpu_reference(calib_sample, t)[0] for t in cands} if len(cands) > 1 else {1: None}
+        threads = max(calib, key=lambda t: calib[t] or 0.0)
+        # warm-up runs are whole fresh party processes: a small sample suffices
+        warm_sample = min(args.cpu_sample, max(calib_sample // 4, 1 << 10))
         for _ in range(args.warmup):
-            wl.cpu_reference(args.cpu_sample, threads)
+            wl.cpu_reference(warm_sample, threads)
         runs = [wl.cpu_reference(args.cpu_sample, threads) for _ in range(args.steps)]
         v = statistics.mean(r[0] for r in runs)
         sample = runs[0][2]
@@ -822,7 +865,10 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic", "config": config,
             "cpu_baseline": {"value": v, "unit": "rows/s", "cores": 3 * threads, "kind": "reference",
-                             "sample": sample},
+                             "sample": sample, "cpu": cpu_model(), "threads_per_party": threads,
+                             "calibration": {"sample_rows": calib_sample,
+                                             "rows_per_s_by_threads_per_party": calib},
+                             "warmup_sample_rows": warm_sample},
             "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
@@ -899,7 +945,7 @@ def main():
     if not args.no_cpu_baseline and world == 1:
         v, _, sample = wl.cpu_reference(args.cpu_sample, 1)
         line["cpu_baseline"] = {"value": v, "unit": "rows/s", "cores": 3, "kind": "reference",
-                                "sample": sample}
+                                "sample": sample, "cpu": cpu_model(), "threads_per_party": 1}
     print(json.dumps(line))
 
 

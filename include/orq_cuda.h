@@ -149,7 +149,10 @@ int orqcu_prefix_sum_a(orqcu_runtime* rt, int width, size_t n, void* const share
  * library, held on every GPU that loads it until the process exits, so n is
  * limited to 2^26 elements (larger n returns ORQCU_EINVAL and touches nothing).
  * The first call on a device looks up the array's device address, so make
- * that first call before any stream capture. All calls share the array: calls
+ * that first call before any stream capture; the address is looked up again
+ * after the last runtime on the device has been destroyed (a cudaDeviceReset
+ * while a runtime of the device is alive is not supported). All calls share
+ * the array: calls
  * that overlap on the GPU (on any streams) race and must be serialised. No
  * cudaMalloc, cudaFree or other allocating routine is called. */
 int orqcu_prefix_sum_a_noalloc(orqcu_runtime* rt, int width, size_t n, void* const shares[3]);
@@ -258,10 +261,11 @@ typedef struct {
  * aggregation network over n rows (a power of two) of width-byte shares (4 or
  * 8). keys: nkeys B-shared key columns, 3 pointers each (keys[3*j+p]); b_specs
  * are boolean aggregations (copy, valid, bit_or), a_specs arithmetic ones
- * (sum, count, copy); reverse selects Direction::Reverse; sel (3 pointers, or
- * NULL) is the table-id column that restricts non-copy aggregations to rows of
- * the same table. One fused launch per network level; at most 4 keys and 8
- * specs of each kind. min/max return ORQCU_EINVAL on the device path. */
+ * (sum, count, copy) — min and max (boolean, by the compare circuit's packed
+ * sign fix-up) are accepted among b_specs; reverse selects
+ * Direction::Reverse; sel (3 pointers, or NULL) is the table-id column that
+ * restricts non-copy aggregations to rows of the same table. One fused launch
+ * per network level; at most 4 keys and 8 specs of each kind. */
 int orqcu_aggregate(orqcu_runtime* rt, int width, size_t n, int nkeys, const void* const* keys,
                     int nb, const orqcu_agg_spec* b_specs, int na, const orqcu_agg_spec* a_specs,
                     int reverse, const void* const* sel);

@@ -69,7 +69,13 @@ int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out) {
         ORQ_CUDA_CHECK(cudaMalloc(&rt->ctx.d_err, sizeof(int)));
         ORQ_CUDA_CHECK(cudaMemset(rt->ctx.d_err, 0, sizeof(int)));
         orqcu::init_ctx_keys(rt->ctx, seed);
-        orqcu::upload_aes_tables(device);
+        orqcu::device_runtime_opened(device);
+        try {
+            orqcu::upload_aes_tables(device);
+        } catch (...) {
+            orqcu::device_runtime_closed(device);
+            throw;
+        }
         *out = rt;
     });
 }
@@ -85,6 +91,7 @@ int orqcu_runtime_destroy(orqcu_runtime* rt) {
         orqcu::release_fy(rt->ctx);
         if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
         if (rt->ctx.d_err) cudaFree(rt->ctx.d_err);
+        orqcu::device_runtime_closed(rt->ctx.device);
         delete rt;
     });
 }

@@ -903,6 +903,18 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     auto& scan_done = R.scan_done;
     auto& st_ev = R.st_ev;
     static_assert(kRing <= kFyRingMax, "ring deeper than the cached events");
+    // On every exit path (an exception included) the generator and scanner
+    // streams are drained before the ring, state and output scratch above go
+    // back to the pool: a later call on the runtime's stream could otherwise
+    // be handed memory those kernels are still writing. Declared after the
+    // scratch buffers, so it runs before their destructors.
+    struct DrainSideStreams {
+        FyRes& r;
+        ~DrainSideStreams() {
+            cudaStreamSynchronize(r.gs);
+            for (int g = 0; g < 3; g++) cudaStreamSynchronize(r.ss[g]);
+        }
+    } drain{R};
     ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
     ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
     for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], ev_start, 0));

@@ -108,11 +108,37 @@ int register_aes_table_uploader(AesTableUploader f) {
     return (int)uploaders().size();
 }
 
+namespace {
+std::mutex g_dev_mu;
+int g_dev_live[kMaxDevices] = {};
+unsigned long long g_dev_epoch[kMaxDevices] = {};
+}  // namespace
+
+void device_runtime_opened(int device) {
+    if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    g_dev_live[device]++;
+}
+
+void device_runtime_closed(int device) {
+    if (device < 0 || device >= kMaxDevices) return;
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    if (g_dev_live[device] > 0 && --g_dev_live[device] == 0) g_dev_epoch[device]++;
+}
+
+unsigned long long device_epoch(int device) {
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    return (device >= 0 && device < kMaxDevices) ? g_dev_epoch[device] : 0ull;
+}
+
 void upload_aes_tables(int device) {
-    static bool done[64] = {false};
+    // epoch + 1 of the last upload per device (0: never uploaded)
+    static unsigned long long done[kMaxDevices] = {};
     static std::mutex mu;
     std::lock_guard<std::mutex> lk(mu);
-    if (device >= 0 && device < 64 && done[device]) return;
+    if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device ordinal out of range");
+    const unsigned long long ep = device_epoch(device) + 1;
+    if (done[device] == ep) return;
     const uint8_t* S = sbox();
     uint32_t T[4 * 256];
     for (int x = 0; x < 256; x++) {
@@ -124,7 +150,7 @@ void upload_aes_tables(int device) {
         T[768 + x] = (t0 << 24) | (t0 >> 8);
     }
     for (AesTableUploader f : uploaders()) f(T);
-    if (device >= 0 && device < 64) done[device] = true;
+    done[device] = ep;
 }
 
 // ---------------------------------------------------------------------------

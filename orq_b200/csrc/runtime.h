@@ -177,6 +177,16 @@ void derive_key(uint64_t seed, int party, int call, uint8_t key[32]);
 void aes256_expand(const uint8_t key[32], uint32_t rk[60]);
 void init_ctx_keys(Ctx& c, uint64_t seed);
 void upload_aes_tables(int device);
+// Per-device set-up (the AES tables, the address of the no-alloc scratch
+// array) is done once per device and remembered with the device's epoch. The
+// epoch advances when the last live runtime on the device is destroyed, so a
+// cudaDeviceReset between runtimes (which drops the context's memory and can
+// move its module globals) makes the next runtime redo the set-up. A reset
+// while a runtime of that device is alive is not supported.
+void device_runtime_opened(int device);
+void device_runtime_closed(int device);
+unsigned long long device_epoch(int device);
+constexpr int kMaxDevices = 64;
 
 // ---- primitives (prims.cu) ----
 void launch_keystream(Ctx& c, int stream_id, unsigned long long nonce0, void* out, size_t nbytes);

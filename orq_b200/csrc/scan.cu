@@ -155,19 +155,24 @@ static __device__ __align__(256) unsigned long long g_noalloc_tsum[3 * kNoAllocT
 
 // Device address of g_noalloc_tsum on `device`, looked up once per device with
 // that device current (host code may not pass the symbol itself to a kernel).
+// The address is remembered with the device's epoch: once the last runtime on
+// the device is destroyed (after which the context may have been reset and
+// the array moved) the next call looks it up again.
 static void* noalloc_scratch(int device) {
-    constexpr int kMaxDevices = 64;
     static std::mutex mu;
     static void* ptrs[kMaxDevices] = {};
+    static unsigned long long epoch[kMaxDevices] = {};
     if (device < 0 || device >= kMaxDevices) throw std::invalid_argument("device ordinal out of range");
     std::lock_guard<std::mutex> lk(mu);
-    if (ptrs[device]) return ptrs[device];
+    const unsigned long long ep = device_epoch(device);
+    if (ptrs[device] && epoch[device] == ep) return ptrs[device];
     int cur = -1;
     ORQ_CUDA_CHECK(cudaGetDevice(&cur));
     if (cur != device) throw std::runtime_error("the runtime's device is not the current device");
     void* p = nullptr;
     ORQ_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_tsum));
     ptrs[device] = p;
+    epoch[device] = ep;
     return p;
 }
 

@@ -83,6 +83,11 @@ CASES = [
     ("a2b64_n20000", "a2b64", 20000, 9, 4, 64, False),
     ("badd32_n500", "badd32", 500, 7, 2, 32, True),
     ("badd64_n333", "badd64", 333, 8, 3, 64, True),
+    # the 2^22-row headline workload and 2^20: every Fisher-Yates permutation
+    # spans many 2^20-draw getNext buffers (about 127 at 2^22)
+    ("radix_n1048576_b40", "radix", 1 << 20, 7, 7, 40, False),
+    ("radix_n4194304_b40", "radix", 1 << 22, 7, 7, 40, False),
+    ("qsort_n1048576_b40", "qsort", 1 << 20, 7, 7, 40, False),
 ]
 
 

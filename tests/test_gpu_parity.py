@@ -134,6 +134,29 @@ def test_radix_large_matches_reference_digests(orq, digests):
         assert [sha(a) for a in arr] == d["arrays"][name], name
 
 
+@pytest.mark.parametrize("tag", ["radix_n1048576_b40", "radix_n4194304_b40"])
+def test_radix_headline_size_matches_reference_digests(orq, digests, tag):
+    """Share-level parity at 2^20 and at the benchmarked 2^22 rows (40-bit
+    keys, seed 7, two payloads): the key, both payloads and the sorting
+    permutation equal the reference's shares, digest for digest. At these
+    sizes each of the 44 Fisher-Yates permutations per group spans many
+    2^20-draw getNext buffers (about 127 at 2^22), so the chained nonces, the
+    buffer-end accounting and the multi-window scan are all pinned."""
+    d = digests[tag]
+    m = d["meta"]
+    out, _ = replay_radix(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+def test_quicksort_2p20_matches_reference_digests(orq, digests):
+    d = digests["qsort_n1048576_b40"]
+    m = d["meta"]
+    out, _ = replay_qsort(GpuBackend(m["shim_seed"]), m["n"], m["data_seed"], m["bits"], 8)
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
 @pytest.mark.parametrize("n,bits", [(1, 40), (2, 3), (1023, 16), (4096, 40)])
 def test_radix_matches_restatement(orq, n, bits):
     gpu, _ = replay_radix(GpuBackend(31), n, 17, bits)

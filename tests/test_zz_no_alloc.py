@@ -44,6 +44,34 @@ def test_noalloc_prefix_sum_equals_pooled_on_two_calls(cuda_lib, w):
         assert np.array_equal(fixed.open().cpu().numpy().view(dt), want)
 
 
+@pytest.mark.parametrize("w", [4, 8])
+def test_noalloc_prefix_sum_takes_no_device_memory(cuda_lib, w):
+    """After one warm-up call (which loads the kernels), a call leaves the
+    runtime's pool empty (any pooled scratch would be cached there after its
+    release), leaves torch's allocator untouched and does not change the
+    device's free memory."""
+    import torch
+
+    import orq_b200 as orq
+
+    rt = orq.Runtime(seed=6)
+    n = (1 << 22) + 9
+    dt = {4: np.uint32, 8: np.uint64}[w]
+    v = rt.secret_share_a(np.arange(n, dtype=dt), 0)
+    ptrs = _p3(v.shares)
+    assert cuda_lib.orqcu_prefix_sum_a_noalloc(rt.h, w, ctypes.c_size_t(n), ptrs) == 0
+    torch.cuda.synchronize()
+    rt.trim()
+    torch.cuda.synchronize()
+    free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+    assert cuda_lib.orqcu_prefix_sum_a_noalloc(rt.h, w, ctypes.c_size_t(n), ptrs) == 0
+    torch.cuda.synchronize()
+    assert rt.trim() == 0, "the call cached pooled scratch"
+    torch.cuda.synchronize()
+    assert torch.cuda.memory_allocated() == alloc0
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_prefix_sum_refuses_oversized(cuda_lib):
     import torch
 
