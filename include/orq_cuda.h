@@ -84,6 +84,17 @@ int orqcu_malloc(orqcu_runtime* rt, size_t bytes, void** dptr);
 int orqcu_free(orqcu_runtime* rt, void* dptr);
 int orqcu_memcpy_h2d(orqcu_runtime* rt, void* dst_dev, const void* src_host, size_t bytes);
 int orqcu_memcpy_d2h(orqcu_runtime* rt, void* dst_host, const void* src_dev, size_t bytes);
+/* Stream-ordered device memory from the runtime's pool (the storage behind
+ * ORQ's Vector / EVector, mapping_access_vector.h:208-260): a block freed here
+ * is reused by later work on the runtime's stream without synchronising the
+ * device. Only pointers from orqcu_pool_alloc may be passed to orqcu_pool_free. */
+int orqcu_pool_alloc(orqcu_runtime* rt, size_t bytes, void** dptr);
+int orqcu_pool_free(orqcu_runtime* rt, void* dptr);
+/* Device-to-device copy and byte fill, asynchronous on the runtime's stream
+ * (Vector's deep operator=, mapping_access_vector.h:1263, and zero-initialised
+ * storage). */
+int orqcu_memcpy_d2d(orqcu_runtime* rt, void* dst_dev, const void* src_dev, size_t bytes);
+int orqcu_memset(orqcu_runtime* rt, void* dst_dev, int byte, size_t bytes);
 
 /* Keystream of `stream` starting at nonce0 (AESPRGAlgorithm::fillBytes,
  * prg_algorithm.h:161-172); does not advance the stream. */

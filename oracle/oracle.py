@@ -298,3 +298,70 @@ class Oracle:
     def sub_b(self, x, y):
         """BSharedVector::operator- (x + ~y + 1 by the adder)."""
         return self._bin(self.lib.oro_sub_b, x, y)
+
+
+class OracleNP:
+    """Restatement of the Beaver-2PC (dummy triples) and Fantastic-4PC local
+    steps (orq_oracle.c, oro_np_*). A vector is a list of the distinct shares:
+    [S0, S1] for 2PC, [X0, X1, X2, X3] for 4PC (X[j] is the share party j
+    lacks)."""
+
+    def __init__(self, seed: int, nparties: int):
+        assert nparties in (2, 4)
+        self.np = nparties
+        self.lib = _lib()
+        self.ctx = _Ctx()
+        self.lib.oro_ctx_init_np(ctypes.byref(self.ctx), ctypes.c_uint64(seed), nparties)
+
+    def _p(self, arrs):
+        return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+    def new(self, n, w):
+        return [np.zeros(n, dtype=_DT[w]) for _ in range(self.np)]
+
+    def secret_share(self, data, arith, party=0):
+        data = np.ascontiguousarray(data)
+        w = data.itemsize
+        s = self.new(len(data), w)
+        self.lib.oro_np_secret_share(ctypes.byref(self.ctx), self.np, int(arith), w, ctypes.c_size_t(len(data)),
+                                     data.ctypes.data_as(ctypes.c_void_p), party, self._p(s))
+        return s
+
+    def open(self, s, arith):
+        w = s[0].itemsize
+        out = np.zeros(len(s[0]), dtype=_DT[w])
+        self.lib.oro_np_open(self.np, int(arith), w, ctypes.c_size_t(len(s[0])), self._p(s),
+                             out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def _mult(self, x, y, arith):
+        w = x[0].itemsize
+        z = self.new(len(x[0]), w)
+        self.lib.oro_np_mult(ctypes.byref(self.ctx), self.np, int(arith), w, ctypes.c_size_t(len(x[0])),
+                             self._p(x), self._p(y), self._p(z))
+        return z
+
+    def and_b(self, x, y):
+        return self._mult(x, y, False)
+
+    def mul_a(self, x, y):
+        return self._mult(x, y, True)
+
+    def b2a_bit(self, x):
+        w = x[0].itemsize
+        y = self.new(len(x[0]), w)
+        self.lib.oro_np_b2a_bit(ctypes.byref(self.ctx), self.np, w, ctypes.c_size_t(len(x[0])), self._p(x),
+                                self._p(y))
+        return y
+
+    def _local(self, op, x, y):
+        w = x[0].itemsize
+        z = self.new(len(x[0]), w)
+        self.lib.oro_np_local(self.np, op, w, ctypes.c_size_t(len(x[0])), self._p(x), self._p(y), self._p(z))
+        return z
+
+    def xor_b(self, x, y):
+        return self._local(0, x, y)
+
+    def add_a(self, x, y):
+        return self._local(1, x, y)

@@ -1666,3 +1666,185 @@ void oro_a2b(oro_ctx* c, int w, size_t n, void* const x[3], void* y[3]) {
     free3(F);
     free3(G);
 }
+
+/* ========================================================================= */
+/* Beaver 2PC (core/protocols/beaver_2pc.h) with dummy triples and
+ * Fantastic-4PC (core/protocols/dalskov_4pc.h): the local steps of all
+ * parties in one process. */
+
+/* Keys (rand_setup.h:306-381). 2PC: call 0 local PRG, call 1 group {0,1} on
+ * P0 (the everyone group is the same set and P0's call 2 is discarded).
+ * 4PC: call 0 local PRG; P0 draws the group keys of {0,1,2}, {2,3,0},
+ * {3,0,1} and the everyone group (calls 1-4), P1 that of {1,2,3} (call 1);
+ * then setup_4pc_common_prgs (rand_setup.h:154-221) draws one more key per
+ * party (P0 call 5, P1 call 2, P2 call 1, P3 call 1): party q's key seeds the
+ * PRG of {q, q-1, q-2}, the one that excludes q+1. */
+void oro_ctx_init_np(oro_ctx* c, uint64_t seed, int nparties) {
+    static const int who2[3][2] = {{0, 1}, {0, 0}, {1, 0}};
+    static const int who4[8][2] = {{3, 1}, {0, 5}, {1, 2}, {2, 1}, {0, 0}, {1, 0}, {2, 0}, {3, 0}};
+    memset(c, 0, sizeof(*c));
+    const int ns = nparties == 2 ? 3 : 8;
+    for (int s = 0; s < ns; s++) {
+        uint8_t key[32];
+        const int* wh = nparties == 2 ? who2[s] : who4[s];
+        oro_derive_key(seed, wh[0], wh[1], key);
+        oro_aes256_expand(key, c->rk[s]);
+    }
+}
+
+static u128 ar(int arith, u128 a, u128 b) { return arith ? a + b : a ^ b; }
+static u128 sr(int arith, u128 a, u128 b) { return arith ? a - b : a ^ b; }
+static u128 mr(int arith, u128 a, u128 b) { return arith ? a * b : a & b; }
+
+/* 2PC secret_share_b/a (beaver_2pc.h:214-260): the owner d keeps
+ * r = localPRG_d.getNext(n) and sends data - r (data ^ r).
+ * 4PC (dalskov_4pc.h:152-201): s0, s1, s2 from the owner's local PRG,
+ * s3 = data - s0 - s1 - s2; party d+k lacks s_k, so X[(d+k)%4] = s_k. */
+void oro_np_secret_share(oro_ctx* c, int np, int arith, int w, size_t n, const void* data, int d,
+                         void* const* s) {
+    if (np == 2) {
+        oro_stream_fill(c, ORO_P2_LOCAL0 + d, s[d], n, w);
+        for (size_t i = 0; i < n; i++) st(s[1 - d], i, w, sr(arith, ld(data, i, w), ld(s[d], i, w)));
+        return;
+    }
+    void* sk[4];
+    for (int k = 0; k < 4; k++) sk[k] = s[(d + k) % 4];
+    for (int k = 0; k < 3; k++) oro_stream_fill(c, ORO_P4_LOCAL0 + d, sk[k], n, w);
+    for (size_t i = 0; i < n; i++) {
+        u128 v = ld(data, i, w);
+        for (int k = 0; k < 3; k++) v = sr(arith, v, ld(sk[k], i, w));
+        st(sk[3], i, w, v);
+    }
+}
+
+void oro_np_open(int np, int arith, int w, size_t n, void* const* s, void* out) {
+    for (size_t i = 0; i < n; i++) {
+        u128 v = 0;
+        for (int k = 0; k < np; k++) v = ar(arith, v, ld(s[k], i, w));
+        st(out, i, w, v);
+    }
+}
+
+/* op: 0 xor, 1 add, 2 sub (local on every share) */
+void oro_np_local(int np, int op, int w, size_t n, void* const* x, void* const* y, void* const* z) {
+    for (int k = 0; k < np; k++)
+        for (size_t i = 0; i < n; i++) {
+            u128 a = ld(x[k], i, w), b = ld(y[k], i, w);
+            st(z[k], i, w, op == 0 ? a ^ b : op == 1 ? a + b : a - b);
+        }
+}
+
+/* next_party / excluded_party (dalskov_4pc.h:11-24) */
+static int f4_next(int i, int j) {
+    int a = i < j ? i : j, b = i < j ? j : i;
+    return b == (a + 1) % 4 ? (b + 1) % 4 : (a + 1) % 4;
+}
+
+/* 4PC inp<E>(v, Pi, Pj, Pg, Ph) (dalskov_4pc.h:300-340) accumulated into r:
+ * X'[g] = R from the PRG that excludes g, X'[h] = v - R (v ^ R), others 0. */
+static void f4_inp_acc(oro_ctx* c, int arith, int w, size_t n, const void* v, int g, int h, void* r[4]) {
+    void* R = xalloc(n * (size_t)w);
+    oro_stream_fill(c, ORO_P4_NOT0 + g, R, n, w);
+    for (size_t i = 0; i < n; i++) {
+        u128 rr = ld(R, i, w);
+        st(r[g], i, w, ar(arith, ld(r[g], i, w), rr));
+        st(r[h], i, w, ar(arith, ld(r[h], i, w), sr(arith, ld(v, i, w), rr)));
+    }
+    free(R);
+}
+
+void oro_np_mult(oro_ctx* c, int np, int arith, int w, size_t n, void* const* x, void* const* y,
+                 void* const* z) {
+    if (np == 2) {
+        /* DummyOLE::getNext(2n) (dummy_ole.h): B, C, D from the common PRG,
+         * A = C*D - B (B ^ C&D); P0 gets (A, C), P1 (B, D). Beaver triple
+         * (beaver_triple_generator.h:getNext): P0 a=C[:n] b=C[n:]
+         * c=a*b+A[:n]+A[n:]; P1 a=D[n:] b=D[:n] c=a*b+B[:n]+B[n:].
+         * multiply_a / and_b (beaver_2pc.h:50-59,108-117): A' = open(x+a),
+         * B' = open(y+b), z_p = y_p*A' - a_p*B' + c_p. */
+        const size_t m = 2 * n;
+        uint8_t* B = xalloc(m * (size_t)w);
+        uint8_t* C = xalloc(m * (size_t)w);
+        uint8_t* D = xalloc(m * (size_t)w);
+        oro_stream_fill(c, ORO_P2_COMMON, B, m, w);
+        oro_stream_fill(c, ORO_P2_COMMON, C, m, w);
+        oro_stream_fill(c, ORO_P2_COMMON, D, m, w);
+        for (size_t i = 0; i < n; i++) {
+            u128 Cl = ld(C, i, w), Cr = ld(C, n + i, w), Dl = ld(D, i, w), Dr = ld(D, n + i, w);
+            u128 Bl = ld(B, i, w), Br = ld(B, n + i, w);
+            u128 Al = sr(arith, mr(arith, Cl, Dl), Bl), Arr = sr(arith, mr(arith, Cr, Dr), Br);
+            if (!arith) {
+                Al = Bl ^ (Cl & Dl);
+                Arr = Br ^ (Cr & Dr);
+            }
+            u128 a[2] = {Cl, Dr}, b[2] = {Cr, Dl};
+            u128 cc[2] = {ar(arith, ar(arith, mr(arith, Cl, Cr), Al), Arr),
+                          ar(arith, ar(arith, mr(arith, Dr, Dl), Bl), Br)};
+            u128 x0 = ld(x[0], i, w), x1 = ld(x[1], i, w), y0 = ld(y[0], i, w), y1 = ld(y[1], i, w);
+            u128 Ao = ar(arith, ar(arith, x0, a[0]), ar(arith, x1, a[1]));
+            u128 Bo = ar(arith, ar(arith, y0, b[0]), ar(arith, y1, b[1]));
+            u128 yy[2] = {y0, y1};
+            for (int p = 0; p < 2; p++)
+                st(z[p], i, w, ar(arith, sr(arith, mr(arith, yy[p], Ao), mr(arith, a[p], Bo)), cc[p]));
+        }
+        free(B);
+        free(C);
+        free(D);
+        return;
+    }
+    /* 4PC multiply_a / and_b (dalskov_4pc.h:384-420,479-506): for the pairs
+     * (0,1) (0,2) (0,3) (1,2) (1,3) (2,3), inp of X_h*Y_g + X_g*Y_h into the
+     * result, then Z_k += X_k*Y_k. */
+    void* r[4];
+    void* v = xalloc(n * (size_t)w);
+    for (int k = 0; k < 4; k++) r[k] = xalloc(n * (size_t)w);
+    for (int i = 0; i < 4; i++)
+        for (int j = i + 1; j < 4; j++) {
+            int g = f4_next(i, j), h = 6 - i - j - g;
+            for (size_t e = 0; e < n; e++) {
+                u128 xh = ld(x[h], e, w), xg = ld(x[g], e, w), yh = ld(y[h], e, w), yg = ld(y[g], e, w);
+                st(v, e, w, ar(arith, mr(arith, xh, yg), mr(arith, xg, yh)));
+            }
+            f4_inp_acc(c, arith, w, n, v, g, h, r);
+        }
+    for (int k = 0; k < 4; k++) {
+        for (size_t e = 0; e < n; e++)
+            st(z[k], e, w, ar(arith, ld(r[k], e, w), mr(arith, ld(x[k], e, w), ld(y[k], e, w))));
+        free(r[k]);
+    }
+    free(v);
+}
+
+void oro_np_b2a_bit(oro_ctx* c, int np, int w, size_t n, void* const* x, void* const* y) {
+    void* t[4];
+    for (int k = 0; k < np; k++) t[k] = xalloc(n * (size_t)w);
+    if (np == 2) {
+        /* beaver_2pc.h:147-158: xm = x & 1, P1 negates its share, xm * xm */
+        for (size_t i = 0; i < n; i++) {
+            st(t[0], i, w, ld(x[0], i, w) & 1);
+            st(t[1], i, w, (u128)0 - (ld(x[1], i, w) & 1));
+        }
+    } else {
+        /* dalskov_4pc.h:562-590: s0 = X2^X3 (bits, held by P0 and P1) shared by
+         * inp(s0, 1, 0) (g = 2, h = 3), s1 = X0^X1 shared by inp(s1, 3, 2)
+         * (g = 0, h = 1); share0 - share1, squared */
+        void* s0 = xalloc(n * (size_t)w);
+        void* s1 = xalloc(n * (size_t)w);
+        void* u[4];
+        for (int k = 0; k < 4; k++) u[k] = xalloc(n * (size_t)w);
+        for (size_t i = 0; i < n; i++) {
+            st(s0, i, w, (ld(x[2], i, w) ^ ld(x[3], i, w)) & 1);
+            st(s1, i, w, (ld(x[0], i, w) ^ ld(x[1], i, w)) & 1);
+        }
+        f4_inp_acc(c, 1, w, n, s0, 2, 3, t);
+        f4_inp_acc(c, 1, w, n, s1, 0, 1, u);
+        for (int k = 0; k < 4; k++) {
+            for (size_t i = 0; i < n; i++) st(t[k], i, w, ld(t[k], i, w) - ld(u[k], i, w));
+            free(u[k]);
+        }
+        free(s0);
+        free(s1);
+    }
+    oro_np_mult(c, np, 1, w, n, t, t, y);
+    for (int k = 0; k < np; k++) free(t[k]);
+}

@@ -147,6 +147,25 @@ void oro_bitonic_sort_rows(oro_ctx* c, int w, size_t n, int nkeys, void* const* 
                            const int* desc, int na, void* const* data_a, int nb,
                            void* const* data_b);
 
+/* ---- Beaver 2PC with dummy triples and Fantastic-4PC: the local steps ----
+ * A context for `nparties` = 2 or 4 holds that protocol's streams:
+ *   2PC: ORO_P2_COMMON (group {0,1}, P0's keygen call 1), ORO_P2_LOCAL0/1;
+ *   4PC: ORO_P4_NOT0..3 (the PRG shared by the three parties other than e,
+ *        keyed by party e-1's setup_4pc_common_prgs key), ORO_P4_LOCAL0..3.
+ * A 2PC vector is S[0], S[1] (party p holds S[p]); a 4PC vector is X[0..3]
+ * where X[j] is the share party j lacks (party p holds X[p+1], X[p+2],
+ * X[p+3] as its local shares 0, 1, 2). */
+enum { ORO_P2_COMMON = 0, ORO_P2_LOCAL0 = 1, ORO_P2_LOCAL1 = 2 };
+enum { ORO_P4_NOT0 = 0, ORO_P4_LOCAL0 = 4 };
+void oro_ctx_init_np(oro_ctx* c, uint64_t seed, int nparties);
+void oro_np_secret_share(oro_ctx* c, int np, int arith, int w, size_t n, const void* data, int d,
+                         void* const* s);
+void oro_np_open(int np, int arith, int w, size_t n, void* const* s, void* out);
+void oro_np_mult(oro_ctx* c, int np, int arith, int w, size_t n, void* const* x, void* const* y,
+                 void* const* z);
+void oro_np_b2a_bit(oro_ctx* c, int np, int w, size_t n, void* const* x, void* const* y);
+void oro_np_local(int np, int op, int w, size_t n, void* const* x, void* const* y, void* const* z);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,7 +9,9 @@
  *     -> made deterministic: key = SplitMix64 stream keyed by (seed, party, call
  *        index), seed from ORQ_SHIM_SEED and party from STARTMPC_HOST_RANK, so
  *        the GPU runtime can derive the same keys (oro_derive_key);
- *   - crypto_stream_xchacha20*, crypto_generichash* (2PC/4PC only) -> abort.
+ *   - crypto_generichash* (4PC transcript hashes) -> SHA-512 through OpenSSL
+ *     (consistent between parties; shares never depend on it);
+ *   - crypto_stream_xchacha20* -> abort (not on the path).
  */
 #pragma once
 
@@ -101,25 +103,44 @@ static inline int crypto_stream_xchacha20(unsigned char* c, unsigned long long c
     fprintf(stderr, "[shim] xchacha20 is not provided\n");
     abort();
 }
+/* crypto_generichash* (the 4PC transcript hashes, dalskov_4pc.h:107-111):
+ * here SHA-512 truncated to the requested length through OpenSSL. The hashes
+ * only let honest parties compare their views; every party computes the same
+ * function, so the checks pass and no share depends on it. */
+static inline EVP_MD_CTX** orq_shim_hash_ctx(crypto_generichash_state* s) {
+    return (EVP_MD_CTX**)(void*)s->opaque;
+}
 static inline int crypto_generichash_init(crypto_generichash_state* s, const unsigned char* key,
                                           size_t keylen, size_t outlen) {
-    (void)s, (void)key, (void)keylen, (void)outlen;
-    fprintf(stderr, "[shim] generichash is not provided\n");
-    abort();
+    (void)outlen;
+    EVP_MD_CTX** c = orq_shim_hash_ctx(s);
+    *c = EVP_MD_CTX_new();
+    if (!*c || !EVP_DigestInit_ex(*c, EVP_sha512(), NULL)) abort();
+    if (key && keylen) EVP_DigestUpdate(*c, key, keylen);
+    return 0;
 }
 static inline int crypto_generichash_update(crypto_generichash_state* s, const unsigned char* in,
                                             unsigned long long inlen) {
-    (void)s, (void)in, (void)inlen;
-    abort();
+    EVP_MD_CTX** c = orq_shim_hash_ctx(s);
+    if (inlen && !EVP_DigestUpdate(*c, in, (size_t)inlen)) abort();
+    return 0;
 }
 static inline int crypto_generichash_final(crypto_generichash_state* s, unsigned char* out,
                                            size_t outlen) {
-    (void)s, (void)out, (void)outlen;
-    abort();
+    EVP_MD_CTX** c = orq_shim_hash_ctx(s);
+    unsigned char md[64];
+    unsigned int len = 0;
+    if (!EVP_DigestFinal_ex(*c, md, &len)) abort();
+    EVP_MD_CTX_free(*c);
+    *c = NULL;
+    memcpy(out, md, outlen < 64 ? outlen : 64);
+    return 0;
 }
 static inline int crypto_generichash(unsigned char* out, size_t outlen, const unsigned char* in,
                                      unsigned long long inlen, const unsigned char* key,
                                      size_t keylen) {
-    (void)out, (void)outlen, (void)in, (void)inlen, (void)key, (void)keylen;
-    abort();
+    crypto_generichash_state st;
+    crypto_generichash_init(&st, key, keylen, outlen);
+    crypto_generichash_update(&st, in, inlen);
+    return crypto_generichash_final(&st, out, outlen);
 }

@@ -71,21 +71,57 @@ def parse_dump(path: str) -> dict:
 DRIVER_QS = os.path.join(HERE, "_ref", "ref_driver_qs")  # EncodedTable sorts by quicksort
 
 
+DRIVER_2PC = os.path.join(HERE, "_ref", "ref_driver_2pc")  # Beaver 2PC, dummy triples
+DRIVER_4PC = os.path.join(HERE, "_ref", "ref_driver_4pc")  # Fantastic-4PC
+
+
+def parse_dump_k(path: str) -> dict:
+    """Records written by ref_driver_np.cpp: name, element width, n, k, then
+    the k local share columns of the party (raw little-endian)."""
+    out = {}
+    with open(path, "rb") as f:
+        data = f.read()
+    off = 0
+    while off < len(data):
+        (nl,) = struct.unpack_from("<I", data, off)
+        off += 4
+        name = data[off : off + nl].decode()
+        off += nl
+        w, n, k = struct.unpack_from("<IQI", data, off)
+        off += 16
+        cols = []
+        for _ in range(k):
+            cols.append(np.frombuffer(data, dtype=_DT[w], count=n, offset=off).copy())
+            off += n * w
+        out[name] = cols
+    return out
+
+
+def run_np(nparties: int, op: str, n: int, data_seed: int, shim_seed: int = 1, timeout: float = 600.0):
+    """Run ref_driver_np (Beaver 2PC or Fantastic-4PC) on 2 or 4 parties.
+    Returns (list of per-party dicts of local share columns, stdout of P0)."""
+    driver = {2: DRIVER_2PC, 4: DRIVER_4PC}[nparties]
+    return run(op, n, data_seed, shim_seed=shim_seed, timeout=timeout, driver=driver, nparties=nparties,
+               parser=parse_dump_k)
+
+
 def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
         threads: int = 1, batch: int = -1, timeout: float = 600.0, outdir: str | None = None,
-        driver: str | None = None):
-    """Run one op on 3 parties. Returns (list of per-party dicts, stdout of P0)."""
+        driver: str | None = None, nparties: int = 3, parser=None):
+    """Run one op on 3 parties (or `nparties` with another driver). Returns
+    (list of per-party dicts, stdout of P0)."""
     driver = driver or DRIVER
+    parser = parser or parse_dump
     if not os.path.exists(driver):
         raise FileNotFoundError(driver + " (run `make -C oracle ref`)")
     tmp = outdir or tempfile.mkdtemp(prefix="orqref_")
     base = _free_base_port()
     procs = []
-    for rank in range(3):
+    for rank in range(nparties):
         env = dict(os.environ)
         env.update({
             "STARTMPC_EXEC_MODE": "0",
-            "STARTMPC_HOST_COUNT": "3",
+            "STARTMPC_HOST_COUNT": str(nparties),
             "STARTMPC_HOST_RANK": str(rank),
             "STARTMPC_BASE_PORT": str(base),
             "ORQ_SHIM_SEED": str(shim_seed),
@@ -94,7 +130,7 @@ def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
         procs.append(subprocess.Popen(cmd, env=env, stdout=subprocess.PIPE,
                                       stderr=subprocess.PIPE, start_new_session=True))
     deadline = time.time() + timeout
-    outs = [None, None, None]
+    outs = [None] * nparties
     try:
         for i, p in enumerate(procs):
             left = max(1.0, deadline - time.time())
@@ -107,7 +143,7 @@ def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
     for i, p in enumerate(procs):
         if p.returncode != 0:
             raise RuntimeError(f"party {i} exited {p.returncode}: {outs[i][1].decode()[-2000:]}")
-    dumps = [parse_dump(os.path.join(tmp, f"p{r}.bin")) for r in range(3)]
+    dumps = [parser(os.path.join(tmp, f"p{r}.bin")) for r in range(nparties)]
     return dumps, outs[0][0].decode()
 
 
@@ -128,3 +164,22 @@ if __name__ == "__main__":
     print(o)
     for k in d[0]:
         print(k, d[0][k][0][:4])
+
+
+def distinct_shares_np(dumps: list, name: str, nparties: int):
+    """The distinct shares of a 2PC or 4PC vector from the parties' dumps.
+    2PC: party p holds S[p]. 4PC: party p's local share k is X[(p + k + 1) % 4]
+    (X[j] is the share party j lacks); the three holders of each X[j] must
+    agree."""
+    if nparties == 2:
+        return [dumps[0][name][0], dumps[1][name][0]]
+    X = [None] * 4
+    for p in range(4):
+        for k in range(3):
+            j = (p + k + 1) % 4
+            col = dumps[p][name][k]
+            if X[j] is None:
+                X[j] = col
+            elif not np.array_equal(X[j], col):
+                raise AssertionError(f"{name}: holders of X[{j}] disagree (party {p})")
+    return X

@@ -188,6 +188,37 @@ int orqcu_memcpy_d2h(orqcu_runtime* rt, void* dst, const void* src, size_t bytes
     });
 }
 
+int orqcu_pool_alloc(orqcu_runtime* rt, size_t bytes, void** dptr) {
+    return guard([&] {
+        need_rt(rt);
+        need(dptr != nullptr, "null output");
+        cudaSetDevice(rt->ctx.device);
+        *dptr = rt->ctx.alloc(bytes ? bytes : 1);
+    });
+}
+int orqcu_pool_free(orqcu_runtime* rt, void* dptr) {
+    return guard([&] {
+        need_rt(rt);
+        rt->ctx.release(dptr);
+    });
+}
+int orqcu_memcpy_d2d(orqcu_runtime* rt, void* dst, const void* src, size_t bytes) {
+    return guard([&] {
+        need_rt(rt);
+        if (!bytes) return;
+        need(dst != nullptr && src != nullptr, "null pointer");
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, rt->ctx.stream));
+    });
+}
+int orqcu_memset(orqcu_runtime* rt, void* dst, int byte, size_t bytes) {
+    return guard([&] {
+        need_rt(rt);
+        if (!bytes) return;
+        need(dst != nullptr, "null pointer");
+        ORQ_CUDA_CHECK(cudaMemsetAsync(dst, byte & 0xff, bytes, rt->ctx.stream));
+    });
+}
+
 int orqcu_keystream(orqcu_runtime* rt, int stream, uint64_t nonce0, size_t nbytes, void* out) {
     return guard([&] {
         need_rt(rt);

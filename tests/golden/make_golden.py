@@ -90,6 +90,17 @@ CASES = [
     ("qsort_n1048576_b40", "qsort", 1 << 20, 7, 7, 40, False),
 ]
 
+# Beaver 2PC (dummy triples) and Fantastic-4PC primitive sequences
+# (oracle/ref_driver_np.cpp): (tag, parties, n, data_seed, shim_seed, full?)
+NP_CASES = [
+    ("p2_prims_n1000", 2, 1000, 7, 3, True),
+    ("p2_prims_n1", 2, 1, 11, 4, True),
+    ("p2_prims_n300000", 2, 300000, 9, 5, False),
+    ("p4_prims_n1000", 4, 1000, 7, 3, True),
+    ("p4_prims_n1", 4, 1, 11, 4, True),
+    ("p4_prims_n300000", 4, 300000, 9, 5, False),
+]
+
 
 def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
@@ -142,6 +153,21 @@ def main():
             digests[tag]["arrays"][name] = [digest(s) for s in S]
             if full:
                 arrays[f"{tag}/{name}"] = stacked
+        print(tag, "ok", flush=True)
+    for tag, npar, n, dseed, sseed, full in NP_CASES:
+        if only and tag not in only:
+            continue
+        dumps, _ = run_ref.run_np(npar, "prims", n, dseed, shim_seed=sseed)
+        meta = {"op": "prims", "parties": npar, "n": n, "data_seed": dseed, "shim_seed": sseed}
+        digests[tag] = {"meta": meta, "arrays": {}}
+        for name in dumps[0]:
+            if "open" in name:
+                S = [dumps[0][name][0]]
+            else:
+                S = run_ref.distinct_shares_np(dumps, name, npar)
+            digests[tag]["arrays"][name] = [digest(s) for s in S]
+            if full:
+                arrays[f"{tag}/{name}"] = np.stack(S)
         print(tag, "ok", flush=True)
     np.savez_compressed(os.path.join(HERE, "ref_golden.npz"), **arrays)
     with open(os.path.join(HERE, "ref_digests.json"), "w") as f:

@@ -561,3 +561,65 @@ def replay_badd(be, n, seed, w):
     out = {"sum": be.np(s), "diff": be.np(d), "open_sum": be.open(s, False)[None],
            "open_diff": be.open(d, False)[None]}
     return out, (x, y)
+
+
+def replay_prims_np(be, n, seed):
+    """The "prims" op of ref_driver_np.cpp (Beaver 2PC / Fantastic-4PC) on a
+    backend with share / and_b / xor_b / mul_a / add_a / b2a_bit / open:
+    widths 4, 8, 1 with data seeds seed, seed+1, seed+2."""
+    out = {}
+    for w, tag, sd in ((4, "w4_", seed), (8, "w8_", seed + 1), (1, "w1_", seed + 2)):
+        st = splitmix64_fast(sd, 2 * n)
+        x, y = st[:n].astype(_U[w]), st[n:].astype(_U[w])
+        xb = be.share(x, False, 0)
+        yb = be.share(y, False, 1)
+        out[tag + "xb"], out[tag + "yb"] = be.np(xb), be.np(yb)
+        zb = be.and_b(xb, yb)
+        out[tag + "and"] = be.np(zb)
+        out[tag + "xor"] = be.np(be.xor_b(xb, yb))
+        xa = be.share(x, True, 1)
+        ya = be.share(y, True, 0)
+        out[tag + "xa"], out[tag + "ya"] = be.np(xa), be.np(ya)
+        za = be.mul_a(xa, ya)
+        out[tag + "mul"] = be.np(za)
+        out[tag + "add"] = be.np(be.add_a(xa, ya))
+        ba = be.b2a_bit(xb)
+        out[tag + "b2a"] = be.np(ba)
+        out[tag + "open_and"] = be.open(zb, False)[None]
+        out[tag + "open_mul"] = be.open(za, True)[None]
+        out[tag + "open_b2a"] = be.open(ba, True)[None]
+    return out
+
+
+class OracleNPBackend:
+    """The 2PC / 4PC restatement (oracle.oracle.OracleNP) behind the replay
+    interface; shares are lists of numpy arrays."""
+
+    def __init__(self, seed, nparties):
+        from oracle.oracle import OracleNP
+
+        self.o = OracleNP(seed, nparties)
+
+    def share(self, data, arith, party):
+        return self.o.secret_share(data, arith, party)
+
+    def and_b(self, x, y):
+        return self.o.and_b(x, y)
+
+    def xor_b(self, x, y):
+        return self.o.xor_b(x, y)
+
+    def mul_a(self, x, y):
+        return self.o.mul_a(x, y)
+
+    def add_a(self, x, y):
+        return self.o.add_a(x, y)
+
+    def b2a_bit(self, x):
+        return self.o.b2a_bit(x)
+
+    def open(self, x, arith):
+        return self.o.open(x, arith)
+
+    def np(self, x):
+        return np.stack(x)

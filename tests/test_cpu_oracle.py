@@ -342,3 +342,27 @@ def test_boolean_add_sub_match_reference_shares(oracle_lib, golden, digests, tag
         assert same(arr, golden[f"{tag}/{name}"]), name
     assert np.array_equal(out["open_sum"][0].view(x.dtype), x + y)
     assert np.array_equal(out["open_diff"][0].view(x.dtype), x - y)
+
+
+@pytest.mark.parametrize("tag", ["p2_prims_n1000", "p2_prims_n1", "p4_prims_n1000", "p4_prims_n1"])
+def test_np_prims_match_reference_shares(oracle_lib, golden, digests, tag):
+    """Beaver 2PC (dummy triples) and Fantastic-4PC: the restatement's shares
+    of every vector of the primitive sequence equal the reference's."""
+    from replay import OracleNPBackend, replay_prims_np
+
+    m = digests[tag]["meta"]
+    out = replay_prims_np(OracleNPBackend(m["shim_seed"], m["parties"]), m["n"], m["data_seed"])
+    assert set(out) == set(digests[tag]["arrays"])
+    for name, arr in out.items():
+        assert same(arr, golden[f"{tag}/{name}"]), name
+
+
+@pytest.mark.parametrize("tag", ["p2_prims_n300000", "p4_prims_n300000"])
+def test_np_prims_large_match_reference_digests(oracle_lib, digests, tag):
+    from replay import OracleNPBackend, replay_prims_np
+
+    d = digests[tag]
+    m = d["meta"]
+    out = replay_prims_np(OracleNPBackend(m["shim_seed"], m["parties"]), m["n"], m["data_seed"])
+    for name, arr in out.items():
+        assert [sha(a) for a in arr] == d["arrays"][name], name
