@@ -337,6 +337,123 @@ def join_expected(pk, g, v, fk, q):
     return keys, tot, sums.astype(np.int64)
 
 
+# The reference's published micro_primitives figures (README.md:213-236), 3PC,
+# one worker, 32-bit elements, seconds per call on the authors' 8-core machine.
+PUBLISHED_PRIMS = {1 << 20: {"AND": 0.01723, "MULT": 0.01167, "EQ": 0.04605, "GR": 0.07226, "RCA": 0.1298},
+                   1 << 24: {"AND": 0.1686, "MULT": 0.1992, "EQ": 1.14, "GR": 1.499, "RCA": 1.913}}
+
+
+class PrimsWorkload:
+    """ORQ's micro_primitives sequence (bench/micro/micro_primitives.cpp) on
+    n 32-bit elements, 3PC: AND (and_b), MULT (multiply_a), EQ (==), GR (>)
+    and RCA (binary +), the protocol steps of north_star's first hot-path
+    item. One step = the five calls; a row is one element of one call."""
+
+    name = "prims"
+    PRIMS = ("AND", "MULT", "EQ", "GR", "RCA")
+
+    def __init__(self, args, seed):
+        self.n = args.n if args.n != DEFAULT_N else 1 << 24
+        self.seed = seed
+        self.units = 5 * self.n
+        self.flush_l2 = False  # 5 x 3 x 64 MB of input shares per step
+        self.config = {"workload": f"3PC primitives AND, MULT, EQ, GR, RCA on 2^{self.n.bit_length() - 1} "
+                                   "int32 elements (ORQ's micro_primitives), one element of one call = one row",
+                       "rows_per_gpu": self.units, "elements": self.n,
+                       "l2": "inputs larger than L2 (192 MB of shares per operand)", "seed": seed}
+
+    def setup(self, rt, orq):
+        import numpy as np
+
+        self.orq, self.rt, self.np = orq, rt, np
+        st = splitmix(self.seed, 2 * self.n)
+        self.x = st[:self.n].astype(np.uint32)
+        self.y = st[self.n:].astype(np.uint32)
+        self.xb, self.yb = rt.secret_share_b(self.x, 0), rt.secret_share_b(self.y, 1)
+        self.xa, self.ya = rt.secret_share_a(self.x, 0), rt.secret_share_a(self.y, 1)
+
+    def ops(self):
+        xb, yb, xa, ya = self.xb, self.yb, self.xa, self.ya
+        return {"AND": lambda: xb & yb, "MULT": lambda: xa * ya, "EQ": lambda: xb == yb,
+                "GR": lambda: xb > yb, "RCA": lambda: xb + yb}
+
+    def step(self):
+        self.out = {k: f() for k, f in self.ops().items()}
+
+    def check(self):
+        np = self.np
+        x, y = self.x, self.y
+        o = {k: v.open().cpu().numpy().view(np.uint32) for k, v in self.out.items()}
+        xs, ys = x.view(np.int32), y.view(np.int32)
+        with np.errstate(over="ignore"):
+            return (np.array_equal(o["AND"], x & y) and np.array_equal(o["MULT"], x * y)
+                    and np.array_equal(o["EQ"], (x == y).astype(np.uint32))
+                    and np.array_equal(o["GR"], (xs > ys).astype(np.uint32))
+                    and np.array_equal(o["RCA"], x + y))
+
+    def breakdown(self):
+        """Seconds per primitive call (CUDA events, median of 5), beside the
+        reference's published figure at the same size."""
+        import torch
+
+        out = {}
+        pub = PUBLISHED_PRIMS.get(self.n, {})
+        for k, f in self.ops().items():
+            ts = []
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                f()
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1) / 1e3)
+            sec = statistics.median(ts)
+            out[k] = {"seconds": sec, "elements_per_s": self.n / sec}
+            if k in pub:
+                out[k]["published_s"] = pub[k]
+                out[k]["speedup_vs_published"] = pub[k] / sec
+        return out
+
+    def e2e_setup(self, dev):
+        import torch
+
+        np, n = self.np, self.n
+        self.pin = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (self.x, self.y)]
+        self.dbuf = [torch.empty(n, dtype=torch.int32, device=dev) for _ in range(2)]
+        self.outs = {k: torch.empty(n, dtype=torch.int32).pin_memory() for k in self.PRIMS}
+        self.h2d = 2 * n * 4
+        self.d2h = 5 * n * 4
+
+    def e2e_step(self):
+        rt = self.rt
+        for h, d in zip(self.pin, self.dbuf):
+            d.copy_(h, non_blocking=True)
+        xb, yb = rt.secret_share_b(self.dbuf[0], 0), rt.secret_share_b(self.dbuf[1], 1)
+        xa, ya = rt.secret_share_a(self.dbuf[0], 0), rt.secret_share_a(self.dbuf[1], 1)
+        res = {"AND": xb & yb, "MULT": xa * ya, "EQ": xb == yb, "GR": xb > yb, "RCA": xb + yb}
+        for k, v in res.items():
+            self.outs[k].copy_(v.open(), non_blocking=True)
+
+    def e2e_check(self):
+        np = self.np
+        return bool(np.array_equal(self.outs["AND"].numpy().view(np.uint32), self.x & self.y))
+
+    def cpu_reference(self, sample, threads):
+        from oracle import run_ref
+
+        n = max(1024, min(sample, 1 << 22))
+        t0 = time.time()
+        _, out = run_ref.run("prims_time", n, self.seed, shim_seed=7, bits=32, threads=threads, timeout=1800)
+        prims = None
+        for line in out.splitlines():
+            if line.startswith('{"prims"'):
+                prims = json.loads(line)["prims"]
+        sec = sum(prims.values()) if prims else time.time() - t0
+        self.ref_prims = prims
+        return 5 * n / sec, sec, (f"n={n} int32 elements, ORQ's own AND, MULT, EQ, GR, RCA (5 calls), 3 party "
+                                  f"processes x {threads} worker threads, batch -1, NoCopy sockets over 127.0.0.1")
+
+
 class JoinWorkload:
     """Config 3: A (2^22 rows) inner-join B (2^24 rows) on pk = fk, copying
     the group key and value; VQ = value * quantity; group-by SUM(VQ), COUNT."""
@@ -617,7 +734,7 @@ class ServeReference:
 
 
 WORKLOADS = {"radix": RadixWorkload, "qsort": QuicksortWorkload, "bitonic": BitonicWorkload,
-             "join": JoinWorkload}
+             "join": JoinWorkload, "prims": PrimsWorkload}
 
 
 def max_over_ranks(x):
@@ -731,6 +848,8 @@ def run_orq(args, rank, world, local_rank):
         e2e = {"value": world * wl.units * ke / (ems / 1e3), "unit": "rows/s",
                "h2d_bytes_per_step": wl.h2d, "d2h_bytes_per_step": wl.d2h, "ms_per_step": ems / ke}
     ok = max_over_ranks(0.0 if ok else 1.0) == 0.0  # every replica's output checked
+    if hasattr(wl, "breakdown"):
+        wl.extra = {"primitives": wl.breakdown()}
     if dist is not None:
         dist.destroy_process_group()
     return wl, ms, launches, prof, clk, e2e, ok
@@ -940,12 +1059,17 @@ def main():
         "correct": ok, "gpu_launches": launches, "clocks": clk,
     }
     line.update(roofline(prof, args.steps, wl.units if wl.name == "radix" else None))
+    if wl.name == "prims":
+        line["dtype"] = "int32"
+    line.update(getattr(wl, "extra", {}))
     if e2e:
         line["e2e"] = e2e
     if not args.no_cpu_baseline and world == 1:
         v, _, sample = wl.cpu_reference(args.cpu_sample, 1)
         line["cpu_baseline"] = {"value": v, "unit": "rows/s", "cores": 3, "kind": "reference",
                                 "sample": sample, "cpu": cpu_model(), "threads_per_party": 1}
+        if getattr(wl, "ref_prims", None):
+            line["cpu_baseline"]["seconds_per_primitive"] = wl.ref_prims
     print(json.dumps(line))
 
 

@@ -333,6 +333,50 @@ int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before);
  * every SM in turn. Results do not depend on it. No reference counterpart. */
 int orqcu_runtime_set_sm_limit(orqcu_runtime* rt, int sms);
 
+/* ---- Beaver 2PC and Fantastic-4PC ------------------------------------------
+ * The local steps of ORQ's other protocol classes, every party in this
+ * process. A runtime made by orqcu_runtime_create_np runs one of them:
+ *   nparties = 2: Beaver_2PC (include/core/protocols/beaver_2pc.h) with the
+ *     dummy triples of a USE_DUMMY_TRIPLES build (random/correlation/
+ *     dummy_ole.h, beaver_triple_generator.h); a vector is S[0], S[1] and
+ *     party p holds S[p];
+ *   nparties = 4: Fantastic_4PC (include/core/protocols/dalskov_4pc.h); a
+ *     vector is X[0..3], X[j] being the share party j lacks (party p holds
+ *     X[p+1], X[p+2], X[p+3] as its local shares 0, 1, 2, get_shares at
+ *     dalskov_4pc.h:152-168).
+ * Keys follow the same deterministic key generator as the 3PC runtime, in
+ * each protocol's keygen order (rand_setup.h:154-238,306-381), so shares equal
+ * the reference's with one worker and batch size -1. `shares`, `x`, `y`, `z`
+ * are arrays of nparties device pointers; widths 1, 2, 4 or 8. The 3PC entry
+ * points refuse such a runtime and these refuse a 3PC one (ORQCU_EINVAL). */
+int orqcu_runtime_create_np(uint64_t seed, int device, int nparties, orqcu_runtime** out);
+/* 2, 3 or 4 */
+int orqcu_runtime_parties(orqcu_runtime* rt, int* nparties);
+/* secret_share_b / secret_share_a (beaver_2pc.h:214-260, dalskov_4pc.h:152-201)
+ * from data_party's local PRG; data_dev is its plaintext on the device. */
+int orqcu_np_secret_share(orqcu_runtime* rt, int arith, int width, size_t n, const void* data_dev,
+                          int data_party, void* const* shares);
+/* open_shares_a / open_shares_b (beaver_2pc.h:172-183, dalskov_4pc.h:660-676). */
+int orqcu_np_open(orqcu_runtime* rt, int arith, int width, size_t n, const void* const* shares,
+                  void* out_dev);
+/* and_b / multiply_a (beaver_2pc.h:50-59,108-117 with the dummy triple of the
+ * call; dalskov_4pc.h:384-420,479-506 with the six inp sharings), one fused
+ * launch each; z must not alias x or y. */
+int orqcu_np_and_b(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z);
+int orqcu_np_multiply_a(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                        void* const* z);
+/* b2a_bit (beaver_2pc.h:147-158, dalskov_4pc.h:562-590): LSB of a boolean
+ * sharing to an arithmetic one, one fused launch; y must not alias x. */
+int orqcu_np_b2a_bit(orqcu_runtime* rt, int width, size_t n, const void* const* x, void* const* y);
+/* xor_b / add_a / sub_a: local on every share. */
+int orqcu_np_xor_b(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z);
+int orqcu_np_add_a(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z);
+int orqcu_np_sub_a(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z);
+
 #ifdef __cplusplus
 }
 #endif

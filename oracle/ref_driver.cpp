@@ -582,6 +582,34 @@ int main(int argc, char** argv) {
         }
         auto x1 = o1.open();
         d.plain("open_o1", x1);
+    } else if (op == "prims_time") {
+        // ORQ's micro_primitives sequence on n 32-bit elements: AND, MULT, EQ,
+        // GR, RCA (binary +), each timed; prints one JSON line of seconds
+        uint64_t st = seed;
+        auto x = gen<int32_t>(n, st, ~0ull);
+        auto y = gen<int32_t>(n, st, ~0ull);
+        BSharedVector<int32_t> xb = secret_share_b(x, 0), yb = secret_share_b(y, 1);
+        ASharedVector<int32_t> xa = secret_share_a(x, 0), ya = secret_share_a(y, 1);
+        double t[5];
+        auto tick = [] { return std::chrono::steady_clock::now(); };
+        auto sec = [](auto a, auto b) { return std::chrono::duration<double>(b - a).count(); };
+        auto a0 = tick();
+        auto r0 = xb & yb;
+        auto a1 = tick();
+        auto r1 = xa * ya;
+        auto a2 = tick();
+        auto r2 = xb == yb;
+        auto a3 = tick();
+        auto r3 = xb > yb;
+        auto a4 = tick();
+        auto r4 = xb + yb;
+        auto a5 = tick();
+        t[0] = sec(a0, a1), t[1] = sec(a1, a2), t[2] = sec(a2, a3), t[3] = sec(a3, a4), t[4] = sec(a4, a5);
+        secs = sec(a0, a5);
+        if (pid == 0)
+            printf("{\"prims\": {\"AND\": %.6f, \"MULT\": %.6f, \"EQ\": %.6f, \"GR\": %.6f, \"RCA\": %.6f}}\n",
+                   t[0], t[1], t[2], t[3], t[4]);
+        (void)r0, (void)r1, (void)r2, (void)r3, (void)r4;
     } else if (op == "shuffle") {
         uint64_t st = seed;
         auto x = gen<int32_t>(n, st, ~0ull);

@@ -645,3 +645,79 @@ def radix_sort(v: BSharedVector, order: int = ASC, bits: int | None = None) -> E
     _check(rt.lib.orqcu_radix_sort(rt.h, v.width, ctypes.c_size_t(v.size()), _p3(v.shares),
                                    bits, int(order == DESC), _p3(perm)))
     return ElementwisePermutation(rt, perm)
+
+
+# ---------------------------------------------------------------------------
+# Beaver 2PC (dummy triples) and Fantastic-4PC: the local steps of ORQ's other
+# protocol classes (include/core/protocols/beaver_2pc.h, dalskov_4pc.h), every
+# party in this process. A vector is an (nparties, n) tensor of its distinct
+# shares: S[0], S[1] for 2PC; X[0..3] for 4PC, X[j] being the share party j
+# lacks.
+class NPRuntime(Runtime):
+    """Runtime of the Beaver-2PC (nparties=2) or Fantastic-4PC (4) protocol."""
+
+    def __init__(self, nparties: int, seed: int = 1, device: int = 0):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise OrqError("orq_b200 needs a CUDA device (no CPU fallback)")
+        if nparties not in (2, 4):
+            raise ValueError("nparties must be 2 or 4")
+        self.lib = load_library()
+        self.device = device
+        self.nparties = nparties
+        torch.cuda.set_device(device)
+        h = ctypes.c_void_p()
+        _check(self.lib.orqcu_runtime_create_np(ctypes.c_uint64(seed), device, nparties, ctypes.byref(h)))
+        self.h = h
+        _check(self.lib.orqcu_runtime_set_stream(self.h, ctypes.c_void_p(
+            torch.cuda.current_stream(device).cuda_stream)))
+
+    def _pn(self, t):
+        return (ctypes.c_void_p * self.nparties)(*[t[j].data_ptr() for j in range(self.nparties)])
+
+    def _new(self, n, w):
+        torch = _torch()
+        dt = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}[w]
+        return torch.empty((self.nparties, n), dtype=dt, device=f"cuda:{self.device}")
+
+    def secret_share(self, data, arith: bool, party: int = 0):
+        """secret_share_b / secret_share_a from `party`'s local PRG."""
+        w = data.itemsize if isinstance(data, np.ndarray) else data.element_size()
+        d = self._to_dev(data, w)
+        s = self._new(d.shape[0], w)
+        _check(self.lib.orqcu_np_secret_share(self.h, int(arith), w, ctypes.c_size_t(d.shape[0]),
+                                              ctypes.c_void_p(d.data_ptr()), party, self._pn(s)))
+        return s
+
+    def open(self, s, arith: bool):
+        torch = _torch()
+        out = torch.empty(s.shape[1], dtype=s.dtype, device=s.device)
+        _check(self.lib.orqcu_np_open(self.h, int(arith), s.element_size(), ctypes.c_size_t(s.shape[1]),
+                                      self._pn(s), ctypes.c_void_p(out.data_ptr())))
+        return out
+
+    def _bin(self, fn, x, y):
+        z = self._new(x.shape[1], x.element_size())
+        _check(fn(self.h, x.element_size(), ctypes.c_size_t(x.shape[1]), self._pn(x), self._pn(y), self._pn(z)))
+        return z
+
+    def and_b(self, x, y):
+        return self._bin(self.lib.orqcu_np_and_b, x, y)
+
+    def multiply_a(self, x, y):
+        return self._bin(self.lib.orqcu_np_multiply_a, x, y)
+
+    def xor_b(self, x, y):
+        return self._bin(self.lib.orqcu_np_xor_b, x, y)
+
+    def add_a(self, x, y):
+        return self._bin(self.lib.orqcu_np_add_a, x, y)
+
+    def sub_a(self, x, y):
+        return self._bin(self.lib.orqcu_np_sub_a, x, y)
+
+    def b2a_bit(self, x):
+        y = self._new(x.shape[1], x.element_size())
+        _check(self.lib.orqcu_np_b2a_bit(self.h, x.element_size(), ctypes.c_size_t(x.shape[1]), self._pn(x),
+                                         self._pn(y)))
+        return y

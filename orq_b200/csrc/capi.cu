@@ -1,6 +1,7 @@
 // capi.cu — extern "C" entry points (include/orq_cuda.h).
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -38,7 +39,13 @@ int guard(F&& f) {
 void need(bool ok, const char* msg) {
     if (!ok) throw std::invalid_argument(msg);
 }
-void need_rt(orqcu_runtime* rt) { need(rt != nullptr, "null runtime"); }
+// any runtime (memory, streams, profiling)
+void need_rt_any(orqcu_runtime* rt) { need(rt != nullptr, "null runtime"); }
+// a replicated-3PC runtime (every 3PC protocol and operator entry)
+void need_rt(orqcu_runtime* rt) {
+    need_rt_any(rt);
+    need(rt->ctx.nparties == 3, "this runtime runs the 2PC/4PC protocol; use the orqcu_np_* entry points");
+}
 void need_w(int w) { need(w == 1 || w == 2 || w == 4 || w == 8 || w == 16, "width must be 1,2,4,8,16"); }
 void need_sh(const void* const s[3], size_t n, const char* what) {
     if (n == 0) return;
@@ -54,30 +61,122 @@ extern "C" {
 int orqcu_version(void) { return 1; }
 const char* orqcu_last_error(void) { return g_err.c_str(); }
 
+static void create_runtime(uint64_t seed, int device, int nparties, orqcu_runtime** out) {
+    need(out != nullptr, "null output");
+    need(nparties == 2 || nparties == 3 || nparties == 4, "parties must be 2, 3 or 4");
+    int ndev = 0;
+    ORQ_CUDA_CHECK(cudaGetDeviceCount(&ndev));
+    need(device >= 0 && device < ndev, "no such CUDA device");
+    ORQ_CUDA_CHECK(cudaSetDevice(device));
+    std::unique_ptr<orqcu_runtime> rt(new orqcu_runtime());
+    rt->ctx.device = device;
+    ORQ_CUDA_CHECK(cudaDeviceGetAttribute(&rt->ctx.num_sms, cudaDevAttrMultiProcessorCount, device));
+    ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&rt->ctx.stream, cudaStreamNonBlocking));
+    rt->ctx.owns_stream = true;
+    ORQ_CUDA_CHECK(cudaMalloc(&rt->ctx.d_err, sizeof(int)));
+    ORQ_CUDA_CHECK(cudaMemset(rt->ctx.d_err, 0, sizeof(int)));
+    if (nparties == 3) orqcu::init_ctx_keys(rt->ctx, seed);
+    else orqcu::init_ctx_keys_np(rt->ctx, seed, nparties);
+    orqcu::device_runtime_opened(device);
+    try {
+        orqcu::upload_aes_tables(device);
+    } catch (...) {
+        orqcu::device_runtime_closed(device);
+        throw;
+    }
+    *out = rt.release();
+}
+
 int orqcu_runtime_create(uint64_t seed, int device, orqcu_runtime** out) {
+    return guard([&] { create_runtime(seed, device, 3, out); });
+}
+
+int orqcu_runtime_create_np(uint64_t seed, int device, int nparties, orqcu_runtime** out) {
+    return guard([&] { create_runtime(seed, device, nparties, out); });
+}
+
+int orqcu_runtime_parties(orqcu_runtime* rt, int* nparties) {
     return guard([&] {
-        need(out != nullptr, "null output");
-        int ndev = 0;
-        ORQ_CUDA_CHECK(cudaGetDeviceCount(&ndev));
-        need(device >= 0 && device < ndev, "no such CUDA device");
-        ORQ_CUDA_CHECK(cudaSetDevice(device));
-        auto* rt = new orqcu_runtime();
-        rt->ctx.device = device;
-        ORQ_CUDA_CHECK(cudaDeviceGetAttribute(&rt->ctx.num_sms, cudaDevAttrMultiProcessorCount, device));
-        ORQ_CUDA_CHECK(cudaStreamCreateWithFlags(&rt->ctx.stream, cudaStreamNonBlocking));
-        rt->ctx.owns_stream = true;
-        ORQ_CUDA_CHECK(cudaMalloc(&rt->ctx.d_err, sizeof(int)));
-        ORQ_CUDA_CHECK(cudaMemset(rt->ctx.d_err, 0, sizeof(int)));
-        orqcu::init_ctx_keys(rt->ctx, seed);
-        orqcu::device_runtime_opened(device);
-        try {
-            orqcu::upload_aes_tables(device);
-        } catch (...) {
-            orqcu::device_runtime_closed(device);
-            throw;
-        }
-        *out = rt;
+        need_rt_any(rt);
+        need(nparties != nullptr, "null output");
+        *nparties = rt->ctx.nparties;
     });
+}
+
+// ---- Beaver 2PC / Fantastic-4PC ----------------------------------------------
+static void need_np_rt(orqcu_runtime* rt) {
+    need_rt_any(rt);
+    need(rt->ctx.nparties == 2 || rt->ctx.nparties == 4,
+         "this runtime runs replicated 3PC; create one with orqcu_runtime_create_np");
+}
+static void need_shares(const void* const* s, int np, size_t n, const char* what) {
+    if (n == 0) return;
+    need(s != nullptr, what);
+    for (int k = 0; k < np; k++) need(s[k] != nullptr, what);
+}
+
+int orqcu_np_secret_share(orqcu_runtime* rt, int arith, int width, size_t n, const void* data_dev,
+                          int data_party, void* const* shares) {
+    return guard([&] {
+        need_np_rt(rt);
+        need_shares(shares, rt->ctx.nparties, n, "null share pointer");
+        need(n == 0 || data_dev != nullptr, "null data");
+        orqcu::op_np_secret_share(rt->ctx, arith != 0, width, n, data_dev, data_party, shares);
+    });
+}
+
+int orqcu_np_open(orqcu_runtime* rt, int arith, int width, size_t n, const void* const* shares, void* out_dev) {
+    return guard([&] {
+        need_np_rt(rt);
+        need_shares(shares, rt->ctx.nparties, n, "null share pointer");
+        need(n == 0 || out_dev != nullptr, "null output");
+        orqcu::op_np_open(rt->ctx, arith != 0, width, n, shares, out_dev);
+    });
+}
+
+static int np_bin(orqcu_runtime* rt, int mode, int width, size_t n, const void* const* x, const void* const* y,
+                  void* const* z) {
+    return guard([&] {
+        need_np_rt(rt);
+        need_shares(x, rt->ctx.nparties, n, "null x");
+        if (mode != 2) need_shares(y, rt->ctx.nparties, n, "null y");
+        need_shares(z, rt->ctx.nparties, n, "null z");
+        orqcu::op_np_mult(rt->ctx, mode, width, n, x, y, z);
+    });
+}
+int orqcu_np_and_b(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z) {
+    return np_bin(rt, 0, width, n, x, y, z);
+}
+int orqcu_np_multiply_a(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                        void* const* z) {
+    return np_bin(rt, 1, width, n, x, y, z);
+}
+int orqcu_np_b2a_bit(orqcu_runtime* rt, int width, size_t n, const void* const* x, void* const* y) {
+    return np_bin(rt, 2, width, n, x, nullptr, y);
+}
+
+static int np_local(orqcu_runtime* rt, int op, int width, size_t n, const void* const* x, const void* const* y,
+                    void* const* z) {
+    return guard([&] {
+        need_np_rt(rt);
+        need_shares(x, rt->ctx.nparties, n, "null x");
+        need_shares(y, rt->ctx.nparties, n, "null y");
+        need_shares(z, rt->ctx.nparties, n, "null z");
+        orqcu::op_np_local(rt->ctx, op, width, n, x, y, z);
+    });
+}
+int orqcu_np_xor_b(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z) {
+    return np_local(rt, 0, width, n, x, y, z);
+}
+int orqcu_np_add_a(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z) {
+    return np_local(rt, 1, width, n, x, y, z);
+}
+int orqcu_np_sub_a(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
+                   void* const* z) {
+    return np_local(rt, 2, width, n, x, y, z);
 }
 
 int orqcu_runtime_destroy(orqcu_runtime* rt) {
@@ -98,7 +197,7 @@ int orqcu_runtime_destroy(orqcu_runtime* rt) {
 
 int orqcu_runtime_set_stream(orqcu_runtime* rt, void* s) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         cudaSetDevice(rt->ctx.device);
         ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
         if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
@@ -109,7 +208,7 @@ int orqcu_runtime_set_stream(orqcu_runtime* rt, void* s) {
 
 int orqcu_synchronize(orqcu_runtime* rt) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
         rt->ctx.check_device_error();
     });
@@ -117,7 +216,7 @@ int orqcu_synchronize(orqcu_runtime* rt) {
 
 int orqcu_get_nonce(orqcu_runtime* rt, int stream, uint64_t* nonce) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         need(stream >= 0 && stream < orqcu::NSTREAMS && nonce, "bad stream id");
         *nonce = rt->ctx.nonce[stream];
     });
@@ -125,7 +224,7 @@ int orqcu_get_nonce(orqcu_runtime* rt, int stream, uint64_t* nonce) {
 
 int orqcu_kernels_launched(orqcu_runtime* rt, uint64_t* count) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         need(count != nullptr, "null output");
         *count = rt->ctx.kernels_launched;
     });
@@ -133,7 +232,7 @@ int orqcu_kernels_launched(orqcu_runtime* rt, uint64_t* count) {
 
 int orqcu_profile_enable(orqcu_runtime* rt, int on) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         rt->ctx.prof_collect();
         rt->ctx.profiling = on != 0;
     });
@@ -141,7 +240,7 @@ int orqcu_profile_enable(orqcu_runtime* rt, int on) {
 
 int orqcu_profile_report(orqcu_runtime* rt, char* buf, size_t len) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         need(buf != nullptr && len > 0, "null buffer");
         rt->ctx.prof_collect();
         std::string out;
@@ -159,7 +258,7 @@ int orqcu_profile_report(orqcu_runtime* rt, char* buf, size_t len) {
 
 int orqcu_malloc(orqcu_runtime* rt, size_t bytes, void** dptr) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         need(dptr != nullptr, "null output");
         cudaSetDevice(rt->ctx.device);
         ORQ_CUDA_CHECK(cudaMalloc(dptr, bytes ? bytes : 1));
@@ -167,13 +266,13 @@ int orqcu_malloc(orqcu_runtime* rt, size_t bytes, void** dptr) {
 }
 int orqcu_free(orqcu_runtime* rt, void* dptr) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         ORQ_CUDA_CHECK(cudaFree(dptr));
     });
 }
 int orqcu_memcpy_h2d(orqcu_runtime* rt, void* dst, const void* src, size_t bytes) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         if (!bytes) return;
         ORQ_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, rt->ctx.stream));
         ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
@@ -181,7 +280,7 @@ int orqcu_memcpy_h2d(orqcu_runtime* rt, void* dst, const void* src, size_t bytes
 }
 int orqcu_memcpy_d2h(orqcu_runtime* rt, void* dst, const void* src, size_t bytes) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         if (!bytes) return;
         ORQ_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, rt->ctx.stream));
         ORQ_CUDA_CHECK(cudaStreamSynchronize(rt->ctx.stream));
@@ -190,7 +289,7 @@ int orqcu_memcpy_d2h(orqcu_runtime* rt, void* dst, const void* src, size_t bytes
 
 int orqcu_pool_alloc(orqcu_runtime* rt, size_t bytes, void** dptr) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         need(dptr != nullptr, "null output");
         cudaSetDevice(rt->ctx.device);
         *dptr = rt->ctx.alloc(bytes ? bytes : 1);
@@ -198,13 +297,13 @@ int orqcu_pool_alloc(orqcu_runtime* rt, size_t bytes, void** dptr) {
 }
 int orqcu_pool_free(orqcu_runtime* rt, void* dptr) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         rt->ctx.release(dptr);
     });
 }
 int orqcu_memcpy_d2d(orqcu_runtime* rt, void* dst, const void* src, size_t bytes) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         if (!bytes) return;
         need(dst != nullptr && src != nullptr, "null pointer");
         ORQ_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, rt->ctx.stream));
@@ -212,7 +311,7 @@ int orqcu_memcpy_d2d(orqcu_runtime* rt, void* dst, const void* src, size_t bytes
 }
 int orqcu_memset(orqcu_runtime* rt, void* dst, int byte, size_t bytes) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         if (!bytes) return;
         need(dst != nullptr, "null pointer");
         ORQ_CUDA_CHECK(cudaMemsetAsync(dst, byte & 0xff, bytes, rt->ctx.stream));
@@ -221,7 +320,7 @@ int orqcu_memset(orqcu_runtime* rt, void* dst, int byte, size_t bytes) {
 
 int orqcu_keystream(orqcu_runtime* rt, int stream, uint64_t nonce0, size_t nbytes, void* out) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         need(stream >= 0 && stream < orqcu::NSTREAMS, "bad stream id");
         need(out != nullptr || nbytes == 0, "null output");
         orqcu::launch_keystream(rt->ctx, stream, nonce0, out, nbytes);
@@ -534,18 +633,19 @@ int orqcu_bitonic_sort_batch(orqcu_runtime* rt, int width, int count, const size
 
 int orqcu_runtime_reseed(orqcu_runtime* rt, uint64_t seed) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         for (auto& sp : rt->ctx.perm_queue) rt->ctx.free_perm(sp);
         rt->ctx.perm_queue.clear();
         rt->ctx.perm_queue_n = 0;
-        orqcu::init_ctx_keys(rt->ctx, seed);
+        if (rt->ctx.nparties == 3) orqcu::init_ctx_keys(rt->ctx, seed);
+        else orqcu::init_ctx_keys_np(rt->ctx, seed, rt->ctx.nparties);
         for (int s = 0; s < orqcu::NSTREAMS; s++) rt->ctx.nonce[s] = 0;
     });
 }
 
 int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         if (cached_before) *cached_before = rt->ctx.pool.cached_bytes();
         rt->ctx.pool.trim(rt->ctx.stream);
     });
@@ -553,7 +653,7 @@ int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before) {
 
 int orqcu_runtime_set_sm_limit(orqcu_runtime* rt, int sms) {
     return guard([&] {
-        need_rt(rt);
+        need_rt_any(rt);
         int total = 0;
         ORQ_CUDA_CHECK(cudaDeviceGetAttribute(&total, cudaDevAttrMultiProcessorCount, rt->ctx.device));
         need(sms >= 0, "negative SM limit");

@@ -99,6 +99,32 @@ void init_ctx_keys(Ctx& c, uint64_t seed) {
     }
 }
 
+// Beaver 2PC (rand_setup.h:229-238,306-330): call 0 local PRG, call 1 the
+// {0,1} group on P0 (P0's call 2, the everyone group of the same set, is
+// discarded). Fantastic-4PC (rand_setup.h:154-221): call 0 local PRG, P0 draws
+// the keys of {0,1,2}, {2,3,0}, {3,0,1} and the everyone group (calls 1-4),
+// P1 that of {1,2,3}; setup_4pc_common_prgs then draws one key per party (P0
+// call 5, P1 call 2, P2 call 1, P3 call 1): party q's key seeds the PRG of
+// the three parties other than q+1.
+void init_ctx_keys_np(Ctx& c, uint64_t seed, int nparties) {
+    static const int who2[3][2] = {{0, 1}, {0, 0}, {1, 0}};
+    static const int who4[8][2] = {{3, 1}, {0, 5}, {1, 2}, {2, 1}, {0, 0}, {1, 0}, {2, 0}, {3, 0}};
+    if (nparties != 2 && nparties != 4) throw std::invalid_argument("parties must be 2 or 4");
+    c.seed = seed;
+    c.nparties = nparties;
+    const int ns = nparties == 2 ? 3 : 8;
+    for (int s = 0; s < NSTREAMS; s++) {
+        c.nonce[s] = 0;
+        std::memset(c.rk[s].k, 0, sizeof(c.rk[s].k));
+    }
+    for (int s = 0; s < ns; s++) {
+        uint8_t key[32];
+        const int* wh = nparties == 2 ? who2[s] : who4[s];
+        derive_key(seed, wh[0], wh[1], key);
+        aes256_expand(key, c.rk[s].k);
+    }
+}
+
 static std::vector<AesTableUploader>& uploaders() {
     static std::vector<AesTableUploader> v;
     return v;

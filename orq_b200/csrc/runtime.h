@@ -35,6 +35,11 @@ enum StreamId {
     LOCAL2 = 9,
     NSTREAMS = 10
 };
+// The same slots hold the streams of the other protocol classes:
+// Beaver 2PC: the {0,1} PRG and the parties' local PRGs;
+// Fantastic-4PC: the PRG of the three parties other than e (NOT0 + e) and the
+// local PRGs (LOCAL0 + p).
+enum { P2_COMMON = 0, P2_LOCAL0 = 1, P4_NOT0 = 0, P4_LOCAL0 = 4 };
 
 // Device allocation that returns to the pool when dropped.
 struct DevBuf {
@@ -109,6 +114,7 @@ struct FyRes {
 
 struct Ctx {
     int device = 0;
+    int nparties = 3;  // 3: replicated 3PC; 2: Beaver 2PC; 4: Fantastic-4PC
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
@@ -176,6 +182,14 @@ struct ProfScope {
 void derive_key(uint64_t seed, int party, int call, uint8_t key[32]);
 void aes256_expand(const uint8_t key[32], uint32_t rk[60]);
 void init_ctx_keys(Ctx& c, uint64_t seed);
+// keys of the Beaver-2PC (nparties 2) or Fantastic-4PC (4) streams
+void init_ctx_keys_np(Ctx& c, uint64_t seed, int nparties);
+
+// ---- Beaver 2PC / Fantastic-4PC local steps (proto24.cu) ----
+void op_np_secret_share(Ctx& c, bool arith, int w, size_t n, const void* data, int party, void* const* s);
+void op_np_open(Ctx& c, bool arith, int w, size_t n, const void* const* s, void* out);
+void op_np_local(Ctx& c, int op, int w, size_t n, const void* const* x, const void* const* y, void* const* z);
+void op_np_mult(Ctx& c, int mode, int w, size_t n, const void* const* x, const void* const* y, void* const* z);
 void upload_aes_tables(int device);
 // Per-device set-up (the AES tables, the address of the no-alloc scratch
 // array) is done once per device and remembered with the device's epoch. The

@@ -623,3 +623,38 @@ class OracleNPBackend:
 
     def np(self, x):
         return np.stack(x)
+
+
+class GpuNPBackend:
+    """The device 2PC / 4PC runtime (orq_b200.NPRuntime) behind the replay
+    interface."""
+
+    def __init__(self, seed, nparties, device=0):
+        import orq_b200 as orq
+
+        self.rt = orq.NPRuntime(nparties, seed=seed, device=device)
+
+    def share(self, data, arith, party):
+        return self.rt.secret_share(data, arith, party)
+
+    def and_b(self, x, y):
+        return self.rt.and_b(x, y)
+
+    def xor_b(self, x, y):
+        return self.rt.xor_b(x, y)
+
+    def mul_a(self, x, y):
+        return self.rt.multiply_a(x, y)
+
+    def add_a(self, x, y):
+        return self.rt.add_a(x, y)
+
+    def b2a_bit(self, x):
+        return self.rt.b2a_bit(x)
+
+    def open(self, x, arith):
+        return self.rt.open(x, arith).cpu().numpy()
+
+    def np(self, x):
+        a = x.cpu().numpy()
+        return a.view(_U[a.dtype.itemsize])
