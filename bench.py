@@ -560,7 +560,8 @@ def run_batch(args, rank, world, local_rank):
     """Config 4: 512 independent sorts (256 bitonic with sizes padded to 2^k,
     256 radix), lengths log-uniform over 2^10..2^20, int32 keys uniform over
     32 bits. Batched path: one bitonic_sort_batch (persistent work-list kernel
-    per network round, autotuned CTA size, CUDA graph) then the radix sorts;
+    per network round, autotuned CTA size, CUDA graph) then one
+    radix_sort_batch (the radix items back to back, one synchronisation);
     plain path: 512 per-call operators in the same order (bitonic items, then
     radix items), which yields the same shares. Timed with CUDA events on the
     runtime's stream; both paths' opened outputs are checked."""
@@ -595,8 +596,7 @@ def run_batch(args, rank, world, local_rank):
 
     def batched():
         orq.bitonic_sort_batch([vecs[i] for i in bit_idx], orq.ASC, use_graph=True)
-        for i in rad_idx:
-            orq.radix_sort(vecs[i], orq.ASC, 32)
+        orq.radix_sort_batch([vecs[i] for i in rad_idx], orq.ASC, 32)
 
     def plain():
         for i in bit_idx:

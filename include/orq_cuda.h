@@ -187,6 +187,15 @@ int orqcu_apply_elementwise_perm(orqcu_runtime* rt, int x_arith, int x_width, si
 int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int bits,
                      int descending, void* const perm_out[3]);
 
+/* `count` independent radix sorts (keys[3*i+p], width key_width 4 or 8, n[i]
+ * rows, bits[i], descending[i]); perms_out[3*i+p] receives item i's A-shared
+ * int32 sorting permutation. The shares equal those of `count`
+ * orqcu_radix_sort calls in list order (the same PRG draws in the same
+ * order); items run back to back with one synchronisation at the end. No
+ * reference counterpart (ORQ sorts one vector per call). Synchronous. */
+int orqcu_radix_sort_batch(orqcu_runtime* rt, int key_width, int count, const size_t* n, void* const* keys,
+                           const int* bits, const int* descending, void* const* perms_out);
+
 /* quicksort (quicksort.h:214-246): sorts the B-shared key (width 4 or 8) in
  * the signed order, ascending or descending, and writes the A-shared int32
  * sorting permutation to perm_out. The protocol of quicksort_body

@@ -625,6 +625,24 @@ def bitonic_sort_batch(vectors, order=ASC, use_graph: bool = True):
                                            int(bool(use_graph))))
 
 
+def radix_sort_batch(vectors, order=ASC, bits=None):
+    """Radix sorts of many independent B-shared key columns (same width), in
+    place; returns their sorting permutations. Shares equal those of calling
+    radix_sort on each column in list order; item i's bit passes overlap item
+    i+1's permutation generation. `order` and `bits` are one value or a list."""
+    if not vectors:
+        return []
+    rt, w = vectors[0].rt, vectors[0].width
+    k = len(vectors)
+    orders = order if isinstance(order, (list, tuple)) else [order] * k
+    bl = bits if isinstance(bits, (list, tuple)) else [bits if bits is not None else 8 * w] * k
+    perms = [ElementwisePermutation(rt, rt._alloc(v.size(), 4)) for v in vectors]
+    ns = (ctypes.c_size_t * k)(*[v.size() for v in vectors])
+    _check(rt.lib.orqcu_radix_sort_batch(rt.h, w, k, ns, _flat(vectors), (ctypes.c_int * k)(*bl),
+                                         (ctypes.c_int * k)(*[int(o == DESC) for o in orders]), _flat(perms)))
+    return perms
+
+
 def quicksort(v: BSharedVector, order: int = ASC) -> ElementwisePermutation:
     """orq::operators::quicksort (quicksort.h:214-246): sorts v in place and
     returns the A-shared sorting permutation."""

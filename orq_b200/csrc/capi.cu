@@ -498,6 +498,22 @@ int orqcu_radix_sort(orqcu_runtime* rt, int key_width, size_t n, void* const key
     });
 }
 
+
+int orqcu_radix_sort_batch(orqcu_runtime* rt, int key_width, int count, const size_t* n, void* const* keys,
+                           const int* bits, const int* descending, void* const* perms_out) {
+    return guard([&] {
+        need_rt(rt);
+        need(count >= 0, "negative count");
+        if (count == 0) return;
+        need(n && keys && bits && descending && perms_out, "null argument");
+        for (int k = 0; k < count; k++) {
+            need_sh(keys + 3 * k, n[k], "null key share pointer");
+            need_sh(perms_out + 3 * k, n[k], "null permutation share pointer");
+        }
+        orqcu::op_radix_sort_batch(rt->ctx, key_width, count, n, keys, bits, descending, perms_out);
+    });
+}
+
 int orqcu_quicksort(orqcu_runtime* rt, int key_width, size_t n, void* const key[3], int descending,
                     void* const perm_out[3]) {
     return guard([&] {

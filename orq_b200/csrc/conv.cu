@@ -7,10 +7,9 @@
 // The adder works on bit-packed words: bit i of 8W consecutive elements forms
 // one word (pack_from), and each of the 8W-1 carry rounds is one AND over the
 // ceil(n / 8W) words, c_i = ((c_{i-1} ^ a_i) & (a ^ b)_i) ^ a_i. Here a warp
-// owns one word: lane l holds element l (and element 32 + l for 8-byte
-// shares), a ballot packs a bit of 32 elements, the three lanes 0..2 compute
-// the round's keystream block of the three PAIR streams, and the sum bits are
-// unpacked back into the lanes' elements, all rounds in registers.
+// owns the words of one keystream block (k_rca); a ballot packs a bit of 32
+// elements, and the sum bits are unpacked back into the lanes' elements, all
+// rounds in registers.
 #include <type_traits>
 
 #include "launch.cuh"
@@ -30,87 +29,123 @@ struct RcaArgs {
     int carry_in;          // subtraction: the carry starts as all ones (inplace_invert)
 };
 
+// A warp owns the WPW = 16 / W consecutive packed words that one keystream
+// block of a carry round covers (4 words of 32 elements for int32, 2 of 64
+// for int64); lane l holds element 32h + l of each of them (four elements a
+// lane). Before the rounds, the warp computes every keystream block it needs
+// once, spread over the lanes: stream q's block of round i is computed by
+// lane i % 32 into slot q * RPL + i / 32; round i then takes it by shuffle.
 template <int W>
 __global__ void __launch_bounds__(kAesThreads, 1) k_rca(RcaArgs a) {
     using T = typename std::conditional<W == 4, uint32_t, unsigned long long>::type;
-    constexpr int B = 8 * W;        // elements per packed word
-    constexpr int H = B / 32;       // elements per lane
+    constexpr int B = 8 * W;              // elements per packed word
+    constexpr int H = B / 32;             // elements per lane and word
+    constexpr int WPW = 16 / W;           // words per warp (one keystream block)
+    constexpr int RPL = (B - 1 + 31) / 32;  // rounds per lane and stream
     extern __shared__ __align__(16) uint32_t sm[];
     aes_stage_tables(sm);
     const AesSmem S(sm);
     const int lane = threadIdx.x & 31;
+    const unsigned long long groups = (a.cw + WPW - 1) / WPW;
     const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
-    for (unsigned long long c = (unsigned long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-         c < a.cw; c += warps) {
-        T x[H][3], ab[H][3], sum[H][3];
-        bool ok[H];
+    for (unsigned long long gi = (unsigned long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+         gi < groups; gi += warps) {
+        const unsigned long long c0 = gi * WPW;
+        // keystream of all rounds: ks[q * RPL + r] = stream q, round 32 r + lane
+        uint4 ks[3 * RPL];
 #pragma unroll
-        for (int h = 0; h < H; h++) {
-            const unsigned long long e = c * B + 32ull * h + lane;
-            ok[h] = e < a.n;
+        for (int q = 0; q < 3; q++)
 #pragma unroll
-            for (int p = 0; p < 3; p++) {
-                x[h][p] = ok[h] ? reinterpret_cast<const T*>(a.a[p])[e] : (T)0;
-                ab[h][p] = x[h][p] ^ (ok[h] ? reinterpret_cast<const T*>(a.b[p])[e] : (T)0);
-                sum[h][p] = 0;
+            for (int r = 0; r < RPL; r++) {
+                const int i = 32 * r + lane;
+                ks[q * RPL + r] = make_uint4(0, 0, 0, 0);
+                if (i < B - 1)
+                    ks[q * RPL + r] = keystream_block_n(S, a.pair[q].rk, a.pair[q].nonce + (unsigned long long)i * a.C,
+                                                        c0 * W / 16);
             }
-        }
-        const T c0 = a.carry_in ? ~(T)0 : (T)0;
-        T carry[3] = {c0, c0, c0};
+        T x[WPW][H][3], ab[WPW][H][3], sum[WPW][H][3];
+#pragma unroll
+        for (int j = 0; j < WPW; j++)
+#pragma unroll
+            for (int h = 0; h < H; h++) {
+                const unsigned long long e = (c0 + j) * B + 32ull * h + lane;
+                const bool ok = e < a.n;
+#pragma unroll
+                for (int p = 0; p < 3; p++) {
+                    x[j][h][p] = ok ? reinterpret_cast<const T*>(a.a[p])[e] : (T)0;
+                    ab[j][h][p] = x[j][h][p] ^ (ok ? reinterpret_cast<const T*>(a.b[p])[e] : (T)0);
+                    sum[j][h][p] = 0;
+                }
+            }
+        const T cin = a.carry_in ? ~(T)0 : (T)0;
+        T carry[WPW][3];
+#pragma unroll
+        for (int j = 0; j < WPW; j++) carry[j][0] = carry[j][1] = carry[j][2] = cin;
 #pragma unroll 1
         for (int i = 0; i < B; i++) {
-            T axb[3], ai[3];
+            // this round's keystream words: block of stream q from lane i % 32
+            uint32_t kb[3][4];
+            if (i < B - 1) {
 #pragma unroll
-            for (int p = 0; p < 3; p++) {
-                axb[p] = ai[p] = 0;
-#pragma unroll
-                for (int h = 0; h < H; h++) {
-                    axb[p] |= (T)__ballot_sync(0xffffffffu, (ab[h][p] >> i) & 1) << (32 * h);
-                    ai[p] |= (T)__ballot_sync(0xffffffffu, (x[h][p] >> i) & 1) << (32 * h);
+                for (int q = 0; q < 3; q++) {
+                    uint4 blk = ks[q * RPL];
+                    if constexpr (RPL > 1) {
+                        if (i >= 32) blk = ks[q * RPL + 1];
+                    }
+                    kb[q][0] = __shfl_sync(0xffffffffu, blk.x, i & 31);
+                    kb[q][1] = __shfl_sync(0xffffffffu, blk.y, i & 31);
+                    kb[q][2] = __shfl_sync(0xffffffffu, blk.z, i & 31);
+                    kb[q][3] = __shfl_sync(0xffffffffu, blk.w, i & 31);
                 }
             }
 #pragma unroll
-            for (int p = 0; p < 3; p++) {
-                const T s = axb[p] ^ carry[p];
+            for (int j = 0; j < WPW; j++) {
+                T axb[3], ai[3];
 #pragma unroll
-                for (int h = 0; h < H; h++) sum[h][p] |= ((s >> (32 * h + lane)) & 1) << i;
+                for (int p = 0; p < 3; p++) {
+                    axb[p] = ai[p] = 0;
+#pragma unroll
+                    for (int h = 0; h < H; h++) {
+                        axb[p] |= (T)__ballot_sync(0xffffffffu, (ab[j][h][p] >> i) & 1) << (32 * h);
+                        ai[p] |= (T)__ballot_sync(0xffffffffu, (x[j][h][p] >> i) & 1) << (32 * h);
+                    }
+                }
+#pragma unroll
+                for (int p = 0; p < 3; p++) {
+                    const T s = axb[p] ^ carry[j][p];
+#pragma unroll
+                    for (int h = 0; h < H; h++) sum[j][h][p] |= ((s >> (32 * h + lane)) & 1) << i;
+                }
+                if (i == B - 1) continue;  // no carry out of the top bit
+                // word c0 + j of each stream's round-i draw: W bytes at j*W of the block
+                T K[3];
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    if constexpr (W == 4) K[q] = (T)kb[q][j];
+                    else K[q] = (T)(((unsigned long long)kb[q][2 * j + 1] << 32) | kb[q][2 * j]);
+                }
+                // c_i = ((c ^ a_i) & axb_i) ^ a_i, the AND with r_p = K[p-1] ^ K[p]
+                T u[3], z[3];
+#pragma unroll
+                for (int p = 0; p < 3; p++) u[p] = carry[j][p] ^ ai[p];
+#pragma unroll
+                for (int p = 0; p < 3; p++) {
+                    const int q = (p + 1) % 3, pm = (p + 2) % 3;
+                    z[p] = (K[pm] ^ K[p]) ^ (u[p] & axb[p]) ^ (u[p] & axb[q]) ^ (u[q] & axb[p]);
+                }
+#pragma unroll
+                for (int p = 0; p < 3; p++) carry[j][p] = z[p] ^ ai[p];
             }
-            if (i == B - 1) break;  // no carry out of the top bit
-            // the round's keystream: word c (W bytes at c*W) of each PAIR call
-            uint32_t kw[2] = {0, 0};
-            if (lane < 3) {
-                const uint4 blk = keystream_block_n(S, a.pair[lane].rk, a.pair[lane].nonce + (unsigned long long)i * a.C,
-                                                    c * W / 16);
-                const uint32_t wds[4] = {blk.x, blk.y, blk.z, blk.w};
-                const int o = (int)((c * W / 4) & 3);
-                kw[0] = wds[o];
-                kw[1] = W == 8 ? wds[o + 1] : 0u;
-            }
-            T K[3];
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                const uint32_t lo = __shfl_sync(0xffffffffu, kw[0], q);
-                const uint32_t hi = __shfl_sync(0xffffffffu, kw[1], q);
-                K[q] = W == 8 ? (T)(((unsigned long long)hi << 32) | lo) : (T)lo;
-            }
-            // c_i = ((c ^ a_i) & axb_i) ^ a_i, the AND with r_p = K[p-1] ^ K[p]
-            T u[3], z[3];
-#pragma unroll
-            for (int p = 0; p < 3; p++) u[p] = carry[p] ^ ai[p];
-#pragma unroll
-            for (int p = 0; p < 3; p++) {
-                const int q = (p + 1) % 3, pm = (p + 2) % 3;
-                z[p] = (K[pm] ^ K[p]) ^ (u[p] & axb[p]) ^ (u[p] & axb[q]) ^ (u[q] & axb[p]);
-            }
-#pragma unroll
-            for (int p = 0; p < 3; p++) carry[p] = z[p] ^ ai[p];
         }
 #pragma unroll
-        for (int h = 0; h < H; h++)
-            if (ok[h]) {
-                const unsigned long long e = c * B + 32ull * h + lane;
+        for (int j = 0; j < WPW; j++)
 #pragma unroll
-                for (int p = 0; p < 3; p++) reinterpret_cast<T*>(a.sum[p])[e] = sum[h][p];
+            for (int h = 0; h < H; h++) {
+                const unsigned long long e = (c0 + j) * B + 32ull * h + lane;
+                if (e < a.n) {
+#pragma unroll
+                    for (int p = 0; p < 3; p++) reinterpret_cast<T*>(a.sum[p])[e] = sum[j][h][p];
+                }
             }
     }
 }
@@ -140,9 +175,11 @@ void op_rca(Ctx& c, int w, size_t n, CSh3 A, CSh3 Bv, Sh3 sum, bool carry_in) {
     a.C = chunks_of(cw * (unsigned long long)w);
     a.carry_in = carry_in;
     if (n) {
-        const double blocks = 3.0 * (double)(B - 1) * (double)cw;
-        if (w == 4) launch_aes(c, "boolean_adder", 9.0 * w * n, blocks, k_rca<4>, cw * 32, a);
-        else launch_aes(c, "boolean_adder", 9.0 * w * n, blocks, k_rca<8>, cw * 32, a);
+        // one warp per 16 / W words; each computes 3 (B - 1) blocks
+        const unsigned long long groups = (cw + 16 / w - 1) / (16 / w);
+        const double blocks = 3.0 * (double)(B - 1) * (double)groups;
+        if (w == 4) launch_aes(c, "boolean_adder", 9.0 * w * n, blocks, k_rca<4>, groups * 32, a);
+        else launch_aes(c, "boolean_adder", 9.0 * w * n, blocks, k_rca<8>, groups * 32, a);
     }
     for (int q = 0; q < 3; q++) c.nonce[PAIR0 + q] += (B - 1) * a.C;
 }

@@ -443,4 +443,29 @@ void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 p
     });
 }
 
+// ---------------------------------------------------------------------------
+// Batched radix sorts: `count` items in list order, the shares of `count`
+// plain calls. Items run back to back on the runtime's stream with no host
+// synchronisation between them (a plain call ends with one). Overlapping item
+// k's bit passes with item k+1's Fisher-Yates chain is allowed by the PRG
+// order (the chain only needs nonces the host knows once item k's chain has
+// ended) and was measured: on a second stream, with or without a static SM
+// split, it made the ragged batch slower (both halves want every SM for AES,
+// and the data side's CTAs delay the scanner launches the chain waits on).
+void op_radix_sort_batch(Ctx& c, int kw, int count, const size_t* n, void* const* keys, const int* bits,
+                         const int* desc, void* const* perms_out) {
+    if (count <= 0) return;
+    for (int k = 0; k < count; k++) {
+        if (kw != 4 && kw != 8) throw std::invalid_argument("radix sort keys must be int32 or int64");
+        if (bits[k] < 1 || bits[k] > kw * 8) throw std::invalid_argument("bits out of range");
+        if (n[k] >= (1ull << 31)) throw std::invalid_argument("sorts support n < 2^31");
+    }
+    for (int k = 0; k < count; k++) {
+        Sh3 key{{keys[3 * k], keys[3 * k + 1], keys[3 * k + 2]}};
+        Sh3 po{{perms_out[3 * k], perms_out[3 * k + 1], perms_out[3 * k + 2]}};
+        op_radix_sort(c, kw, n[k], key, bits[k], desc[k] != 0, po);
+    }
+    c.check_device_error();
+}
+
 }  // namespace orqcu

@@ -238,6 +238,10 @@ void op_prefix_sum_noalloc(Ctx& c, int w, size_t n, Sh3 s);
 
 // ---- sorting (radix.cu) ----
 void op_radix_sort(Ctx& c, int kw, size_t n, Sh3 key, int bits, bool desc, Sh3 perm_out /*int32*/);
+// `count` radix sorts whose shares equal `count` op_radix_sort calls in list
+// order, run back to back without host synchronisation between items.
+void op_radix_sort_batch(Ctx& c, int kw, int count, const size_t* n, void* const* keys, const int* bits,
+                         const int* desc, void* const* perms_out);
 
 // ---- compare circuit and bitonic sort (cmp.cu) ----
 void op_compare(Ctx& c, int w, size_t n, CSh3 x, CSh3 y, Sh3 eq, Sh3 gt);

@@ -791,3 +791,38 @@ def test_boolean_add_sub_match_reference_shares(orq, golden, digests, tag, w):
         assert same(arr, golden[f"{tag}/{name}"]), name
     assert np.array_equal(out["open_sum"][0].view(x.dtype), x + y)
     assert np.array_equal(out["open_diff"][0].view(x.dtype), x - y)
+
+
+def test_radix_sort_batch_equals_sequential_calls(orq):
+    """orqcu_radix_sort_batch: ragged items (40-bit int64 keys, a 1-bit and a
+    16-bit item, ascending and descending, a one-row item) give
+    exactly the shares, permutations and nonces of the same radix_sort calls
+    made one after another, and the runtime stays usable for plain calls."""
+    import torch
+
+    sizes = [3000, 7, 70001, 1, 513, 20000]
+    bits = [40, 40, 16, 40, 1, 40]
+    desc = [False, False, True, False, False, True]
+    keys = [radix_inputs(max(n, 1), 100 + i, b)[0][:n] for i, (n, b) in enumerate(zip(sizes, bits))]
+    rt_b = orq.Runtime(seed=23)
+    rt_s = orq.Runtime(seed=23)
+    vb = [rt_b.secret_share_b(k, 0) for k in keys]
+    vs = [rt_s.secret_share_b(k, 0) for k in keys]
+    pb = orq.radix_sort_batch(vb, [orq.DESC if d else orq.ASC for d in desc], bits)
+    ps = [orq.radix_sort(v, orq.DESC if d else orq.ASC, b) for v, d, b in zip(vs, desc, bits)]
+    torch.cuda.synchronize()
+    for i in range(len(sizes)):
+        assert torch.equal(vb[i].shares, vs[i].shares), i
+        assert torch.equal(pb[i].shares, ps[i].shares), i
+    for s in range(10):
+        assert rt_b.nonce(s) == rt_s.nonce(s), s
+    # plain calls after the batch continue from the same state
+    a = rt_b.secret_share_b(keys[0], 0)
+    b = rt_s.secret_share_b(keys[0], 0)
+    orq.radix_sort(a, orq.ASC, 40)
+    orq.radix_sort(b, orq.ASC, 40)
+    assert torch.equal(a.shares, b.shares)
+    ko = vb[0].open().cpu().numpy().view(np.int64)
+    assert np.array_equal(np.sort(keys[0].view(np.int64)), ko)
+    ko = vb[5].open().cpu().numpy().view(np.int64)
+    assert np.array_equal(np.sort(keys[5].view(np.int64))[::-1], ko)
