@@ -674,18 +674,25 @@ def run_serve(args, rank, world, local_rank):
     srv.close()
     capacity = cap_stats["requests"] / cap_stats["makespan_s"]
     rate = 0.8 * capacity
-    out = {"capacity_req_per_s": capacity, "rate_req_per_s": rate}
-    for name, slots in (("serving", args.slots), ("plain", 1)):
-        trace = make_trace(args.serve_requests, rate, seed=5 + rank, max_log=args.serve_max_log)
-        srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol,
-                     share_sms=bool(args.share_sms))
-        clocks = ClockSampler(local_rank)
-        clocks.start()
-        st = srv.run(trace, check=True)
-        st["clocks"] = clocks.stop()
-        srv.close()
-        st["ok"] = all(r.ok for r in trace)
-        out[name] = st
+    out = {"capacity_req_per_s": capacity, "rate_req_per_s": rate, "repeats": []}
+    # each repeat serves a fresh trace (its own arrivals and sizes) both ways;
+    # the spread over repeats is the run-to-run noise of the comparison
+    for r in range(max(1, args.serve_repeats)):
+        rep = {}
+        for name, slots in (("serving", args.slots), ("plain", 1)):
+            trace = make_trace(args.serve_requests, rate, seed=5 + rank + 1000 * r, max_log=args.serve_max_log)
+            srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol,
+                         share_sms=bool(args.share_sms))
+            clocks = ClockSampler(local_rank)
+            clocks.start()
+            st = srv.run(trace, check=True)
+            st["clocks"] = clocks.stop()
+            srv.close()
+            st["ok"] = all(r_.ok for r_ in trace)
+            rep[name] = st
+            if r == 0:
+                out[name] = st
+        out["repeats"].append(rep)
     return out
 
 
@@ -944,6 +951,8 @@ def main():
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-max-log", type=int, default=22)
+    ap.add_argument("--serve-repeats", type=int, default=3,
+                    help="serve: fresh traces served both ways, for the run-to-run spread")
     ap.add_argument("--share-sms", type=int, default=0,
                     help="serve: partition the SMs between slots (1) or let every slot use all of them (0)")
     ap.add_argument("--sort-protocol", default="quick", choices=["quick", "radix"],
@@ -1003,9 +1012,11 @@ def main():
             for k in ("ms_batched", "ms_plain"):
                 res[k] = max_over_ranks(res[k])
         else:
+            for rp in res.get("repeats", []):  # every rank takes the same steps
+                for part in ("serving", "plain"):
+                    for k in ("makespan_s", "p50_ms", "p99_ms"):
+                        rp[part][k] = max_over_ranks(rp[part][k])
             for part in ("serving", "plain"):
-                for k in ("makespan_s", "p50_ms", "p99_ms"):
-                    res[part][k] = max_over_ranks(res[part][k])
                 res[part]["rows_per_s"] = res[part]["rows"] / res[part]["makespan_s"]
         if dist is not None:
             dist.destroy_process_group()
@@ -1044,6 +1055,17 @@ def main():
                     "plain": {"value": pl["rows_per_s"], "unit": "rows/s", "p50_ms": pl["p50_ms"],
                               "p99_ms": pl["p99_ms"], "makespan_s": pl["makespan_s"]},
                     "timing": "host wall clock from each request's arrival to its opened result on the host"}
+            reps = res.get("repeats", [])
+            if reps:
+                rows_s = [rp["serving"]["rows"] / rp["serving"]["makespan_s"] for rp in reps]
+                rows_p = [rp["plain"]["rows"] / rp["plain"]["makespan_s"] for rp in reps]
+                ratio = [a / b for a, b in zip(rows_s, rows_p)]
+                line["repeats"] = [{"serving_rows_per_s": a, "plain_rows_per_s": b, "serving_over_plain": c,
+                                    "serving_p50_ms": rp["serving"]["p50_ms"], "serving_p99_ms": rp["serving"]["p99_ms"],
+                                    "plain_p50_ms": rp["plain"]["p50_ms"], "plain_p99_ms": rp["plain"]["p99_ms"]}
+                                   for a, b, c, rp in zip(rows_s, rows_p, ratio, reps)]
+                line["serving_over_plain"] = {"mean": statistics.mean(ratio), "min": min(ratio), "max": max(ratio)}
+                line["correct"] = line["correct"] and all(rp["serving"]["ok"] and rp["plain"]["ok"] for rp in reps)
         print(json.dumps(line))
         return
 

@@ -194,7 +194,9 @@ __device__ __forceinline__ void compare_rows(const T (&X)[E][3], const T (&Y)[E]
         for (int p = 0; p < 3; p++) Gt[k][p] = (s1[p] >> (rowbase + k)) & 1;
 }
 
-template <int W>
+// MINMAX: whether the level has a min or max aggregation; without one the
+// compare circuit is compiled out (it holds most of the registers)
+template <int W, bool MINMAX>
 __global__ void __launch_bounds__(kAggThreads, 1) k_agg_level(AggLevelArgs a) {
     using T = typename std::conditional<W == 4, uint32_t, unsigned long long>::type;
     constexpr int E = 16 / W;               // rows per unit
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) k_agg_level(AggLevelArgs a) {
 #pragma unroll
                     for (int p = 0; p < 3; p++) R[k][p] ^= X[k][p];
                 }
-            } else if (f == AGG_MIN || f == AGG_MAX) {
+            } else if (MINMAX && (f == AGG_MIN || f == AGG_MAX)) {
                 // bg = b > a (_compare with this = b), ! for min; then
                 // a = multiplex(g, a, multiplex(bg, a, b))
                 T Gt[E][3];
@@ -612,7 +614,10 @@ void op_aggregate(Ctx& c, int w, size_t n, int nkeys, const void* const* keys, i
         const unsigned long long units = ceil_div((unsigned long long)dr * w, 16);
         const double bytes = (double)dr * w * 3.0 * (2.0 * nkeys + (sel ? 2.0 : 0.0) + 3.0 * (na + nb));
         {
-            auto kern = w == 4 ? k_agg_level<4> : k_agg_level<8>;
+            bool minmax = false;
+            for (int s2 = 0; s2 < nb; s2++) minmax = minmax || bs[s2].func == AGG_MIN || bs[s2].func == AGG_MAX;
+            auto kern = w == 4 ? (minmax ? k_agg_level<4, true> : k_agg_level<4, false>)
+                               : (minmax ? k_agg_level<8, true> : k_agg_level<8, false>);
             prep_aes_kernel(kern);
             const unsigned grid = (unsigned)std::min<unsigned long long>(ceil_div(units, kAggThreads), (unsigned long long)c.num_sms);
             ProfScope ps(c, "agg_level", bytes, 3.0 * calls * units + 3.0 * packed * units);

@@ -195,7 +195,7 @@ struct FyScanArgs {
     const uint32_t* last;  // [3][tiles] masked value of each tile's last draw
     const uint32_t* cnt;
     FyState* state;     // [3]
-    uint32_t* acc;      // [3][count][n] accepted offsets v_i (swap with i + v_i)
+    uint32_t* acc;      // [count][3][n] accepted offsets v_i (swap with i + v_i)
     uint32_t* refills;  // [3][count] getNext buffers used
     unsigned long long* stats;  // optional [3][kFyStats] diagnostic counters (ORQ_FY_STATS)
 };
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         const unsigned long long t_a0 = clock64();
         const uint32_t tot_a = tot_c + s_uacc;
         const uint32_t need = n - i;
-        uint32_t* acc = a.acc + ((size_t)g * a.count + m) * (size_t)n;
+        uint32_t* acc = a.acc + ((size_t)m * 3 + g) * (size_t)n;
         {
             uint32_t rc = cbase, ru = ubase;
 #pragma unroll
@@ -786,7 +786,9 @@ FyRes& fy_res(Ctx& c) {
     ORQ_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&R.gs, cudaStreamNonBlocking, prio_lo));
     for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&R.ss[g], cudaStreamNonBlocking, prio_hi));
+    ORQ_CUDA_CHECK(cudaStreamCreateWithPriority(&R.fs, cudaStreamNonBlocking, prio_lo));
     ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&R.ev_start, cudaEventDisableTiming));
+    ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&R.fin_done, cudaEventDisableTiming));
     for (int k = 0; k < kFyRingMax; k++) {
         ORQ_CUDA_CHECK(cudaEventCreateWithFlags(&R.gen_done[k], cudaEventDisableTiming));
         for (int g = 0; g < 3; g++) {
@@ -805,7 +807,9 @@ void release_fy(Ctx& c) {
     if (!R.ready) return;
     cudaStreamSynchronize(R.gs);
     for (int g = 0; g < 3; g++) cudaStreamSynchronize(R.ss[g]);
+    cudaStreamSynchronize(R.fs);
     cudaEventDestroy(R.ev_start);
+    cudaEventDestroy(R.fin_done);
     for (int k = 0; k < kFyRingMax; k++) {
         cudaEventDestroy(R.gen_done[k]);
         for (int g = 0; g < 3; g++) {
@@ -815,6 +819,7 @@ void release_fy(Ctx& c) {
     }
     cudaStreamDestroy(R.gs);
     for (int g = 0; g < 3; g++) cudaStreamDestroy(R.ss[g]);
+    cudaStreamDestroy(R.fs);
     cudaFreeHost(R.hst);
     R = FyRes{};
 }
@@ -908,16 +913,74 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     // back to the pool: a later call on the runtime's stream could otherwise
     // be handed memory those kernels are still writing. Declared after the
     // scratch buffers, so it runs before their destructors.
+    //
+    // Finalize runs on its own low-priority stream for the permutations the
+    // scanners have completed, while the chain goes on (the generator leaves
+    // SMs idle while the scanners work through dense windows). acc is laid out
+    // [permutation][group], so B permutations of all three groups are one
+    // contiguous batch; the scratch holds one batch.
+    const size_t fin_b = std::max<size_t>(1, std::min<size_t>({(size_t)4, count,
+                                                               ((size_t)1 << 27) / (3 * std::max<size_t>(n, 1))}));
+    const size_t fin_el = 3 * fin_b * n;
+    const uint32_t fin_chunks = (uint32_t)ceil_div(n, (size_t)kFinChunk);
+    Scratch f_cur(c, fin_el * 4), f_part(c, 3 * fin_b * fin_chunks * 4), f_bucket(c, fin_el * 4),
+        f_par(c, fin_el * 4), f_A(c, fin_el * 4), f_ptrs(c, 2 * 3 * count * sizeof(void*));
+    {
+        std::vector<int32_t*> hp(2 * 3 * count);
+        for (size_t m = 0; m < count; m++)
+            for (int g = 0; g < 3; g++) {
+                hp[3 * m + g] = out[m].perm[g];
+                hp[3 * count + 3 * m + g] = out[m].inv[g];
+            }
+        ORQ_CUDA_CHECK(cudaMemcpyAsync(f_ptrs.p, hp.data(), hp.size() * sizeof(void*), cudaMemcpyHostToDevice,
+                                       c.stream));
+        ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // hp is pageable and leaves scope
+    }
+    cudaStream_t fs = R.fs;
+    size_t fin_next = 0;  // permutations [0, fin_next) are queued for finalize
+    auto launch_fin = [&](size_t m0, size_t m1) {
+        const size_t P = 3 * (m1 - m0);
+        const size_t el = P * n;
+        FinArgs fa;
+        fa.acc = acc.as<uint32_t>() + 3 * m0 * n;
+        fa.n = (uint32_t)n;
+        fa.P = (uint32_t)P;
+        fa.chunks = fin_chunks;
+        fa.cur = f_cur.as<uint32_t>();
+        fa.part = f_part.as<uint32_t>();
+        fa.bucket = f_bucket.as<int32_t>();
+        fa.par = f_par.as<int32_t>();
+        fa.A = f_A.as<int32_t>();
+        fa.perm_out = f_ptrs.as<int32_t*>() + 3 * m0;
+        fa.inv_out = f_ptrs.as<int32_t*>() + 3 * count + 3 * m0;
+        fa.err = c.d_err;
+        const unsigned gg = plain_grid(c, el);
+        const unsigned gc = (unsigned)(P * fin_chunks);
+        ProfScope ps(c, "fy_finalize", 0.0, 0.0, fs);
+        ORQ_CUDA_CHECK(cudaMemsetAsync(f_cur.p, 0, el * 4, fs));
+        k_fin_count<<<gg, 256, 0, fs>>>(fa);
+        k_fin_part<<<gc, kFinThreads, 0, fs>>>(fa);
+        k_fin_top<<<(unsigned)P, kFinThreads, 0, fs>>>(fa);
+        k_fin_starts<<<gc, kFinThreads, 0, fs>>>(fa);
+        k_fin_place<<<gg, 256, 0, fs>>>(fa);
+        k_fin_par<<<gg, 256, 0, fs>>>(fa);
+        k_fin_roots<<<gg, 256, 0, fs>>>(fa);
+        k_fin_final<<<gg, 256, 0, fs>>>(fa);
+        ORQ_CUDA_CHECK(cudaGetLastError());
+        c.kernels_launched += 8;
+    };
     struct DrainSideStreams {
         FyRes& r;
         ~DrainSideStreams() {
             cudaStreamSynchronize(r.gs);
             for (int g = 0; g < 3; g++) cudaStreamSynchronize(r.ss[g]);
+            cudaStreamSynchronize(r.fs);
         }
     } drain{R};
     ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
     ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
     for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], ev_start, 0));
+    ORQ_CUDA_CHECK(cudaStreamWaitEvent(fs, ev_start, 0));
 
     prep_aes_kernel(k_fy_gen);
     ORQ_CUDA_CHECK(cudaFuncSetAttribute(k_fy_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem));
@@ -1024,12 +1087,19 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         while (!finished && checked + lag <= w) {
             const int pb = (int)(checked % kRing);
             bool all = true;
+            size_t mmin = count;  // permutations every group has completed
             for (int g = 0; g < 3; g++) {
                 ORQ_CUDA_CHECK(cudaEventSynchronize(st_ev[g][pb]));
                 all = all && hst[3 * pb + g].done;
+                mmin = std::min<size_t>(mmin, hst[3 * pb + g].done ? count : hst[3 * pb + g].m);
             }
             finished = all;
             checked++;
+            if (!finished && fin_next + fin_b <= mmin) {
+                // their accepted offsets were written before this window's states
+                for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(fs, st_ev[g][pb], 0));
+                for (; fin_next + fin_b <= mmin; fin_next += fin_b) launch_fin(fin_next, fin_next + fin_b);
+            }
         }
     }
     const unsigned long long w = tl_idx.size();
@@ -1069,52 +1139,11 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
         }
     }
 
-    // finalize, a few permutations at a time to bound scratch
-    const size_t per_batch = std::max<size_t>(1, std::min<size_t>(3 * count, (size_t)(1ull << 27) / std::max<size_t>(n, 1)));
-    for (size_t p0 = 0; p0 < 3 * count; p0 += per_batch) {
-        const size_t P = std::min(per_batch, 3 * count - p0);
-        const size_t el = P * n;
-        const uint32_t chunks = (uint32_t)ceil_div(n, (size_t)kFinChunk);
-        Scratch cur(c, el * 4), part(c, P * chunks * 4), bucket(c, el * 4), par(c, el * 4), A(c, el * 4),
-            ptrs(c, 2 * P * sizeof(void*));
-        std::vector<int32_t*> hp(2 * P);
-        for (size_t k = 0; k < P; k++) {
-            // acc is laid out [group][perm]; permutation index pm = p0 + k
-            const size_t pm = p0 + k, g = pm / count, m = pm % count;
-            hp[k] = out[m].perm[g];
-            hp[P + k] = out[m].inv[g];
-        }
-        ORQ_CUDA_CHECK(cudaMemcpyAsync(ptrs.p, hp.data(), hp.size() * sizeof(void*),
-                                       cudaMemcpyHostToDevice, c.stream));
-        FinArgs fa;
-        fa.acc = acc.as<uint32_t>() + p0 * n;
-        fa.n = (uint32_t)n;
-        fa.P = (uint32_t)P;
-        fa.chunks = chunks;
-        fa.cur = cur.as<uint32_t>();
-        fa.part = part.as<uint32_t>();
-        fa.bucket = bucket.as<int32_t>();
-        fa.par = par.as<int32_t>();
-        fa.A = A.as<int32_t>();
-        fa.perm_out = ptrs.as<int32_t*>();
-        fa.inv_out = ptrs.as<int32_t*>() + P;
-        fa.err = c.d_err;
-        const unsigned gg = plain_grid(c, el);
-        const unsigned gc = (unsigned)(P * chunks);
-        ProfScope ps(c, "fy_finalize", 0.0);
-        ORQ_CUDA_CHECK(cudaMemsetAsync(cur.p, 0, el * 4, c.stream));
-        k_fin_count<<<gg, 256, 0, c.stream>>>(fa);
-        k_fin_part<<<gc, kFinThreads, 0, c.stream>>>(fa);
-        k_fin_top<<<(unsigned)P, kFinThreads, 0, c.stream>>>(fa);
-        k_fin_starts<<<gc, kFinThreads, 0, c.stream>>>(fa);
-        k_fin_place<<<gg, 256, 0, c.stream>>>(fa);
-        k_fin_par<<<gg, 256, 0, c.stream>>>(fa);
-        k_fin_roots<<<gg, 256, 0, c.stream>>>(fa);
-        k_fin_final<<<gg, 256, 0, c.stream>>>(fa);
-        ORQ_CUDA_CHECK(cudaGetLastError());
-        c.kernels_launched += 8;
-        ORQ_CUDA_CHECK(cudaStreamSynchronize(c.stream));  // scratch reuse
-    }
+    // the permutations completed since the last batch, then the runtime's
+    // stream waits for the finalize stream
+    for (; fin_next < count; fin_next += fin_b) launch_fin(fin_next, std::min(count, fin_next + fin_b));
+    ORQ_CUDA_CHECK(cudaEventRecord(R.fin_done, fs));
+    ORQ_CUDA_CHECK(cudaStreamWaitEvent(c.stream, R.fin_done, 0));
     c.check_device_error();
 
 }

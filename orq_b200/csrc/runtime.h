@@ -105,7 +105,9 @@ struct FyRes {
     bool ready = false;
     cudaStream_t gs = nullptr;
     cudaStream_t ss[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t fs = nullptr;  // finalize of completed permutations, during the chain
     cudaEvent_t ev_start = nullptr;
+    cudaEvent_t fin_done = nullptr;
     cudaEvent_t gen_done[kFyRingMax] = {};
     cudaEvent_t scan_done[3][kFyRingMax] = {};
     cudaEvent_t st_ev[3][kFyRingMax] = {};
