@@ -222,7 +222,9 @@ constexpr int kScanWarps = kScanThreads / 32;
 constexpr int kFyStats = 10;  // diagnostic counters per group
 constexpr int kQuads = kPerThread / 4;  // lane-quads per thread and step
 constexpr uint32_t kUncCap = 2048;
-constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4;
+// dynamic shared memory: the step's entries, then the lane-quad classes and
+// prefixes (cq below)
+constexpr size_t kScanSmem = (size_t)kMaxStepEntries * 4 + (size_t)kScanWarps * kQuads * 32 * 4;
 
 // entries per step at level L: uncertain entries of a step are about
 // cs^2 / (2 n/4^L); keep that near 512
@@ -233,10 +235,10 @@ __device__ __forceinline__ uint32_t step_entries(uint32_t n, uint32_t L) {
     return s;
 }
 
-// 4-byte global -> shared copy that completes asynchronously (cp.async)
-__device__ __forceinline__ void cp_async4(uint32_t* dst_smem, const uint32_t* src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+// 4-byte global -> shared copy that completes asynchronously (cp.async);
+// dst is a shared-window address
+__device__ __forceinline__ void cp_async4(uint32_t dst, const uint32_t* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 // bulk prefetch of [addr, addr + bytes) into L2; addr and bytes multiples of 16
@@ -248,9 +250,12 @@ __device__ __forceinline__ void prefetch_l2(uintptr_t addr, uint32_t bytes) {
 // class of entry q with value v in a step of cs entries at bound T: bit 0
 // certainly accepted (v + q <= T: at most q acceptances precede it), bit 4
 // uncertain (v <= T but not certain); rejected otherwise
+// (v < n < 2^31 and q < 2^15 for real entries, so v + q fits 32 bits; the
+// padding entries beyond cs are excluded first)
 __device__ __forceinline__ uint32_t fy_class(uint32_t q, uint32_t v, uint32_t cs, uint32_t T) {
-    const bool cert = q < cs && (unsigned long long)v + q <= T;
-    const bool unc = q < cs && !cert && v <= T;
+    const bool in = q < cs;
+    const bool cert = in && v + q <= T;
+    const bool unc = in && !cert && v <= T;
     return (uint32_t)cert | ((uint32_t)unc << 4);
 }
 
@@ -283,7 +288,11 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
     __shared__ uint32_t P[kMaxWindowTiles + 1];  // prefix of level-L counts over the window
     __shared__ uint32_t unc_v[kUncCap], unc_cp[kUncCap], unc_pre[kUncCap + 1];
     __shared__ uint32_t wtot[kScanWarps], wpre[kScanWarps];
-    __shared__ uint8_t codes[kScanWarps][kQuads][32];  // entry classes per warp, iteration and lane
+    // per warp, quad iteration and lane: bits 0-7 the four entries' classes,
+    // bits 8-18 the certain and bits 19-29 the uncertain entries of the warp
+    // before this lane-quad (at most 1024 each); in the dynamic allocation
+    // after the entries (static shared memory is limited to 48 KB)
+    auto cq = reinterpret_cast<uint32_t (*)[kQuads][32]>(sv + kMaxStepEntries);
     __shared__ uint32_t s_last_q, s_uacc, s_tot;
     const uint32_t g = a.g0 + blockIdx.x;
     const uint32_t n = a.n;
@@ -359,15 +368,26 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         // its tile cursor forward). Warp w stages and then processes entries
         // [1024w, 1024w + 1024), so a warp-level sync publishes them.
         {
+            // the lane's current tile: entry e lives at EV[boff + e] while
+            // e < tend; the tile advances only when a lane crosses into the next
             const size_t off = a.lay.off[L];
             uint32_t t = tau;
+            uint32_t tend = P[t + 1];
+            size_t boff = (size_t)t * a.lay.slot + off - (size_t)P[t];  // wraps; boff + e does not
+            const uint32_t sv_sh = (uint32_t)__cvta_generic_to_shared(sv);
 #pragma unroll
             for (int u = 0; u < kPerThread; u++) {
                 const uint32_t q = qw + 32u * u;
                 if (q < cs) {
                     const uint32_t e = e0 + q;
-                    while (P[t + 1] <= e) t++;
-                    cp_async4(sv + q, EV + (size_t)t * a.lay.slot + off + (e - P[t]));
+                    if (e >= tend) {
+                        do {
+                            t++;
+                        } while (P[t + 1] <= e);
+                        tend = P[t + 1];
+                        boff = (size_t)t * a.lay.slot + off - (size_t)P[t];
+                    }
+                    cp_async4(sv_sh + 4u * q, EV + (boff + e));
                 } else {
                     sv[q] = 0xffffffffu;
                 }
@@ -376,7 +396,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         }
         __syncwarp();
         // In the passes below lane l of warp w holds, at iteration u, the four
-        // consecutive entries q = 1024w + 128u + 4l + r (r = 0..3); codes[w][u][l]
+        // consecutive entries q = 1024w + 128u + 4l + r (r = 0..3); cq[w][u][l]
         // keeps their classification (bit r: certainly accepted, bit 4 + r:
         // uncertain): a lane-quad is one 16-byte shared load, and ranks come
         // from one packed warp scan per 128 entries.
@@ -385,18 +405,19 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         // while the uncertain entries do not fit the list
         uint32_t tot_c, tot_u;
         for (;;) {
-            uint32_t x = 0;
+            uint32_t x = 0;  // the warp's (certain | uncertain << 16) so far
 #pragma unroll
             for (int u = 0; u < kQuads; u++) {
                 const uint32_t q = q0 + 128u * u;
                 const uint4 v4 = *reinterpret_cast<const uint4*>(sv + q);
                 const uint32_t code = fy_class(q, v4.x, cs, T) | (fy_class(q + 1, v4.y, cs, T) << 1) |
                                       (fy_class(q + 2, v4.z, cs, T) << 2) | (fy_class(q + 3, v4.w, cs, T) << 3);
-                codes[warp][u][lane] = (uint8_t)code;
-                x += __popc(code & 0xfu) | (__popc(code >> 4) << 16);
+                uint32_t ex, tot;
+                quad_prefix(code, lane, ex, tot);
+                const uint32_t pre = x + ex;
+                cq[warp][u][lane] = code | ((pre & 0xffffu) << 8) | ((pre >> 16) << 19);
+                x += tot;
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
             if (lane == 0) wtot[warp] = x;
             __syncthreads();
             if (warp == 0) {
@@ -425,15 +446,13 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         // ---- list the uncertain entries in order, with the certain accepts
         // before each
         if (tot_u) {
-            uint32_t rc = cbase, ru = ubase;
 #pragma unroll
             for (int u = 0; u < kQuads; u++) {
-                const uint32_t code = codes[warp][u][lane];
-                uint32_t ex, tot;
-                quad_prefix(code, lane, ex, tot);
+                const uint32_t cw = cq[warp][u][lane];
+                const uint32_t code = cw & 0xffu;
                 if (code >> 4) {
                     const uint32_t q = q0 + 128u * u;
-                    uint32_t c = rc + (ex & 0xffffu), k = ru + (ex >> 16);
+                    uint32_t c = cbase + ((cw >> 8) & 0x7ffu), k = ubase + (cw >> 19);
 #pragma unroll
                     for (int r = 0; r < 4; r++) {
                         if ((code >> (4 + r)) & 1u) {
@@ -444,8 +463,6 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                         c += (code >> r) & 1u;
                     }
                 }
-                rc += tot & 0xffffu;
-                ru += tot >> 16;
             }
         }
         __syncthreads();
@@ -464,15 +481,16 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                 uint32_t okmask = __ballot_sync(0xffffffffu, cert);
                 const uint32_t undmask = __ballot_sync(0xffffffffu, und);
                 if (undmask) {
-                    // decide the chunk lane by lane
-                    okmask = 0;
-                    uint32_t cur = acc_so_far;
-                    for (int j = 0; j < 32; j++) {
+                    // decide the undetermined lanes in order; the certain ones
+                    // (already in okmask) and the rejected ones do not depend
+                    // on the lanes before them
+                    uint32_t pend = undmask;
+                    while (pend) {
+                        const int j = __ffs(pend) - 1;
+                        pend &= pend - 1;
                         const long long sj = __shfl_sync(0xffffffffu, slack, j);
-                        if (base + j < tot_u && sj >= (long long)cur) {
-                            okmask |= 1u << j;
-                            cur++;
-                        }
+                        const uint32_t before = acc_so_far + __popc(okmask & ((1u << j) - 1u));
+                        if (sj >= (long long)before) okmask |= 1u << j;
                     }
                 }
                 if (valid) {
@@ -499,33 +517,48 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         const uint32_t need = n - i;
         uint32_t* acc = a.acc + ((size_t)m * 3 + g) * (size_t)n;
         {
-            uint32_t rc = cbase, ru = ubase;
+            uint32_t* acci = acc + i;
 #pragma unroll
             for (int u = 0; u < kQuads; u++) {
-                const uint32_t code = codes[warp][u][lane];
-                uint32_t ex, tot;
-                quad_prefix(code, lane, ex, tot);
+                const uint32_t cw = cq[warp][u][lane];
+                const uint32_t code = cw & 0xffu;
                 if (code) {
                     const uint32_t q = q0 + 128u * u;
                     const uint4 v4 = *reinterpret_cast<const uint4*>(sv + q);
                     const uint32_t vv[4] = {v4.x, v4.y, v4.z, v4.w};
-                    uint32_t c = rc + (ex & 0xffffu), k = ru + (ex >> 16);  // certain / uncertain before q + r
+                    // certain / uncertain entries before q + r
+                    uint32_t c = cbase + ((cw >> 8) & 0x7ffu), k = ubase + (cw >> 19);
+                    if ((code >> 4) == 0) {
+                        // no uncertain entry in the quad: one lookup of the
+                        // uncertain acceptances before it serves all four
+                        const uint32_t up = unc_pre[k];
 #pragma unroll
-                    for (int r = 0; r < 4; r++) {
-                        const bool cert = (code >> r) & 1u, unc = (code >> (4 + r)) & 1u;
-                        if (cert || (unc && unc_cp[k])) {
-                            const uint32_t rank = c + unc_pre[k];
-                            if (rank < need) {
-                                acc[i + rank] = vv[r];
-                                if (rank == need - 1) s_last_q = q + r;
+                        for (int r = 0; r < 4; r++) {
+                            if ((code >> r) & 1u) {
+                                const uint32_t rank = c + up;
+                                if (rank < need) {
+                                    acci[rank] = vv[r];
+                                    if (rank == need - 1) s_last_q = q + r;
+                                }
+                                c++;
                             }
                         }
-                        c += cert;
-                        k += unc;
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 4; r++) {
+                            const bool cert = (code >> r) & 1u, unc = (code >> (4 + r)) & 1u;
+                            if (cert || (unc && unc_cp[k])) {
+                                const uint32_t rank = c + unc_pre[k];
+                                if (rank < need) {
+                                    acci[rank] = vv[r];
+                                    if (rank == need - 1) s_last_q = q + r;
+                                }
+                            }
+                            c += cert;
+                            k += unc;
+                        }
                     }
                 }
-                rc += tot & 0xffffu;
-                ru += tot >> 16;
             }
         }
         if (tot_a >= need) {
