@@ -13,8 +13,9 @@
 // secret_share_b / secret_share_a / public_share / secret_share,
 // orq::operators (sorts, shuffle, permutations, compare_rows, swap,
 // multiplex, table_sort, distinct), orq::aggregators and EncodedTable<T> with
-// sort / aggregate / joins / open_with_schema. One process plays all three
-// parties of replicated 3PC; every protocol step runs in liborq_cuda.so (link
+// sort / aggregate / joins / open_with_schema. One process plays all the
+// parties (replicated 3PC, or 2PC / 4PC with -DPROTOCOL_NUM=2|4); every
+// protocol step runs in liborq_cuda.so (link
 // with -L<dir> -lorq_cuda) through the C ABI of orq_cuda.h. With the same
 // keys and one worker thread at batch size -1 on the CPU side, shares equal a
 // CPU run's bit for bit.
@@ -36,7 +37,7 @@ namespace debug {
 }  // namespace debug
 
 namespace service {
-namespace loopback_3pc {
+namespace loopback {
 template <typename T>
 using BSharedVector = orq::BSharedVector<T>;
 template <typename T>
@@ -61,11 +62,30 @@ using orq::relational::isBShared;
 using orq::relational::JoinOptions;
 using orq::operators::ASC;
 using orq::operators::DESC;
-}  // namespace loopback_3pc
+}  // namespace loopback
+// the protocol namespaces of mpc.h: one loopback API serves all three
+namespace loopback_3pc = loopback;
+namespace loopback_2pc = loopback;
+namespace loopback_4pc = loopback;
 }  // namespace service
 }  // namespace orq
 
+// PROTOCOL_NUM (mpc.h:70-169) picks the protocol at compile time, as in the
+// reference: 3 replicated 3PC (default), 2 Beaver 2PC with dummy triples, 4
+// Fantastic-4PC. The 2PC / 4PC runtimes run sharing, open, and_b, xor_b,
+// multiply_a, add_a, sub_a and b2a_bit; other operators throw RuntimeError.
+#ifndef PROTOCOL_NUM
+#define PROTOCOL_NUM 3
+#endif
+#if PROTOCOL_NUM == 2
+#define COMPILED_MPC_PROTOCOL_NAMESPACE orq::service::loopback_2pc
+#elif PROTOCOL_NUM == 4
+#define COMPILED_MPC_PROTOCOL_NAMESPACE orq::service::loopback_4pc
+#elif PROTOCOL_NUM == 3
 #define COMPILED_MPC_PROTOCOL_NAMESPACE orq::service::loopback_3pc
+#else
+#error "PROTOCOL_NUM must be 2, 3 or 4"
+#endif
 
 // orq_init (include/backend/common/setup.h:8-58): the reference reads the
 // party/thread/batch arguments and connects the parties; the loopback build
@@ -73,7 +93,7 @@ using orq::operators::DESC;
 // ORQ_SEED (default 1) exactly as the deterministic key generator of the
 // reference's test build derives them; ORQ_DEVICE picks the CUDA device.
 inline void orq_init(uint64_t seed, int device = 0) {
-    orq::service::runtime_holder() = std::make_unique<orq::service::LoopbackRunTime>(seed, device);
+    orq::service::runtime_holder() = std::make_unique<orq::service::LoopbackRunTime>(seed, device, PROTOCOL_NUM);
 }
 inline void orq_init(int argc = 0, char** argv = nullptr) {
     (void)argc;

@@ -112,12 +112,19 @@ namespace service {
 class LoopbackRunTime {
     orqcu_runtime* rt_ = nullptr;
     uint64_t seed_;
+    int nparties_;
     std::mt19937_64 local_rng_;
 
    public:
-    explicit LoopbackRunTime(uint64_t seed, int device = 0) : seed_(seed), local_rng_(seed ^ 0x5DEECE66Dull) {
-        orqcu_check(orqcu_runtime_create(seed, device, &rt_));
+    // nparties 3: replicated 3PC; 2: Beaver 2PC with dummy triples; 4:
+    // Fantastic-4PC (the latter two run the protocols' local steps: sharing,
+    // open, and_b, multiply_a, b2a_bit and the local ops)
+    explicit LoopbackRunTime(uint64_t seed, int device = 0, int nparties = 3)
+        : seed_(seed), nparties_(nparties), local_rng_(seed ^ 0x5DEECE66Dull) {
+        if (nparties == 3) orqcu_check(orqcu_runtime_create(seed, device, &rt_));
+        else orqcu_check(orqcu_runtime_create_np(seed, device, nparties, &rt_));
     }
+    int nparties() const { return nparties_; }
     ~LoopbackRunTime() {
         if (rt_) orqcu_runtime_destroy(rt_);
     }
@@ -130,7 +137,7 @@ class LoopbackRunTime {
     // One process holds every party; opened values are available to it, so
     // checks written for "party 0" run here.
     int getPartyID() const { return 0; }
-    int getNumParties() const { return 3; }
+    int getNumParties() const { return nparties_; }
 
     // RunTime::populateLocalRandom (runtime.h): plaintext randomness for test
     // inputs, from a host generator seeded by the runtime seed.
@@ -182,9 +189,10 @@ struct ShareStore {
     void* base = nullptr;
     size_t cap = 0;
     int width = 0;
-    ShareStore(orqcu_runtime* r, size_t n, int w) : rt(r), cap(n), width(w) {
-        orqcu_check(orqcu_pool_alloc(rt, 3 * std::max<size_t>(n, 1) * (size_t)w, &base));
-        orqcu_check(orqcu_memset(rt, base, 0, 3 * std::max<size_t>(n, 1) * (size_t)w));
+    int np = 3;  // distinct share arrays: 3 (3PC), 2 (2PC) or 4 (4PC)
+    ShareStore(orqcu_runtime* r, size_t n, int w, int parties) : rt(r), cap(n), width(w), np(parties) {
+        orqcu_check(orqcu_pool_alloc(rt, (size_t)np * std::max<size_t>(n, 1) * (size_t)w, &base));
+        orqcu_check(orqcu_memset(rt, base, 0, (size_t)np * std::max<size_t>(n, 1) * (size_t)w));
     }
     ~ShareStore() {
         if (base) orqcu_pool_free(rt, base);
@@ -193,8 +201,8 @@ struct ShareStore {
     ShareStore& operator=(const ShareStore&) = delete;
 };
 
-// A (possibly offset) view of n elements of a ShareStore: the three share
-// pointers the C ABI takes.
+// A (possibly offset) view of n elements of a ShareStore: the share pointers
+// the C ABI takes (three for 3PC, two or four for 2PC / 4PC).
 struct Shares {
     std::shared_ptr<ShareStore> st;
     size_t off = 0, n = 0;
@@ -202,17 +210,22 @@ struct Shares {
 
     Shares() = default;
     Shares(size_t n_, int w) : n(n_), width(w) {
-        st = std::make_shared<ShareStore>(service::runTime->handle(), n_, w);
+        st = std::make_shared<ShareStore>(service::runTime->handle(), n_, w, service::runTime->nparties());
     }
+    int np() const { return st ? st->np : 3; }
     void* ptr(int p) const {
         return static_cast<char*>(st->base) + ((size_t)p * st->cap + off) * (size_t)width;
     }
     struct P3 {
-        void* p[3];
+        void* p[4];
         operator void* const*() const { return p; }
         operator const void* const*() const { return const_cast<const void* const*>(p); }
     };
-    P3 p3() const { return {{ptr(0), ptr(1), ptr(2)}}; }
+    P3 p3() const {
+        P3 r{{nullptr, nullptr, nullptr, nullptr}};
+        for (int p = 0; p < np(); p++) r.p[p] = ptr(p);
+        return r;
+    }
     Shares slice(size_t b, size_t e) const {
         if (b > e || e > n) throw std::out_of_range("slice out of range");
         Shares s = *this;
@@ -228,18 +241,19 @@ struct Shares {
     }
     // elementwise copy of o's shares into this view (Vector::operator=)
     void assign(const Shares& o) const {
-        if (o.n != n || o.width != width) throw std::invalid_argument("assignment of a different size or type");
-        for (int p = 0; p < 3; p++)
+        if (o.n != n || o.width != width || o.np() != np())
+            throw std::invalid_argument("assignment of a different size or type");
+        for (int p = 0; p < np(); p++)
             orqcu_check(orqcu_memcpy_d2d(st->rt, ptr(p), o.ptr(p), n * (size_t)width));
     }
     void zero() const {
-        for (int p = 0; p < 3; p++) orqcu_check(orqcu_memset(st->rt, ptr(p), 0, n * (size_t)width));
+        for (int p = 0; p < np(); p++) orqcu_check(orqcu_memset(st->rt, ptr(p), 0, n * (size_t)width));
     }
-    // the three shares on the host, S[p][i] (tests and share files)
+    // the distinct shares on the host, S[p][i] (tests and share files)
     template <typename T>
     std::vector<std::vector<T>> download() const {
-        std::vector<std::vector<T>> h(3, std::vector<T>(n));
-        for (int p = 0; p < 3; p++)
+        std::vector<std::vector<T>> h(np(), std::vector<T>(n));
+        for (int p = 0; p < np(); p++)
             orqcu_check(orqcu_memcpy_d2h(st->rt, h[p].data(), ptr(p), n * sizeof(T)));
         return h;
     }

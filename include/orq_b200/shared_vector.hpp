@@ -67,6 +67,8 @@ class SharedVectorBase {
     void need_same(const SharedVectorBase& o) const {
         if (o.size() != size()) throw std::invalid_argument("vector sizes differ");
     }
+    // replicated 3PC, or the 2PC / 4PC runtime (orqcu_np_* entry points)
+    bool np3() const { return s_.np() == 3; }
 
    public:
     using value_type = T;
@@ -99,7 +101,8 @@ class SharedVectorBase {
         if (!size()) return out;
         void* d = nullptr;
         orqcu_check(orqcu_pool_alloc(rt(), size() * sizeof(T), &d));
-        int rc = orqcu_open(rt(), Arith, share_width<T>(), size(), s_.p3(), d);
+        int rc = np3() ? orqcu_open(rt(), Arith, share_width<T>(), size(), s_.p3(), d)
+                       : orqcu_np_open(rt(), Arith, share_width<T>(), size(), s_.p3(), d);
         if (rc == ORQCU_OK) rc = orqcu_memcpy_d2h(rt(), out.data(), d, size() * sizeof(T));
         orqcu_pool_free(rt(), d);
         orqcu_check(rc);
@@ -131,10 +134,10 @@ class BSharedVector : public SharedVectorBase<T, BSharedVector<T>, false> {
     BSharedVector(const std::unique_ptr<BSharedVector>& p) : Base(p->shares()) {}
 
     // and_b (replicated_3pc.h:166-191) fused with the zero-sharing
-    U operator&(const BSharedVector& o) const { return this->binary(o, orqcu_and_b); }
-    U operator^(const BSharedVector& o) const { return this->binary(o, orqcu_xor_b); }
-    BSharedVector& operator&=(const BSharedVector& o) { return this->in_place(o, orqcu_and_b); }
-    BSharedVector& operator^=(const BSharedVector& o) { return this->in_place(o, orqcu_xor_b); }
+    U operator&(const BSharedVector& o) const { return this->binary(o, this->np3() ? orqcu_and_b : orqcu_np_and_b); }
+    U operator^(const BSharedVector& o) const { return this->binary(o, this->np3() ? orqcu_xor_b : orqcu_np_xor_b); }
+    BSharedVector& operator&=(const BSharedVector& o) { return *this = *(*this & o); }
+    BSharedVector& operator^=(const BSharedVector& o) { return this->in_place(o, this->np3() ? orqcu_xor_b : orqcu_np_xor_b); }
     BSharedVector& operator&=(const U& o) { return *this &= *o; }
     BSharedVector& operator^=(const U& o) { return *this ^= *o; }
     // operator| (b_shared_vector.h:438-441): ~(~a & ~b)
@@ -205,12 +208,12 @@ class ASharedVector : public SharedVectorBase<T, ASharedVector<T>, true> {
     ASharedVector(const std::unique_ptr<ASharedVector>& p) : Base(p->shares()) {}
 
     // multiply_a (replicated_3pc.h:44-67); add_a / sub_a are local
-    U operator*(const ASharedVector& o) const { return this->binary(o, orqcu_multiply_a); }
-    U operator+(const ASharedVector& o) const { return this->binary(o, orqcu_add_a); }
-    U operator-(const ASharedVector& o) const { return this->binary(o, orqcu_sub_a); }
-    ASharedVector& operator*=(const ASharedVector& o) { return this->in_place(o, orqcu_multiply_a); }
-    ASharedVector& operator+=(const ASharedVector& o) { return this->in_place(o, orqcu_add_a); }
-    ASharedVector& operator-=(const ASharedVector& o) { return this->in_place(o, orqcu_sub_a); }
+    U operator*(const ASharedVector& o) const { return this->binary(o, this->np3() ? orqcu_multiply_a : orqcu_np_multiply_a); }
+    U operator+(const ASharedVector& o) const { return this->binary(o, this->np3() ? orqcu_add_a : orqcu_np_add_a); }
+    U operator-(const ASharedVector& o) const { return this->binary(o, this->np3() ? orqcu_sub_a : orqcu_np_sub_a); }
+    ASharedVector& operator*=(const ASharedVector& o) { return *this = *(*this * o); }
+    ASharedVector& operator+=(const ASharedVector& o) { return this->in_place(o, this->np3() ? orqcu_add_a : orqcu_np_add_a); }
+    ASharedVector& operator-=(const ASharedVector& o) { return this->in_place(o, this->np3() ? orqcu_sub_a : orqcu_np_sub_a); }
     ASharedVector& operator*=(const U& o) { return *this *= *o; }
     ASharedVector& operator+=(const U& o) { return *this += *o; }
     ASharedVector& operator-=(const U& o) { return *this -= *o; }
@@ -230,7 +233,10 @@ class ASharedVector : public SharedVectorBase<T, ASharedVector<T>, true> {
 template <typename T>
 ASharedVector<T> BSharedVector<T>::b2a_bit() const {
     ASharedVector<T> r(this->size());
-    orqcu_check(orqcu_b2a_bit(this->rt(), share_width<T>(), this->size(), this->s_.p3(), r.shares().p3()));
+    if (this->np3())
+        orqcu_check(orqcu_b2a_bit(this->rt(), share_width<T>(), this->size(), this->s_.p3(), r.shares().p3()));
+    else
+        orqcu_check(orqcu_np_b2a_bit(this->rt(), share_width<T>(), this->size(), this->s_.p3(), r.shares().p3()));
     return r;
 }
 
@@ -256,19 +262,25 @@ class ElementwisePermutation : public ASharedVector<int32_t> {
 // ---------------------------------------------------------------------------
 // secret_share_b / secret_share_a (replicated_3pc.h:401-448): the owner
 // `party` shares its plaintext with its local PRG.
+namespace detail {
+template <typename T>
+EVector<T> share(const Vector<T>& data, int party, int arith) {
+    EVector<T> e{Shares(data.size(), share_width<T>())};
+    DeviceInput<T> in(data);
+    if (e.s.np() == 3)
+        orqcu_check(orqcu_secret_share(e.s.st->rt, arith, share_width<T>(), data.size(), in.p, party, e.s.p3()));
+    else
+        orqcu_check(orqcu_np_secret_share(e.s.st->rt, arith, share_width<T>(), data.size(), in.p, party, e.s.p3()));
+    return e;
+}
+}  // namespace detail
 template <typename T>
 EVector<T> secret_share_b(const Vector<T>& data, int party = 0) {
-    EVector<T> e{Shares(data.size(), share_width<T>())};
-    detail::DeviceInput<T> in(data);
-    orqcu_check(orqcu_secret_share(e.s.st->rt, 0, share_width<T>(), data.size(), in.p, party, e.s.p3()));
-    return e;
+    return detail::share(data, party, 0);
 }
 template <typename T>
 EVector<T> secret_share_a(const Vector<T>& data, int party = 0) {
-    EVector<T> e{Shares(data.size(), share_width<T>())};
-    detail::DeviceInput<T> in(data);
-    orqcu_check(orqcu_secret_share(e.s.st->rt, 1, share_width<T>(), data.size(), in.p, party, e.s.p3()));
-    return e;
+    return detail::share(data, party, 1);
 }
 // secret_share_vec(x, sx) of the reference's tests: share into an existing
 // vector, boolean or arithmetic by its type
@@ -280,12 +292,17 @@ template <typename T>
 void secret_share_vec(const Vector<T>& data, ASharedVector<T>& out, int party = 0) {
     out = ASharedVector<T>(secret_share_a(data, party));
 }
-// public_share (replicated_3pc.h:456-470): S0 = x, S1 = S2 = 0
+// public_share (replicated_3pc.h:456-470): S0 = x, S1 = S2 = 0; for 2PC
+// (beaver_2pc.h:262-270) S0 = x, S1 = 0; for 4PC (dalskov_4pc.h:786-797)
+// X0 = x and the other shares 0
 template <typename T>
 EVector<T> public_share(const Vector<T>& data) {
     EVector<T> e{Shares(data.size(), share_width<T>())};
     detail::DeviceInput<T> in(data);
-    orqcu_check(orqcu_public_share(e.s.st->rt, share_width<T>(), data.size(), in.p, e.s.p3()));
+    if (e.s.np() == 3)
+        orqcu_check(orqcu_public_share(e.s.st->rt, share_width<T>(), data.size(), in.p, e.s.p3()));
+    else if (data.size())
+        orqcu_check(orqcu_memcpy_d2d(e.s.st->rt, e.s.ptr(0), in.p, data.size() * sizeof(T)));
     return e;
 }
 

@@ -12,7 +12,9 @@
 //       distinct shares of every vector so their digests can be compared with
 //       the reference's (run with ORQ_SEED = the reference's key seed, and
 //       compiled with -DORQ_B200_DEFAULT_SORT_PROTO=RADIXSORT like the
-//       reference driver).
+//       reference driver). Compiled with -DPROTOCOL_NUM=2 or 4, "prims" is
+//       the sequence of oracle/ref_driver_np.cpp and dumps the 2 or 4
+//       distinct shares.
 #include <algorithm>
 #include <cstdio>
 #include <fstream>
@@ -68,7 +70,9 @@ struct Dumper {
     void shares(const std::string& name, const SV& v) {
         using T = typename SV::value_type;
         auto h = v.shares().template download<T>();
-        rec(name, sizeof(T), v.size(), {h[0].data(), h[1].data(), h[2].data()});
+        std::vector<const void*> a;
+        for (auto& col : h) a.push_back(col.data());
+        rec(name, sizeof(T), v.size(), a);
     }
     template <typename T>
     void plain(const std::string& name, const orq::Vector<T>& a) {
@@ -77,8 +81,10 @@ struct Dumper {
 };
 
 // ---- the reference driver's sequences -------------------------------------
+// xa_owner: 2 in the 3PC driver (oracle/ref_driver.cpp), 1 in the 2PC / 4PC
+// driver (oracle/ref_driver_np.cpp)
 template <typename T>
-static void run_prims(size_t n, uint64_t seed, Dumper& d, const std::string& tag) {
+static void run_prims(size_t n, uint64_t seed, Dumper& d, const std::string& tag, int xa_owner) {
     uint64_t st = seed;
     auto x = gen<T>(n, st, ~0ull);
     auto y = gen<T>(n, st, ~0ull);
@@ -90,7 +96,7 @@ static void run_prims(size_t n, uint64_t seed, Dumper& d, const std::string& tag
     d.shares(tag + "and", zb);
     BSharedVector<T> xo = xb ^ yb;
     d.shares(tag + "xor", xo);
-    ASharedVector<T> xa = secret_share_a(x, 2);
+    ASharedVector<T> xa = secret_share_a(x, xa_owner);
     ASharedVector<T> ya = secret_share_a(y, 0);
     d.shares(tag + "xa", xa);
     d.shares(tag + "ya", ya);
@@ -334,9 +340,10 @@ int main(int argc, char** argv) {
             const int bits = argc > 6 ? std::atoi(argv[6]) : 40;
             Dumper d(argv[5]);
             if (op == "prims") {
-                run_prims<int32_t>(n, seed, d, "w4_");
-                run_prims<int64_t>(n, seed + 1, d, "w8_");
-                run_prims<int8_t>(n, seed + 2, d, "w1_");
+                const int xa_owner = PROTOCOL_NUM == 3 ? 2 : 1;
+                run_prims<int32_t>(n, seed, d, "w4_", xa_owner);
+                run_prims<int64_t>(n, seed + 1, d, "w8_", xa_owner);
+                run_prims<int8_t>(n, seed + 2, d, "w1_", xa_owner);
             } else if (op == "radix") {
                 run_radix(n, seed, bits, d);
             } else if (op == "join_agg") {

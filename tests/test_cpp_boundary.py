@@ -24,7 +24,8 @@ LIBDIR = os.path.join(ROOT, "orq_b200")
 
 def build(variant: str = "default") -> str:
     """Compile the C++ program; the "radix" variant sets the sort protocol of
-    EncodedTable sorts to RADIXSORT, as the reference driver is built."""
+    EncodedTable sorts to RADIXSORT, as the reference driver is built; "p2" /
+    "p4" build it for Beaver 2PC / Fantastic-4PC (PROTOCOL_NUM)."""
     from orq_b200 import build as b
 
     b.build()
@@ -34,6 +35,8 @@ def build(variant: str = "default") -> str:
            SRC, "-L", LIBDIR, "-lorq_cuda", f"-Wl,-rpath,{LIBDIR}", "-o", exe]
     if variant == "radix":
         cmd.insert(1, "-DORQ_B200_DEFAULT_SORT_PROTO=RADIXSORT")
+    elif variant in ("p2", "p4"):
+        cmd.insert(1, f"-DPROTOCOL_NUM={variant[1]}")
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]
     return exe
@@ -48,7 +51,7 @@ def test_c_header_compiles_as_c(tmp_path):
     assert r.returncode == 0, r.stderr
 
 
-@pytest.mark.parametrize("variant", ["default", "radix"])
+@pytest.mark.parametrize("variant", ["default", "radix", "p2", "p4"])
 def test_cpp_program_compiles_and_links(variant):
     exe = build(variant)
     assert os.path.exists(exe)
@@ -108,6 +111,26 @@ def test_cpp_program_matches_reference_shares(digests, tmp_path, tag):
     out = tmp_path / "d.bin"
     env = dict(os.environ, ORQ_SEED=str(m["shim_seed"]))
     r = subprocess.run([exe, "dump", m["op"], str(m["n"]), str(m["data_seed"]), str(out), str(m["bits"])],
+                       capture_output=True, text=True, timeout=900, env=env)
+    assert r.returncode == 0, r.stderr[-3000:]
+    got = read_dump(out)
+    want = digests[tag]["arrays"]
+    assert set(got) == set(want)
+    for name, arrs in got.items():
+        assert [hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest() for a in arrs] == want[name], name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", ["p2_prims_n1000", "p2_prims_n300000", "p4_prims_n1000", "p4_prims_n300000"])
+def test_cpp_program_np_matches_reference_shares(digests, tmp_path, tag):
+    """The 2PC / 4PC prims sequence of the reference's PROTOCOL_NUM=2|4 build,
+    written against ORQ's C++ API compiled with the same PROTOCOL_NUM, gives
+    the reference's distinct shares (S0, S1 or X0..X3) digest for digest."""
+    m = digests[tag]["meta"]
+    exe = build(f"p{m['parties']}")
+    out = tmp_path / "d.bin"
+    env = dict(os.environ, ORQ_SEED=str(m["shim_seed"]))
+    r = subprocess.run([exe, "dump", m["op"], str(m["n"]), str(m["data_seed"]), str(out)],
                        capture_output=True, text=True, timeout=900, env=env)
     assert r.returncode == 0, r.stderr[-3000:]
     got = read_dump(out)
