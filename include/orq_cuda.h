@@ -386,6 +386,59 @@ int orqcu_np_add_a(orqcu_runtime* rt, int width, size_t n, const void* const* x,
 int orqcu_np_sub_a(orqcu_runtime* rt, int width, size_t n, const void* const* x, const void* const* y,
                    void* const* z);
 
+/* ---- One party of replicated 3PC beside CPU parties ---------------------------
+ * A party runtime plays ONE party p of Replicated_3PC: it holds p's two
+ * shares x[0] = S[p], x[1] = S[p+1] and only the keys p holds, and each entry
+ * computes p's local step of a primitive; the exchange that follows is the
+ * caller's, over its own communicator (the NoCopy wire format of
+ * core/communication/no_copy_communicator/no_copy_communicator.h:120-266 is
+ * raw little-endian arrays; include/orq_b200/nocopy.hpp speaks it), so a GPU
+ * party runs with CPU parties of the reference. Party runtimes refuse the
+ * all-party entries above and those refuse a party runtime (ORQCU_EINVAL). */
+int orqcu_party_runtime_create(int party, int device, orqcu_runtime** out);
+/* The keys of setup_random_generation (backend/common/rand_setup.h:306-381)
+ * that party p holds, as 32-byte AES-256 keys: */
+enum {
+    ORQCU_PKEY_LOCAL = 0, /* the local PRG (secret_share on the data owner) */
+    ORQCU_PKEY_NEXT = 1,  /* p's pairwise key, sent to p+1 (zero sharing get(+1)) */
+    ORQCU_PKEY_PREV = 2,  /* the pairwise key received from p-1 (get(-1)) */
+    ORQCU_PKEY_G01 = 3,   /* group PRGs of the groups p belongs to */
+    ORQCU_PKEY_G02 = 4,
+    ORQCU_PKEY_G12 = 5,
+    ORQCU_PKEY_G012 = 6
+};
+int orqcu_party_set_key(orqcu_runtime* rt, int slot, const uint8_t key[32]);
+/* The deterministic key generator of reproducible runs (AESPRGAlgorithm::
+ * aesKeyGen, prg/prg_algorithm.h:192-197, replaced by SplitMix64 of seed,
+ * party and the party's keygen-call index; call 0 is the local PRG). A
+ * deployment draws keys from the OS instead. */
+int orqcu_keygen(uint64_t seed, int party, int call, uint8_t key[32]);
+/* secret_share_b / secret_share_a on the data owner (replicated_3pc.h:401-448):
+ * writes the three shares, s[j] = S[j]; the owner keeps (S[p], S[p+1]), sends
+ * (S[p+1], S[p+2]) to p+1 and (S[p+2], S[p]) to p+2. */
+int orqcu_party_secret_share(orqcu_runtime* rt, int arith, int width, size_t n, const void* data_dev,
+                             void* const s[3]);
+/* and_b / multiply_a (replicated_3pc.h:44-67,166-191): z = p's new share,
+ * before the exchange (send z to p-1, receive S[p+1] from p+1). */
+int orqcu_party_and_b(orqcu_runtime* rt, int width, size_t n, const void* const x[2], const void* const y[2],
+                      void* z);
+int orqcu_party_multiply_a(orqcu_runtime* rt, int width, size_t n, const void* const x[2],
+                           const void* const y[2], void* z);
+/* b2a_bit (replicated_3pc.h:220-251) in two local steps around the exchange
+ * of s0 and s1 (each: send to p-1, receive from p+1): pre writes p's s0, s1;
+ * post takes both exchanged pairs and writes p's share of (s0 - s1)^2 before
+ * the final exchange. */
+int orqcu_party_b2a_pre(orqcu_runtime* rt, int width, size_t n, const void* const x[2], void* s0, void* s1);
+int orqcu_party_b2a_post(orqcu_runtime* rt, int width, size_t n, const void* const s0[2],
+                         const void* const s1[2], void* z);
+/* xor_b / add_a / sub_a on both local shares (op 0, 1, 2). */
+int orqcu_party_local(orqcu_runtime* rt, int op, int width, size_t n, const void* const x[2],
+                      const void* const y[2], void* const z[2]);
+/* open_shares_b / open_shares_a (replicated_3pc.h:310-330) after sending x[1]
+ * to p-1 and receiving `third` (S[p+2]) from p+1. */
+int orqcu_party_open(orqcu_runtime* rt, int arith, int width, size_t n, const void* const x[2],
+                     const void* third, void* out_dev);
+
 #ifdef __cplusplus
 }
 #endif

@@ -618,6 +618,8 @@ int main(int argc, char** argv) {
         d.shares("shuffled", xb);
         auto o = xb.open();
         d.plain("open_shuffled", o);
+    } else if (op == "setup") {
+        // orq_init alone: the key exchange of setup_random_generation
     } else {
         fprintf(stderr, "unknown op %s\n", op.c_str());
         return 2;

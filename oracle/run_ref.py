@@ -107,11 +107,13 @@ def run_np(nparties: int, op: str, n: int, data_seed: int, shim_seed: int = 1, t
 
 def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
         threads: int = 1, batch: int = -1, timeout: float = 600.0, outdir: str | None = None,
-        driver: str | None = None, nparties: int = 3, parser=None):
+        driver: str | None = None, nparties: int = 3, parser=None, exe: dict | None = None):
     """Run one op on 3 parties (or `nparties` with another driver). Returns
-    (list of per-party dicts, stdout of P0)."""
+    (list of per-party dicts, stdout of P0). `exe` maps a rank to another
+    program that plays that party with the driver's arguments and
+    environment (ORQ_SEED carries the key seed to it); parser None with exe
+    given skips reading the dumps."""
     driver = driver or DRIVER
-    parser = parser or parse_dump
     if not os.path.exists(driver):
         raise FileNotFoundError(driver + " (run `make -C oracle ref`)")
     tmp = outdir or tempfile.mkdtemp(prefix="orqref_")
@@ -125,8 +127,10 @@ def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
             "STARTMPC_HOST_RANK": str(rank),
             "STARTMPC_BASE_PORT": str(base),
             "ORQ_SHIM_SEED": str(shim_seed),
+            "ORQ_SEED": str(shim_seed),
         })
-        cmd = [driver, str(threads), "1", str(batch), op, str(n), str(data_seed), tmp, str(bits)]
+        prog = (exe or {}).get(rank, driver)
+        cmd = [prog, str(threads), "1", str(batch), op, str(n), str(data_seed), tmp, str(bits)]
         procs.append(subprocess.Popen(cmd, env=env, stdout=subprocess.PIPE,
                                       stderr=subprocess.PIPE, start_new_session=True))
     deadline = time.time() + timeout
@@ -143,6 +147,9 @@ def run(op: str, n: int, data_seed: int, shim_seed: int = 1, bits: int = 40,
     for i, p in enumerate(procs):
         if p.returncode != 0:
             raise RuntimeError(f"party {i} exited {p.returncode}: {outs[i][1].decode()[-2000:]}")
+    if exe and parser is None:
+        return tmp, outs[0][0].decode()
+    parser = parser or parse_dump
     dumps = [parser(os.path.join(tmp, f"p{r}.bin")) for r in range(nparties)]
     return dumps, outs[0][0].decode()
 

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liborq_cuda.so")
-UNITS = ["runtime.cu", "prims.cu", "perm.cu", "radix.cu", "scan.cu", "cmp.cu", "agg.cu", "tsort.cu", "qsort.cu", "conv.cu", "proto24.cu", "capi.cu"]
+UNITS = ["runtime.cu", "prims.cu", "perm.cu", "radix.cu", "scan.cu", "cmp.cu", "agg.cu", "tsort.cu", "qsort.cu", "conv.cu", "proto24.cu", "party.cu", "capi.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -45,6 +45,7 @@ void need_rt_any(orqcu_runtime* rt) { need(rt != nullptr, "null runtime"); }
 void need_rt(orqcu_runtime* rt) {
     need_rt_any(rt);
     need(rt->ctx.nparties == 3, "this runtime runs the 2PC/4PC protocol; use the orqcu_np_* entry points");
+    need(rt->ctx.party < 0, "this runtime plays one party; use the orqcu_party_* entry points");
 }
 void need_w(int w) { need(w == 1 || w == 2 || w == 4 || w == 8 || w == 16, "width must be 1,2,4,8,16"); }
 void need_sh(const void* const s[3], size_t n, const char* what) {
@@ -61,7 +62,7 @@ extern "C" {
 int orqcu_version(void) { return 1; }
 const char* orqcu_last_error(void) { return g_err.c_str(); }
 
-static void create_runtime(uint64_t seed, int device, int nparties, orqcu_runtime** out) {
+static void create_runtime(uint64_t seed, int device, int nparties, orqcu_runtime** out, int party = -1) {
     need(out != nullptr, "null output");
     need(nparties == 2 || nparties == 3 || nparties == 4, "parties must be 2, 3 or 4");
     int ndev = 0;
@@ -75,8 +76,15 @@ static void create_runtime(uint64_t seed, int device, int nparties, orqcu_runtim
     rt->ctx.owns_stream = true;
     ORQ_CUDA_CHECK(cudaMalloc(&rt->ctx.d_err, sizeof(int)));
     ORQ_CUDA_CHECK(cudaMemset(rt->ctx.d_err, 0, sizeof(int)));
-    if (nparties == 3) orqcu::init_ctx_keys(rt->ctx, seed);
-    else orqcu::init_ctx_keys_np(rt->ctx, seed, nparties);
+    if (party >= 0) {
+        // one party: its keys arrive through orqcu_party_set_key
+        rt->ctx.party = party;
+        for (int s = 0; s < orqcu::NSTREAMS; s++) std::memset(rt->ctx.rk[s].k, 0, sizeof(rt->ctx.rk[s].k));
+    } else if (nparties == 3) {
+        orqcu::init_ctx_keys(rt->ctx, seed);
+    } else {
+        orqcu::init_ctx_keys_np(rt->ctx, seed, nparties);
+    }
     orqcu::device_runtime_opened(device);
     try {
         orqcu::upload_aes_tables(device);
@@ -100,6 +108,129 @@ int orqcu_runtime_parties(orqcu_runtime* rt, int* nparties) {
         need_rt_any(rt);
         need(nparties != nullptr, "null output");
         *nparties = rt->ctx.nparties;
+    });
+}
+
+// ---- one party of 3PC --------------------------------------------------------
+static void need_party_rt(orqcu_runtime* rt) {
+    need_rt_any(rt);
+    need(rt->ctx.party >= 0, "this runtime plays every party; create one with orqcu_party_runtime_create");
+}
+static void need2(const void* const* s, size_t n, const char* what) {
+    if (n == 0) return;
+    need(s != nullptr && s[0] && s[1], what);
+}
+
+int orqcu_party_runtime_create(int party, int device, orqcu_runtime** out) {
+    return guard([&] {
+        need(party >= 0 && party <= 2, "party must be 0, 1 or 2");
+        create_runtime(0, device, 3, out, party);
+    });
+}
+
+int orqcu_party_set_key(orqcu_runtime* rt, int slot, const uint8_t key[32]) {
+    return guard([&] {
+        need_party_rt(rt);
+        need(key != nullptr, "null key");
+        const int p = rt->ctx.party;
+        int s;
+        switch (slot) {
+            case ORQCU_PKEY_LOCAL: s = orqcu::LOCAL0 + p; break;
+            case ORQCU_PKEY_NEXT: s = orqcu::PAIR0 + p; break;
+            case ORQCU_PKEY_PREV: s = orqcu::PAIR0 + (p + 2) % 3; break;
+            case ORQCU_PKEY_G01: s = orqcu::G01; break;
+            case ORQCU_PKEY_G02: s = orqcu::G02; break;
+            case ORQCU_PKEY_G12: s = orqcu::G12; break;
+            case ORQCU_PKEY_G012: s = orqcu::G012; break;
+            default: throw std::invalid_argument("unknown key slot");
+        }
+        orqcu::aes256_expand(key, rt->ctx.rk[s].k);
+        rt->ctx.nonce[s] = 0;
+    });
+}
+
+int orqcu_keygen(uint64_t seed, int party, int call, uint8_t key[32]) {
+    return guard([&] {
+        need(key != nullptr, "null key");
+        need(party >= 0 && call >= 0, "party and call must be non-negative");
+        orqcu::derive_key(seed, party, call, key);
+    });
+}
+
+int orqcu_party_secret_share(orqcu_runtime* rt, int arith, int width, size_t n, const void* data_dev,
+                             void* const s[3]) {
+    return guard([&] {
+        need_party_rt(rt);
+        need_w(width);
+        need_sh(s, n, "null share pointer");
+        need(n == 0 || data_dev != nullptr, "null data");
+        orqcu::op_party_share(rt->ctx, arith != 0, width, n, data_dev, m3(s));
+    });
+}
+
+static int party_mult(orqcu_runtime* rt, bool arith, int width, size_t n, const void* const x[2],
+                      const void* const y[2], void* z) {
+    return guard([&] {
+        need_party_rt(rt);
+        need_w(width);
+        need2(x, n, "null share pointer");
+        need2(y, n, "null share pointer");
+        need(n == 0 || z != nullptr, "null output");
+        orqcu::op_party_mult(rt->ctx, arith, width, n, x, y, z);
+    });
+}
+int orqcu_party_and_b(orqcu_runtime* rt, int width, size_t n, const void* const x[2], const void* const y[2],
+                      void* z) {
+    return party_mult(rt, false, width, n, x, y, z);
+}
+int orqcu_party_multiply_a(orqcu_runtime* rt, int width, size_t n, const void* const x[2],
+                           const void* const y[2], void* z) {
+    return party_mult(rt, true, width, n, x, y, z);
+}
+
+int orqcu_party_b2a_pre(orqcu_runtime* rt, int width, size_t n, const void* const x[2], void* s0, void* s1) {
+    return guard([&] {
+        need_party_rt(rt);
+        need_w(width);
+        need2(x, n, "null share pointer");
+        need(n == 0 || (s0 && s1), "null output");
+        orqcu::op_party_b2a_pre(rt->ctx, width, n, x, s0, s1);
+    });
+}
+
+int orqcu_party_b2a_post(orqcu_runtime* rt, int width, size_t n, const void* const s0[2],
+                         const void* const s1[2], void* z) {
+    return guard([&] {
+        need_party_rt(rt);
+        need_w(width);
+        need2(s0, n, "null share pointer");
+        need2(s1, n, "null share pointer");
+        need(n == 0 || z != nullptr, "null output");
+        orqcu::op_party_b2a_post(rt->ctx, width, n, s0, s1, z);
+    });
+}
+
+int orqcu_party_local(orqcu_runtime* rt, int op, int width, size_t n, const void* const x[2],
+                      const void* const y[2], void* const z[2]) {
+    return guard([&] {
+        need_party_rt(rt);
+        need_w(width);
+        need(op >= 0 && op <= 2, "op must be 0 (xor), 1 (add) or 2 (sub)");
+        need2(x, n, "null share pointer");
+        need2(y, n, "null share pointer");
+        need2(z, n, "null output");
+        orqcu::op_party_local(rt->ctx, op, width, n, x, y, z);
+    });
+}
+
+int orqcu_party_open(orqcu_runtime* rt, int arith, int width, size_t n, const void* const x[2],
+                     const void* third, void* out_dev) {
+    return guard([&] {
+        need_party_rt(rt);
+        need_w(width);
+        need2(x, n, "null share pointer");
+        need(n == 0 || (third && out_dev), "null pointer");
+        orqcu::op_party_open(rt->ctx, arith != 0, width, n, x, third, out_dev);
     });
 }
 
@@ -650,6 +781,7 @@ int orqcu_bitonic_sort_batch(orqcu_runtime* rt, int width, int count, const size
 int orqcu_runtime_reseed(orqcu_runtime* rt, uint64_t seed) {
     return guard([&] {
         need_rt_any(rt);
+        need(rt->ctx.party < 0, "a one-party runtime takes its keys from orqcu_party_set_key");
         for (auto& sp : rt->ctx.perm_queue) rt->ctx.free_perm(sp);
         rt->ctx.perm_queue.clear();
         rt->ctx.perm_queue_n = 0;

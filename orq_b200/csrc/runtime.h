@@ -117,6 +117,7 @@ struct FyRes {
 struct Ctx {
     int device = 0;
     int nparties = 3;  // 3: replicated 3PC; 2: Beaver 2PC; 4: Fantastic-4PC
+    int party = -1;    // >= 0: plays only this party of 3PC (party.cu); -1: all parties
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
@@ -211,6 +212,13 @@ void op_public_share(Ctx& c, int w, size_t n, const void* data_dev, Sh3 s);
 void op_open(Ctx& c, bool arith, int w, size_t n, CSh3 s, void* out_dev);
 void op_mult(Ctx& c, bool arith, int w, size_t n, CSh3 x, CSh3 y, Sh3 z);
 void op_local(Ctx& c, int op, int w, size_t n, CSh3 x, CSh3 y, Sh3 z);  // 0 xor,1 add,2 sub
+// one party of 3PC (party.cu): local steps before the caller's exchange
+void op_party_mult(Ctx& c, bool arith, int w, size_t n, const void* const x[2], const void* const y[2], void* z);
+void op_party_b2a_pre(Ctx& c, int w, size_t n, const void* const x[2], void* s0, void* s1);
+void op_party_b2a_post(Ctx& c, int w, size_t n, const void* const s0[2], const void* const s1[2], void* z);
+void op_party_local(Ctx& c, int op, int w, size_t n, const void* const x[2], const void* const y[2], void* const z[2]);
+void op_party_share(Ctx& c, bool arith, int w, size_t n, const void* data_dev, Sh3 s);
+void op_party_open(Ctx& c, bool arith, int w, size_t n, const void* const x[2], const void* third, void* out_dev);
 void op_not(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
 void op_b2a_bit(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
 void op_a2b(Ctx& c, int w, size_t n, CSh3 x, Sh3 y);
