@@ -11,17 +11,19 @@
 // nonces depend on how many draws the previous one used.
 //
 // GPU design:
-//  * fy_gen  (all SMs but three): AES keystream of a window of buffers, drop
-//    draws with v >= n (they can never be accepted), compact the survivors of
-//    each 32768-draw tile in order, record a tile bitmap and the tile minimum.
+//  * fy_gen  (all SMs but three): AES keystream of a window of buffers; per
+//    32768-draw tile, nested lists (in draw order) of the draws below n/4^L,
+//    and the tile's last draw.
 //  * fy_scan (one 1024-thread CTA per group): replays the sequential
-//    acceptance exactly over the survivors, 8192 at a time; a survivor is
-//    certainly accepted if v + (its index in the step) <= n-1-i, certainly
-//    rejected if v > n-1-i, and the rare ones in between are decided in order
-//    by one thread. Tiles whose minimum exceeds n-1-i are skipped.
-//    Window w+1 is generated while window w is scanned.
+//    acceptance exactly over the sparsest level that holds every candidate; an
+//    entry is certainly accepted if v + (its index in the step) <= n-1-i,
+//    certainly rejected if v > n-1-i, and the few in between are decided in
+//    order by one warp. Windows are generated up to five ahead of the scans.
+//  * fy_small (M <= 2^17, a predictable number of buffers per permutation):
+//    every (permutation, group) in its own CTA at once from predicted start
+//    buffers, re-run from the first wrong prediction until all are verified.
 //  * fy_finalize: turns the accepted offsets into the final permutation in
-//    parallel (see k_fy_final) and writes its inverse.
+//    parallel and writes its inverse.
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -183,6 +185,101 @@ __global__ void __launch_bounds__(kGenThreads, 1) k_fy_gen(FyGenArgs a) {
         if (threadIdx.x < a.lay.nl)
             a.cnt[slot * kMaxLevels + threadIdx.x] = min(sbase[threadIdx.x], a.lay.cap[threadIdx.x]);
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Small permutations (M = 2^bit_width(n) <= 2^17). A permutation then takes
+// d ≈ M·H_n draws (std ≈ 1.3·M) and 1 + floor(d / 2^20) getNext buffers, a
+// count that is predictable: permutation m of a group is assumed to start at
+// buffer m·b̂ of the chain, and every (permutation, group) pair runs at once,
+// one CTA each, with no host round trip. Warps 1.. generate the draws chunk
+// by chunk into shared memory (two chunk buffers), warp 0 replays the
+// acceptance 32 draws at a time (lane j is certainly accepted if v + j <= T,
+// rejected if v > T, and the rest are decided in order) and reports the
+// buffers the permutation used. The host then checks the assumed starts
+// against the used counts; from the first permutation of a group whose start
+// was wrong, the rest are run again from the corrected start (each pass
+// fixes at least that one). A permutation needing more than `max_chunks`
+// chunks sets `overflow`, and the general chain redoes everything.
+constexpr uint32_t kSmallChunk = 8192;  // draws per chunk
+constexpr int kSmallThreads = 512;
+constexpr uint32_t kSmallMaxM = 1u << 17;
+constexpr uint32_t kChunksPerBuffer = (1u << 20) / kSmallChunk;  // 128
+constexpr size_t kSmallSmem = (size_t)kAesSmemBytes + 2 * kSmallChunk * 4;
+
+struct FySmallArgs {
+    StreamArg st[3];  // chain start of each group (buffer 0)
+    uint32_t n, mask, count, max_chunks;
+    uint32_t m0[3];        // per group, the first permutation to run
+    const uint32_t* start;  // [3][count] assumed start buffer
+    uint32_t* used;         // [3][count] buffers used
+    uint32_t* acc;          // [count][3][n] accepted offsets v_i
+    uint32_t* overflow;     // set when a permutation needs more than max_chunks
+};
+
+__global__ void __launch_bounds__(kSmallThreads, 1) k_fy_small(FySmallArgs a) {
+    const uint32_t m = blockIdx.x / 3, g = blockIdx.x % 3;
+    if (m < a.m0[g]) return;  // already verified (uniform per CTA)
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t s_dlast;
+    aes_stage_tables(sm);
+    const AesSmem S(sm);
+    uint32_t* buf = sm + kAesSmemBytes / 4;  // [2][kSmallChunk]
+    StreamArg st = a.st[g];
+    st.nonce += 4ull * a.start[g * a.count + m];  // 4 nonces per buffer
+    const uint32_t n = a.n;
+    uint32_t* acc = a.acc + ((size_t)m * 3 + g) * n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t i = 0;  // accepted so far (warp 0)
+    // iteration k produces chunk k into buf[k & 1] and consumes chunk k - 1
+    // from buf[(k - 1) & 1]; the barrier that opens an iteration publishes
+    // chunk k - 1, frees the buffer chunk k - 2 held, and stops every thread
+    // at once when the permutation is complete
+    for (uint32_t k = 0; k <= a.max_chunks; k++) {
+        if (__syncthreads_or(warp == 0 && i >= n)) break;
+        if (warp > 0) {
+            if (k < a.max_chunks) {
+                uint4* dst = reinterpret_cast<uint4*>(buf + (k & 1) * kSmallChunk);
+                const unsigned long long blk0 = (unsigned long long)k * (kSmallChunk / 4);
+                for (uint32_t b = threadIdx.x - 32; b < kSmallChunk / 4; b += kSmallThreads - 32) {
+                    const uint4 ks = keystream_block(S, st, blk0 + b);
+                    dst[b] = make_uint4(ks.x & a.mask, ks.y & a.mask, ks.z & a.mask, ks.w & a.mask);
+                }
+            }
+        } else if (k > 0) {
+            const uint32_t* src = buf + ((k - 1) & 1) * kSmallChunk;
+            const uint32_t d0 = (k - 1) * kSmallChunk;  // draw index of the chunk's first draw
+            for (uint32_t base = 0; base < kSmallChunk && i < n; base += 32) {
+                const uint32_t v = src[base + lane];  // v <= mask < 2^17: v + lane cannot wrap
+                const uint32_t T = n - 1 - i;
+                const bool cert = v + (uint32_t)lane <= T;
+                uint32_t ok = __ballot_sync(0xffffffffu, cert);
+                uint32_t pend = __ballot_sync(0xffffffffu, !cert && v <= T);
+                while (pend) {
+                    const int j = __ffs(pend) - 1;
+                    pend &= pend - 1;
+                    const uint32_t vj = __shfl_sync(0xffffffffu, v, j);
+                    if (vj + (uint32_t)__popc(ok & ((1u << j) - 1u)) <= T) ok |= 1u << j;
+                }
+                if ((ok >> lane) & 1u) {
+                    const uint32_t r = i + (uint32_t)__popc(ok & lt);
+                    if (r < n) {
+                        acc[r] = v;
+                        if (r == n - 1) s_dlast = d0 + base + (uint32_t)lane;
+                    }
+                }
+                i += (uint32_t)__popc(ok);
+            }
+        }
+    }
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        // gen_perm refills each time its index reaches the end of a buffer,
+        // the last accepted draw included: 1 + floor(draws / 2^20) buffers
+        if (i >= n) a.used[g * a.count + m] = 1u + (s_dlast + 1u) / (1u << 20);
+        else atomicOr(a.overflow, 1u);
     }
 }
 
@@ -912,21 +1009,11 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     // sparse tail (generation-bound). The three groups are scanned on three
     // streams: their dense phases fall in different windows, and a shared
     // launch per window would cost the slowest group every time.
+    // (allocated below, after the small-permutation path, which needs none)
     constexpr int kRing = 6;
-    std::vector<std::unique_ptr<Scratch>> ring_ev, ring_last, ring_cnt;
-    for (int k = 0; k < kRing; k++) {
-        ring_ev.emplace_back(new Scratch(c, ents_b + 256));  // slack for 16-byte rounded prefetches
-        ring_last.emplace_back(new Scratch(c, (size_t)3 * tiles * 4));
-        ring_cnt.emplace_back(new Scratch(c, cnt_b));
-    }
-    Scratch state(c, 3 * sizeof(FyState));
     Scratch acc(c, (size_t)3 * count * n * 4);
-    Scratch refills(c, (size_t)3 * count * 4);
-    ORQ_CUDA_CHECK(cudaMemsetAsync(state.p, 0, 3 * sizeof(FyState), c.stream));
     const bool want_stats = std::getenv("ORQ_FY_STATS") != nullptr;
     const auto t_start = std::chrono::steady_clock::now();
-    Scratch stats(c, 3 * kFyStats * 8);
-    if (want_stats) ORQ_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 3 * kFyStats * 8, c.stream));
 
     // generator and scanner run on private non-blocking streams so they overlap
     // whatever the caller's stream is (the legacy default stream included)
@@ -1014,6 +1101,102 @@ void gen_sharded_perms(Ctx& c, size_t n, size_t count, std::vector<ShardedPerm>&
     ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
     for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], ev_start, 0));
     ORQ_CUDA_CHECK(cudaStreamWaitEvent(fs, ev_start, 0));
+
+    if ((1ull << bitsw) <= kSmallMaxM) {
+        // every permutation of every group at once from predicted start
+        // buffers, corrected pass by pass (k_fy_small)
+        const uint32_t bhat = 1u + (uint32_t)(M * H / (double)(1u << 20));
+        std::vector<uint32_t> hstart(3 * count), hused(3 * count);
+        for (int g = 0; g < 3; g++)
+            for (size_t m = 0; m < count; m++) hstart[g * count + m] = (uint32_t)m * bhat;
+        Scratch d_start(c, hstart.size() * 4), d_used(c, hused.size() * 4), ovf(c, 4);
+        // the pool hands out memory in the runtime stream's order
+        ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
+        ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
+        ORQ_CUDA_CHECK(cudaMemsetAsync(ovf.p, 0, 4, gs));
+        ORQ_CUDA_CHECK(cudaFuncSetAttribute(k_fy_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem));
+        FySmallArgs sa;
+        for (int g = 0; g < 3; g++) {
+            sa.st[g] = c.stream_arg(G01 + g);
+            sa.m0[g] = 0;
+        }
+        sa.n = (uint32_t)n;
+        sa.mask = mask;
+        sa.count = (uint32_t)count;
+        sa.max_chunks = (bhat + 6) * kChunksPerBuffer;
+        sa.start = d_start.as<uint32_t>();
+        sa.used = d_used.as<uint32_t>();
+        sa.acc = acc.as<uint32_t>();
+        sa.overflow = ovf.as<uint32_t>();
+        bool ok = false;
+        for (int pass = 0; pass < 64; pass++) {
+            ORQ_CUDA_CHECK(cudaMemcpyAsync(d_start.p, hstart.data(), hstart.size() * 4, cudaMemcpyHostToDevice, gs));
+            {
+                ProfScope ps(c, "fy_small", 0.0, 0.0, gs);
+                k_fy_small<<<(unsigned)(3 * count), kSmallThreads, kSmallSmem, gs>>>(sa);
+            }
+            ORQ_CUDA_CHECK(cudaGetLastError());
+            c.kernels_launched++;
+            uint32_t overflow = 0;
+            ORQ_CUDA_CHECK(cudaMemcpyAsync(hused.data(), d_used.p, hused.size() * 4, cudaMemcpyDeviceToHost, gs));
+            ORQ_CUDA_CHECK(cudaMemcpyAsync(&overflow, ovf.p, 4, cudaMemcpyDeviceToHost, gs));
+            ORQ_CUDA_CHECK(cudaStreamSynchronize(gs));
+            if (overflow) break;
+            // permutations before m0[g] are verified, and so is m0[g]'s start;
+            // the first one whose assumed start differs from the true one is
+            // where the next pass begins
+            bool again = false;
+            for (int g = 0; g < 3; g++) {
+                uint32_t* st = hstart.data() + g * count;
+                const uint32_t* us = hused.data() + g * count;
+                size_t m = sa.m0[g];
+                if (m >= count) continue;
+                uint32_t expect = st[m];
+                for (; m < count; m++) {
+                    if (st[m] != expect) break;
+                    expect = st[m] + us[m];
+                }
+                sa.m0[g] = (uint32_t)m;
+                if (m < count) {
+                    again = true;
+                    for (size_t k = m; k < count; k++) st[k] = expect + (uint32_t)(k - m) * bhat;
+                }
+            }
+            if (!again) {
+                ok = true;
+                break;
+            }
+        }
+        if (ok) {
+            for (int g = 0; g < 3; g++)
+                c.nonce[G01 + g] += 4ull * (hstart[g * count + count - 1] + hused[g * count + count - 1]);
+            for (; fin_next < count; fin_next += fin_b) launch_fin(fin_next, std::min(count, fin_next + fin_b));
+            ORQ_CUDA_CHECK(cudaEventRecord(R.fin_done, fs));
+            ORQ_CUDA_CHECK(cudaStreamWaitEvent(c.stream, R.fin_done, 0));
+            c.check_device_error();
+            return;
+        }
+        // a permutation ran past max_chunks (or the passes did not settle):
+        // the general chain below redoes all of them (no nonce was consumed)
+    }
+
+    std::vector<std::unique_ptr<Scratch>> ring_ev, ring_last, ring_cnt;
+    for (int k = 0; k < kRing; k++) {
+        ring_ev.emplace_back(new Scratch(c, ents_b + 256));  // slack for 16-byte rounded prefetches
+        ring_last.emplace_back(new Scratch(c, (size_t)3 * tiles * 4));
+        ring_cnt.emplace_back(new Scratch(c, cnt_b));
+    }
+    Scratch state(c, 3 * sizeof(FyState));
+    Scratch refills(c, (size_t)3 * count * 4);
+    ORQ_CUDA_CHECK(cudaMemsetAsync(state.p, 0, 3 * sizeof(FyState), c.stream));
+    Scratch stats(c, 3 * kFyStats * 8);
+    if (want_stats) ORQ_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 3 * kFyStats * 8, c.stream));
+    // the side streams start after these allocations and memsets, and are
+    // drained before the buffers above go back to the pool (declared after them)
+    ORQ_CUDA_CHECK(cudaEventRecord(ev_start, c.stream));
+    ORQ_CUDA_CHECK(cudaStreamWaitEvent(gs, ev_start, 0));
+    for (int g = 0; g < 3; g++) ORQ_CUDA_CHECK(cudaStreamWaitEvent(ss[g], ev_start, 0));
+    DrainSideStreams drain_ring{R};
 
     prep_aes_kernel(k_fy_gen);
     ORQ_CUDA_CHECK(cudaFuncSetAttribute(k_fy_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem));
