@@ -651,13 +651,15 @@ def run_serve(args, rank, world, local_rank):
     """Config 5: Poisson arrivals of mixed requests (60% sort, 30% group-by
     over 2^10 groups, 10% PK-FK join with a 4x foreign-key side), sizes
     log-uniform over 2^12..2^22 rows, int64 keys. Capacity is measured first
-    on the plain per-request path (one slot, all requests queued at once);
-    the trace then arrives at 80% of that capacity and is served (a) by the
-    continuous-batching server and (b) by the plain path. Every result is
-    checked against its plaintext answer."""
+    on the plain per-request path (one slot, all requests queued at once) and
+    on the continuous-batching server (the same requests, all at once): the
+    saturated rows/s of both. The trace then arrives at 80% of the plain
+    capacity and is served (a) by the continuous-batching server and (b) by
+    the plain path (latency at load). Every result is checked against its
+    plaintext answer after the timed runs."""
     import torch
 
-    from orq_b200.serve import Server, make_trace
+    from orq_b200.serve import Server, check_result, make_trace
 
     torch.cuda.set_device(local_rank)
     # warm-up: a small trace through both paths (tables, pools, kernels)
@@ -674,25 +676,31 @@ def run_serve(args, rank, world, local_rank):
     # is the run-to-run noise of the comparison
     for r in range(max(1, args.serve_repeats)):
         seed = 5 + rank + 1000 * r
-        calib = make_trace(args.serve_requests, 0.0, seed=seed, max_log=args.serve_max_log)
-        srv = Server(slots=1, device=local_rank, protocol=args.sort_protocol)
-        cap_stats = srv.run(calib)
-        srv.close()
+        sat = {}
+        for name, slots in (("plain", 1), ("serving", args.slots)):
+            calib = make_trace(args.serve_requests, 0.0, seed=seed, max_log=args.serve_max_log)
+            srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol,
+                         share_sms=bool(args.share_sms) and slots > 1)
+            st = srv.run(calib)
+            srv.close()
+            st["ok"] = all(check_result(r_, r_.result) for r_ in calib)
+            sat[name] = st
+        cap_stats = sat["plain"]
         capacity = cap_stats["requests"] / cap_stats["makespan_s"]
         rate = 0.8 * capacity
         if r == 0:
             out["capacity_req_per_s"], out["rate_req_per_s"] = capacity, rate
-        rep = {"capacity_req_per_s": capacity}
+        rep = {"capacity_req_per_s": capacity, "saturated": sat}
         for name, slots in (("serving", args.slots), ("plain", 1)):
             trace = make_trace(args.serve_requests, rate, seed=seed, max_log=args.serve_max_log)
             srv = Server(slots=slots, device=local_rank, protocol=args.sort_protocol,
                          share_sms=bool(args.share_sms))
             clocks = ClockSampler(local_rank)
             clocks.start()
-            st = srv.run(trace, check=True)
+            st = srv.run(trace)
             st["clocks"] = clocks.stop()
             srv.close()
-            st["ok"] = all(r_.ok for r_ in trace)
+            st["ok"] = all(check_result(r_, r_.result) for r_ in trace)
             rep[name] = st
             if r == 0:
                 out[name] = st
@@ -1024,6 +1032,7 @@ def main():
                 for part in ("serving", "plain"):
                     for k in ("makespan_s", "p50_ms", "p99_ms"):
                         rp[part][k] = max_over_ranks(rp[part][k])
+                    rp["saturated"][part]["makespan_s"] = max_over_ranks(rp["saturated"][part]["makespan_s"])
             for part in ("serving", "plain"):
                 res[part]["rows_per_s"] = res[part]["rows"] / res[part]["makespan_s"]
         if dist is not None:
@@ -1074,7 +1083,20 @@ def main():
                                     "plain_p50_ms": rp["plain"]["p50_ms"], "plain_p99_ms": rp["plain"]["p99_ms"]}
                                    for a, b, c, rp in zip(rows_s, rows_p, ratio, reps)]
                 line["serving_over_plain"] = {"mean": statistics.mean(ratio), "min": min(ratio), "max": max(ratio)}
-                line["correct"] = line["correct"] and all(rp["serving"]["ok"] and rp["plain"]["ok"] for rp in reps)
+                # throughput: every request queued at once, both ways
+                sat_s = [world * rp["saturated"]["serving"]["rows"] / rp["saturated"]["serving"]["makespan_s"]
+                         for rp in reps]
+                sat_p = [world * rp["saturated"]["plain"]["rows"] / rp["saturated"]["plain"]["makespan_s"]
+                         for rp in reps]
+                sat_r = [a / b for a, b in zip(sat_s, sat_p)]
+                line["saturated"] = {"serving_rows_per_s": sat_s, "plain_rows_per_s": sat_p,
+                                     "serving_over_plain": {"mean": statistics.mean(sat_r), "min": min(sat_r),
+                                                            "max": max(sat_r)},
+                                     "note": "the same requests all queued at time 0: served by the slots "
+                                             "vs one after another on the plain path"}
+                line["correct"] = line["correct"] and all(
+                    rp["serving"]["ok"] and rp["plain"]["ok"] and rp["saturated"]["serving"]["ok"]
+                    and rp["saturated"]["plain"]["ok"] for rp in reps)
         print(json.dumps(line))
         return
 

@@ -251,26 +251,38 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_fy_small(FySmallArgs a) {
         } else if (k > 0) {
             const uint32_t* src = buf + ((k - 1) & 1) * kSmallChunk;
             const uint32_t d0 = (k - 1) * kSmallChunk;  // draw index of the chunk's first draw
-            for (uint32_t base = 0; base < kSmallChunk && i < n; base += 32) {
-                const uint32_t v = src[base + lane];  // v <= mask < 2^17: v + lane cannot wrap
-                const uint32_t T = n - 1 - i;
-                const bool cert = v + (uint32_t)lane <= T;
-                uint32_t ok = __ballot_sync(0xffffffffu, cert);
-                uint32_t pend = __ballot_sync(0xffffffffu, !cert && v <= T);
-                while (pend) {
-                    const int j = __ffs(pend) - 1;
-                    pend &= pend - 1;
-                    const uint32_t vj = __shfl_sync(0xffffffffu, v, j);
-                    if (vj + (uint32_t)__popc(ok & ((1u << j) - 1u)) <= T) ok |= 1u << j;
-                }
-                if ((ok >> lane) & 1u) {
-                    const uint32_t r = i + (uint32_t)__popc(ok & lt);
-                    if (r < n) {
-                        acc[r] = v;
-                        if (r == n - 1) s_dlast = d0 + base + (uint32_t)lane;
+            // 128 draws at a time (lane l holds draws 32u + l): T only
+            // decreases, so a group with no draw <= T now has no acceptance
+            // and is skipped whole (most groups, late in a permutation)
+            for (uint32_t base = 0; base < kSmallChunk && i < n; base += 128) {
+                uint32_t v4[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) v4[u] = src[base + 32u * u + lane];
+                const uint32_t mn = min(min(v4[0], v4[1]), min(v4[2], v4[3]));
+                if (!__any_sync(0xffffffffu, mn <= n - 1 - i)) continue;
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (i >= n) break;
+                    const uint32_t v = v4[u];  // v <= mask < 2^17: v + lane cannot wrap
+                    const uint32_t T = n - 1 - i;
+                    const bool cert = v + (uint32_t)lane <= T;
+                    uint32_t ok = __ballot_sync(0xffffffffu, cert);
+                    uint32_t pend = __ballot_sync(0xffffffffu, !cert && v <= T);
+                    while (pend) {
+                        const int j = __ffs(pend) - 1;
+                        pend &= pend - 1;
+                        const uint32_t vj = __shfl_sync(0xffffffffu, v, j);
+                        if (vj + (uint32_t)__popc(ok & ((1u << j) - 1u)) <= T) ok |= 1u << j;
                     }
+                    if ((ok >> lane) & 1u) {
+                        const uint32_t r = i + (uint32_t)__popc(ok & lt);
+                        if (r < n) {
+                            acc[r] = v;
+                            if (r == n - 1) s_dlast = d0 + base + 32u * u + (uint32_t)lane;
+                        }
+                    }
+                    i += (uint32_t)__popc(ok);
                 }
-                i += (uint32_t)__popc(ok);
             }
         }
     }

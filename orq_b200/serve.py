@@ -3,11 +3,13 @@ aggregate and PK-FK join requests.
 
 A server owns S slots. Each slot is a worker thread with its own runtime
 (keys, nonces, device memory pool) on its own CUDA stream. Requests wait in
-one FIFO queue; the head request is admitted as soon as a slot is free and
-its estimated device memory fits in the part of the HBM budget that running
+one queue; the oldest request is admitted as soon as a slot is free and its
+estimated device memory fits in the part of the HBM budget that running
 requests have not reserved, so requests that arrive while others run start
 as soon as a slot and memory free up, and their kernels overlap on the
-device. A slot re-keys its runtime with the request's own seed before
+device. One exception: at most one large request (LARGE_ROWS rows or more,
+which fills the GPU by itself) runs at a time, and smaller requests behind a
+waiting large one (within LOOKAHEAD) take the free slots meanwhile. A slot re-keys its runtime with the request's own seed before
 running it (orqcu_runtime_reseed): a request's shares and opened result are
 the same whether it runs alone or in a mix. A slot keeps its device memory
 pool warm between requests (re-allocating and re-mapping gigabytes per
@@ -153,6 +155,30 @@ class _Slot:
         if sm_limit:
             self.rt.set_sm_limit(sm_limit)
         self.busy = False
+        self.large = False  # running a request of at least LARGE_ROWS rows
+
+
+# Requests of at least this many rows fill the GPU on their own (their
+# Fisher-Yates chains and sorts use every SM): two of them side by side only
+# contend, while a small request (latency-bound, a few SMs) overlaps a large
+# one well. The dispatcher therefore keeps at most one large request in
+# flight and lets small ones behind it in the queue take the other slots.
+LARGE_ROWS = 1 << 19
+LOOKAHEAD = 16
+
+
+def pick_next(queue, slots):
+    """Index in `queue` of the request to admit next, or None: the oldest one,
+    unless a large request is running and it is large too, in which case the
+    oldest small one within LOOKAHEAD."""
+    large_running = any(s.busy and s.large for s in slots)
+    for k, cand in enumerate(queue):
+        if k >= LOOKAHEAD:
+            break
+        if large_running and cand.rows >= LARGE_ROWS:
+            continue
+        return k
+    return None
 
 
 class Server:
@@ -211,6 +237,7 @@ class Server:
                     state["error"] = e
                 with lock:
                     slot.busy = False
+                    slot.large = False
                     state["reserved"] -= req.est_bytes
                     state["done"] += 1
                     lock.notify_all()
@@ -225,15 +252,23 @@ class Server:
                 while i < len(reqs) and reqs[i].arrival <= now:
                     queue.append(reqs[i])
                     i += 1
-                # admit from the head while a slot and memory are free
+                # admit while a slot and memory are free: the oldest request
+                # that fits, except that a large one waits while another large
+                # one runs (smaller ones within LOOKAHEAD go ahead of it)
                 while queue:
-                    head = queue[0]
                     free_slot = next((s for s in self.slots if not s.busy), None)
-                    fits = state["reserved"] + head.est_bytes <= self.budget or state["reserved"] == 0
-                    if free_slot is None or not fits:
+                    if free_slot is None:
                         break
-                    queue.popleft()
+                    pick = pick_next(queue, self.slots)
+                    if pick is None:
+                        break
+                    head = queue[pick]
+                    fits = state["reserved"] + head.est_bytes <= self.budget or state["reserved"] == 0
+                    if not fits:
+                        break
+                    del queue[pick]
                     free_slot.busy = True
+                    free_slot.large = head.rows >= LARGE_ROWS
                     state["reserved"] += head.est_bytes
                     head.t_admit = time.perf_counter() - t0
                     head.slot = free_slot.idx

@@ -366,3 +366,20 @@ def test_np_prims_large_match_reference_digests(oracle_lib, digests, tag):
     out = replay_prims_np(OracleNPBackend(m["shim_seed"], m["parties"]), m["n"], m["data_seed"])
     for name, arr in out.items():
         assert [sha(a) for a in arr] == d["arrays"][name], name
+
+
+def test_serving_admission_keeps_one_large_request_in_flight():
+    """The dispatcher's pick: FIFO, except that a large request waits while
+    another large one runs and smaller ones within the lookahead go first."""
+    from types import SimpleNamespace as NS
+
+    from orq_b200.serve import LARGE_ROWS, LOOKAHEAD, pick_next
+
+    big, small = NS(rows=LARGE_ROWS), NS(rows=LARGE_ROWS // 2)
+    idle, runs_big, runs_small = NS(busy=False, large=False), NS(busy=True, large=True), NS(busy=True, large=False)
+    assert pick_next([big, small], [idle, idle]) == 0
+    assert pick_next([big, small], [runs_small, idle]) == 0
+    assert pick_next([big, big, small], [runs_big, idle]) == 2
+    assert pick_next([big, big], [runs_big, idle]) is None
+    assert pick_next([big] * LOOKAHEAD + [small], [runs_big, idle]) is None
+    assert pick_next([], [idle]) is None
