@@ -331,9 +331,13 @@ int orqcu_bitonic_sort_batch(orqcu_runtime* rt, int width, int count, const size
  * not depend on what ran before it. No reference counterpart (one
  * orq_init per process there). */
 int orqcu_runtime_reseed(orqcu_runtime* rt, uint64_t seed);
-/* Return the runtime's cached (unused) device memory to the device, ordered
- * on the runtime's stream (no device-wide synchronisation); writes the bytes
- * that were cached to *cached_before when non-NULL. */
+/* Return the runtime's cached (unused) device memory to the device's memory
+ * pool, ordered on the runtime's stream (no device-wide synchronisation),
+ * where other runtimes' allocations reuse it without mapping it again; writes
+ * the bytes that were cached to *cached_before when non-NULL. The pool gives
+ * its unused memory back to the system when the last runtime on the device
+ * is destroyed. A runtime that misses its cache while holding 8 GiB or more
+ * of other sizes trims itself the same way before allocating. */
 int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before);
 
 /* Size this runtime's grids for `sms` SMs (0 = all; at least 4) instead of the

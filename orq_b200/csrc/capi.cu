@@ -85,6 +85,7 @@ static void create_runtime(uint64_t seed, int device, int nparties, orqcu_runtim
     } else {
         orqcu::init_ctx_keys_np(rt->ctx, seed, nparties);
     }
+    orqcu::keep_pool_memory(device);
     orqcu::device_runtime_opened(device);
     try {
         orqcu::upload_aes_tables(device);

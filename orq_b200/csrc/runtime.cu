@@ -149,7 +149,10 @@ void device_runtime_opened(int device) {
 void device_runtime_closed(int device) {
     if (device < 0 || device >= kMaxDevices) return;
     std::lock_guard<std::mutex> lk(g_dev_mu);
-    if (g_dev_live[device] > 0 && --g_dev_live[device] == 0) g_dev_epoch[device]++;
+    if (g_dev_live[device] > 0 && --g_dev_live[device] == 0) {
+        g_dev_epoch[device]++;
+        release_pool_memory(device);  // the last runtime on the device is gone
+    }
 }
 
 unsigned long long device_epoch(int device) {
@@ -199,16 +202,27 @@ static size_t bucket(size_t bytes) {
 
 void* Pool::get(size_t bytes, cudaStream_t stream) {
     const size_t b = bucket(bytes);
+    bool evict = false;
     {
         std::lock_guard<std::mutex> lk(mu_);
-        auto it = free_.find(b);
-        if (it != free_.end()) {
+        // the smallest cached block of at least b bytes, if it wastes at most half of b
+        auto it = free_.lower_bound(b);
+        if (it != free_.end() && it->first <= b + b / 2) {
             void* p = it->second;
+            live_[p] = it->first;
             free_.erase(it);
-            live_[p] = b;
             return p;
         }
+        size_t cached = 0;
+        for (auto& kv : free_) cached += kv.first;
+        evict = cached >= kEvictBytes;
     }
+    // a miss with much memory cached in other sizes (a runtime that serves
+    // requests of changing sizes): hand the cache back to the device's pool
+    // first, stream-ordered, so the new block reuses that memory instead of
+    // growing the footprint (the device pool keeps it mapped, see
+    // keep_pool_memory)
+    if (evict) trim(stream);
     void* p = nullptr;
     cudaError_t e = cudaMallocAsync(&p, b, stream);
     if (e != cudaSuccess) {
@@ -228,6 +242,27 @@ void Pool::put(void* p) {
     if (it == live_.end()) return;
     free_.emplace(it->second, p);
     live_.erase(it);
+}
+
+// The device's default memory pool keeps memory freed into it mapped (by
+// default it returns it to the system at the next synchronisation, and the
+// next allocation maps it again at a cost of milliseconds per gigabyte).
+// Per process; set once per device.
+void keep_pool_memory(int device) {
+    static std::mutex mu;
+    static bool done[kMaxDevices] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= kMaxDevices || done[device]) return;
+    cudaMemPool_t pool;
+    ORQ_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = ~0ull;
+    ORQ_CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    done[device] = true;
+}
+
+void release_pool_memory(int device) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
 }
 
 void Pool::trim(cudaStream_t stream) {

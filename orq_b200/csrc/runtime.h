@@ -55,11 +55,19 @@ class Pool {
     size_t cached_bytes();
     ~Pool();
 
+    // on a miss with at least this much cached in other sizes, the cache is
+    // handed back to the device's pool before allocating
+    static constexpr size_t kEvictBytes = size_t(8) << 30;
+
    private:
     std::mutex mu_;
     std::multimap<size_t, void*> free_;
     std::map<void*, size_t> live_;
 };
+// the device's default memory pool keeps freed memory mapped (once per device)
+void keep_pool_memory(int device);
+// returns the device pool's unused memory to the system
+void release_pool_memory(int device);
 
 // A sharded permutation: one local permutation per 2-party group
 // ({0,1},{0,2},{1,2}), each with its inverse, all device-resident int32.
