@@ -391,6 +391,12 @@ __device__ __forceinline__ uint32_t tile_in(const uint32_t* P, uint32_t lo, uint
     return lo;
 }
 
+// quads (128 entries) of warp w's range [1024w, 1024w + 1024) below cs
+__device__ __forceinline__ int wquads(int w, uint32_t cs) {
+    const uint32_t b = (uint32_t)w * 1024u;
+    return b >= cs ? 0 : (int)min((uint32_t)kQuads, (cs - b + 127u) / 128u);
+}
+
 __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
     extern __shared__ __align__(16) uint32_t sv[];  // step entries, sv[q]
     __shared__ uint32_t red[33];
@@ -484,8 +490,11 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             uint32_t tend = P[t + 1];
             size_t boff = (size_t)t * a.lay.slot + off - (size_t)P[t];  // wraps; boff + e does not
             const uint32_t sv_sh = (uint32_t)__cvta_generic_to_shared(sv);
+            // entries past cs are never read as entries (their class is
+            // forced to rejected), so they are not staged
 #pragma unroll
             for (int u = 0; u < kPerThread; u++) {
+                if ((uint32_t)warp * 1024u + 32u * u >= cs) break;  // warp-uniform
                 const uint32_t q = qw + 32u * u;
                 if (q < cs) {
                     const uint32_t e = e0 + q;
@@ -497,8 +506,6 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
                         boff = (size_t)t * a.lay.slot + off - (size_t)P[t];
                     }
                     cp_async4(sv_sh + 4u * q, EV + (boff + e));
-                } else {
-                    sv[q] = 0xffffffffu;
                 }
             }
             cp_async_wait_all();
@@ -515,8 +522,12 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         uint32_t tot_c, tot_u;
         for (;;) {
             uint32_t x = 0;  // the warp's (certain | uncertain << 16) so far
+            // the warp's quads holding entries (warp-uniform; the passes below
+            // skip the rest, whose classes would all be zero)
+            const int nq = wquads(warp, cs);
 #pragma unroll
             for (int u = 0; u < kQuads; u++) {
+                if (u >= nq) break;
                 const uint32_t q = q0 + 128u * u;
                 const uint4 v4 = *reinterpret_cast<const uint4*>(sv + q);
                 const uint32_t code = fy_class(q, v4.x, cs, T) | (fy_class(q + 1, v4.y, cs, T) << 1) |
@@ -554,9 +565,11 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
         const unsigned long long t_li0 = clock64();
         // ---- list the uncertain entries in order, with the certain accepts
         // before each
+        const int nq = wquads(warp, cs);
         if (tot_u) {
 #pragma unroll
             for (int u = 0; u < kQuads; u++) {
+                if (u >= nq) break;
                 const uint32_t cw = cq[warp][u][lane];
                 const uint32_t code = cw & 0xffu;
                 if (code >> 4) {
@@ -629,6 +642,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) k_fy_scan(FyScanArgs a) {
             uint32_t* acci = acc + i;
 #pragma unroll
             for (int u = 0; u < kQuads; u++) {
+                if (u >= nq) break;
                 const uint32_t cw = cq[warp][u][lane];
                 const uint32_t code = cw & 0xffu;
                 if (code) {
