@@ -259,7 +259,38 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_fy_small(FySmallArgs a) {
 #pragma unroll
                 for (int u = 0; u < 4; u++) v4[u] = src[base + 32u * u + lane];
                 const uint32_t mn = min(min(v4[0], v4[1]), min(v4[2], v4[3]));
-                if (!__any_sync(0xffffffffu, mn <= n - 1 - i)) continue;
+                const uint32_t T0 = n - 1 - i;
+                if (!__any_sync(0xffffffffu, mn <= T0)) continue;
+                // draw q = 32u + l of the group is certainly accepted if
+                // v + q <= T0 (at most q acceptances precede it) and rejected if
+                // v > T0; when no draw lies in between, every fate is known and
+                // the ranks are prefix counts in draw order (one pass, no
+                // dependence between the four rounds)
+                uint32_t cm[4];
+                bool und = false;
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const uint32_t q = 32u * u + (uint32_t)lane;
+                    const bool cert = v4[u] + q <= T0;
+                    cm[u] = __ballot_sync(0xffffffffu, cert);
+                    und = und || (!cert && v4[u] <= T0);
+                }
+                if (!__any_sync(0xffffffffu, und)) {
+                    uint32_t run = i;
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        if ((cm[u] >> lane) & 1u) {
+                            const uint32_t r = run + (uint32_t)__popc(cm[u] & lt);
+                            if (r < n) {
+                                acc[r] = v4[u];
+                                if (r == n - 1) s_dlast = d0 + base + 32u * u + (uint32_t)lane;
+                            }
+                        }
+                        run += (uint32_t)__popc(cm[u]);
+                    }
+                    i = run;
+                    continue;
+                }
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     if (i >= n) break;
