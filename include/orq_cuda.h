@@ -337,7 +337,8 @@ int orqcu_runtime_reseed(orqcu_runtime* rt, uint64_t seed);
  * the bytes that were cached to *cached_before when non-NULL. The pool gives
  * its unused memory back to the system when the last runtime on the device
  * is destroyed. A runtime that misses its cache while holding 8 GiB or more
- * of other sizes trims itself the same way before allocating. */
+ * of other sizes returns its least recently released blocks the same way,
+ * as much as the new block needs, before allocating. */
 int orqcu_runtime_trim(orqcu_runtime* rt, size_t* cached_before);
 
 /* Size this runtime's grids for `sms` SMs (0 = all; at least 4) instead of the

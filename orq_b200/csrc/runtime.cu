@@ -1,6 +1,8 @@
 // runtime.cu — context set-up: key schedule, AES tables, device buffer pool.
 #include <cstring>
 
+#include <algorithm>
+
 #include "runtime.h"
 
 namespace orqcu {
@@ -211,18 +213,34 @@ void* Pool::get(size_t bytes, cudaStream_t stream) {
             void* p = it->second;
             live_[p] = it->first;
             free_.erase(it);
+            tick_.erase(p);
             return p;
         }
         size_t cached = 0;
         for (auto& kv : free_) cached += kv.first;
         evict = cached >= kEvictBytes;
+        if (evict) {
+            // a miss with much memory cached in other sizes (a runtime that
+            // serves requests of changing sizes): hand the least recently
+            // released blocks back to the device's pool, stream-ordered, until
+            // they cover the new block, which then reuses that memory instead
+            // of growing the footprint (the device pool keeps it mapped, see
+            // keep_pool_memory); blocks a steady workload keeps reusing stay
+            std::vector<std::pair<uint64_t, std::multimap<size_t, void*>::iterator>> order;
+            order.reserve(free_.size());
+            for (auto f = free_.begin(); f != free_.end(); ++f) order.emplace_back(tick_[f->second], f);
+            std::sort(order.begin(), order.end(),
+                      [](const auto& x, const auto& y) { return x.first < y.first; });
+            size_t freed = 0;
+            for (auto& o : order) {
+                if (freed >= b) break;
+                freed += o.second->first;
+                cudaFreeAsync(o.second->second, stream);
+                tick_.erase(o.second->second);
+                free_.erase(o.second);
+            }
+        }
     }
-    // a miss with much memory cached in other sizes (a runtime that serves
-    // requests of changing sizes): hand the cache back to the device's pool
-    // first, stream-ordered, so the new block reuses that memory instead of
-    // growing the footprint (the device pool keeps it mapped, see
-    // keep_pool_memory)
-    if (evict) trim(stream);
     void* p = nullptr;
     cudaError_t e = cudaMallocAsync(&p, b, stream);
     if (e != cudaSuccess) {
@@ -241,6 +259,7 @@ void Pool::put(void* p) {
     auto it = live_.find(p);
     if (it == live_.end()) return;
     free_.emplace(it->second, p);
+    tick_[p] = ++clock_;
     live_.erase(it);
 }
 
@@ -269,6 +288,7 @@ void Pool::trim(cudaStream_t stream) {
     std::lock_guard<std::mutex> lk(mu_);
     for (auto& kv : free_) cudaFreeAsync(kv.second, stream);
     free_.clear();
+    tick_.clear();
 }
 
 size_t Pool::cached_bytes() {

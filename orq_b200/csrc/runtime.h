@@ -55,14 +55,16 @@ class Pool {
     size_t cached_bytes();
     ~Pool();
 
-    // on a miss with at least this much cached in other sizes, the cache is
-    // handed back to the device's pool before allocating
+    // on a miss with at least this much cached in other sizes, the least
+    // recently released blocks are handed back to the device's pool first
     static constexpr size_t kEvictBytes = size_t(8) << 30;
 
    private:
     std::mutex mu_;
     std::multimap<size_t, void*> free_;
     std::map<void*, size_t> live_;
+    std::map<void*, uint64_t> tick_;  // when each cached block was released
+    uint64_t clock_ = 0;
 };
 // the device's default memory pool keeps freed memory mapped (once per device)
 void keep_pool_memory(int device);
