@@ -322,8 +322,9 @@ int orqcu_runtime_destroy(orqcu_runtime* rt) {
         orqcu::release_fy(rt->ctx);
         if (rt->ctx.owns_stream) cudaStreamDestroy(rt->ctx.stream);
         if (rt->ctx.d_err) cudaFree(rt->ctx.d_err);
-        orqcu::device_runtime_closed(rt->ctx.device);
-        delete rt;
+        const int device = rt->ctx.device;
+        delete rt;  // its pool's blocks go back to the device pool first
+        orqcu::device_runtime_closed(device);
     });
 }
 
