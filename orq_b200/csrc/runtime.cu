@@ -204,7 +204,6 @@ static size_t bucket(size_t bytes) {
 
 void* Pool::get(size_t bytes, cudaStream_t stream) {
     const size_t b = bucket(bytes);
-    bool evict = false;
     {
         std::lock_guard<std::mutex> lk(mu_);
         // the smallest cached block of at least b bytes, if it wastes at most half of b
@@ -212,32 +211,31 @@ void* Pool::get(size_t bytes, cudaStream_t stream) {
         if (it != free_.end() && it->first <= b + b / 2) {
             void* p = it->second;
             live_[p] = it->first;
-            free_.erase(it);
-            tick_.erase(p);
+            forget(it);
             return p;
         }
-        size_t cached = 0;
-        for (auto& kv : free_) cached += kv.first;
-        evict = cached >= kEvictBytes;
-        if (evict) {
-            // a miss with much memory cached in other sizes (a runtime that
-            // serves requests of changing sizes): hand the least recently
-            // released blocks back to the device's pool, stream-ordered, until
-            // they cover the new block, which then reuses that memory instead
-            // of growing the footprint (the device pool keeps it mapped, see
-            // keep_pool_memory); blocks a steady workload keeps reusing stay
-            std::vector<std::pair<uint64_t, std::multimap<size_t, void*>::iterator>> order;
-            order.reserve(free_.size());
-            for (auto f = free_.begin(); f != free_.end(); ++f) order.emplace_back(tick_[f->second], f);
-            std::sort(order.begin(), order.end(),
-                      [](const auto& x, const auto& y) { return x.first < y.first; });
+        // a miss with much memory cached in other sizes (a runtime that
+        // serves requests of changing sizes): hand the least recently
+        // released blocks back to the device's pool, stream-ordered, until
+        // they cover the new block, which then reuses that memory instead of
+        // growing the footprint (the device pool keeps it mapped, see
+        // keep_pool_memory); blocks a steady workload keeps reusing stay
+        if (cached_ >= kEvictBytes) {
             size_t freed = 0;
-            for (auto& o : order) {
-                if (freed >= b) break;
-                freed += o.second->first;
-                cudaFreeAsync(o.second->second, stream);
-                tick_.erase(o.second->second);
-                free_.erase(o.second);
+            while (freed < b && !lru_.empty()) {
+                void* q = lru_.begin()->second;
+                const size_t sz = meta_[q].first;
+                auto r = free_.equal_range(sz);
+                auto f = r.first;
+                while (f != r.second && f->second != q) ++f;
+                if (f == r.second) {  // not in the size index: drop the stale entry
+                    lru_.erase(lru_.begin());
+                    meta_.erase(q);
+                    continue;
+                }
+                freed += sz;
+                cudaFreeAsync(q, stream);
+                forget(f);
             }
         }
     }
@@ -254,12 +252,28 @@ void* Pool::get(size_t bytes, cudaStream_t stream) {
     return p;
 }
 
+// drop a cached block from the size index, the release order and the count
+void Pool::forget(std::multimap<size_t, void*>::iterator it) {
+    void* p = it->second;
+    auto m = meta_.find(p);
+    if (m != meta_.end()) {
+        lru_.erase(m->second.second);
+        meta_.erase(m);
+    }
+    cached_ -= it->first;
+    free_.erase(it);
+}
+
 void Pool::put(void* p) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = live_.find(p);
     if (it == live_.end()) return;
-    free_.emplace(it->second, p);
-    tick_[p] = ++clock_;
+    const size_t sz = it->second;
+    free_.emplace(sz, p);
+    const uint64_t t = ++clock_;
+    lru_.emplace(t, p);
+    meta_[p] = {sz, t};
+    cached_ += sz;
     live_.erase(it);
 }
 
@@ -288,14 +302,14 @@ void Pool::trim(cudaStream_t stream) {
     std::lock_guard<std::mutex> lk(mu_);
     for (auto& kv : free_) cudaFreeAsync(kv.second, stream);
     free_.clear();
-    tick_.clear();
+    lru_.clear();
+    meta_.clear();
+    cached_ = 0;
 }
 
 size_t Pool::cached_bytes() {
     std::lock_guard<std::mutex> lk(mu_);
-    size_t b = 0;
-    for (auto& kv : free_) b += kv.first;
-    return b;
+    return cached_;
 }
 
 Pool::~Pool() {

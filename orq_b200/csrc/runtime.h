@@ -61,10 +61,13 @@ class Pool {
 
    private:
     std::mutex mu_;
-    std::multimap<size_t, void*> free_;
+    std::multimap<size_t, void*> free_;               // cached blocks by size
     std::map<void*, size_t> live_;
-    std::map<void*, uint64_t> tick_;  // when each cached block was released
+    std::map<uint64_t, void*> lru_;                    // cached blocks by release time
+    std::map<void*, std::pair<size_t, uint64_t>> meta_;  // cached block: size, release time
+    size_t cached_ = 0;
     uint64_t clock_ = 0;
+    void forget(std::multimap<size_t, void*>::iterator it);
 };
 // the device's default memory pool keeps freed memory mapped (once per device)
 void keep_pool_memory(int device);
