@@ -346,8 +346,9 @@ PUBLISHED_PRIMS = {1 << 20: {"AND": 0.01723, "MULT": 0.01167, "EQ": 0.04605, "GR
 class PrimsWorkload:
     """ORQ's micro_primitives sequence (bench/micro/micro_primitives.cpp) on
     n 32-bit elements, 3PC: AND (and_b), MULT (multiply_a), EQ (==), GR (>)
-    and RCA (binary +), the protocol steps of north_star's first hot-path
-    item. One step = the five calls; a row is one element of one call."""
+    and RCA (binary +): the protocols' local AND / MUL steps fused with their
+    correlated randomness, and the compare circuits built on them. One step =
+    the five calls; a row is one element of one call."""
 
     name = "prims"
     PRIMS = ("AND", "MULT", "EQ", "GR", "RCA")

@@ -859,7 +859,7 @@ def test_empty_vectors(orq):
 
 
 def test_radix_2p24_properties(orq):
-    """The north_star target size: 2^24 rows, 40-bit keys, two payloads.
+    """The largest radix workload: 2^24 rows, 40-bit keys, two payloads.
     Opened keys sorted and stable, payloads carried, the permutation a
     bijection (share-level parity is pinned by digests at 2^20 and 2^22)."""
     n, bits = 1 << 24, 40
